@@ -1,0 +1,196 @@
+/*
+ * pppm_b200.h - C ABI of the B200-native PPPM-TDBEM time-step library (libpppm_b200.so).
+ *
+ * The reference (hellojxt/PPPM-TDBEM) exposes its hot path only as the C++ class
+ * PPPMSolver (src/algorithm/pppm.h:11-165) driven by the demo loop
+ * (experiments/demo/main.cu:170-275).  This header is the C boundary that replaces that
+ * class for foreign callers (the C++ scene host in pppm-tdbem_b200/host, the Python
+ * ctypes binding and torch.autograd.Function, test harnesses).  Each entry point cites the
+ * reference member it replaces.
+ *
+ * Conventions
+ *   - Every call returns an int status (PPPM_OK == 0) and never throws or exits.
+ *   - Grids are res^3, cell (x, y, z) at linear index (x * res + y) * res + z (z fastest),
+ *     the reference layout (src/core/array3D.h:76).
+ *   - Vertices are float[3 * nv] (x, y, z interleaved); triangles int[3 * nt].
+ *   - Time index t starts at -1; each step writes grid slot t + 1 then increments t
+ *     (src/algorithm/fdtd.h:55,73-87).  Histories are rings of 32 slots per triangle
+ *     (src/algorithm/bem.h:55).
+ *   - A handle owns all its device memory and one CUDA stream.  Calls on one handle are not
+ *     thread-safe; distinct handles may be used from distinct host threads.
+ */
+#ifndef PPPM_B200_H
+#define PPPM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes ----- */
+#define PPPM_OK 0
+#define PPPM_ERR_ARG 1      /* bad argument (null pointer, index out of range, bad size)  */
+#define PPPM_ERR_CUDA 2     /* a CUDA runtime call failed; see pppm_last_error_message()   */
+#define PPPM_ERR_CAPACITY 3 /* a mesh exceeds a structural limit (see pppm_limits)         */
+#define PPPM_ERR_NAN 4      /* a non-finite value reached the listener / state            */
+#define PPPM_ERR_STATE 5    /* call out of order (e.g. step before set_mesh)              */
+#define PPPM_ERR_TIMEOUT 6  /* a bounded device-side wait gave up                         */
+#define PPPM_ERR_NOMEM 7    /* device allocation failed                                   */
+
+/* ------------------------------------------------------------------ parameters ------- */
+#define PPPM_PRECISION_FP32 0 /* FP32 grids/histories, fp16+scale weights (the reference's) */
+#define PPPM_PRECISION_FP64 1 /* FP64 everywhere, unquantised weights: the error yardstick  */
+
+#define PPPM_WEIGHTS_REF32 0 /* TDBEM weights in FP32 with the reference's arithmetic       */
+#define PPPM_WEIGHTS_FP64 1  /* singular and near-singular face integrals in FP64           */
+
+typedef struct pppm_params {
+    int res;               /* grid resolution (cells per axis), >= 8                      */
+    float dl;              /* cell size h                                                 */
+    float dt;              /* time step                                                   */
+    float min_pos[3];      /* world position of the grid's lower corner                   */
+    int pml_width;         /* PML layers; 0 = the reference's absorbing boundary (ABC)     */
+    float reflect_coeff;   /* Dirichlet far-field factor, reference default 0.83          */
+    float c;               /* speed of sound, reference hard-codes 340.3 (macro.h:82)     */
+    float rho;             /* air density 1.225 (macro.h:83)                              */
+    int precision;         /* PPPM_PRECISION_*                                            */
+    int weights;           /* PPPM_WEIGHTS_*                                              */
+    int device;            /* CUDA device ordinal                                         */
+    void *stream;          /* cudaStream_t to use, or NULL to create one                  */
+} pppm_params;
+
+typedef struct pppm_handle pppm_handle;
+
+/* Fill *p with the reference defaults (PPPMSolver constructor defaults, pppm.h:39-44). */
+int pppm_params_default(pppm_params *p);
+
+/* Replaces PPPMSolver::PPPMSolver(res, dl, dt, min_pos, pml_width, reflect_coeff)
+ * (pppm.h:39-54).  Allocates the three grid time levels. */
+int pppm_create(const pppm_params *p, pppm_handle **out);
+
+/* Replaces PPPMSolver::clear() + delete (pppm.h:111-126). */
+int pppm_destroy(pppm_handle *h);
+
+/* Replaces PPPMSolver::set_mesh(verts, tris) (pppm.h:75-95): triangle geometry, per-cell
+ * lists, 3^3 / 4^3 neighbour lists, GridCache and FaceCache weights, zeroed histories. */
+int pppm_set_mesh(pppm_handle *h, const float *verts, int nv, const int *tris, int nt);
+
+/* Replaces PPPMSolver::update_mesh(verts) (pppm.h:97-109): same topology, new vertex
+ * positions; lists rebuilt, caches refreshed under the reference's recompute criteria
+ * (pppm_cache.h:65-70, 123-128).  verts_on_device != 0: verts is a device pointer. */
+int pppm_update_mesh(pppm_handle *h, const float *verts, int verts_on_device);
+
+/* Replaces nsteps calls of PPPMSolver::update_grid_and_face(acc) (pppm.h:138-145).
+ * acc holds nsteps rows of nt per-triangle normal accelerations (row s drives step s);
+ * acc_on_device != 0: acc is a device pointer.  Listener values are recorded on the device
+ * after every step (the demo's per-step read, experiments/demo/main.cu:266). */
+int pppm_step(pppm_handle *h, const float *acc, int acc_on_device, int nsteps);
+
+/* Listener cells (experiments/demo/main.cu:148: int3(checkCoord * res)). */
+int pppm_add_listener(pppm_handle *h, int x, int y, int z);
+int pppm_clear_listeners(pppm_handle *h);
+/* Number of recorded steps so far and listener count. */
+int pppm_listener_count(pppm_handle *h, int *nsteps, int *nlisteners);
+/* Copy recorded samples [first, first + count) x nlisteners into out (host). */
+int pppm_read_listeners(pppm_handle *h, int first, int count, float *out);
+int pppm_rewind_listeners(pppm_handle *h);
+
+/* Current time index t (fdtd.t). */
+int pppm_get_time(pppm_handle *h, int *t);
+int pppm_set_time(pppm_handle *h, int t);
+
+/* Replaces pg.fdtd.reset() + neumann.reset() + dirichlet.reset() (demo/main.cu:240-242):
+ * zero grids and histories; t is kept (the demo restores it explicitly). */
+int pppm_reset_fields(pppm_handle *h);
+
+/* Whole solver state (grids, histories, PML fields, t) into / from a caller-owned host
+ * buffer: cross-fade restart (demo/main.cu:215-244) and adjoint checkpoints. */
+int pppm_state_size(pppm_handle *h, size_t *bytes);
+int pppm_save_state(pppm_handle *h, void *dst, size_t bytes);
+int pppm_restore_state(pppm_handle *h, const void *src, size_t bytes);
+
+/* ----------------------------------------------------------- read-out for parity ----- */
+#define PPPM_DUMP_GRID_T 0        /* float/double res^3: grid slot t                     */
+#define PPPM_DUMP_GRID_TM1 1      /* grid slot t-1                                       */
+#define PPPM_DUMP_GRID_TM2 2      /* grid slot t-2                                       */
+#define PPPM_DUMP_NEUMANN 3       /* nt x 32 ring                                        */
+#define PPPM_DUMP_DIRICHLET 4     /* nt x 32 ring                                        */
+#define PPPM_DUMP_TRI_GEOM 5      /* float nt x 7: centre xyz, normal xyz, area          */
+#define PPPM_DUMP_TRI_CELLS 6     /* int nt x 6: grid coord xyz, base coord xyz          */
+#define PPPM_DUMP_CELL_COUNTS 7   /* int res^3 triangles per cell                        */
+#define PPPM_DUMP_N3_CELLS 8      /* int n3 x 4: x, y, z, 3^3 list length                */
+#define PPPM_DUMP_N3_TRIS 9       /* int p3: concatenated 3^3 lists                      */
+#define PPPM_DUMP_B4_CELLS 10     /* int b4 x 4: x, y, z, base-cell list length          */
+#define PPPM_DUMP_B4_TRIS 11      /* int: concatenated base-cell lists                   */
+#define PPPM_DUMP_N4_TRIS 12      /* int p4: concatenated 4^3 lists, one per base cell   */
+#define PPPM_DUMP_GRID_CACHE 13   /* nt x 54 x 72 B LayerWeightHalf records (FP32 mode)  */
+#define PPPM_DUMP_FACE_PAIRS 14   /* int pf x 2: (centre, neighbour) in hot-path order   */
+#define PPPM_DUMP_FACE_CACHE 15   /* pf x 72 B weights in the same order (FP32 mode)     */
+#define PPPM_DUMP_INTERP 16       /* float nt x 8 trilinear face weights                 */
+#define PPPM_DUMP_CELL_TYPE 17    /* int res^3 labels AIR 0 SOLID 1 GHOST 2 UNKNOWN 3    */
+#define PPPM_DUMP_CELL_NEAREST 18 /* int res^3 nearest triangle (-1 if none)             */
+#define PPPM_DUMP_CELL_GHOST 19   /* int res^3 ghost index (-1 if not GHOST)             */
+#define PPPM_DUMP_CELL_POINTS 20  /* float res^3 x 7: nearest xyz, reflect xyz, distance */
+#define PPPM_DUMP_COUNTS 21       /* int[8]: n3, p3, b4, p4(pairs per centre), pf, nt, nv, ghost count */
+
+int pppm_dump_size(pppm_handle *h, int what, size_t *bytes);
+int pppm_dump(pppm_handle *h, int what, void *dst, size_t bytes);
+
+/* Overwrite one grid slot (what = PPPM_DUMP_GRID_T/TM1/TM2) or one history ring
+ * (PPPM_DUMP_NEUMANN / PPPM_DUMP_DIRICHLET) from host memory; used to set initial
+ * conditions and by the parity harness.  Element type follows the handle's precision. */
+int pppm_load(pppm_handle *h, int what, const void *src, size_t bytes);
+
+/* Parity mode: replace the GridCache / FaceCache tables with tables read out of the
+ * reference (same record layout as PPPM_DUMP_GRID_CACHE and PPPM_DUMP_FACE_CACHE).
+ * face_pairs lists (centre, neighbour) for each face record.  FP32 handles only. */
+int pppm_import_grid_cache(pppm_handle *h, const void *records, size_t bytes);
+int pppm_import_face_cache(pppm_handle *h, const int *face_pairs, const void *records, int npairs);
+
+/* ------------------------------------------------------------ cell labels ------------ */
+/* Replaces fill_cell_data (ghost_cell_util.cu:214-230): nearest triangle within +-3 cells,
+ * AIR / SOLID / GHOST / UNKNOWN labels, z-column sweep, ghost indices.  Reads the current
+ * mesh.  *ghost_count receives the number of GHOST cells (may be NULL). */
+int pppm_classify_cells(pppm_handle *h, int *ghost_count);
+
+/* Replaces GhostCellSolver::fill_in_fresh_cell (ghost_cell.cu:207-218) for a moving mesh:
+ * re-label after the last update_mesh and fill cells that turned from non-AIR to AIR in grid
+ * slots t and t-1 by inverse-distance interpolation at the reflection point, minus
+ * rho * a * |xf - xr|.  acc / acc_old: current and previous per-triangle accelerations
+ * (host).  *fresh_count receives the number of fresh cells (may be NULL). */
+int pppm_fill_fresh_cells(pppm_handle *h, const float *acc, const float *acc_old, int *fresh_count);
+
+/* ------------------------------------------------------------ batched scenes --------- */
+/* Many independent scenes advanced together by one persistent kernel per step under a
+ * captured CUDA graph; no reference counterpart (the reference runs one scene per process).
+ * Scenes are ordinary handles that already hold their mesh; nsteps[i] may differ. */
+typedef struct pppm_batch pppm_batch;
+int pppm_batch_create(pppm_handle **scenes, int nscenes, pppm_batch **out);
+int pppm_batch_destroy(pppm_batch *b);
+/* acc[i]: nsteps[i] x nt_i rows for scene i (device pointers when acc_on_device != 0). */
+int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, int acc_on_device);
+
+/* ------------------------------------------------------------ adjoint ---------------- */
+/* Gradient of L = sum_s sum_l g[s][l] * p_l(s) over the next nsteps forward steps from the
+ * current state, with geometry and labels held fixed: dL/dacc[s][tri].  No reference
+ * counterpart.  acc: nsteps x nt forward inputs (host); dL_dsignal: nsteps x nlisteners
+ * (host); dL_dacc out: nsteps x nt (host).  Checkpoints every `checkpoint_every` steps; the
+ * forward state is advanced by nsteps on return. */
+int pppm_adjoint(pppm_handle *h, const float *acc, int nsteps, const float *dL_dsignal, int checkpoint_every,
+                 float *dL_dacc);
+
+/* ------------------------------------------------------------ diagnostics ------------ */
+const char *pppm_status_string(int status);
+const char *pppm_last_error_message(void);
+/* Kernel launches issued by this handle since creation (for launch accounting). */
+int pppm_launch_count(pppm_handle *h, long long *count);
+/* Last-step timing breakdown in microseconds measured with CUDA events when enabled. */
+int pppm_enable_timing(pppm_handle *h, int enable);
+int pppm_kernel_times(pppm_handle *h, float *us_stencil, float *us_face, float *us_near, int *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PPPM_B200_H */

@@ -1,0 +1,1024 @@
+// GridCache / FaceCache: the TDBEM weight tables the per-step correction reads.
+//
+// Reference semantics kept (src/algorithm/pppm_cache.{h,cu}):
+//   GridCache     one record pair per (triangle, 27 neighbour cells): the FDTD-near weights
+//                 (8 stencil targets at scales {2, s, s, s, s, s, s, -6s}, s = (c dt / h)^2,
+//                 shifted by one step, minus the BEM-near weights two steps back) and the
+//                 BEM-near weights; targets inside the triangle's own cell are skipped
+//                 (pppm_cache.cu:64-123).  Refreshed for a triangle when its centre moved
+//                 > 1% h, its normal moved > 0.01 or its area changed > 1% (pppm_cache.h:65-70).
+//   FaceCache     one record per (centre face, neighbour face) ever seen in the centre's 4^3
+//                 block: the face-to-face integral minus the neighbour's point integrals at
+//                 those of the centre's 8 interpolation corners farther than 1.5 h from the
+//                 neighbour centre in some axis (pppm_cache.cu:234-271).  Records persist
+//                 across mesh updates and are refreshed only when new or when the pair's
+//                 normal dot product moved > 0.01 or its centre distance > 1%
+//                 (pppm_cache.h:123-128, pppm_cache.cu:183-232).  Trilinear interpolation
+//                 weights of every face are recomputed on every update (pppm_cache.cu:157-181).
+// B200 layout: the persistent face records live in a pool addressed through a per-centre
+// open-addressing table (kFaceCacheSlots keys per face, the reference's per-face bound);
+// after each refresh the records the step needs are gathered into dense arrays in hot-path
+// order, so the per-step kernels stream them.
+#include "handle.cuh"
+
+namespace pb
+{
+
+namespace
+{
+
+// ---- fp16 row packing (bem.h:171-191)
+__device__ inline void pack_half(const float *s, const float *d, __half2 *out, float2 *scale)
+{
+    float ms = 0, md = 0;
+    for (int i = 0; i < kTaps; i++)
+    {
+        ms = max(ms, abs(s[i]));
+        md = max(md, abs(d[i]));
+    }
+    if (ms == 0)
+        ms = 1;
+    if (md == 0)
+        md = 1;
+    for (int i = 0; i < kTaps; i++)
+    {
+        float a = s[i] / ms, b = d[i] / md;
+        out[i] = __halves2half2(__float2half_rn(a), __float2half_rn(b));
+    }
+    *scale = make_float2(ms, md);
+}
+
+__device__ inline void pack_double(const double *s, const double *d, double2 *out)
+{
+    for (int i = 0; i < kTaps; i++)
+        out[i] = make_double2(s[i], d[i]);
+}
+
+struct DevConsts
+{
+    float lambda;
+    float wave_re[kTaps], wave_im[kTaps];
+    float threshold;
+    double lambda_d;
+    double wave_re_d[kTaps], wave_im_d[kTaps];
+    float c, dt, h;
+    f3 mn;
+    int res;
+};
+
+__device__ inline void load_tri(const float *verts, const int *tris, int t, f3 *v, int *idx)
+{
+    idx[0] = tris[3 * t];
+    idx[1] = tris[3 * t + 1];
+    idx[2] = tris[3 * t + 2];
+    v[0] = load3(verts, idx[0]);
+    v[1] = load3(verts, idx[1]);
+    v[2] = load3(verts, idx[2]);
+}
+
+// spectrum k <= 8 -> full 16 with conjugates, FFT, scaling (bem.h:306-321)
+__device__ inline void spectrum_to_weights(cf *sp, float lambda, float *w)
+{
+    for (int k = kTaps / 2 + 1; k < kTaps; k++)
+        sp[k] = cf{sp[kTaps - k].re, -sp[kTaps - k].im};
+    ref32::scaled_fft(sp, lambda, w);
+}
+
+__device__ inline void spectrum_to_weights_d(cd *sp, double lambda, double *w)
+{
+    for (int k = kTaps / 2 + 1; k < kTaps; k++)
+        sp[k] = cd{sp[kTaps - k].re, -sp[kTaps - k].im};
+    f64::scaled_fft(sp, lambda, w);
+}
+
+// ---------------------------------------------------------------- grid cache ---------
+__global__ void gc_flag_kernel(const float *center, const float *normal, const float *area, const float *snap, int nt,
+                               float h, int empty, int *flag)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    if (empty)
+    {
+        flag[i] = 1;
+        return;
+    }
+    f3 oc = f3{snap[7 * i], snap[7 * i + 1], snap[7 * i + 2]};
+    f3 on = f3{snap[7 * i + 3], snap[7 * i + 4], snap[7 * i + 5]};
+    float oa = snap[7 * i + 6];
+    f3 c = load3(center, i), n = load3(normal, i);
+    float a = area[i];
+    flag[i] = (len3(oc - c) > 0.01 * h || len3(on - n) > 0.01 || abs(oa - a) > 0.01 * a) ? 1 : 0;
+}
+
+// one thread per (triangle, weight index); FP32 records with the reference's arithmetic
+__global__ void gc_compute_kernel(DevConsts dc, const float *verts, const int *tris, const int *cellc,
+                                  const float *center, const float *normal, const float *area, const int *flag, int nt,
+                                  __half2 *gc_w, float2 *gc_scale, float *snap)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nt * 27)
+        return;
+    int tri = (int)(gid / 27), woff = (int)(gid % 27);
+    if (!flag[tri])
+        return;
+    f3 v[3];
+    int idx[3];
+    load_tri(verts, tris, tri, v, idx);
+    int tx = cellc[3 * tri], ty = cellc[3 * tri + 1], tz = cellc[3 * tri + 2];
+    int nx = tx + woff % 3 - 1, ny = ty + woff / 3 % 3 - 1, nz = tz + woff / 9 - 1;
+    int dcx[8] = {nx, nx - 1, nx + 1, nx, nx, nx, nx, nx};
+    int dcy[8] = {ny, ny, ny, ny - 1, ny + 1, ny, ny, ny};
+    int dcz[8] = {nz, nz, nz, nz, nz, nz - 1, nz + 1, nz};
+    float scale = dc.c * dc.c * dc.dt * dc.dt / (dc.h * dc.h);
+    float dsc[8] = {2, scale, scale, scale, scale, scale, scale, -6 * scale};
+    f3 pts[8];
+    float sc[8];
+    int n = 0;
+    for (int i = 0; i < 8; i++)
+    {
+        if (!(dcx[i] == tx && dcy[i] == ty && dcz[i] == tz))
+        {
+            pts[n] = cell_center(dcx[i], dcy[i], dcz[i], dc.h, dc.mn);
+            sc[n] = dsc[i];
+            n++;
+        }
+    }
+    cf ss[kTaps], sd[kTaps];
+    for (int k = 0; k <= kTaps / 2; k++)
+    {
+        cf kk{dc.wave_re[k], dc.wave_im[k]};
+        ss[k] = ref32::face_to_points(v, pts, sc, n, true, kk, false);
+        sd[k] = ref32::face_to_points(v, pts, sc, n, true, kk, true);
+    }
+    float ws[kTaps], wd[kTaps];
+    spectrum_to_weights(ss, dc.lambda, ws);
+    spectrum_to_weights(sd, dc.lambda, wd);
+    // move(-1)
+    for (int i = kTaps - 1; i >= 1; i--)
+    {
+        ws[i] = ws[i - 1];
+        wd[i] = wd[i - 1];
+    }
+    ws[0] = 0;
+    wd[0] = 0;
+    bool inside = (nx == tx && ny == ty && nz == tz);
+    float ps[kTaps], pd[kTaps];
+    if (!inside)
+    {
+        f3 p = cell_center(nx, ny, nz, dc.h, dc.mn);
+        cf qs[kTaps], qd[kTaps];
+        for (int k = 0; k <= kTaps / 2; k++)
+        {
+            cf kk{dc.wave_re[k], dc.wave_im[k]};
+            qs[k] = ref32::face_to_points(v, &p, nullptr, 1, false, kk, false);
+            qd[k] = ref32::face_to_points(v, &p, nullptr, 1, false, kk, true);
+        }
+        spectrum_to_weights(qs, dc.lambda, ps);
+        spectrum_to_weights(qd, dc.lambda, pd);
+        for (int i = 2; i < kTaps; i++)
+        {
+            ws[i] += ps[i - 2] * -1.0f;
+            wd[i] += pd[i - 2] * -1.0f;
+        }
+    }
+    size_t rec = (size_t)tri * 54 + woff;
+    pack_half(ws, wd, gc_w + rec * kTaps, gc_scale + rec);
+    float bs[kTaps], bd[kTaps];
+    for (int i = 0; i < kTaps; i++)
+    {
+        bs[i] = 0;
+        bd[i] = 0;
+    }
+    if (!inside)
+        for (int i = 0; i < kTaps; i++)
+        {
+            bs[i] += ps[i] * 1.0f;
+            bd[i] += pd[i] * 1.0f;
+        }
+    pack_half(bs, bd, gc_w + (rec + 27) * kTaps, gc_scale + rec + 27);
+    if (woff == 0)
+    {
+        f3 c = load3(center, tri), nn = load3(normal, tri);
+        snap[7 * tri] = c.x;
+        snap[7 * tri + 1] = c.y;
+        snap[7 * tri + 2] = c.z;
+        snap[7 * tri + 3] = nn.x;
+        snap[7 * tri + 4] = nn.y;
+        snap[7 * tri + 5] = nn.z;
+        snap[7 * tri + 6] = area[tri];
+    }
+}
+
+// FP64 scheme: the same records entirely in double, unquantised
+__global__ void gc_compute_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *cellc,
+                                    const float *center, const float *normal, const float *area, const int *flag,
+                                    int nt, double2 *gc_w, float *snap)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nt * 27)
+        return;
+    int tri = (int)(gid / 27), woff = (int)(gid % 27);
+    if (!flag[tri])
+        return;
+    using namespace f64;
+    f3 vf[3];
+    int idx[3];
+    load_tri(verts, tris, tri, vf, idx);
+    d3 v[3] = {dd(vf[0]), dd(vf[1]), dd(vf[2])};
+    int tx = cellc[3 * tri], ty = cellc[3 * tri + 1], tz = cellc[3 * tri + 2];
+    int nx = tx + woff % 3 - 1, ny = ty + woff / 3 % 3 - 1, nz = tz + woff / 9 - 1;
+    int dcx[8] = {nx, nx - 1, nx + 1, nx, nx, nx, nx, nx};
+    int dcy[8] = {ny, ny, ny, ny - 1, ny + 1, ny, ny, ny};
+    int dcz[8] = {nz, nz, nz, nz, nz, nz - 1, nz + 1, nz};
+    double h = dc.h;
+    double scale = (double)dc.c * dc.c * dc.dt * dc.dt / (h * h);
+    double dsc[8] = {2, scale, scale, scale, scale, scale, scale, -6 * scale};
+    d3 mn{dc.mn.x, dc.mn.y, dc.mn.z};
+    auto ctr = [&](int i, int j, int k) { return d3{(i + 0.5) * h + mn.x, (j + 0.5) * h + mn.y, (k + 0.5) * h + mn.z}; };
+    d3 pts[8];
+    double sc[8];
+    int n = 0;
+    for (int i = 0; i < 8; i++)
+        if (!(dcx[i] == tx && dcy[i] == ty && dcz[i] == tz))
+        {
+            pts[n] = ctr(dcx[i], dcy[i], dcz[i]);
+            sc[n] = dsc[i];
+            n++;
+        }
+    cd ss[kTaps], sd[kTaps];
+    for (int k = 0; k <= kTaps / 2; k++)
+    {
+        cd kk{dc.wave_re_d[k], dc.wave_im_d[k]};
+        ss[k] = face_to_points(v, pts, sc, n, kk, false);
+        sd[k] = face_to_points(v, pts, sc, n, kk, true);
+    }
+    double ws[kTaps], wd[kTaps];
+    spectrum_to_weights_d(ss, dc.lambda_d, ws);
+    spectrum_to_weights_d(sd, dc.lambda_d, wd);
+    for (int i = kTaps - 1; i >= 1; i--)
+    {
+        ws[i] = ws[i - 1];
+        wd[i] = wd[i - 1];
+    }
+    ws[0] = 0;
+    wd[0] = 0;
+    bool inside = (nx == tx && ny == ty && nz == tz);
+    double ps[kTaps] = {0}, pd[kTaps] = {0};
+    if (!inside)
+    {
+        d3 p = ctr(nx, ny, nz);
+        double one = 1.0;
+        cd qs[kTaps], qd[kTaps];
+        for (int k = 0; k <= kTaps / 2; k++)
+        {
+            cd kk{dc.wave_re_d[k], dc.wave_im_d[k]};
+            qs[k] = face_to_points(v, &p, &one, 1, kk, false);
+            qd[k] = face_to_points(v, &p, &one, 1, kk, true);
+        }
+        spectrum_to_weights_d(qs, dc.lambda_d, ps);
+        spectrum_to_weights_d(qd, dc.lambda_d, pd);
+        for (int i = 2; i < kTaps; i++)
+        {
+            ws[i] -= ps[i - 2];
+            wd[i] -= pd[i - 2];
+        }
+    }
+    size_t rec = (size_t)tri * 54 + woff;
+    pack_double(ws, wd, gc_w + rec * kTaps);
+    pack_double(ps, pd, gc_w + (rec + 27) * kTaps);
+    if (woff == 0)
+    {
+        f3 c = load3(center, tri), nn = load3(normal, tri);
+        snap[7 * tri] = c.x;
+        snap[7 * tri + 1] = c.y;
+        snap[7 * tri + 2] = c.z;
+        snap[7 * tri + 3] = nn.x;
+        snap[7 * tri + 4] = nn.y;
+        snap[7 * tri + 5] = nn.z;
+        snap[7 * tri + 6] = area[tri];
+    }
+}
+
+// dense copy of the 3^3 pair records in hot-path order
+template <typename Rec>
+__global__ void gather_w3_kernel(const int *p3_tri, const unsigned char *p3_woff, long long p3, const Rec *gc_w,
+                                 const float2 *gc_scale, Rec *w3, float2 *w3_scale)
+{
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= p3 * kTaps)
+        return;
+    long long pair = p / kTaps;
+    int k = (int)(p % kTaps);
+    size_t rec = (size_t)p3_tri[pair] * 54 + p3_woff[pair];
+    w3[(pair * 2) * kTaps + k] = gc_w[rec * kTaps + k];
+    w3[(pair * 2 + 1) * kTaps + k] = gc_w[(rec + 27) * kTaps + k];
+    if (k == 0 && gc_scale)
+    {
+        w3_scale[pair * 2] = gc_scale[rec];
+        w3_scale[pair * 2 + 1] = gc_scale[rec + 27];
+    }
+}
+
+// ---------------------------------------------------------------- face cache ---------
+// trilinear weights of the 2x2x2 corner cells at the face's 1-point Gauss node
+// (pppm_cache.cu:157-181)
+__global__ void interp_kernel(const float *verts, const int *tris, const int *basec, int nt, float h, f3 mn,
+                              float *interp, double *interp_d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    f3 v[3];
+    int idx[3];
+    load_tri(verts, tris, i, v, idx);
+    float jac = ref32::jacobian(v);
+    const float gx = (float)PB_TRI_X;
+    f3 q = ref32::local_to_global(gx, gx, v);
+    f3 base = cell_center(basec[3 * i], basec[3 * i + 1], basec[3 * i + 2], h, mn);
+    f3 d = (q - base) / h;
+    float wt[8];
+    wt[0] = (1 - d.x) * (1 - d.y) * (1 - d.z);
+    wt[1] = (1 - d.x) * (1 - d.y) * d.z;
+    wt[2] = (1 - d.x) * d.y * (1 - d.z);
+    wt[3] = (1 - d.x) * d.y * d.z;
+    wt[4] = d.x * (1 - d.y) * (1 - d.z);
+    wt[5] = d.x * (1 - d.y) * d.z;
+    wt[6] = d.x * d.y * (1 - d.z);
+    wt[7] = d.x * d.y * d.z;
+    float s = 0.5 * 1.0f * jac;
+    for (int k = 0; k < 8; k++)
+    {
+        float w = 0;
+        w += s * wt[k];
+        interp[8 * i + k] = w;
+    }
+    if (interp_d)
+    {
+        using namespace f64;
+        d3 vd[3] = {dd(v[0]), dd(v[1]), dd(v[2])};
+        double jd = jacobian(vd);
+        d3 qd = ltg(1.0 / 3, 1.0 / 3, vd);
+        double hh = h;
+        double bx = (basec[3 * i] + 0.5) * hh + mn.x, by = (basec[3 * i + 1] + 0.5) * hh + mn.y,
+               bz = (basec[3 * i + 2] + 0.5) * hh + mn.z;
+        double ex = (qd.x - bx) / hh, ey = (qd.y - by) / hh, ez = (qd.z - bz) / hh;
+        double wd8[8] = {(1 - ex) * (1 - ey) * (1 - ez), (1 - ex) * (1 - ey) * ez, (1 - ex) * ey * (1 - ez),
+                         (1 - ex) * ey * ez,             ex * (1 - ey) * (1 - ez), ex * (1 - ey) * ez,
+                         ex * ey * (1 - ez),             ex * ey * ez};
+        for (int k = 0; k < 8; k++)
+            interp_d[8 * i + k] = 0.5 * jd * wd8[k];
+    }
+}
+
+__device__ inline unsigned hash_slot(int key) { return ((unsigned)key * 2654435761u) >> 22; }  // 10 bits
+
+// one warp per centre face: find or insert each (centre, neighbour) pair in the centre's
+// table, decide whether its record must be recomputed.
+__global__ void fc_lookup_kernel(const int *face_start, const int *face_nbr, int nt, const float *center,
+                                 const float *normal, int *keys, int *slots, int *pool_count, long long pool_cap,
+                                 float2 *pool_meta, int *face_pool, int *pair_flag, int *status)
+{
+    int warp = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (warp >= nt)
+        return;
+    int ctr = warp;
+    f3 cc = load3(center, ctr), cn = load3(normal, ctr);
+    int *tk = keys + (size_t)ctr * kFaceCacheSlots;
+    int *ts = slots + (size_t)ctr * kFaceCacheSlots;
+    for (int p = face_start[ctr] + lane; p < face_start[ctr + 1]; p += 32)
+    {
+        int nbr = face_nbr[p];
+        unsigned hsh = hash_slot(nbr);
+        int slot = -1;
+        bool fresh = false;
+        for (int probe = 0; probe < kFaceCacheSlots; probe++)
+        {
+            unsigned pos = (hsh + probe) & (kFaceCacheSlots - 1);
+            int cur = tk[pos];
+            if (cur == nbr)
+            {
+                // inserted by an earlier refresh (this refresh inserts each pair once)
+                slot = ts[pos];
+                break;
+            }
+            if (cur == -1)
+            {
+                int prev = atomicCAS(&tk[pos], -1, nbr);
+                if (prev == -1)
+                {
+                    slot = atomicAdd(pool_count, 1);
+                    ts[pos] = slot;
+                    fresh = true;
+                    break;
+                }
+                if (prev == nbr)
+                {
+                    slot = ts[pos];
+                    break;
+                }
+            }
+        }
+        if (slot < 0 || slot >= pool_cap)
+        {
+            atomicCAS(status, 0, PPPM_ERR_CAPACITY);
+            face_pool[p] = 0;
+            pair_flag[p] = 0;
+            continue;
+        }
+        f3 nc = load3(center, nbr), nn = load3(normal, nbr);
+        float angle = dot3(nn, cn);
+        float dist = len3(nc - cc);
+        int recompute = 0;
+        if (fresh)
+            recompute = 1;
+        else
+        {
+            float2 m = pool_meta[slot];
+            recompute = (abs(m.x - angle) > 0.01 || abs(m.y - dist) > 0.01 * dist) ? 1 : 0;
+        }
+        if (recompute)
+            pool_meta[slot] = make_float2(angle, dist);
+        face_pool[p] = slot;
+        pair_flag[p] = recompute;
+    }
+}
+
+__global__ void compact_pairs_kernel(const int *flag, const int *pos, long long n, int *out)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && flag[i])
+        out[pos[i]] = (int)i;
+}
+
+__device__ inline int centre_of(const int *face_start, int nt, int p)
+{
+    int lo = 0, hi = nt;  // largest i with face_start[i] <= p
+    while (hi - lo > 1)
+    {
+        int mid = (lo + hi) >> 1;
+        if (face_start[mid] <= p)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Phase A: face-to-face spectra, one thread per (recomputed pair, layer, k <= 8).
+// mode: 0 = ref32 throughout, 1 = FP64 for panels sharing vertices (stored as float)
+__global__ void fc_spectra_kernel(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
+                                  const int *face_nbr, const int *work, int nwork, int mode, cf *spec)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nwork * 18)
+        return;
+    int w = (int)(gid / 18), r = (int)(gid % 18);
+    int layer = r / 9, k = r % 9;
+    int p = work[w];
+    int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
+    f3 sv[3], tv[3];
+    int si[3], ti[3];
+    load_tri(verts, tris, nbr, sv, si);
+    load_tri(verts, tris, ctr, tv, ti);
+    cf out;
+    if (mode == 1 && ref32::common_vertices(si, ti) > 0)
+    {
+        using namespace f64;
+        d3 s[3] = {dd(sv[0]), dd(sv[1]), dd(sv[2])}, t[3] = {dd(tv[0]), dd(tv[1]), dd(tv[2])};
+        cd v = face_to_face(s, si, t, ti, cd{dc.wave_re_d[k], dc.wave_im_d[k]}, dc.threshold, layer == 1);
+        out = cf{(float)v.re, (float)v.im};
+    }
+    else
+        out = ref32::face_to_face(sv, si, tv, ti, cf{dc.wave_re[k], dc.wave_im[k]}, dc.threshold, layer == 1);
+    spec[(size_t)w * 18 + r] = out;
+}
+
+__global__ void fc_spectra_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
+                                    const int *face_nbr, const int *work, int nwork, cd *spec)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nwork * 18)
+        return;
+    int w = (int)(gid / 18), r = (int)(gid % 18);
+    int layer = r / 9, k = r % 9;
+    int p = work[w];
+    int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
+    f3 sv[3], tv[3];
+    int si[3], ti[3];
+    load_tri(verts, tris, nbr, sv, si);
+    load_tri(verts, tris, ctr, tv, ti);
+    using namespace f64;
+    d3 s[3] = {dd(sv[0]), dd(sv[1]), dd(sv[2])}, t[3] = {dd(tv[0]), dd(tv[1]), dd(tv[2])};
+    spec[(size_t)w * 18 + r] =
+        face_to_face(s, si, t, ti, cd{dc.wave_re_d[k], dc.wave_im_d[k]}, (double)dc.h * 0.1, layer == 1);
+}
+
+// Phase B: corner point integrals, FFT, packing into the pool record
+__global__ void fc_finish_kernel(DevConsts dc, const float *verts, const int *tris, const float *center,
+                                 const int *basec, const float *interp, const int *face_start, int nt,
+                                 const int *face_nbr, const int *face_pool, const int *work, int nwork, const cf *spec,
+                                 __half2 *pool_w, float2 *pool_scale)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwork)
+        return;
+    int p = work[w];
+    int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
+    f3 sv[3];
+    int si[3];
+    load_tri(verts, tris, nbr, sv, si);
+    f3 nbc = load3(center, nbr);
+    f3 pts[8];
+    float sc[8];
+    int n = 0;
+    int bx = basec[3 * ctr], by = basec[3 * ctr + 1], bz = basec[3 * ctr + 2];
+    for (int dx = 0; dx < 2; dx++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dz = 0; dz < 2; dz++)
+            {
+                int widx = dx * 4 + dy * 2 + dz;
+                f3 c = cell_center(bx + dx, by + dy, bz + dz, dc.h, dc.mn);
+                if (abs(c.x - nbc.x) > dc.h * 1.5 || abs(c.y - nbc.y) > dc.h * 1.5 || abs(c.z - nbc.z) > dc.h * 1.5)
+                {
+                    pts[n] = c;
+                    sc[n] = -interp[8 * ctr + widx];
+                    n++;
+                }
+            }
+    cf ss[kTaps], sd[kTaps];
+    for (int k = 0; k <= kTaps / 2; k++)
+    {
+        cf a = spec[(size_t)w * 18 + k], b = spec[(size_t)w * 18 + 9 + k];
+        cf kk{dc.wave_re[k], dc.wave_im[k]};
+        cf ps = ref32::face_to_points(sv, pts, sc, n, true, kk, false);
+        cf pd = ref32::face_to_points(sv, pts, sc, n, true, kk, true);
+        ss[k] = cf{a.re + ps.re, a.im + ps.im};
+        sd[k] = cf{b.re + pd.re, b.im + pd.im};
+    }
+    float ws[kTaps], wd[kTaps];
+    spectrum_to_weights(ss, dc.lambda, ws);
+    spectrum_to_weights(sd, dc.lambda, wd);
+    int slot = face_pool[p];
+    pack_half(ws, wd, pool_w + (size_t)slot * kTaps, pool_scale + slot);
+}
+
+__global__ void fc_finish_kernel_d(DevConsts dc, const float *verts, const int *tris, const float *center,
+                                   const int *basec, const double *interp, const int *face_start, int nt,
+                                   const int *face_nbr, const int *face_pool, const int *work, int nwork,
+                                   const cd *spec, double2 *pool_w)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwork)
+        return;
+    using namespace f64;
+    int p = work[w];
+    int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
+    f3 svf[3];
+    int si[3];
+    load_tri(verts, tris, nbr, svf, si);
+    d3 sv[3] = {dd(svf[0]), dd(svf[1]), dd(svf[2])};
+    d3 nbc = (1.0 / 3) * (sv[0] + sv[1] + sv[2]);
+    double h = dc.h;
+    d3 pts[8];
+    double sc[8];
+    int n = 0;
+    int bx = basec[3 * ctr], by = basec[3 * ctr + 1], bz = basec[3 * ctr + 2];
+    for (int dx = 0; dx < 2; dx++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dz = 0; dz < 2; dz++)
+            {
+                int widx = dx * 4 + dy * 2 + dz;
+                d3 c{(bx + dx + 0.5) * h + dc.mn.x, (by + dy + 0.5) * h + dc.mn.y, (bz + dz + 0.5) * h + dc.mn.z};
+                if (fabs(c.x - nbc.x) > h * 1.5 || fabs(c.y - nbc.y) > h * 1.5 || fabs(c.z - nbc.z) > h * 1.5)
+                {
+                    pts[n] = c;
+                    sc[n] = -interp[8 * ctr + widx];
+                    n++;
+                }
+            }
+    cd ss[kTaps], sd[kTaps];
+    for (int k = 0; k <= kTaps / 2; k++)
+    {
+        cd a = spec[(size_t)w * 18 + k], b = spec[(size_t)w * 18 + 9 + k];
+        cd kk{dc.wave_re_d[k], dc.wave_im_d[k]};
+        cd ps = face_to_points(sv, pts, sc, n, kk, false);
+        cd pd = face_to_points(sv, pts, sc, n, kk, true);
+        ss[k] = cd{a.re + ps.re, a.im + ps.im};
+        sd[k] = cd{b.re + pd.re, b.im + pd.im};
+    }
+    double ws[kTaps], wd[kTaps];
+    spectrum_to_weights_d(ss, dc.lambda_d, ws);
+    spectrum_to_weights_d(sd, dc.lambda_d, wd);
+    pack_double(ws, wd, pool_w + (size_t)face_pool[p] * kTaps);
+}
+
+template <typename Rec>
+__global__ void gather_face_kernel(const int *face_pool, long long pf, const Rec *pool_w, const float2 *pool_scale,
+                                   Rec *face_w, float2 *face_scale)
+{
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= pf * kTaps)
+        return;
+    long long p = g / kTaps;
+    int k = (int)(g % kTaps);
+    int slot = face_pool[p];
+    face_w[p * kTaps + k] = pool_w[(size_t)slot * kTaps + k];
+    if (k == 0 && pool_scale)
+        face_scale[p] = pool_scale[slot];
+}
+
+// 0.5 * area - sum_j factor_j with factor_j = double-layer weight 0 of pair j, summed in
+// list order in the working precision (pppm.cu:172-193)
+__global__ void denom_kernel(const int *face_start, int nt, const float *area, const __half2 *face_w,
+                             const float2 *face_scale, const double2 *face_wd, double *denom)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    if (face_wd)
+    {
+        double s = 0;
+        for (int p = face_start[i]; p < face_start[i + 1]; p++)
+            s += face_wd[(size_t)p * kTaps].y;
+        denom[i] = 0.5 * (double)area[i] - s;
+    }
+    else
+    {
+        float s = 0;
+        for (int p = face_start[i]; p < face_start[i + 1]; p++)
+            s += (float)__high2half(face_w[(size_t)p * kTaps]) * face_scale[p].y;
+        denom[i] = 0.5 * area[i] - s;
+    }
+}
+
+DevConsts make_consts(const Handle &h)
+{
+    DevConsts dc;
+    dc.lambda = h.tc.lambda;
+    dc.lambda_d = h.tc.lambda_d;
+    for (int k = 0; k < kTaps; k++)
+    {
+        dc.wave_re[k] = h.tc.wave_re[k];
+        dc.wave_im[k] = h.tc.wave_im[k];
+        dc.wave_re_d[k] = h.tc.wave_re_d[k];
+        dc.wave_im_d[k] = h.tc.wave_im_d[k];
+    }
+    dc.threshold = h.tc.threshold;
+    dc.c = h.prm.c;
+    dc.dt = h.prm.dt;
+    dc.h = h.prm.dl;
+    dc.mn = f3{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
+    dc.res = h.res;
+    return dc;
+}
+
+}  // namespace
+
+int cache_refresh(Handle &h)
+{
+    cudaStream_t s = h.stream;
+    const int nt = h.nt, T = 256;
+    const size_t rec_bytes = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    DevConsts dc = make_consts(h);
+
+    // ---- one-time allocations
+    if (!h.d_gc_w)
+    {
+        PB_TRY(dev_alloc(&h.d_gc_w, (size_t)nt * 54 * rec_bytes));
+        if (!h.fp64)
+            PB_TRY(dalloc(&h.d_gc_scale, (size_t)nt * 54));
+        PB_TRY(dalloc(&h.d_gc_snap, (size_t)nt * 7));
+        PB_TRY(dalloc(&h.d_gc_flag, (size_t)nt));
+        PB_TRY(dalloc(&h.d_fc_keys, (size_t)nt * kFaceCacheSlots));
+        PB_TRY(dalloc(&h.d_fc_slot, (size_t)nt * kFaceCacheSlots));
+        PB_CUDA(cudaMemsetAsync(h.d_fc_keys, 0xff, sizeof(int) * (size_t)nt * kFaceCacheSlots, s));
+        PB_TRY(dalloc(&h.d_pool_count, 1));
+        PB_CUDA(cudaMemsetAsync(h.d_pool_count, 0, sizeof(int), s));
+        PB_TRY(dalloc(&h.d_face_interp, (size_t)nt * 8));
+        if (h.fp64)
+            PB_TRY(dalloc(&h.d_face_interp_d, (size_t)nt * 8));
+        PB_TRY(dalloc(&h.d_face_denom, (size_t)nt));
+        h.pool_used = 0;
+        h.gc_empty = true;
+    }
+
+    // ---- grid cache
+    gc_flag_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_center, h.d_normal, h.d_area, h.d_gc_snap, nt, h.prm.dl,
+                                               h.gc_empty ? 1 : 0, h.d_gc_flag);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    if (h.fp64)
+        gc_compute_kernel_d<<<div_up((long long)nt * 27, 128), 128, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc,
+                                                                             h.d_center, h.d_normal, h.d_area,
+                                                                             h.d_gc_flag, nt, (double2 *)h.d_gc_w,
+                                                                             h.d_gc_snap);
+    else
+        gc_compute_kernel<<<div_up((long long)nt * 27, 128), 128, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc,
+                                                                           h.d_center, h.d_normal, h.d_area,
+                                                                           h.d_gc_flag, nt, (__half2 *)h.d_gc_w,
+                                                                           h.d_gc_scale, h.d_gc_snap);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    h.gc_empty = false;
+    if (h.p3 > 0)
+    {
+        if (h.fp64)
+            gather_w3_kernel<double2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(
+                h.d_p3_tri, h.d_p3_woff, h.p3, (const double2 *)h.d_gc_w, nullptr, (double2 *)h.d_w3, nullptr);
+        else
+            gather_w3_kernel<__half2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(h.d_p3_tri, h.d_p3_woff, h.p3,
+                                                                            (const __half2 *)h.d_gc_w, h.d_gc_scale,
+                                                                            (__half2 *)h.d_w3, h.d_w3_scale);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+
+    // ---- face cache
+    const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
+    interp_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_verts, h.d_tris, h.d_basec, nt, h.prm.dl, mn, h.d_face_interp,
+                                               h.d_face_interp_d);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    if (h.pf > 0)
+    {
+        // every pair may be new: make room for pf more records
+        long long need = h.pool_used + h.pf;
+        if (need > h.pool_cap)
+        {
+            long long nc = need + need / 2 + 1024;
+            void *nw = nullptr;
+            float2 *nsc = nullptr, *nmeta = nullptr;
+            PB_TRY(dev_alloc(&nw, (size_t)nc * rec_bytes));
+            if (!h.fp64)
+                PB_TRY(dalloc(&nsc, (size_t)nc));
+            PB_TRY(dalloc(&nmeta, (size_t)nc));
+            if (h.pool_used > 0)
+            {
+                PB_CUDA(cudaMemcpyAsync(nw, h.d_pool_w, (size_t)h.pool_used * rec_bytes, cudaMemcpyDeviceToDevice, s));
+                if (!h.fp64)
+                    PB_CUDA(cudaMemcpyAsync(nsc, h.d_pool_scale, (size_t)h.pool_used * sizeof(float2),
+                                            cudaMemcpyDeviceToDevice, s));
+                PB_CUDA(cudaMemcpyAsync(nmeta, h.d_pool_meta, (size_t)h.pool_used * sizeof(float2),
+                                        cudaMemcpyDeviceToDevice, s));
+            }
+            PB_CUDA(cudaStreamSynchronize(s));
+            dev_free(h.d_pool_w);
+            dev_free(h.d_pool_scale);
+            dev_free(h.d_pool_meta);
+            h.d_pool_w = nw;
+            h.d_pool_scale = nsc;
+            h.d_pool_meta = nmeta;
+            h.pool_cap = nc;
+        }
+        PB_CUDA(cudaMemsetAsync(h.d_status, 0, sizeof(int), s));
+        fc_lookup_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(
+            h.d_face_start, h.d_face_nbr, nt, h.d_center, h.d_normal, h.d_fc_keys, h.d_fc_slot, h.d_pool_count,
+            h.pool_cap, h.d_pool_meta, h.d_face_pool, h.d_pair_flag, h.d_status);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+        int st = 0;
+        PB_TRY(read_int(h, h.d_status, &st));
+        if (st)
+        {
+            set_error("face cache: more than %d distinct neighbours seen by one face", kFaceCacheSlots);
+            return st;
+        }
+        int used = 0;
+        PB_TRY(read_int(h, h.d_pool_count, &used));
+        h.pool_used = used;
+
+        // compact the recompute list
+        int *pos = h.d_flags;  // res^3 scratch is free after mesh_build
+        int *work = h.d_flags + (h.pf + 1);
+        if (2 * (h.pf + 1) > 4 * (h.n_cells + 1))
+        {
+            set_error("face pair scratch too small");
+            return PPPM_ERR_CAPACITY;
+        }
+        PB_TRY(exclusive_scan(h, h.d_pair_flag, pos, h.pf));
+        int nwork = 0;
+        PB_TRY(read_int(h, pos + h.pf, &nwork));
+        if (nwork > 0)
+        {
+            compact_pairs_kernel<<<div_up(h.pf, T), T, 0, s>>>(h.d_pair_flag, pos, h.pf, work);
+            h.launches++;
+            size_t need_spec = (size_t)nwork * 18 * (h.fp64 ? sizeof(cd) : sizeof(cf));
+            if (need_spec > h.spec_bytes)
+            {
+                dev_free(h.d_spec);
+                h.d_spec = nullptr;
+                PB_TRY(dev_alloc(&h.d_spec, need_spec + need_spec / 2));
+                h.spec_bytes = need_spec + need_spec / 2;
+            }
+            if (h.fp64)
+            {
+                fc_spectra_kernel_d<<<div_up((long long)nwork * 18, 128), 128, 0, s>>>(
+                    dc, h.d_verts, h.d_tris, h.d_face_start, nt, h.d_face_nbr, work, nwork, (cd *)h.d_spec);
+                fc_finish_kernel_d<<<div_up(nwork, 128), 128, 0, s>>>(
+                    dc, h.d_verts, h.d_tris, h.d_center, h.d_basec, h.d_face_interp_d, h.d_face_start, nt,
+                    h.d_face_nbr, h.d_face_pool, work, nwork, (const cd *)h.d_spec, (double2 *)h.d_pool_w);
+            }
+            else
+            {
+                int mode = h.prm.weights == PPPM_WEIGHTS_FP64 ? 1 : 0;
+                fc_spectra_kernel<<<div_up((long long)nwork * 18, 128), 128, 0, s>>>(
+                    dc, h.d_verts, h.d_tris, h.d_face_start, nt, h.d_face_nbr, work, nwork, mode, (cf *)h.d_spec);
+                fc_finish_kernel<<<div_up(nwork, 128), 128, 0, s>>>(
+                    dc, h.d_verts, h.d_tris, h.d_center, h.d_basec, h.d_face_interp, h.d_face_start, nt,
+                    h.d_face_nbr, h.d_face_pool, work, nwork, (const cf *)h.d_spec, (__half2 *)h.d_pool_w,
+                    h.d_pool_scale);
+            }
+            h.launches += 2;
+            PB_CHECK_LAUNCH();
+        }
+        if (h.fp64)
+            gather_face_kernel<double2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+                h.d_face_pool, h.pf, (const double2 *)h.d_pool_w, nullptr, (double2 *)h.d_face_w, nullptr);
+        else
+            gather_face_kernel<__half2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+                h.d_face_pool, h.pf, (const __half2 *)h.d_pool_w, h.d_pool_scale, (__half2 *)h.d_face_w,
+                h.d_face_scale);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+    denom_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_face_start, nt, h.d_area,
+                                              h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
+                                              h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
+
+int cache_free(Handle &h)
+{
+    void *ptrs[] = {h.d_gc_w,      h.d_gc_scale,  h.d_gc_snap,   h.d_gc_flag,    h.d_fc_keys,
+                    h.d_fc_slot,   h.d_pool_w,    h.d_pool_scale, h.d_pool_meta, h.d_pool_count,
+                    h.d_face_interp, h.d_face_interp_d, h.d_face_denom, h.d_spec};
+    for (void *p : ptrs)
+        dev_free(p);
+    h.d_gc_w = nullptr;
+    h.d_gc_scale = nullptr;
+    h.d_gc_snap = nullptr;
+    h.d_gc_flag = nullptr;
+    h.d_fc_keys = h.d_fc_slot = h.d_pool_count = nullptr;
+    h.d_pool_w = nullptr;
+    h.d_pool_scale = h.d_pool_meta = nullptr;
+    h.d_face_interp = nullptr;
+    h.d_face_interp_d = nullptr;
+    h.d_face_denom = nullptr;
+    h.d_spec = nullptr;
+    h.pool_cap = h.pool_used = 0;
+    h.spec_bytes = 0;
+    return PPPM_OK;
+}
+
+}  // namespace pb
+
+// ---------------------------------------------------------------- parity import -------
+namespace pb
+{
+
+namespace
+{
+// reference LayerWeightHalf record: half s[16], float ms, half d[16], float md (72 bytes,
+// bem.h:163-169)
+struct RefRecord
+{
+    __half s[kTaps];
+    float ms;
+    __half d[kTaps];
+    float md;
+};
+static_assert(sizeof(RefRecord) == 72, "reference record layout");
+
+__global__ void import_records_kernel(const RefRecord *in, long long n, const long long *dst_index, __half2 *w,
+                                      float2 *scale)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    long long r = dst_index ? dst_index[i] : i;
+    RefRecord rec = in[i];
+    for (int k = 0; k < kTaps; k++)
+        w[r * kTaps + k] = __halves2half2(rec.s[k], rec.d[k]);
+    scale[r] = make_float2(rec.ms, rec.md);
+}
+
+__global__ void snapshot_kernel(const float *center, const float *normal, const float *area, int nt, float *snap)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    for (int k = 0; k < 3; k++)
+    {
+        snap[7 * i + k] = center[3 * i + k];
+        snap[7 * i + 3 + k] = normal[3 * i + k];
+    }
+    snap[7 * i + 6] = area[i];
+}
+}  // namespace
+
+int cache_regather(Handle &h)
+{
+    cudaStream_t s = h.stream;
+    const int T = 256;
+    if (h.p3 > 0)
+    {
+        if (h.fp64)
+            gather_w3_kernel<double2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(
+                h.d_p3_tri, h.d_p3_woff, h.p3, (const double2 *)h.d_gc_w, nullptr, (double2 *)h.d_w3, nullptr);
+        else
+            gather_w3_kernel<__half2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(h.d_p3_tri, h.d_p3_woff, h.p3,
+                                                                            (const __half2 *)h.d_gc_w, h.d_gc_scale,
+                                                                            (__half2 *)h.d_w3, h.d_w3_scale);
+        h.launches++;
+    }
+    if (h.pf > 0)
+    {
+        if (h.fp64)
+            gather_face_kernel<double2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+                h.d_face_pool, h.pf, (const double2 *)h.d_pool_w, nullptr, (double2 *)h.d_face_w, nullptr);
+        else
+            gather_face_kernel<__half2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+                h.d_face_pool, h.pf, (const __half2 *)h.d_pool_w, h.d_pool_scale, (__half2 *)h.d_face_w,
+                h.d_face_scale);
+        h.launches++;
+    }
+    denom_kernel<<<div_up(h.nt, T), T, 0, s>>>(h.d_face_start, h.nt, h.d_area,
+                                                h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
+                                                h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
+
+int cache_import_grid(Handle &h, const void *records)
+{
+    if (h.fp64)
+        return PPPM_ERR_ARG;
+    cudaStream_t s = h.stream;
+    size_t n = (size_t)h.nt * 54;
+    void *tmp = nullptr;
+    PB_TRY(dev_alloc(&tmp, n * sizeof(RefRecord)));
+    PB_CUDA(cudaMemcpyAsync(tmp, records, n * sizeof(RefRecord), cudaMemcpyHostToDevice, s));
+    import_records_kernel<<<div_up((long long)n, 256), 256, 0, s>>>((const RefRecord *)tmp, (long long)n, nullptr,
+                                                                      (__half2 *)h.d_gc_w, h.d_gc_scale);
+    snapshot_kernel<<<div_up(h.nt, 256), 256, 0, s>>>(h.d_center, h.d_normal, h.d_area, h.nt, h.d_gc_snap);
+    h.launches += 2;
+    PB_CHECK_LAUNCH();
+    PB_CUDA(cudaStreamSynchronize(s));
+    dev_free(tmp);
+    h.gc_empty = false;
+    return cache_regather(h);
+}
+
+int cache_import_face(Handle &h, const int *pairs, const void *records, int n)
+{
+    if (h.fp64)
+        return PPPM_ERR_ARG;
+    cudaStream_t s = h.stream;
+    // (centre, neighbour) -> pool slot of the current face list
+    std::vector<int> start(h.nt + 1), nbr(h.pf), pool(h.pf);
+    PB_CUDA(cudaMemcpyAsync(start.data(), h.d_face_start, sizeof(int) * (h.nt + 1), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(nbr.data(), h.d_face_nbr, sizeof(int) * h.pf, cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(pool.data(), h.d_face_pool, sizeof(int) * h.pf, cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    std::vector<long long> dst(n);
+    for (int i = 0; i < n; i++)
+    {
+        int c = pairs[2 * i], j = pairs[2 * i + 1];
+        if (c < 0 || c >= h.nt)
+            return PPPM_ERR_ARG;
+        long long found = -1;
+        for (int p = start[c]; p < start[c + 1]; p++)
+            if (nbr[p] == j)
+            {
+                found = pool[p];
+                break;
+            }
+        if (found < 0)
+        {
+            set_error("imported face pair (%d, %d) is not in the current 4^3 lists", c, j);
+            return PPPM_ERR_ARG;
+        }
+        dst[i] = found;
+    }
+    void *tmp = nullptr;
+    long long *ddst = nullptr;
+    PB_TRY(dev_alloc(&tmp, (size_t)n * sizeof(RefRecord)));
+    PB_TRY(dalloc(&ddst, (size_t)n));
+    PB_CUDA(cudaMemcpyAsync(tmp, records, (size_t)n * sizeof(RefRecord), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ddst, dst.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, s));
+    import_records_kernel<<<div_up(n, 256), 256, 0, s>>>((const RefRecord *)tmp, n, ddst, (__half2 *)h.d_pool_w,
+                                                         h.d_pool_scale);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    PB_CUDA(cudaStreamSynchronize(s));
+    dev_free(tmp);
+    dev_free(ddst);
+    return cache_regather(h);
+}
+
+}  // namespace pb

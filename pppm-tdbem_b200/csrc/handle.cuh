@@ -1,0 +1,217 @@
+// The solver handle: every device array of one scene, and the internal entry points the
+// C ABI (capi.cu) strings together.
+//
+// HBM layout (one scene):
+//   grid[3]        res^3 real each, x-major / z-contiguous (reference layout); ring by t.
+//                  Between the near-field kernel of step t and the stencil kernel of step
+//                  t+1 the dead slot t+1 carries, at corrected cells only, the FDTD-near
+//                  correction of step t+1 (see step.cu).
+//   pml[3]         res^3 x 6 real (PML only)
+//   neumann/dirichlet  nt x 32 real rings
+//   cell CSR       cell_start[res^3 + 1] / cell_tris[nt] (sorted by triangle id per cell),
+//                  same for base cells
+//   3^3 pairs      n3 corrected cells: n3_cell, n3_start[n3 + 1]; p3 pairs: p3_tri,
+//                  p3_woff; dense weights w3_half[p3][2][32] + w3_scale[p3][2][2]
+//                  (FDTD-near then BEM-near, fp16 + per-row scale, the reference's format)
+//   face pairs     face_start[nt + 1] per centre triangle; pf pairs: face_nbr; dense
+//                  weights face_half[pf][32] + face_scale[pf][2]; per centre: 8 corner cells,
+//                  8 trilinear weights, denominator 0.5 * area - sum(factor)
+//   caches         grid cache nt x 54 records (persistent, with the geometry snapshot of the
+//                  last refresh); face cache per-centre open-addressing table
+//                  (kFaceCacheSlots keys) into a growable record pool
+#pragma once
+#include <vector>
+#include "common.cuh"
+#include "tdbem.cuh"
+
+namespace pb
+{
+
+// Device view of one scene used by the step kernels (POD, passed by value).
+template <typename Real>
+struct SceneView
+{
+    int res;
+    int n_cells;
+    Real *g0, *g1, *g2;  // grid slots for (t+1), t, t-1 after mapping by the launcher
+    const unsigned *corr_mask;
+    // 3^3 pairs
+    int n3;
+    const int *n3_cell;
+    const int *n3_start;
+    const int *p3_tri;
+    const void *w3;        // FP32: __half2[p3][2][16]; FP64: double[p3][2][32]
+    const float2 *w3_scale;  // FP32 only: [p3][2] (single scale, double scale)
+    // faces
+    int nt;
+    const int *face_start;
+    const int *face_nbr;
+    const void *face_w;        // FP32: __half2[pf][16]; FP64: double[pf][32]
+    const float2 *face_scale;  // FP32 only
+    const int *face_corner;    // nt x 8 linear cells
+    const float *face_interp;  // nt x 8 (FP32) ; FP64 uses face_interp_d
+    const double *face_interp_d;
+    const double *face_denom;  // nt
+    Real *neumann;             // nt x 32
+    Real *dirichlet;           // nt x 32
+    float reflect;
+    // listeners
+    int n_listen;
+    const int *listen_cell;  // linear cell
+    const int *listen_n3;    // compact index in the corrected-cell list or -1
+    Real *series;            // [step][listener]
+};
+
+struct Handle
+{
+    pppm_params prm{};
+    bool fp64 = false;
+    size_t real_size = 4;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int res = 0;
+    long long n_cells = 0;
+    int t = -1;
+    long long launches = 0;
+    TdbemConsts tc{};
+
+    void *grid[3] = {nullptr, nullptr, nullptr};  // ring slots, index (t + 3) % 3
+    void *pml[3] = {nullptr, nullptr, nullptr};
+
+    // ---- mesh
+    bool mesh_set = false;
+    int nv = 0, nt = 0;
+    float *d_verts = nullptr;  // 3 nv
+    int *d_tris = nullptr;     // 3 nt
+    float *d_center = nullptr, *d_normal = nullptr, *d_area = nullptr;  // 3nt, 3nt, nt
+    int *d_cellc = nullptr, *d_basec = nullptr;  // 3nt each: grid coord, base coord
+    int *d_cell = nullptr, *d_base = nullptr;    // linear, -1 when outside the grid
+    int *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_tris = nullptr;
+    int *d_base_count = nullptr, *d_base_start = nullptr, *d_base_tris = nullptr;
+    int *d_cursor = nullptr;     // scratch res^3
+    int *d_scan_tmp = nullptr;   // scan scratch
+    size_t scan_tmp_elems = 0;
+    int *d_flags = nullptr;      // res^3 scratch
+
+    // ---- corrected cells and 3^3 pairs
+    int n3 = 0;
+    long long p3 = 0;
+    int *d_n3_cell = nullptr, *d_n3_start = nullptr;
+    int *d_p3_tri = nullptr;
+    unsigned char *d_p3_woff = nullptr;
+    void *d_w3 = nullptr;
+    float2 *d_w3_scale = nullptr;
+    long long p3_cap = 0;
+    unsigned *d_corr_mask = nullptr;
+
+    // ---- base cells and 4^3 lists
+    int b4 = 0;
+    long long p4 = 0;  // sum over base cells of 4^3 list lengths
+    int *d_b4_cell = nullptr, *d_b4_start = nullptr, *d_n4_tris = nullptr;
+    long long n4_cap = 0;
+
+    // ---- face pairs (per centre triangle)
+    long long pf = 0;
+    int *d_face_start = nullptr, *d_face_nbr = nullptr, *d_face_pool = nullptr;
+    void *d_face_w = nullptr;
+    float2 *d_face_scale = nullptr;
+    long long pf_cap = 0;
+    int *d_face_corner = nullptr;
+    float *d_face_interp = nullptr;
+    double *d_face_interp_d = nullptr;
+    double *d_face_denom = nullptr;
+
+    // ---- persistent caches
+    bool gc_empty = true;
+    void *d_gc_w = nullptr;        // FP32: __half2[nt][54][16]; FP64: double[nt][54][32]
+    float2 *d_gc_scale = nullptr;  // FP32: [nt][54]
+    float *d_gc_snap = nullptr;    // nt x 7 centre, normal, area at last refresh
+    int *d_gc_flag = nullptr;      // nt recompute flags
+    int *d_fc_keys = nullptr;      // nt x kFaceCacheSlots neighbour ids, -1 = empty
+    int *d_fc_slot = nullptr;      // nt x kFaceCacheSlots pool slots
+    void *d_pool_w = nullptr;      // pool records (layout as face_w)
+    float2 *d_pool_scale = nullptr;
+    float2 *d_pool_meta = nullptr;  // (normal angle, distance) at last refresh
+    int *d_pool_count = nullptr;    // device counter
+    long long pool_cap = 0;
+    long long pool_used = 0;
+    int *d_pair_flag = nullptr;  // pf scratch: 1 = recompute
+    int *d_status = nullptr;     // device-side status word (capacity / timeout)
+    void *d_spec = nullptr;      // recompute scratch spectra
+    size_t spec_bytes = 0;
+
+    // ---- histories
+    void *d_neumann = nullptr, *d_dirichlet = nullptr;
+
+    // ---- listeners
+    std::vector<int> listen_xyz;
+    std::vector<int> listen_corr;  // 1 if the listener cell is a corrected cell
+    int *d_listen_cell = nullptr, *d_listen_n3 = nullptr;
+    void *d_series = nullptr;
+    long long series_cap = 0;  // steps
+    long long series_count = 0;
+
+    // ---- cell labels
+    int *d_cell_type = nullptr, *d_cell_nearest = nullptr, *d_cell_ghost = nullptr;
+    float *d_cell_points = nullptr;  // res^3 x 7
+    int *d_cell_type_old = nullptr;
+    int ghost_count = 0;
+
+    // ---- timing
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float us_stencil = 0, us_face = 0, us_near = 0;
+
+    // ---- scratch for accelerations
+    float *d_acc = nullptr;
+    long long acc_cap = 0;
+
+    void *slot(int time) const { return grid[((time % 3) + 3) % 3]; }
+    void *pml_slot(int time) const { return pml[((time % 3) + 3) % 3]; }
+};
+
+// ---------------------------------------------------------------- internal API -------
+int dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+template <typename T>
+int dalloc(T **p, size_t count)
+{
+    return dev_alloc((void **)p, count * sizeof(T));
+}
+template <typename T>
+int dgrow(T **p, long long &cap, long long need, cudaStream_t s)
+{
+    if (need <= cap)
+        return PPPM_OK;
+    long long nc = need + need / 2 + 64;
+    dev_free(*p);
+    *p = nullptr;
+    int rc = dev_alloc((void **)p, (size_t)nc * sizeof(T));
+    if (rc)
+        return rc;
+    cap = nc;
+    (void)s;
+    return PPPM_OK;
+}
+
+// mesh.cu
+int mesh_build(Handle &h);                      // geometry + all lists from d_verts/d_tris
+int exclusive_scan(Handle &h, const int *in, int *out, long long n);  // out[n] = total
+int read_int(Handle &h, const int *d, int *out);
+
+// cache.cu
+int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators
+int cache_free(Handle &h);
+int cache_regather(Handle &h);  // dense gathers + denominators from the persistent caches
+int cache_import_grid(Handle &h, const void *records);                         // nt x 54 x 72 B
+int cache_import_face(Handle &h, const int *pairs, const void *records, int n);  // n x 72 B
+
+// step.cu
+int step_prime(Handle &h);
+int step_run(Handle &h, const float *acc_dev, int nsteps);
+
+// cells.cu
+int cells_classify(Handle &h, int *ghost_count);
+int cells_fresh(Handle &h, const float *acc, const float *acc_old, int *fresh_count);
+
+}  // namespace pb

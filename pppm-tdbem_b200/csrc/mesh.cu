@@ -1,0 +1,549 @@
+// Mesh-side structures of one scene, rebuilt on every set_mesh / update_mesh:
+// triangle geometry, per-cell and per-base-cell triangle lists (CSR, triangle ids ascending
+// inside a cell, so the lists are deterministic), the corrected-cell set with its 3^3
+// triangle pairs, the non-empty base cells with their 4^3 lists, and per-triangle face
+// pair lists with interpolation corners.
+//
+// Reference semantics followed (src/algorithm/particle_grid.{h,cu}):
+//   triangle record       particle_grid.cu:40-88 (centre = (v0+v1+v2)/3, normal =
+//                         normalize(cross), area = |cross|/2, grid coord by truncation,
+//                         base coord = coord - (centre < cell centre))
+//   3^3 list of a cell    particle_grid.cu:139-182: cells in [1, res-2]^3 whose 27-cell block
+//                         holds a triangle, sub-cells visited x fastest
+//   4^3 list of a base    particle_grid.cu:184-223: base cells in [1, res-2]^3 with a
+//                         non-empty base list, block (-1..2)^3, x fastest
+// The reference fills lists by atomic append, so its in-cell order varies run to run; the
+// sets are identical.
+#include "handle.cuh"
+
+namespace pb
+{
+
+namespace
+{
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void scan_tiles_kernel(const int *in, int *out, int *tile_sums, long long n_in, long long n_out)
+{
+    __shared__ int warp_tot[kScanThreads / 32];
+    long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++)
+    {
+        long long idx = base + i;
+        v[i] = (idx < n_in) ? in[idx] : 0;
+        sum += v[i];
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off)
+            x += y;
+    }
+    if (lane == 31)
+        warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0)
+    {
+        int w = (lane < kScanThreads / 32) ? warp_tot[lane] : 0;
+        int s = w;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            int y = __shfl_up_sync(0xffffffffu, s, off);
+            if (lane >= off)
+                s += y;
+        }
+        if (lane < kScanThreads / 32)
+            warp_tot[lane] = s - w;
+        if (lane == kScanThreads / 32 - 1 && tile_sums)
+            tile_sums[blockIdx.x] = s;
+    }
+    __syncthreads();
+    int run = x - sum + warp_tot[warp];
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++)
+    {
+        long long idx = base + i;
+        if (idx < n_out)
+            out[idx] = run;
+        run += v[i];
+    }
+}
+
+__global__ void scan_add_kernel(int *out, const int *tile_offsets, long long n_out)
+{
+    long long base = (long long)blockIdx.x * kScanTile;
+    int add = tile_offsets[blockIdx.x];
+    for (int i = threadIdx.x; i < kScanTile; i += blockDim.x)
+    {
+        long long idx = base + i;
+        if (idx < n_out)
+            out[idx] += add;
+    }
+}
+
+__device__ inline void flag_error(int *status, int code) { atomicCAS(status, 0, code); }
+
+// ---- triangle geometry (particle_grid.cu:40-88 without the incremental list moves)
+__global__ void geometry_kernel(const float *verts, const int *tris, int nt, int res, float h, f3 mn, float *center,
+                                float *normal, float *area, int *cellc, int *basec, int *cell, int *base, int *status)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    f3 v0 = load3(verts, tris[3 * i]), v1 = load3(verts, tris[3 * i + 1]), v2 = load3(verts, tris[3 * i + 2]);
+    f3 c = (v0 + v1 + v2) / 3.0f;
+    f3 e = cross3(v1 - v0, v2 - v0);
+    f3 n = normalize3(e);
+    float a = len3(e) / 2.0f;
+    f3 rel = (c - mn) / h;
+    int gx = (int)rel.x, gy = (int)rel.y, gz = (int)rel.z;
+    f3 cc = cell_center(gx, gy, gz, h, mn);
+    f3 d = c - cc;
+    int bx = gx - (d.x < 0), by = gy - (d.y < 0), bz = gz - (d.z < 0);
+    store3(center, i, c);
+    store3(normal, i, n);
+    area[i] = a;
+    cellc[3 * i] = gx;
+    cellc[3 * i + 1] = gy;
+    cellc[3 * i + 2] = gz;
+    basec[3 * i] = bx;
+    basec[3 * i + 1] = by;
+    basec[3 * i + 2] = bz;
+    // every structure below reads up to two cells around a triangle: keep triangles at
+    // least two cells inside the grid (the reference reads those cells without checks)
+    bool ok = gx >= 2 && gy >= 2 && gz >= 2 && gx <= res - 3 && gy <= res - 3 && gz <= res - 3 && bx >= 1 &&
+              by >= 1 && bz >= 1 && bx <= res - 3 && by <= res - 3 && bz <= res - 3 && isfinite(c.x) &&
+              isfinite(c.y) && isfinite(c.z);
+    if (!ok)
+    {
+        flag_error(status, PPPM_ERR_ARG);
+        cell[i] = -1;
+        base[i] = -1;
+        return;
+    }
+    cell[i] = (gx * res + gy) * res + gz;
+    base[i] = (bx * res + by) * res + bz;
+}
+
+__global__ void count_kernel(const int *key, int n, int *count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && key[i] >= 0)
+        atomicAdd(&count[key[i]], 1);
+}
+
+__global__ void fill_kernel(const int *key, int n, const int *start, int *cursor, int *list)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && key[i] >= 0)
+        list[start[key[i]] + atomicAdd(&cursor[key[i]], 1)] = i;
+}
+
+// sort each cell's segment ascending (segments are short: a few to ~100 entries)
+__global__ void sort_segments_kernel(const int *start, long long n_cells, int *list)
+{
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells)
+        return;
+    int b = start[c], e = start[c + 1];
+    for (int i = b + 1; i < e; i++)
+    {
+        int v = list[i], j = i - 1;
+        while (j >= b && list[j] > v)
+        {
+            list[j + 1] = list[j];
+            j--;
+        }
+        list[j + 1] = v;
+    }
+}
+
+__device__ inline int cell_len(const int *start, int res, int x, int y, int z)
+{
+    if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res)
+        return 0;
+    int c = (x * res + y) * res + z;
+    return start[c + 1] - start[c];
+}
+
+// corrected-cell flags and 3^3 counts; base-cell flags and 4^3 counts
+__global__ void block_counts_kernel(const int *cell_start, const int *base_start, int res, int *flag3, int *len3,
+                                    int *flag4, int *len4)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)res * res * res;
+    if (i >= n)
+        return;
+    int x = (int)(i / ((long long)res * res)), y = (int)((i / res) % res), z = (int)(i % res);
+    bool inner = x >= 1 && y >= 1 && z >= 1 && x <= res - 2 && y <= res - 2 && z <= res - 2;
+    int s3 = 0, s4 = 0;
+    if (inner)
+    {
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dz = -1; dz <= 1; dz++)
+                    s3 += cell_len(cell_start, res, x + dx, y + dy, z + dz);
+    }
+    bool has_base = inner && (base_start[i + 1] - base_start[i]) > 0;
+    if (has_base)
+    {
+        for (int dx = -1; dx <= 2; dx++)
+            for (int dy = -1; dy <= 2; dy++)
+                for (int dz = -1; dz <= 2; dz++)
+                    s4 += cell_len(cell_start, res, x + dx, y + dy, z + dz);
+    }
+    flag3[i] = s3 > 0;
+    len3[i] = s3;
+    flag4[i] = has_base;
+    len4[i] = s4;
+}
+
+__global__ void compact_kernel(const int *flag, const int *pos, const int *len, long long n, int *out_cell, int *out_len)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i])
+        return;
+    out_cell[pos[i]] = (int)i;
+    out_len[pos[i]] = len[i];
+}
+
+// 3^3 pairs of each corrected cell, sub-cells x fastest (particle_grid.cu:164-182);
+// woff = GridCache weight index of (cell - triangle cell) (pppm_cache.h:38-42)
+__global__ void fill_pairs3_kernel(const int *n3_cell, const int *n3_start, int n3, int res, const int *cell_start,
+                                   const int *cell_tris, int *p3_tri, unsigned char *p3_woff, unsigned *mask)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3)
+        return;
+    int c = n3_cell[i];
+    int x = c / (res * res), y = (c / res) % res, z = c % res;
+    int o = n3_start[i];
+    for (int idx = 0; idx < 27; idx++)
+    {
+        int dx = idx % 3 - 1, dy = idx / 3 % 3 - 1, dz = idx / 9 - 1;
+        int sc = ((x + dx) * res + (y + dy)) * res + (z + dz);
+        unsigned char woff = (unsigned char)((1 - dx) + 3 * (1 - dy) + 9 * (1 - dz));
+        for (int j = cell_start[sc]; j < cell_start[sc + 1]; j++)
+        {
+            p3_tri[o] = cell_tris[j];
+            p3_woff[o] = woff;
+            o++;
+        }
+    }
+    atomicOr(&mask[c >> 5], 1u << (c & 31));
+}
+
+// 4^3 lists of the non-empty base cells (particle_grid.cu:198-223)
+__global__ void fill_n4_kernel(const int *b4_cell, const int *b4_start, int b4, int res, const int *cell_start,
+                               const int *cell_tris, int *n4_tris)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b4)
+        return;
+    int c = b4_cell[i];
+    int x = c / (res * res), y = (c / res) % res, z = c % res;
+    int o = b4_start[i];
+    for (int idx = 0; idx < 64; idx++)
+    {
+        int sx = x + idx % 4 - 1, sy = y + idx / 4 % 4 - 1, sz = z + idx / 16 - 1;
+        if (sx < 0 || sy < 0 || sz < 0 || sx >= res || sy >= res || sz >= res)
+            continue;
+        int sc = (sx * res + sy) * res + sz;
+        for (int j = cell_start[sc]; j < cell_start[sc + 1]; j++)
+            n4_tris[o++] = cell_tris[j];
+    }
+}
+
+// per centre triangle: length of its base cell's 4^3 list
+__global__ void face_len_kernel(const int *base, int nt, const int *b4_pos, const int *b4_flag, const int *b4_start,
+                                int *face_len)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    int b = base[i];
+    if (b < 0 || !b4_flag[b])
+    {
+        face_len[i] = 0;
+        return;
+    }
+    int k = b4_pos[b];
+    face_len[i] = b4_start[k + 1] - b4_start[k];
+}
+
+__global__ void face_fill_kernel(const int *base, const int *basec, int nt, int res, const int *b4_pos,
+                                 const int *b4_flag, const int *b4_start, const int *n4_tris, const int *face_start,
+                                 int *face_nbr, int *face_corner)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt)
+        return;
+    int b = base[i];
+    int bx = basec[3 * i], by = basec[3 * i + 1], bz = basec[3 * i + 2];
+    for (int w = 0; w < 8; w++)
+    {
+        int dx = w >> 2, dy = (w >> 1) & 1, dz = w & 1;
+        face_corner[8 * i + w] = ((bx + dx) * res + (by + dy)) * res + (bz + dz);
+    }
+    if (b < 0 || !b4_flag[b])
+        return;
+    int k = b4_pos[b];
+    int o = face_start[i];
+    for (int j = b4_start[k]; j < b4_start[k + 1]; j++)
+        face_nbr[o++] = n4_tris[j];
+}
+
+}  // namespace
+
+int read_int(Handle &h, const int *d, int *out)
+{
+    PB_CUDA(cudaMemcpyAsync(out, d, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    return PPPM_OK;
+}
+
+// out[0..n] exclusive prefix sums of in[0..n), out[n] = total.  Scratch: h.d_scan_tmp.
+static int scan_level(Handle &h, const int *in, int *out, long long n_in, int *scratch, long long scratch_left)
+{
+    long long n_out = n_in + 1;
+    long long nb = (n_out + kScanTile - 1) / kScanTile;
+    if (nb > 1)
+    {
+        if (scratch_left < 2 * (nb + 1))
+        {
+            set_error("scan scratch exhausted");
+            return PPPM_ERR_CAPACITY;
+        }
+        int *sums = scratch, *offs = scratch + nb + 1;
+        scan_tiles_kernel<<<(unsigned)nb, kScanThreads, 0, h.stream>>>(in, out, sums, n_in, n_out);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+        PB_TRY(scan_level(h, sums, offs, nb, scratch + 2 * (nb + 1), scratch_left - 2 * (nb + 1)));
+        scan_add_kernel<<<(unsigned)nb, 256, 0, h.stream>>>(out, offs, n_out);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+    else
+    {
+        scan_tiles_kernel<<<1, kScanThreads, 0, h.stream>>>(in, out, nullptr, n_in, n_out);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+    return PPPM_OK;
+}
+
+int exclusive_scan(Handle &h, const int *in, int *out, long long n)
+{
+    long long need = 4 * (n / kScanTile + 8) + 64;
+    if ((long long)h.scan_tmp_elems < need)
+    {
+        dev_free(h.d_scan_tmp);
+        h.d_scan_tmp = nullptr;
+        PB_TRY(dalloc(&h.d_scan_tmp, (size_t)need));
+        h.scan_tmp_elems = (size_t)need;
+    }
+    return scan_level(h, in, out, n, h.d_scan_tmp, (long long)h.scan_tmp_elems);
+}
+
+int mesh_build(Handle &h)
+{
+    cudaStream_t s = h.stream;
+    const int res = h.res, nt = h.nt;
+    const long long nc = h.n_cells;
+    const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
+    const int T = 256;
+
+    // per-mesh arrays sized by nt and res^3 (allocated once per set_mesh)
+    if (!h.d_center)
+    {
+        PB_TRY(dalloc(&h.d_center, 3 * (size_t)nt));
+        PB_TRY(dalloc(&h.d_normal, 3 * (size_t)nt));
+        PB_TRY(dalloc(&h.d_area, (size_t)nt));
+        PB_TRY(dalloc(&h.d_cellc, 3 * (size_t)nt));
+        PB_TRY(dalloc(&h.d_basec, 3 * (size_t)nt));
+        PB_TRY(dalloc(&h.d_cell, (size_t)nt));
+        PB_TRY(dalloc(&h.d_base, (size_t)nt));
+        PB_TRY(dalloc(&h.d_cell_tris, (size_t)nt));
+        PB_TRY(dalloc(&h.d_base_tris, (size_t)nt));
+        PB_TRY(dalloc(&h.d_cell_count, (size_t)nc));
+        PB_TRY(dalloc(&h.d_base_count, (size_t)nc));
+        PB_TRY(dalloc(&h.d_cell_start, (size_t)nc + 1));
+        PB_TRY(dalloc(&h.d_base_start, (size_t)nc + 1));
+        PB_TRY(dalloc(&h.d_cursor, (size_t)nc + 1));
+        PB_TRY(dalloc(&h.d_flags, 4 * ((size_t)nc + 1)));
+        PB_TRY(dalloc(&h.d_face_start, (size_t)nt + 1));
+        PB_TRY(dalloc(&h.d_face_corner, 8 * (size_t)nt));
+        PB_TRY(dalloc(&h.d_status, 4));
+    }
+    PB_CUDA(cudaMemsetAsync(h.d_status, 0, 4 * sizeof(int), s));
+
+    geometry_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_verts, h.d_tris, nt, res, h.prm.dl, mn, h.d_center, h.d_normal,
+                                                 h.d_area, h.d_cellc, h.d_basec, h.d_cell, h.d_base, h.d_status);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    int st = 0;
+    PB_TRY(read_int(h, h.d_status, &st));
+    if (st)
+    {
+        set_error("mesh leaves the grid interior: every triangle must lie at least two cells inside the grid");
+        return st;
+    }
+
+    // ---- per-cell and per-base-cell CSR, ids ascending inside a cell
+    for (int pass = 0; pass < 2; pass++)
+    {
+        const int *key = pass == 0 ? h.d_cell : h.d_base;
+        int *count = pass == 0 ? h.d_cell_count : h.d_base_count;
+        int *start = pass == 0 ? h.d_cell_start : h.d_base_start;
+        int *list = pass == 0 ? h.d_cell_tris : h.d_base_tris;
+        PB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * nc, s));
+        PB_CUDA(cudaMemsetAsync(h.d_cursor, 0, sizeof(int) * nc, s));
+        count_kernel<<<div_up(nt, T), T, 0, s>>>(key, nt, count);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+        PB_TRY(exclusive_scan(h, count, start, nc));
+        fill_kernel<<<div_up(nt, T), T, 0, s>>>(key, nt, start, h.d_cursor, list);
+        h.launches++;
+        sort_segments_kernel<<<div_up(nc, T), T, 0, s>>>(start, nc, list);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+
+    // ---- corrected cells (3^3) and base cells (4^3)
+    int *flag3 = h.d_flags, *len3 = h.d_flags + (nc + 1), *flag4 = h.d_flags + 2 * (nc + 1),
+        *len4 = h.d_flags + 3 * (nc + 1);
+    block_counts_kernel<<<div_up(nc, T), T, 0, s>>>(h.d_cell_start, h.d_base_start, res, flag3, len3, flag4, len4);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    // positions of corrected cells -> d_cursor; positions of base cells -> d_count of bases
+    // (the counts were consumed by the CSR build above)
+    int *pos3 = h.d_cursor, *pos4 = h.d_base_count;
+    PB_TRY(exclusive_scan(h, flag3, pos3, nc));
+    int n3 = 0;
+    PB_TRY(read_int(h, pos3 + nc, &n3));
+    // base-cell positions need nc + 1 entries: the base_count array has only nc, so use the
+    // cell_count array (also consumed) for the last entry via a separate scan target
+    PB_TRY(exclusive_scan(h, flag4, h.d_cell_count, nc - 1));
+    (void)pos4;
+    int *b4_pos = h.d_cell_count;  // b4_pos[c] valid for flagged c < nc - 1 (the last cell is never inner)
+    int b4 = 0;
+    PB_TRY(read_int(h, b4_pos + (nc - 1), &b4));
+
+    h.n3 = n3;
+    h.b4 = b4;
+    {
+        long long cap3 = 0;
+        (void)cap3;
+    }
+    // (re)allocate compact arrays
+    dev_free(h.d_n3_cell);
+    dev_free(h.d_n3_start);
+    dev_free(h.d_b4_cell);
+    dev_free(h.d_b4_start);
+    h.d_n3_cell = h.d_n3_start = h.d_b4_cell = h.d_b4_start = nullptr;
+    PB_TRY(dalloc(&h.d_n3_cell, (size_t)n3 + 1));
+    PB_TRY(dalloc(&h.d_n3_start, (size_t)n3 + 1));
+    PB_TRY(dalloc(&h.d_b4_cell, (size_t)b4 + 1));
+    PB_TRY(dalloc(&h.d_b4_start, (size_t)b4 + 1));
+    int *n3_len = h.d_base_count;  // scratch (nc entries available)
+    compact_kernel<<<div_up(nc, T), T, 0, s>>>(flag3, pos3, len3, nc, h.d_n3_cell, n3_len);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    PB_TRY(exclusive_scan(h, n3_len, h.d_n3_start, n3));
+    int p3 = 0;
+    PB_TRY(read_int(h, h.d_n3_start + n3, &p3));
+    h.p3 = p3;
+
+    // b4: compact into b4_cell with lengths in a scratch then scan.  The 3^3 scratch (len3)
+    // is free again after n3_len was written.
+    int *b4_len = len3;
+    compact_kernel<<<div_up(nc - 1, T), T, 0, s>>>(flag4, b4_pos, len4, nc - 1, h.d_b4_cell, b4_len);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    PB_TRY(exclusive_scan(h, b4_len, h.d_b4_start, b4));
+    int p4 = 0;
+    PB_TRY(read_int(h, h.d_b4_start + b4, &p4));
+    h.p4 = p4;
+
+    // ---- 3^3 pairs and corrected-cell mask
+    if (p3 > h.p3_cap)
+    {
+        dev_free(h.d_p3_tri);
+        dev_free(h.d_p3_woff);
+        dev_free(h.d_w3);
+        dev_free(h.d_w3_scale);
+        h.d_p3_tri = nullptr;
+        h.d_p3_woff = nullptr;
+        h.d_w3 = nullptr;
+        h.d_w3_scale = nullptr;
+        long long cap = p3 + p3 / 4 + 256;
+        PB_TRY(dalloc(&h.d_p3_tri, (size_t)cap));
+        PB_TRY(dalloc(&h.d_p3_woff, (size_t)cap));
+        PB_TRY(dev_alloc(&h.d_w3, (size_t)cap * 2 * (h.fp64 ? 16 * sizeof(double2) : 16 * sizeof(__half2))));
+        PB_TRY(dalloc(&h.d_w3_scale, (size_t)cap * 2));
+        h.p3_cap = cap;
+    }
+    PB_CUDA(cudaMemsetAsync(h.d_corr_mask, 0, sizeof(unsigned) * ((nc + 31) / 32), s));
+    fill_pairs3_kernel<<<div_up(n3, T), T, 0, s>>>(h.d_n3_cell, h.d_n3_start, n3, res, h.d_cell_start, h.d_cell_tris,
+                                                   h.d_p3_tri, h.d_p3_woff, h.d_corr_mask);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+
+    // ---- 4^3 lists
+    if (p4 > h.n4_cap)
+    {
+        dev_free(h.d_n4_tris);
+        h.d_n4_tris = nullptr;
+        long long cap = p4 + p4 / 4 + 256;
+        PB_TRY(dalloc(&h.d_n4_tris, (size_t)cap));
+        h.n4_cap = cap;
+    }
+    fill_n4_kernel<<<div_up(b4, T), T, 0, s>>>(h.d_b4_cell, h.d_b4_start, b4, res, h.d_cell_start, h.d_cell_tris,
+                                               h.d_n4_tris);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+
+    // ---- face pairs per centre triangle
+    int *face_len = len3;  // scratch again (b4_len consumed by the scan)
+    face_len_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, nt, b4_pos, flag4, h.d_b4_start, face_len);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    PB_TRY(exclusive_scan(h, face_len, h.d_face_start, nt));
+    int pf = 0;
+    PB_TRY(read_int(h, h.d_face_start + nt, &pf));
+    h.pf = pf;
+    if (pf > h.pf_cap)
+    {
+        dev_free(h.d_face_nbr);
+        dev_free(h.d_face_pool);
+        dev_free(h.d_face_w);
+        dev_free(h.d_face_scale);
+        dev_free(h.d_pair_flag);
+        h.d_face_nbr = h.d_face_pool = h.d_pair_flag = nullptr;
+        h.d_face_w = nullptr;
+        h.d_face_scale = nullptr;
+        long long cap = pf + pf / 4 + 256;
+        PB_TRY(dalloc(&h.d_face_nbr, (size_t)cap));
+        PB_TRY(dalloc(&h.d_face_pool, (size_t)cap));
+        PB_TRY(dalloc(&h.d_pair_flag, (size_t)cap + 1));
+        PB_TRY(dev_alloc(&h.d_face_w, (size_t)cap * (h.fp64 ? 16 * sizeof(double2) : 16 * sizeof(__half2))));
+        PB_TRY(dalloc(&h.d_face_scale, (size_t)cap));
+        h.pf_cap = cap;
+    }
+    face_fill_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, h.d_basec, nt, res, b4_pos, flag4, h.d_b4_start,
+                                                 h.d_n4_tris, h.d_face_start, h.d_face_nbr, h.d_face_corner);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
+
+}  // namespace pb

@@ -1,0 +1,527 @@
+// One PPPM time step as three kernels (the reference issues ~9 launches and ~10 device
+// syncs per step, src/algorithm/pppm.h:138-145):
+//
+//   stencil   p^{t+1} = 2 p^t - p^{t-1} + (c dt)^2 lap p^t on [2, res-3]^3 (FP64 arithmetic
+//             on FP32 storage, fdtd.cu:7-33), the absorbing boundary on layers 1 and res-2
+//             (4x4 solve per cell that also writes the ghost layer of p^t, fdtd.cu:36-150) or
+//             the split-field PML (fdtd.cu:162-232); at corrected cells subtract the FDTD-near
+//             correction that the previous step's near kernel left in this very slot, which
+//             turns p into the reference's far field (pppm.cu:8-50); write neumann[t+1] = acc
+//             (pppm.cu:206-225).
+//   face      per triangle (one warp): far field at the face by trilinear interpolation of
+//             the 8 corner cells, the face-to-face convolution over its 4^3 list, and the
+//             Dirichlet update (pppm.cu:116-193) - three reference kernels fused.
+//   near      per corrected cell (one warp): p = far + 0.98 * sum(BEM-near weights . history)
+//             (pppm.cu:53-113) and, in the same pass over the same pairs and history taps, the
+//             FDTD-near sum of the NEXT step (its taps are t-14..t, all final now), stored in
+//             the grid slot the next stencil writes.  One pass over the pair list per step
+//             instead of two; no copy of the field into a separate far-field grid.
+//
+// Inside a convolution a warp handles two pairs at a time, one lane per tap, so weights
+// (fp16 pairs) and history (16 consecutive ring slots) are read as coalesced 64-byte runs;
+// partial sums stay in registers and are reduced once per triangle / cell.  No atomics.
+#include "handle.cuh"
+
+namespace pb
+{
+
+namespace
+{
+
+struct StepArgs
+{
+    int res;
+    int tnew;  // time index being produced (t + 1)
+    long long step_row;  // row of the listener series for this step
+    double lap_coef;     // (c dt)^2 in double, reference arithmetic
+    double hd;           // h in double
+    float c, dt, h;
+    int pml_width;
+    float damp;
+    int nt;
+    const float *acc;  // nt accelerations of this step (device) or null
+    int n_listen;
+    int listen_cell[8];
+    int listen_corr[8];  // 1 if the listener cell is a corrected cell
+};
+
+template <typename Real>
+__device__ inline Real ld(const Real *g, int res, int x, int y, int z)
+{
+    return g[((long long)x * res + y) * res + z];
+}
+
+// Closed-form 4x4 solve by 2x2 sub-determinants (the method credited at fdtd.cu:36), kept
+// operation for operation so the boundary values round like the reference's.
+template <typename R>
+__device__ inline void solve4(const R a[4][4], const R b[4], R out[4])
+{
+    R s0 = a[0][0] * a[1][1] - a[1][0] * a[0][1];
+    R s1 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
+    R s2 = a[0][0] * a[1][3] - a[1][0] * a[0][3];
+    R s3 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
+    R s4 = a[0][1] * a[1][3] - a[1][1] * a[0][3];
+    R s5 = a[0][2] * a[1][3] - a[1][2] * a[0][3];
+    R c5 = a[2][2] * a[3][3] - a[3][2] * a[2][3];
+    R c4 = a[2][1] * a[3][3] - a[3][1] * a[2][3];
+    R c3 = a[2][1] * a[3][2] - a[3][1] * a[2][2];
+    R c2 = a[2][0] * a[3][3] - a[3][0] * a[2][3];
+    R c1 = a[2][0] * a[3][2] - a[3][0] * a[2][2];
+    R c0 = a[2][0] * a[3][1] - a[3][0] * a[2][1];
+    R invdet = 1.0 / (s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0);
+    R inv[4][4];
+    inv[0][0] = (a[1][1] * c5 - a[1][2] * c4 + a[1][3] * c3) * invdet;
+    inv[0][1] = (-a[0][1] * c5 + a[0][2] * c4 - a[0][3] * c3) * invdet;
+    inv[0][2] = (a[3][1] * s5 - a[3][2] * s4 + a[3][3] * s3) * invdet;
+    inv[0][3] = (-a[2][1] * s5 + a[2][2] * s4 - a[2][3] * s3) * invdet;
+    inv[1][0] = (-a[1][0] * c5 + a[1][2] * c2 - a[1][3] * c1) * invdet;
+    inv[1][1] = (a[0][0] * c5 - a[0][2] * c2 + a[0][3] * c1) * invdet;
+    inv[1][2] = (-a[3][0] * s5 + a[3][2] * s2 - a[3][3] * s1) * invdet;
+    inv[1][3] = (a[2][0] * s5 - a[2][2] * s2 + a[2][3] * s1) * invdet;
+    inv[2][0] = (a[1][0] * c4 - a[1][1] * c2 + a[1][3] * c0) * invdet;
+    inv[2][1] = (-a[0][0] * c4 + a[0][1] * c2 - a[0][3] * c0) * invdet;
+    inv[2][2] = (a[3][0] * s4 - a[3][1] * s2 + a[3][3] * s0) * invdet;
+    inv[2][3] = (-a[2][0] * s4 + a[2][1] * s2 - a[2][3] * s0) * invdet;
+    inv[3][0] = (-a[1][0] * c3 + a[1][1] * c1 - a[1][2] * c0) * invdet;
+    inv[3][1] = (a[0][0] * c3 - a[0][1] * c1 + a[0][2] * c0) * invdet;
+    inv[3][2] = (-a[3][0] * s3 + a[3][1] * s1 - a[3][2] * s0) * invdet;
+    inv[3][3] = (a[2][0] * s3 - a[2][1] * s1 + a[2][2] * s0) * invdet;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+    {
+        out[i] = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            out[i] += inv[i][j] * b[j];
+    }
+}
+
+// Absorbing boundary at a layer-1 / layer-(res-2) cell (fdtd.cu:88-137): unknowns are the
+// ghost values on the outside of each boundary axis (time t) and p^{t+1} of the cell.
+template <typename R>
+__device__ inline R abc_cell(R *cur, const R *prev, int res, int x, int y, int z, R c, R dt, R h)
+{
+    int cc[3] = {x, y, z};
+    int judge[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        judge[d] = -((int)(cc[d] == 1)) + ((int)(cc[d] == res - 2));
+    auto at = [&](const R *g, int d, int s) {
+        int q[3] = {x, y, z};
+        q[d] += s;
+        return g[((long long)q[0] * res + q[1]) * res + q[2]];
+    };
+    const R pc = cur[((long long)x * res + y) * res + z];
+    const R pp = prev[((long long)x * res + y) * res + z];
+    R a[4][4], b[4];
+    R coef = c * c * dt * dt / (h * h);
+    a[3][3] = 1;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        a[3][d] = -coef * (judge[d] != 0);
+    b[3] = -pp + 2 * pc - coef * (6 * pc);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        b[3] += coef * at(cur, d, 1) * (judge[d] <= 0) + coef * at(cur, d, -1) * (judge[d] >= 0);
+    R coef1 = 1 / (dt * dt), coef2 = c / (2 * h * dt), coef3 = -(c * c) / (2 * h * h);
+#pragma unroll
+    for (int idx = 0; idx < 3; idx++)
+    {
+        int ax = idx, ay = (idx + 1) % 3, az = (idx + 2) % 3;
+        a[idx][3] = coef1;
+        a[idx][ax] = coef2;
+        a[idx][ay] = coef3 * (judge[ay] != 0);
+        a[idx][az] = coef3 * (judge[az] != 0);
+        b[idx] = -coef1 * (pp - 2 * pc) +
+                 -coef2 * (at(cur, ax, 1) * (-(judge[ax] < 0)) + at(cur, ax, -1) * (-(judge[ax] > 0)) +
+                           at(prev, ax, 1) * (-judge[ax]) + at(prev, ax, -1) * judge[ax]) +
+                 -coef3 * (at(cur, ay, 1) * (judge[ay] <= 0) + at(cur, ay, -1) * (judge[ay] >= 0) +
+                           at(cur, az, 1) * (judge[az] <= 0) + at(cur, az, -1) * (judge[az] >= 0) - 4 * pc);
+    }
+    R res4[4];
+    solve4<R>(a, b, res4);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (judge[d] != 0)
+        {
+            int q[3] = {x, y, z};
+            q[d] += judge[d];
+            cur[((long long)q[0] * res + q[1]) * res + q[2]] = res4[d];
+        }
+    return res4[3];
+}
+
+// interior leapfrog (fdtd.cu:7-33): float storage, double arithmetic, "6 * p" in the
+// storage precision
+template <typename R>
+__device__ inline R interior_cell(const R *cur, const R *prev, int res, int x, int y, int z, double coefd, double hd)
+{
+    long long i = ((long long)x * res + y) * res + z;
+    long long sx = (long long)res * res;
+    R pc = cur[i];
+    double sum = 0;
+    sum += cur[i - sx];
+    sum += cur[i + sx];
+    sum += cur[i - res];
+    sum += cur[i + res];
+    sum += cur[i - 1];
+    sum += cur[i + 1];
+    sum -= 6 * pc;
+    double lap = sum / (hd * hd);
+    double p = 2 * pc;
+    p += coefd * lap;
+    p += -prev[i];
+    return (R)p;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a, R *cur, const R *prev, R *next,
+                                                       const unsigned *corr_mask, R *neumann, R *series)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int res = a.res, m = res - 2;
+    if (gid < a.nt && a.acc)
+        neumann[(long long)gid * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[gid];
+    if (gid >= (long long)m * m * m)
+        return;
+    int x = 1 + (int)(gid / ((long long)m * m));
+    int y = 1 + (int)((gid / m) % m);
+    int z = 1 + (int)(gid % m);
+    long long c = ((long long)x * res + y) * res + z;
+    bool inner = x >= 2 && y >= 2 && z >= 2 && x <= res - 3 && y <= res - 3 && z <= res - 3;
+    R v;
+    if (inner)
+        v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
+    else
+        v = abc_cell<R>(cur, prev, res, x, y, z, (R)a.c, (R)a.dt, (R)a.h);
+    if ((corr_mask[c >> 5] >> (c & 31)) & 1u)
+    {
+        R corr = next[c];
+        v = v - corr;
+    }
+    next[c] = v;
+    for (int l = 0; l < a.n_listen; l++)
+        if (a.listen_cell[l] == (int)c && !a.listen_corr[l])
+            series[a.step_row * a.n_listen + l] = v;
+}
+
+// split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
+template <typename R>
+__device__ inline R pml_damp(int x, int y, int z, int res, int w, R damp)
+{
+    return (x < w || x >= res - w || y < w || y >= res - w || z < w || z >= res - w) ? damp : (R)0;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) pml_kernel(StepArgs a, const R *cur, const R *prev, R *next, const R *pcur,
+                                                   R *pnext, const unsigned *corr_mask, R *neumann, R *series)
+{
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int res = a.res, m = res - 2, w = a.pml_width;
+    if (gid < a.nt && a.acc)
+        neumann[(long long)gid * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[gid];
+    if (gid >= (long long)m * m * m)
+        return;
+    int q[3] = {1 + (int)(gid / ((long long)m * m)), 1 + (int)((gid / m) % m), 1 + (int)(gid % m)};
+    const R c = a.c, h = a.h, dt = a.dt, damp = a.damp;
+    auto idx = [&](int x, int y, int z) { return ((long long)x * res + y) * res + z; };
+    long long ci = idx(q[0], q[1], q[2]);
+    int sgn[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        sgn[d] = q[d] > res / 2 ? 1 : -1;
+    R cd = pml_damp<R>(q[0], q[1], q[2], res, w, damp);
+    R rhs = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+    {
+        int p1[3] = {q[0], q[1], q[2]}, m1[3] = {q[0], q[1], q[2]}, ps[3] = {q[0], q[1], q[2]}, ms[3] = {q[0], q[1], q[2]};
+        p1[d] += 1;
+        m1[d] -= 1;
+        ps[d] += sgn[d];
+        ms[d] -= sgn[d];
+        rhs += 1 / (h * h) * (cur[idx(p1[0], p1[1], p1[2])] - 2 * cur[ci] + cur[idx(m1[0], m1[1], m1[2])]);
+        rhs += 1 / h *
+               (cd * pcur[6 * idx(ps[0], ps[1], ps[2]) + 3 + d] -
+                pml_damp<R>(ms[0], ms[1], ms[2], res, w, damp) * pcur[6 * idx(ms[0], ms[1], ms[2]) + d]);
+    }
+    R v = cur[ci] * 2 - prev[ci] + c * c * dt * dt * rhs;
+    if (cd != 0)
+    {
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+        {
+            int ps[3] = {q[0], q[1], q[2]}, ms[3] = {q[0], q[1], q[2]};
+            ps[d] += sgn[d];
+            ms[d] -= sgn[d];
+            R dm = pml_damp<R>(ms[0], ms[1], ms[2], res, w, damp);
+            R grad = cur[idx(ps[0], ps[1], ps[2])] - cur[idx(ms[0], ms[1], ms[2])];
+            R r1 = 0;
+            r1 += -1.0f / 2.0f * (dm * pcur[6 * idx(ms[0], ms[1], ms[2]) + d] + cd * pcur[6 * ci + d]);
+            r1 += -1.0f / (h * 2.0f) * grad;
+            pnext[6 * ci + d] = pcur[6 * ci + d] + c * dt * r1;
+            R r2 = 0;
+            r2 += -1.0f / 2.0f * (dm * pcur[6 * ci + 3 + d] + cd * pcur[6 * idx(ps[0], ps[1], ps[2]) + 3 + d]);
+            r2 += -1.0f / (h * 2.0f) * grad;
+            pnext[6 * ci + 3 + d] = pcur[6 * ci + 3 + d] + c * dt * r2;
+        }
+    }
+    if ((corr_mask[ci >> 5] >> (ci & 31)) & 1u)
+        v = v - next[ci];
+    next[ci] = v;
+    for (int l = 0; l < a.n_listen; l++)
+        if (a.listen_cell[l] == (int)ci && !a.listen_corr[l])
+            series[a.step_row * a.n_listen + l] = v;
+}
+
+// ---- convolution helpers: lane k holds tap k of one pair
+__device__ inline float conv_tap(__half2 w, float2 s, float n, float d)
+{
+    return -__low2float(w) * s.x * n + __high2float(w) * s.y * d;
+}
+__device__ inline double conv_tap(double2 w, float2, double n, double d) { return -w.x * n + w.y * d; }
+
+template <typename R>
+struct WRec;
+template <>
+struct WRec<float>
+{
+    using T = __half2;
+    __device__ static T zero() { return __floats2half2_rn(0.f, 0.f); }
+};
+template <>
+struct WRec<double>
+{
+    using T = double2;
+    __device__ static T zero() { return make_double2(0, 0); }
+};
+
+template <typename R>
+__device__ inline R warp_sum(R v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// face stage: one warp per centre triangle
+template <typename R>
+__global__ void __launch_bounds__(256) face_kernel(StepArgs a, const R *next, const int *face_start,
+                                                    const int *face_nbr, const typename WRec<R>::T *face_w,
+                                                    const float2 *face_scale, const int *face_corner,
+                                                    const float *interp, const double *interp_d,
+                                                    const double *denom, const R *neumann, R *dirichlet, float reflect)
+{
+    using W = typename WRec<R>::T;
+    int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (tri >= a.nt)
+        return;
+    const int k = lane & 15, half = lane >> 4;
+    const int tslot = (a.tnew - k) & (kRing - 1);
+    R acc = 0;
+    int b = face_start[tri], e = face_start[tri + 1];
+    for (int p = b + half; p < e; p += 2)
+    {
+        int nbr = face_nbr[p];
+        W w = face_w[(long long)p * kTaps + k];
+        float2 s = face_scale ? face_scale[p] : make_float2(1, 1);
+        R n = neumann[(long long)nbr * kRing + tslot];
+        R d = k == 0 ? (R)0 : dirichlet[(long long)nbr * kRing + tslot];
+        acc += conv_tap(w, s, n, d);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0)
+    {
+        R far_sum = 0;
+        for (int wi = 0; wi < 8; wi++)
+        {
+            R iw = interp_d ? (R)interp_d[8 * tri + wi] : (R)interp[8 * tri + wi];
+            far_sum += iw * next[face_corner[8 * tri + wi]];
+        }
+        R num = far_sum * (R)reflect + acc;
+        dirichlet[(long long)tri * kRing + (a.tnew & (kRing - 1))] = (R)(num / denom[tri]);
+    }
+}
+
+// near stage: one warp per corrected cell.  prime != 0: only the next step's FDTD-near sum.
+template <typename R>
+__global__ void __launch_bounds__(256) near_kernel(StepArgs a, int n3, const int *n3_cell, const int *n3_start,
+                                                    const int *p3_tri, const typename WRec<R>::T *w3,
+                                                    const float2 *w3_scale, const R *neumann, const R *dirichlet,
+                                                    R *cur, R *nextslot, R *series, int prime)
+{
+    using W = typename WRec<R>::T;
+    int ci = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (ci >= n3)
+        return;
+    const int k = lane & 15, half = lane >> 4;
+    const int tslot = (a.tnew - k) & (kRing - 1);
+    R acc_b = 0, acc_f = 0;
+    int b = n3_start[ci], e = n3_start[ci + 1];
+    for (int p = b + half; p < e; p += 2)
+    {
+        int tri = p3_tri[p];
+        R n = neumann[(long long)tri * kRing + tslot];
+        R d = dirichlet[(long long)tri * kRing + tslot];
+        W wf = k < kTaps - 1 ? w3[(long long)p * 2 * kTaps + k + 1] : WRec<R>::zero();
+        float2 sf = w3_scale ? w3_scale[2 * (long long)p] : make_float2(1, 1);
+        acc_f += conv_tap(wf, sf, n, d);
+        if (!prime)
+        {
+            W wb = w3[((long long)p * 2 + 1) * kTaps + k];
+            float2 sb = w3_scale ? w3_scale[2 * (long long)p + 1] : make_float2(1, 1);
+            acc_b += conv_tap(wb, sb, n, d);
+        }
+    }
+    acc_f = warp_sum(acc_f);
+    if (!prime)
+        acc_b = warp_sum(acc_b);
+    if (lane == 0)
+    {
+        int c = n3_cell[ci];
+        nextslot[c] = acc_f;
+        if (!prime)
+        {
+            R v = (R)((double)cur[c] + (double)acc_b * 0.98);
+            cur[c] = v;
+            for (int l = 0; l < a.n_listen; l++)
+                if (a.listen_cell[l] == c)
+                    series[a.step_row * a.n_listen + l] = v;
+        }
+    }
+}
+
+template <typename R>
+StepArgs make_args(Handle &h)
+{
+    StepArgs a{};
+    a.res = h.res;
+    a.tnew = h.t + 1;
+    a.c = h.prm.c;
+    a.dt = h.prm.dt;
+    a.h = h.prm.dl;
+    double cd = h.prm.c, dtd = h.prm.dt;
+    a.lap_coef = cd * cd * dtd * dtd;
+    a.hd = h.prm.dl;
+    a.pml_width = h.prm.pml_width;
+    a.damp = 2.0f / h.prm.dl;
+    a.nt = h.mesh_set ? h.nt : 0;
+    a.n_listen = (int)h.listen_xyz.size() / 3;
+    return a;
+}
+
+template <typename R>
+int fill_listeners(Handle &h, StepArgs &a)
+{
+    if (a.n_listen > 8)
+    {
+        set_error("at most 8 listeners");
+        return PPPM_ERR_ARG;
+    }
+    for (int l = 0; l < a.n_listen; l++)
+    {
+        a.listen_cell[l] = (h.listen_xyz[3 * l] * h.res + h.listen_xyz[3 * l + 1]) * h.res + h.listen_xyz[3 * l + 2];
+        a.listen_corr[l] = l < (int)h.listen_corr.size() ? h.listen_corr[l] : 0;
+    }
+    return PPPM_OK;
+}
+
+template <typename R>
+int run_steps(Handle &h, const float *acc_dev, int nsteps)
+{
+    using W = typename WRec<R>::T;
+    cudaStream_t s = h.stream;
+    StepArgs a = make_args<R>(h);
+    PB_TRY(fill_listeners<R>(h, a));
+    const int m = h.res - 2;
+    long long n_st = std::max<long long>((long long)m * m * m, a.nt);
+    const int T = 256;
+    for (int st = 0; st < nsteps; st++)
+    {
+        a.tnew = h.t + 1;
+        a.step_row = h.series_count;
+        a.acc = acc_dev ? acc_dev + (size_t)st * h.nt : nullptr;
+        R *cur = (R *)h.slot(h.t), *prev = (R *)h.slot(h.t - 1), *next = (R *)h.slot(h.t + 1);
+        R *series = (R *)h.d_series;
+        if (h.timing)
+            cudaEventRecord(h.ev[0], s);
+        if (h.prm.pml_width > 0)
+            pml_kernel<R><<<div_up(n_st, T), T, 0, s>>>(a, cur, prev, next, (const R *)h.pml_slot(h.t),
+                                                        (R *)h.pml_slot(h.t + 1), h.d_corr_mask, (R *)h.d_neumann,
+                                                        series);
+        else
+            stencil_kernel<R><<<div_up(n_st, T), T, 0, s>>>(a, cur, prev, next, h.d_corr_mask, (R *)h.d_neumann,
+                                                            series);
+        h.launches++;
+        if (h.timing)
+            cudaEventRecord(h.ev[1], s);
+        if (h.mesh_set)
+        {
+            face_kernel<R><<<div_up((long long)h.nt * 32, T), T, 0, s>>>(
+                a, next, h.d_face_start, h.d_face_nbr, (const W *)h.d_face_w, h.fp64 ? nullptr : h.d_face_scale,
+                h.d_face_corner, h.d_face_interp, h.fp64 ? h.d_face_interp_d : nullptr, h.d_face_denom,
+                (const R *)h.d_neumann, (R *)h.d_dirichlet, h.prm.reflect_coeff);
+            h.launches++;
+            if (h.timing)
+                cudaEventRecord(h.ev[2], s);
+            if (h.n3 > 0)
+            {
+                near_kernel<R><<<div_up((long long)h.n3 * 32, T), T, 0, s>>>(
+                    a, h.n3, h.d_n3_cell, h.d_n3_start, h.d_p3_tri, (const W *)h.d_w3,
+                    h.fp64 ? nullptr : h.d_w3_scale, (const R *)h.d_neumann, (const R *)h.d_dirichlet, next,
+                    (R *)h.slot(h.t + 2), series, 0);
+                h.launches++;
+            }
+        }
+        if (h.timing)
+            cudaEventRecord(h.ev[3], s);
+        PB_CHECK_LAUNCH();
+        h.t++;
+        h.series_count++;
+    }
+    if (h.timing && nsteps > 0)
+    {
+        PB_CUDA(cudaEventSynchronize(h.ev[3]));
+        cudaEventElapsedTime(&h.us_stencil, h.ev[0], h.ev[1]);
+        if (h.mesh_set)
+        {
+            cudaEventElapsedTime(&h.us_face, h.ev[1], h.ev[2]);
+            cudaEventElapsedTime(&h.us_near, h.ev[2], h.ev[3]);
+        }
+        h.us_stencil *= 1000;
+        h.us_face *= 1000;
+        h.us_near *= 1000;
+    }
+    return PPPM_OK;
+}
+
+template <typename R>
+int prime(Handle &h)
+{
+    using W = typename WRec<R>::T;
+    if (!h.mesh_set || h.n3 == 0)
+        return PPPM_OK;
+    StepArgs a = make_args<R>(h);
+    a.tnew = h.t;  // taps t-k of the current time
+    a.n_listen = 0;
+    near_kernel<R><<<div_up((long long)h.n3 * 32, 256), 256, 0, h.stream>>>(
+        a, h.n3, h.d_n3_cell, h.d_n3_start, h.d_p3_tri, (const W *)h.d_w3, h.fp64 ? nullptr : h.d_w3_scale,
+        (const R *)h.d_neumann, (const R *)h.d_dirichlet, (R *)h.slot(h.t), (R *)h.slot(h.t + 1), nullptr, 1);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
+
+}  // namespace
+
+int step_prime(Handle &h) { return h.fp64 ? prime<double>(h) : prime<float>(h); }
+
+int step_run(Handle &h, const float *acc_dev, int nsteps)
+{
+    return h.fp64 ? run_steps<double>(h, acc_dev, nsteps) : run_steps<float>(h, acc_dev, nsteps);
+}
+
+}  // namespace pb
