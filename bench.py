@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Benchmark of the PPPM-TDBEM time step on B200: Gcell-steps/s and achieved HBM GB/s.
+
+Workload (default, --workload moving): a moving perturbed icosphere (5120 triangles, radius
+0.08 m, translating 0.05 sin(2 pi 3 t) m and rotating 2 rad/s) beside a static 1280-triangle
+plate at res 64, band-limited noise accelerations, motion frames at 1 kHz (69 PPPM steps per
+frame).  One benchmark step = one motion frame: update_mesh (lists + cache refresh) plus the
+69 time steps of that frame.  `value` is device-resident (inputs uploaded before timing);
+`e2e` drives the same frames through the public API from pinned host buffers and reads the
+listener samples back every frame.  --workload static runs the 1280-triangle sphere at
+res 32 without motion (benchmark step = 100 time steps).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank advances its own copy of the scene (replicas, weak
+scaling); value = cells x steps over all ranks / max rank time.  The reference arm runs the
+reference CUDA solver compiled from source (oracle/_ref) on rank 0, or the CPU oracle when
+that build is absent.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "pppm-tdbem_b200", "python"))
+
+from pppm_b200 import scenes  # noqa: E402
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=60, help="timed benchmark steps (motion frames)")
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="moving", choices=["moving", "static"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- distributed ---------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    import torch
+
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(ws, x):
+    import torch
+
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- clocks --------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- workloads -----------
+class Workload:
+    """Frames of the benchmark: per frame the vertex positions and the step range."""
+
+    def __init__(self, kind, nframes):
+        self.kind = kind
+        if kind == "moving":
+            sc = scenes.MovingScene()
+            self.scene = sc
+            steps_needed = int(math.ceil((nframes + 1) / sc.frame_hz / float(sc.dt))) + 2
+            frame = [sc.frame_of_step(s) for s in range(steps_needed)]
+            self.ranges = []
+            for f in range(nframes + 1):
+                idx = [s for s in range(steps_needed) if frame[s] == f]
+                self.ranges.append((idx[0], idx[-1] + 1))
+            self.verts = [sc.frame_verts(f) for f in range(nframes + 1)]
+            self.name = "moving icosphere (5120 tris) + static plate (1280 tris), res 64, 1 kHz motion frames"
+        else:
+            sc = scenes.StaticSphere()
+            self.scene = sc
+            per = 100
+            self.ranges = [(f * per, (f + 1) * per) for f in range(nframes + 1)]
+            self.verts = [sc.verts for _ in range(nframes + 1)]
+            self.name = "static icosphere (1280 tris), res 32"
+        self.total_steps = self.ranges[-1][1]
+        self.res = sc.res
+        self.tris = sc.tris
+        self.listener = sc.listener
+        self.acc = sc.acc(0, self.total_steps)
+
+
+def algorithmic_bytes(counts, res, nt):
+    """Compulsory bytes per launch of each per-step kernel (FP32 scheme)."""
+    m = res - 2
+    n3, p3, pf = counts[0], counts[1], counts[4]
+    abc = 6 * m * m
+    stencil = 12 * m ** 3 + 16 * abc + 4 * n3 + 8 * nt  # p^t, p^{t-1}, p^{t+1}; ghost writes; corrections; acc->ring
+    face = pf * (64 + 8 + 4) + nt * (8 * 4 + 8 * 4 + 8 * 4 + 8 + 8 + 4) + nt * 2 * 64
+    near = p3 * (2 * 64 + 2 * 8 + 4) + n3 * (4 + 4 + 4 + 4 + 4) + nt * 2 * 64
+    return {"stencil": stencil, "face": face, "near": near}
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 2 and not line.startswith("#"):
+                try:
+                    out[f[0]] = float(f[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return float(json.load(open(path))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- our arm -------------
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from pppm_b200 import Solver
+
+    W, K = args.warmup, args.steps
+    wl = Workload(args.workload, W + K)
+    sc = wl.scene
+    stream = torch.cuda.current_stream()
+    dev = torch.device("cuda", local)
+    acc_dev = torch.from_numpy(wl.acc).to(dev)
+    verts_dev = [torch.from_numpy(v).to(dev) for v in wl.verts]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    s = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+    s.set_mesh(wl.verts[0], wl.tris)
+    s.add_listener(*wl.listener)
+
+    def frame(f, timed_events=None):
+        a, b = wl.ranges[f]
+        if f > 0 and wl.kind == "moving":
+            s.update_mesh(verts_dev[f])
+        s.step(acc_dev[a:b])
+
+    for f in range(0, W + 1):  # frame 0 = the set_mesh frame, then W warm-up frames
+        frame(f)
+    torch.cuda.synchronize()
+    launches0 = s.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    total_ms = 0.0
+    steps = 0
+    for f in range(W + 1, W + K + 1):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        frame(f)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        steps += wl.ranges[f][1] - wl.ranges[f][0]
+    barrier(ws)
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    t_max = max_over_ranks(ws, total_ms)
+    cells = float(wl.res) ** 3
+    value = cells * steps * ws / (t_max * 1e-3) / 1e9
+
+    # per-kernel durations (measurement mode: events around each kernel, synchronised)
+    s.enable_timing(True)
+    a, b = wl.ranges[W + K]
+    s.step(acc_dev[a:b])
+    us_st, us_face, us_near, nt_timed = s.kernel_times()
+    s.enable_timing(False)
+    counts = s.dump("counts")
+    alg = algorithmic_bytes(counts, wl.res, len(wl.tris))
+    times = {"stencil": us_st, "face": us_face, "near": us_near}
+    top = max(times, key=lambda k: times[k])
+    peak, peak_kind = measured_peak()
+    achieved = alg[top] / (times[top] * 1e-6) / 1e9
+    traffic = load_traffic().get(top)
+    # update_mesh share of a frame
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    if wl.kind == "moving":
+        s.update_mesh(verts_dev[W + K])
+    e1.record(stream)
+    e1.synchronize()
+    us_update = e0.elapsed_time(e1) * 1e3
+
+    # end-to-end through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        s2 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+        s2.set_mesh(wl.verts[0], wl.tris)
+        s2.add_listener(*wl.listener)
+        acc_pin = torch.from_numpy(wl.acc).pin_memory()
+        verts_pin = [torch.from_numpy(v).pin_memory() for v in wl.verts]
+        out_pin = torch.empty((200,), dtype=torch.float32).pin_memory()
+        h2d = d2h = 0
+        for f in range(0, W + 1):
+            a, b = wl.ranges[f]
+            if f > 0 and wl.kind == "moving":
+                s2.update_mesh(verts_pin[f])
+            s2.step(acc_pin[a:b])
+        barrier(ws)
+        t0 = time.perf_counter()
+        steps2 = 0
+        for f in range(W + 1, W + K + 1):
+            a, b = wl.ranges[f]
+            if wl.kind == "moving":
+                s2.update_mesh(verts_pin[f])
+                h2d += verts_pin[f].numel() * 4
+            s2.step(acc_pin[a:b])
+            h2d += (b - a) * len(wl.tris) * 4
+            done = s2.listeners(first=a, count=b - a)
+            d2h += done.nbytes
+            steps2 += b - a
+        torch.cuda.synchronize()
+        te = max_over_ranks(ws, time.perf_counter() - t0)
+        e2e = {"value": cells * steps2 * ws / te / 1e9, "unit": "Gcell-steps/s",
+               "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K}
+        s2.close()
+        del out_pin
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl)
+
+    s.close()
+    line = {
+        "metric": "Gcell-steps/s, %s (time step + motion-frame refresh)" % wl.name,
+        "value": round(value, 4), "unit": "Gcell-steps/s", "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": round(t_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded meshes, trajectories and accelerations)",
+        "config": {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris)),
+                   "time_steps_per_bench_step": round(steps / K, 2), "time_steps_timed": steps,
+                   "bench_step": "one motion frame: update_mesh + its time steps" if wl.kind == "moving"
+                   else "100 time steps", "l2": "flushed (256 MiB write) between timed iterations",
+                   "parallelism": "replicas x%d" % ws, "precision": "fp32 grids, fp16+scale weights",
+                   "n3_cells": int(counts[0]), "pairs_3x3x3": int(counts[1]), "face_pairs": int(counts[4])},
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes": alg[top],
+                     "kernel_us": {k: round(v, 3) for k, v in times.items()},
+                     "update_mesh_us": round(us_update, 1),
+                     "gb_per_s_all_kernels": round(sum(alg.values()) / (sum(times.values()) * 1e-6) / 1e9, 1)},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+    }
+    return line
+
+
+def cpu_baseline(wl):
+    """The CPU restatement (oracle/) on the host cores: one benchmark step of the same
+    workload (set_mesh untimed)."""
+    from oracle.oracle import Oracle, oracle_threads
+
+    sc = wl.scene
+    o = Oracle(wl.res, sc.h, sc.dt, sc.min_pos)
+    o.set_mesh(wl.verts[0], wl.tris)
+    f = 1
+    a, b = wl.ranges[f]
+    t0 = time.perf_counter()
+    if wl.kind == "moving":
+        o.update_mesh(wl.verts[f])
+    o.step(wl.acc[a:b], listeners=[wl.listener])
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": round(float(wl.res) ** 3 * (b - a) / dt / 1e9, 5), "unit": "Gcell-steps/s",
+            "cores": oracle_threads(), "kind": "port",
+            "sample": "one benchmark step (%d time steps%s) of the same workload, C restatement with OpenMP"
+                      % (b - a, " + update_mesh" if wl.kind == "moving" else "")}
+
+
+# ---------------------------------------------------------------- reference arm -------
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return None
+    W, K = args.warmup, args.steps
+    wl = Workload(args.workload, W + K)
+    sc = wl.scene
+    from oracle import oracle as O
+
+    if O.reference_available():
+        import torch
+
+        r = O.Reference(wl.res, sc.h, sc.dt, sc.min_pos)
+        r.set_mesh(wl.verts[0], wl.tris)
+        if wl.kind == "moving":
+            for v in wl.verts[1:]:
+                r.check_mesh(v)  # validate the whole trajectory against the reference capacities
+            r.set_checks(False)
+        acc_dev = torch.from_numpy(wl.acc).cuda()
+        nt = len(wl.tris)
+        ptr0 = acc_dev.data_ptr()
+
+        def frame(f):
+            a, b = wl.ranges[f]
+            if f > 0 and wl.kind == "moving":
+                r.update_mesh(wl.verts[f])
+            r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
+
+        for f in range(0, W + 1):
+            frame(f)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = 0
+        for f in range(W + 1, W + K + 1):
+            frame(f)
+            steps += wl.ranges[f][1] - wl.ranges[f][0]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        r.close()
+        value = float(wl.res) ** 3 * steps / dt / 1e9
+        kind, cores, sample = "reference", 0, ("reference CUDA solver built from source (oracle/_ref, upstream flags: "
+                                                "device sync after every launch), %d frames" % K)
+    else:
+        from oracle.oracle import Oracle, oracle_threads
+
+        o = Oracle(wl.res, sc.h, sc.dt, sc.min_pos)
+        o.set_mesh(wl.verts[0], wl.tris)
+        t0 = time.perf_counter()
+        steps = 0
+        for f in range(1, min(W + K, 3) + 1):
+            a, b = wl.ranges[f]
+            if wl.kind == "moving":
+                o.update_mesh(wl.verts[f])
+            o.step(wl.acc[a:b], listeners=[wl.listener])
+            steps += b - a
+        dt = time.perf_counter() - t0
+        value = float(wl.res) ** 3 * steps / dt / 1e9
+        kind, cores, sample = "port", oracle_threads(), "CPU restatement, %d frames" % min(W + K, 3)
+    return {"impl": "reference", "metric": "Gcell-steps/s, %s (time step + motion-frame refresh)" % wl.name,
+            "value": round(value, 5), "unit": "Gcell-steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded meshes, trajectories and accelerations)",
+            "config": {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris))},
+            "cpu_baseline": {"value": round(value, 5), "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 5), "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        line = run_reference(args, ws, rank, local)
+    else:
+        line = run_ours(args, ws, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

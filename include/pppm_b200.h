@@ -185,9 +185,11 @@ const char *pppm_status_string(int status);
 const char *pppm_last_error_message(void);
 /* Kernel launches issued by this handle since creation (for launch accounting). */
 int pppm_launch_count(pppm_handle *h, long long *count);
-/* Last-step timing breakdown in microseconds measured with CUDA events when enabled. */
+/* Measurement mode: with timing enabled every step records CUDA events around each of its
+ * kernels and synchronises; pppm_kernel_times returns the mean duration per kernel in
+ * microseconds over the steps timed since pppm_enable_timing, and their number. */
 int pppm_enable_timing(pppm_handle *h, int enable);
-int pppm_kernel_times(pppm_handle *h, float *us_stencil, float *us_face, float *us_near, int *launches);
+int pppm_kernel_times(pppm_handle *h, float *us_stencil, float *us_face, float *us_near, int *timed_steps);
 
 #ifdef __cplusplus
 }

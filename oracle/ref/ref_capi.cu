@@ -131,6 +131,7 @@ struct RefPPPM
 {
     PPPMSolver *solver = nullptr;
     CapacityCheck cap;
+    bool checks = true;
     int nv = 0, nt = 0;
     std::vector<float> verts;
     GArr<float> acc_dev;
@@ -326,14 +327,45 @@ int ref_pppm_update_mesh(void *p, const float *V)
         F[3 * i + 1] = tris[i].y;
         F[3 * i + 2] = tris[i].z;
     }
-    int rc = h->cap.check(V, h->nv, F.data(), h->nt, true);
-    if (rc)
-        return rc;
+    if (h->checks)
+    {
+        int rc = h->cap.check(V, h->nv, F.data(), h->nt, true);
+        if (rc)
+            return rc;
+    }
     return guarded([&] {
         CArr<float3> verts = to_float3(V, h->nv);
         h->solver->update_mesh(verts);
         return last_cuda_status();
     });
+}
+
+// Host-only capacity check of a vertex set against this solver's topology (no reference
+// code runs); used to validate a whole trajectory before timing it with checks disabled.
+int ref_pppm_check_mesh(void *p, const float *V)
+{
+    RefPPPM *h = (RefPPPM *)p;
+    if (!h || !h->solver->mesh_set)
+        return REF_ERR_STATE;
+    auto tris = h->solver->pg.faces.cpu();
+    std::vector<int> F(3 * h->nt);
+    for (int i = 0; i < h->nt; i++)
+    {
+        F[3 * i] = tris[i].x;
+        F[3 * i + 1] = tris[i].y;
+        F[3 * i + 2] = tris[i].z;
+    }
+    return h->cap.check(V, h->nv, F.data(), h->nt, true);
+}
+
+// Enable (default) or disable the per-update host capacity check.
+int ref_pppm_set_checks(void *p, int on)
+{
+    RefPPPM *h = (RefPPPM *)p;
+    if (!h)
+        return REF_ERR_ARG;
+    h->checks = on != 0;
+    return REF_OK;
 }
 
 // One reference step per row of acc (host array, nsteps x nt).  After each step the

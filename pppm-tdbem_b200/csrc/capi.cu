@@ -141,6 +141,36 @@ int refresh_listeners(Handle &h)
     return PPPM_OK;
 }
 
+// release every array sized by the mesh (a failed set_mesh leaves the handle mesh-free)
+void free_mesh(Handle &h)
+{
+    cudaStreamSynchronize(h.stream);
+    cache_free(h);
+    void **ptrs[] = {(void **)&h.d_verts,      (void **)&h.d_tris,        (void **)&h.d_center,
+                     (void **)&h.d_normal,     (void **)&h.d_area,        (void **)&h.d_cellc,
+                     (void **)&h.d_basec,      (void **)&h.d_cell,        (void **)&h.d_base,
+                     (void **)&h.d_cell_count, (void **)&h.d_cell_start,  (void **)&h.d_cell_tris,
+                     (void **)&h.d_base_count, (void **)&h.d_base_start,  (void **)&h.d_base_tris,
+                     (void **)&h.d_cursor,     (void **)&h.d_flags,       (void **)&h.d_n3_cell,
+                     (void **)&h.d_n3_start,   (void **)&h.d_p3_tri,      (void **)&h.d_p3_woff,
+                     (void **)&h.d_w3,         (void **)&h.d_w3_scale,    (void **)&h.d_b4_cell,
+                     (void **)&h.d_b4_start,   (void **)&h.d_n4_tris,     (void **)&h.d_face_start,
+                     (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
+                     (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
+                     (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet};
+    for (void **q : ptrs)
+    {
+        dev_free(*q);
+        *q = nullptr;
+    }
+    h.p3_cap = h.n4_cap = h.pf_cap = 0;
+    h.n3 = h.b4 = 0;
+    h.p3 = h.p4 = h.pf = 0;
+    h.nv = h.nt = 0;
+    h.gc_empty = true;
+    cudaMemsetAsync(h.d_corr_mask, 0, sizeof(unsigned) * ((h.n_cells + 31) / 32), h.stream);
+}
+
 int ensure_series(Handle &h, long long extra)
 {
     int nl = (int)h.listen_xyz.size() / 3;
@@ -302,7 +332,7 @@ int pppm_destroy(pppm_handle *ph)
     Handle &h = ph->h;
     if (h.stream)
         cudaStreamSynchronize(h.stream);
-    cache_free(h);
+    free_mesh(h);
     void *ptrs[] = {h.grid[0],        h.grid[1],         h.grid[2],        h.pml[0],          h.pml[1],
                     h.pml[2],         h.d_verts,         h.d_tris,         h.d_center,        h.d_normal,
                     h.d_area,         h.d_cellc,         h.d_basec,        h.d_cell,          h.d_base,
@@ -349,6 +379,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
             return PPPM_ERR_ARG;
         }
     cudaSetDevice(h.prm.device);
+    free_mesh(h);
     h.nv = nv;
     h.nt = nt;
     PB_TRY(dalloc(&h.d_verts, 3 * (size_t)nv));
@@ -364,7 +395,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
         rc = cache_refresh(h);
     if (rc != PPPM_OK)
     {
-        h.nv = h.nt = 0;
+        free_mesh(h);
         return rc;
     }
     h.mesh_set = true;
@@ -964,6 +995,8 @@ int pppm_enable_timing(pppm_handle *ph, int enable)
 {
     PB_TRY(check_handle(ph));
     ph->h.timing = enable != 0;
+    ph->h.us_stencil = ph->h.us_face = ph->h.us_near = 0;
+    ph->h.timed_steps = 0;
     return PPPM_OK;
 }
 
@@ -971,14 +1004,15 @@ int pppm_kernel_times(pppm_handle *ph, float *us_stencil, float *us_face, float 
 {
     PB_TRY(check_handle(ph));
     Handle &h = ph->h;
+    double n = h.timed_steps > 0 ? (double)h.timed_steps : 1.0;
     if (us_stencil)
-        *us_stencil = h.us_stencil;
+        *us_stencil = (float)(h.us_stencil / n);
     if (us_face)
-        *us_face = h.us_face;
+        *us_face = (float)(h.us_face / n);
     if (us_near)
-        *us_near = h.us_near;
+        *us_near = (float)(h.us_near / n);
     if (launches)
-        *launches = h.mesh_set ? (h.n3 > 0 ? 3 : 2) : 1;
+        *launches = (int)h.timed_steps;
     return PPPM_OK;
 }
 

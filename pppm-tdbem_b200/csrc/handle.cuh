@@ -160,7 +160,8 @@ struct Handle
     // ---- timing
     bool timing = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    float us_stencil = 0, us_face = 0, us_near = 0;
+    float us_stencil = 0, us_face = 0, us_near = 0;  // summed over timed_steps
+    long long timed_steps = 0;
 
     // ---- scratch for accelerations
     float *d_acc = nullptr;

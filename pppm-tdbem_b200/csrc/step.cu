@@ -481,19 +481,22 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
         PB_CHECK_LAUNCH();
         h.t++;
         h.series_count++;
-    }
-    if (h.timing && nsteps > 0)
-    {
-        PB_CUDA(cudaEventSynchronize(h.ev[3]));
-        cudaEventElapsedTime(&h.us_stencil, h.ev[0], h.ev[1]);
-        if (h.mesh_set)
+        if (h.timing)
         {
-            cudaEventElapsedTime(&h.us_face, h.ev[1], h.ev[2]);
-            cudaEventElapsedTime(&h.us_near, h.ev[2], h.ev[3]);
+            // per-kernel durations, accumulated over timed steps (measurement mode only)
+            PB_CUDA(cudaEventSynchronize(h.ev[3]));
+            float a = 0, b = 0, c = 0;
+            cudaEventElapsedTime(&a, h.ev[0], h.ev[1]);
+            if (h.mesh_set)
+            {
+                cudaEventElapsedTime(&b, h.ev[1], h.ev[2]);
+                cudaEventElapsedTime(&c, h.ev[2], h.ev[3]);
+            }
+            h.us_stencil += 1000 * a;
+            h.us_face += 1000 * b;
+            h.us_near += 1000 * c;
+            h.timed_steps++;
         }
-        h.us_stencil *= 1000;
-        h.us_face *= 1000;
-        h.us_near *= 1000;
     }
     return PPPM_OK;
 }

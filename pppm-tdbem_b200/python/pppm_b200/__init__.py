@@ -1,0 +1,298 @@
+"""Python binding of libpppm_b200 (the C ABI in include/pppm_b200.h) through ctypes.
+
+`Solver` mirrors the reference's PPPMSolver (src/algorithm/pppm.h:11-165): construct with the
+grid, `set_mesh`, `update_mesh` on motion frames, `update_grid_and_face(acc)` per step
+(`step(acc_rows)` for many), listener cells read per step like the demo driver
+(experiments/demo/main.cu:266).  Errors raise PPPMError; the CUDA library is required - a
+missing library raises at import, there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_PKG = os.path.dirname(os.path.dirname(_HERE))
+LIB_PATH = os.environ.get("PPPM_B200_LIB", os.path.join(_PKG, "lib", "libpppm_b200.so"))
+
+OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_NAN, ERR_STATE, ERR_TIMEOUT, ERR_NOMEM = range(8)
+PRECISION = {"fp32": 0, "fp64": 1}
+WEIGHTS = {"ref32": 0, "fp64": 1}
+
+DUMP = dict(grid_t=0, grid_tm1=1, grid_tm2=2, neumann=3, dirichlet=4, tri_geom=5, tri_cells=6, cell_counts=7,
+            n3_cells=8, n3_tris=9, b4_cells=10, b4_tris=11, n4_tris=12, grid_cache=13, face_pairs=14,
+            face_cache=15, interp=16, cell_type=17, cell_nearest=18, cell_ghost=19, cell_points=20, counts=21)
+
+# dtype of each dump (None: follows the handle precision; "rec": 72-byte weight records)
+_DUMP_DTYPE = dict(grid_t=None, grid_tm1=None, grid_tm2=None, neumann=None, dirichlet=None, tri_geom=np.float32,
+                   tri_cells=np.int32, cell_counts=np.int32, n3_cells=np.int32, n3_tris=np.int32,
+                   b4_cells=np.int32, b4_tris=np.int32, n4_tris=np.int32, grid_cache="rec", face_pairs=np.int32,
+                   face_cache="rec", interp=np.float32, cell_type=np.int32, cell_nearest=np.int32,
+                   cell_ghost=np.int32, cell_points=np.float32, counts=np.int32)
+
+# the reference's LayerWeightHalf record (bem.h:163-169)
+RECORD = np.dtype([("s", "<f2", 16), ("ms", "<f4"), ("d", "<f2", 16), ("md", "<f4")])
+assert RECORD.itemsize == 72
+
+
+class PPPMError(RuntimeError):
+    def __init__(self, status, where, message):
+        super().__init__("%s: %s (%s)" % (where, message, status))
+        self.status = status
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("res", ctypes.c_int), ("dl", ctypes.c_float), ("dt", ctypes.c_float),
+                ("min_pos", ctypes.c_float * 3), ("pml_width", ctypes.c_int), ("reflect_coeff", ctypes.c_float),
+                ("c", ctypes.c_float), ("rho", ctypes.c_float), ("precision", ctypes.c_int),
+                ("weights", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libpppm_b200.so not built (%s); run pppm-tdbem_b200/build.py" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, ip, fp, i, sz = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_size_t
+    sig = {
+        "pppm_params_default": [ctypes.POINTER(_Params)],
+        "pppm_create": [ctypes.POINTER(_Params), ctypes.POINTER(vp)],
+        "pppm_destroy": [vp],
+        "pppm_set_mesh": [vp, vp, i, vp, i],
+        "pppm_update_mesh": [vp, vp, i],
+        "pppm_step": [vp, vp, i, i],
+        "pppm_add_listener": [vp, i, i, i],
+        "pppm_clear_listeners": [vp],
+        "pppm_listener_count": [vp, ip, ip],
+        "pppm_read_listeners": [vp, i, i, fp],
+        "pppm_rewind_listeners": [vp],
+        "pppm_get_time": [vp, ip],
+        "pppm_set_time": [vp, i],
+        "pppm_reset_fields": [vp],
+        "pppm_state_size": [vp, ctypes.POINTER(sz)],
+        "pppm_save_state": [vp, vp, sz],
+        "pppm_restore_state": [vp, vp, sz],
+        "pppm_dump_size": [vp, i, ctypes.POINTER(sz)],
+        "pppm_dump": [vp, i, vp, sz],
+        "pppm_load": [vp, i, vp, sz],
+        "pppm_import_grid_cache": [vp, vp, sz],
+        "pppm_import_face_cache": [vp, vp, vp, i],
+        "pppm_classify_cells": [vp, ip],
+        "pppm_fill_fresh_cells": [vp, vp, vp, ip],
+        "pppm_batch_create": [ctypes.POINTER(vp), i, ctypes.POINTER(vp)],
+        "pppm_batch_destroy": [vp],
+        "pppm_batch_run": [vp, ctypes.POINTER(vp), ip, i],
+        "pppm_adjoint": [vp, vp, i, vp, i, vp],
+        "pppm_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "pppm_enable_timing": [vp, i],
+        "pppm_kernel_times": [vp, fp, fp, fp, ip],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    lib.pppm_status_string.argtypes = [ctypes.c_int]
+    lib.pppm_status_string.restype = ctypes.c_char_p
+    lib.pppm_last_error_message.argtypes = []
+    lib.pppm_last_error_message.restype = ctypes.c_char_p
+    return lib
+
+
+lib = _load()
+
+
+def check(status, where):
+    if status != OK:
+        msg = lib.pppm_last_error_message().decode() or lib.pppm_status_string(status).decode()
+        raise PPPMError(status, where, msg)
+
+
+def _ptr(a):
+    """Host numpy array -> (pointer, on_device=0); torch CUDA tensor -> (data_ptr, 1)."""
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr()), 1 if a.is_cuda else 0
+    return a.ctypes.data_as(ctypes.c_void_p), 0
+
+
+class Solver:
+    """One scene: FDTD grid + TDBEM near-field correction (reference PPPMSolver)."""
+
+    def __init__(self, res, dl, dt, min_pos=(0.0, 0.0, 0.0), pml_width=0, reflect_coeff=0.83, c=340.3,
+                 rho=1.225, precision="fp32", weights="ref32", device=0, stream=None):
+        p = _Params()
+        check(lib.pppm_params_default(ctypes.byref(p)), "params_default")
+        p.res, p.dl, p.dt = int(res), float(dl), float(dt)
+        for k in range(3):
+            p.min_pos[k] = float(min_pos[k])
+        p.pml_width, p.reflect_coeff, p.c, p.rho = int(pml_width), float(reflect_coeff), float(c), float(rho)
+        p.precision, p.weights, p.device = PRECISION[precision], WEIGHTS[weights], int(device)
+        p.stream = stream
+        self.h = ctypes.c_void_p()
+        check(lib.pppm_create(ctypes.byref(p), ctypes.byref(self.h)), "pppm_create")
+        self.res, self.dl, self.dt = int(res), float(dl), float(dt)
+        self.precision = precision
+        self.real = np.float64 if precision == "fp64" else np.float32
+        self.nt = 0
+        self.nv = 0
+
+    # -- lifecycle
+    def close(self):
+        if self.h:
+            lib.pppm_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- mesh
+    def set_mesh(self, verts, tris):
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+        check(lib.pppm_set_mesh(self.h, v.ctypes.data_as(ctypes.c_void_p), len(v), f.ctypes.data_as(ctypes.c_void_p),
+                                len(f)), "set_mesh")
+        self.nv, self.nt = len(v), len(f)
+
+    def update_mesh(self, verts):
+        if hasattr(verts, "data_ptr"):
+            ptr, dev = _ptr(verts)
+            check(lib.pppm_update_mesh(self.h, ptr, dev), "update_mesh")
+            return
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        if len(v) != self.nv:
+            raise ValueError("vertex count changed")
+        check(lib.pppm_update_mesh(self.h, v.ctypes.data_as(ctypes.c_void_p), 0), "update_mesh")
+
+    # -- stepping
+    def step(self, acc=None, nsteps=None):
+        """acc: (nsteps, nt) host array or CUDA tensor; None only before set_mesh."""
+        if acc is None:
+            check(lib.pppm_step(self.h, None, 0, int(nsteps or 1)), "step")
+            return
+        if hasattr(acc, "data_ptr"):
+            n = acc.shape[0] if acc.dim() == 2 else 1
+            ptr, dev = _ptr(acc)
+            check(lib.pppm_step(self.h, ptr, dev, n), "step")
+            return
+        a = np.ascontiguousarray(acc, dtype=np.float32)
+        if a.ndim == 1:
+            a = a.reshape(1, -1)
+        check(lib.pppm_step(self.h, a.ctypes.data_as(ctypes.c_void_p), 0, a.shape[0]), "step")
+
+    def update_grid_and_face(self, acc):
+        self.step(np.asarray(acc, dtype=np.float32).reshape(1, -1))
+
+    update_step = update_grid_and_face
+
+    # -- listeners
+    def add_listener(self, x, y, z):
+        check(lib.pppm_add_listener(self.h, int(x), int(y), int(z)), "add_listener")
+
+    def listeners(self, first=0, count=None):
+        n, nl = ctypes.c_int(), ctypes.c_int()
+        check(lib.pppm_listener_count(self.h, ctypes.byref(n), ctypes.byref(nl)), "listener_count")
+        if count is None:
+            count = n.value - first
+        out = np.zeros((count, nl.value), np.float32)
+        if count and nl.value:
+            check(lib.pppm_read_listeners(self.h, first, count, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                  "read_listeners")
+        return out
+
+    def rewind_listeners(self):
+        check(lib.pppm_rewind_listeners(self.h), "rewind_listeners")
+
+    # -- time and state
+    @property
+    def t(self):
+        v = ctypes.c_int()
+        check(lib.pppm_get_time(self.h, ctypes.byref(v)), "get_time")
+        return v.value
+
+    @t.setter
+    def t(self, value):
+        check(lib.pppm_set_time(self.h, int(value)), "set_time")
+
+    def reset_fields(self):
+        check(lib.pppm_reset_fields(self.h), "reset_fields")
+
+    def save_state(self):
+        n = ctypes.c_size_t()
+        check(lib.pppm_state_size(self.h, ctypes.byref(n)), "state_size")
+        buf = np.empty(n.value, np.uint8)
+        check(lib.pppm_save_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), n.value), "save_state")
+        return buf
+
+    def restore_state(self, buf):
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        check(lib.pppm_restore_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.size), "restore_state")
+
+    # -- read-out
+    def dump(self, what):
+        code = DUMP[what]
+        n = ctypes.c_size_t()
+        check(lib.pppm_dump_size(self.h, code, ctypes.byref(n)), "dump_size(%s)" % what)
+        raw = np.empty(n.value, np.uint8)
+        if n.value:
+            check(lib.pppm_dump(self.h, code, raw.ctypes.data_as(ctypes.c_void_p), n.value), "dump(%s)" % what)
+        dt = _DUMP_DTYPE[what]
+        if dt is None:
+            dt = self.real
+        if dt == "rec":
+            if self.precision == "fp64":
+                return raw.view(np.float64).reshape(-1, 16, 2)
+            return raw.view(RECORD)
+        return raw.view(dt)
+
+    def grid(self, rel=0):
+        return self.dump({0: "grid_t", -1: "grid_tm1", -2: "grid_tm2"}[rel]).reshape(self.res, self.res, self.res)
+
+    def load(self, what, arr):
+        a = np.ascontiguousarray(arr, dtype=self.real)
+        check(lib.pppm_load(self.h, DUMP[what], a.ctypes.data_as(ctypes.c_void_p), a.nbytes), "load(%s)" % what)
+
+    def import_grid_cache(self, records):
+        r = np.ascontiguousarray(records)
+        check(lib.pppm_import_grid_cache(self.h, r.ctypes.data_as(ctypes.c_void_p), r.nbytes), "import_grid_cache")
+
+    def import_face_cache(self, pairs, records):
+        p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        r = np.ascontiguousarray(records)
+        check(lib.pppm_import_face_cache(self.h, p.ctypes.data_as(ctypes.c_void_p), r.ctypes.data_as(ctypes.c_void_p),
+                                         len(p)), "import_face_cache")
+
+    def classify_cells(self):
+        g = ctypes.c_int()
+        check(lib.pppm_classify_cells(self.h, ctypes.byref(g)), "classify_cells")
+        return g.value
+
+    def fill_fresh_cells(self, acc, acc_old):
+        a = np.ascontiguousarray(acc, dtype=np.float32)
+        b = np.ascontiguousarray(acc_old, dtype=np.float32)
+        n = ctypes.c_int()
+        check(lib.pppm_fill_fresh_cells(self.h, a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p),
+                                        ctypes.byref(n)), "fill_fresh_cells")
+        return n.value
+
+    def launch_count(self):
+        v = ctypes.c_longlong()
+        check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
+        return v.value
+
+    def enable_timing(self, on=True):
+        check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")
+
+    def kernel_times(self):
+        a, b, c, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+        check(lib.pppm_kernel_times(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(n)),
+              "kernel_times")
+        return a.value, b.value, c.value, n.value

@@ -1,0 +1,205 @@
+"""Seeded synthetic scenes for the PPPM-TDBEM step: meshes, rigid motion, accelerations.
+
+The benchmark configurations of this project are synthetic (no dataset is involved):
+  static sphere   icosphere subdivision 3 (642 vertices, 1280 triangles), radius 0.1 m,
+                  res 32, grid length 2x the bounding box, dt = 0.5 h / (sqrt(3) c),
+                  uniform acceleration sin(2 pi 1000 t), listener at int(0.875 res)
+  moving sphere   icosphere subdivision 4 (2562 / 5120) with seeded +-10% radial noise,
+  + plate         radius 0.08 m, translating 0.05 sin(2 pi 3 t) m along x and rotating
+                  2 rad/s about a seeded axis, plus a static 1280-triangle plate; res 64;
+                  band-limited (100 Hz - 8 kHz) unit-RMS Gaussian per-vertex accelerations
+                  averaged to triangles; motion frames sampled at 1 kHz
+  batch           scenes drawn from one seed with res in {24, 32, 48, 64}, perturbed
+                  icospheres of subdivision 2-4 and 1000-4000 steps
+Grid placement follows the reference's demo driver (experiments/demo/main.cu:96-103): grid
+centred on the scene bounding box, length = factor * longest box side, h = length / res,
+and for moving scenes dt = 1 / int(1.01 / (h / sqrt(3) / c)).
+"""
+import math
+
+import numpy as np
+
+C_REF = 340.3  # AIR_WAVE_SPEED (macro.h:82)
+
+
+def icosphere(subdivisions):
+    """Unit icosphere: 10 * 4^n + 2 vertices, 20 * 4^n triangles (outward winding)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, float) / np.linalg.norm(p) for p in v]
+    faces = list(f)
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts, np.float64), np.array(faces, np.int32)
+
+
+def perturbed_sphere(subdivisions, radius, noise, rng):
+    v, f = icosphere(subdivisions)
+    r = radius * (1.0 + noise * rng.uniform(-1.0, 1.0, size=len(v)))
+    return (v * r[:, None]).astype(np.float64), f
+
+
+def plate(nx, nz, size_x, size_z, y):
+    """Flat rectangle in the x-z plane at height y, nx * nz quads, 2 * nx * nz triangles."""
+    xs = np.linspace(-size_x / 2, size_x / 2, nx + 1)
+    zs = np.linspace(-size_z / 2, size_z / 2, nz + 1)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    verts = np.stack([X.ravel(), np.full(X.size, y), Z.ravel()], 1)
+    f = []
+    for i in range(nx):
+        for k in range(nz):
+            a, b = i * (nz + 1) + k, (i + 1) * (nz + 1) + k
+            f += [(a, b + 1, b), (a, a + 1, b + 1)]
+    return verts, np.array(f, np.int32)
+
+
+def rotation_matrix(axis, angle):
+    axis = np.asarray(axis, float) / np.linalg.norm(axis)
+    x, y, z = axis
+    c, s = math.cos(angle), math.sin(angle)
+    C = 1 - c
+    return np.array([[c + x * x * C, x * y * C - z * s, x * z * C + y * s],
+                     [y * x * C + z * s, c + y * y * C, y * z * C - x * s],
+                     [z * x * C - y * s, z * y * C + x * s, c + z * z * C]])
+
+
+def grid_for_bbox(lo, hi, res, factor):
+    """Grid of the demo driver: centred on the box, length = factor * longest side."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    length = float((hi - lo).max()) * factor
+    h = length / res
+    centre = (lo + hi) / 2
+    min_pos = centre - length / 2
+    return np.float32(h), min_pos.astype(np.float32)
+
+
+def demo_dt(h, c=C_REF):
+    """dt = 1 / int(1.01 / (h / sqrt(3) / c)) (experiments/demo/main.cu:103,128)."""
+    frame_rate = int(np.float32(1.01) / (np.float32(h) / np.float32(math.sqrt(3)) / np.float32(c)))
+    return np.float32(1.0 / frame_rate), frame_rate
+
+
+def band_noise(n_series, n_steps, dt, lo_hz, hi_hz, rng):
+    """Unit-RMS Gaussian noise band-limited to [lo_hz, hi_hz] by an FFT mask, per series."""
+    x = rng.standard_normal((n_series, n_steps))
+    X = np.fft.rfft(x, axis=1)
+    freqs = np.fft.rfftfreq(n_steps, dt)
+    X[:, (freqs < lo_hz) | (freqs > hi_hz)] = 0
+    y = np.fft.irfft(X, n_steps, axis=1)
+    rms = np.sqrt((y ** 2).mean(axis=1, keepdims=True))
+    rms[rms == 0] = 1
+    return (y / rms).astype(np.float32)
+
+
+class StaticSphere:
+    """Static pulsating sphere at res 32 (the reference's CPU-sized case)."""
+
+    def __init__(self, res=32, subdivisions=3, radius=0.1, factor=2.0, steps=2000, freq=1000.0, c=C_REF):
+        v, f = icosphere(subdivisions)
+        self.verts = (v * radius).astype(np.float32)
+        self.tris = f
+        self.res = res
+        self.h, self.min_pos = grid_for_bbox(self.verts.min(0), self.verts.max(0), res, factor)
+        self.dt = np.float32(0.5 * self.h / (math.sqrt(3) * c))
+        self.steps = steps
+        self.freq = freq
+        self.listener = (int(0.875 * res),) * 3
+
+    def acc(self, first, count):
+        t = (np.arange(first, first + count, dtype=np.float64)) * float(self.dt)
+        a = np.sin(2 * math.pi * self.freq * t).astype(np.float32)
+        return np.repeat(a[:, None], len(self.tris), 1)
+
+
+class MovingScene:
+    """Moving perturbed sphere plus a static plate (res 64, 1 kHz motion frames)."""
+
+    def __init__(self, res=64, seed=7, subdivisions=4, radius=0.08, noise=0.1, amp=0.05, freq=3.0, omega=2.0,
+                 plate_tris=1280, steps=8820, frame_hz=1000.0, factor=2.0, c=C_REF):
+        rng = np.random.default_rng(seed)
+        sv, sf = perturbed_sphere(subdivisions, radius, noise, rng)
+        self.sphere_verts = sv
+        self.axis = rng.standard_normal(3)
+        self.axis /= np.linalg.norm(self.axis)
+        nq = plate_tris // 2
+        nx = 32 if nq % 32 == 0 else int(math.sqrt(nq))
+        nz = nq // nx
+        rmax = radius * (1 + noise)
+        pv, pf = plate(nx, nz, 2 * (amp + rmax), 2 * rmax, -(rmax + 0.05))
+        self.plate_verts = pv
+        self.nsv = len(sv)
+        self.tris = np.concatenate([sf, pf + len(sv)]).astype(np.int32)
+        self.n_sphere_tris = len(sf)
+        self.amp, self.freq, self.omega = amp, freq, omega
+        lo = np.minimum(np.array([-amp - rmax, -rmax, -rmax]), pv.min(0))
+        hi = np.maximum(np.array([amp + rmax, rmax, rmax]), pv.max(0))
+        self.res = res
+        self.h, self.min_pos = grid_for_bbox(lo, hi, res, factor)
+        self.dt, self.frame_rate = demo_dt(self.h, c)
+        self.steps = steps
+        self.frame_hz = frame_hz
+        self.listener = (int(0.875 * res),) * 3
+        self.seed = seed
+        self._noise = None
+
+    def verts_at(self, time):
+        R = rotation_matrix(self.axis, self.omega * time)
+        sv = self.sphere_verts @ R.T
+        sv[:, 0] += self.amp * math.sin(2 * math.pi * self.freq * time)
+        return np.concatenate([sv, self.plate_verts]).astype(np.float32)
+
+    def frame_of_step(self, step):
+        """Motion frame in force at the start of PPPM step `step` (frame time <= t)."""
+        return int(math.floor(step * float(self.dt) * self.frame_hz + 1e-9))
+
+    def frame_verts(self, frame):
+        return self.verts_at(frame / self.frame_hz)
+
+    def acc(self, first, count):
+        """Per-triangle accelerations for steps [first, first + count): sphere triangles carry
+        band-limited vertex noise averaged to the triangle, the plate is silent."""
+        need = first + count
+        if self._noise is None or self._noise.shape[1] < need:
+            n = max(need, self.steps)
+            rng = np.random.default_rng(self.seed + 1)
+            self._noise = band_noise(self.nsv, n, float(self.dt), 100.0, 8000.0, rng)
+        vn = self._noise[:, first:need]
+        sf = self.tris[: self.n_sphere_tris]
+        tri = (vn[sf[:, 0]] + vn[sf[:, 1]] + vn[sf[:, 2]]) / np.float32(3)
+        out = np.zeros((count, len(self.tris)), np.float32)
+        out[:, : self.n_sphere_tris] = tri.T
+        return out
+
+
+def batch_scenes(n=64, seed=11, c=C_REF):
+    """Independent scenes drawn from one seed: (res, verts, tris, h, min_pos, dt, steps)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        res = int(rng.choice([24, 32, 48, 64]))
+        sub = int(rng.integers(2, 5))
+        v, f = perturbed_sphere(sub, 0.1, 0.1, rng)
+        v = v.astype(np.float32)
+        h, mn = grid_for_bbox(v.min(0), v.max(0), res, 2.0)
+        dt = np.float32(0.5 * h / (math.sqrt(3) * c))
+        steps = int(rng.integers(1000, 4001))
+        out.append(dict(res=res, verts=v, tris=f, h=h, min_pos=mn, dt=dt, steps=steps, freq=float(rng.uniform(500, 2000))))
+    return out

@@ -1,0 +1,56 @@
+"""The C ABI library loads on a machine without a GPU and exports every symbol the header
+declares; the checkers load too.  No compute call is made here."""
+import ctypes
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "pppm_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pppm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = header_functions()
+    for required in ("pppm_create", "pppm_destroy", "pppm_set_mesh", "pppm_update_mesh", "pppm_step",
+                     "pppm_add_listener", "pppm_read_listeners", "pppm_save_state", "pppm_restore_state",
+                     "pppm_reset_fields", "pppm_dump", "pppm_import_grid_cache", "pppm_import_face_cache",
+                     "pppm_batch_create", "pppm_batch_run", "pppm_adjoint"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    import pppm_b200
+
+    lib = ctypes.CDLL(pppm_b200.LIB_PATH)
+    missing = [n for n in header_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    import pppm_b200
+
+    assert pppm_b200.lib.pppm_status_string(0) == b"ok"
+    assert pppm_b200.lib.pppm_status_string(3) == b"capacity exceeded"
+
+
+def test_create_rejects_bad_parameters_without_device_calls():
+    import pppm_b200
+
+    for kw in (dict(res=4, dl=0.01, dt=1e-5), dict(res=32, dl=-1.0, dt=1e-5), dict(res=32, dl=0.01, dt=1e-5, pml_width=40)):
+        try:
+            pppm_b200.Solver(**kw)
+        except pppm_b200.PPPMError as e:
+            assert e.status == pppm_b200.ERR_ARG
+        else:
+            raise AssertionError("accepted %r" % kw)
+
+
+def test_oracle_library_loads():
+    from oracle.oracle import oracle_lib, oracle_threads
+
+    assert oracle_lib() is not None
+    assert oracle_threads() >= 1
