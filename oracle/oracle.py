@@ -68,6 +68,7 @@ def oracle_lib():
             "orc_import_grid_cache": (_i, [_vp, _vp]),
             "orc_import_face_cache": (_i, [_vp, _vp, _vp, _i]),
             "orc_laplace_weight": (_i, [_f, _f, _f, _vp, _vp, _i, _vp, _vp, _vp]),
+            "orc_pair_integral": (_i, [_f, _vp, _vp, _i, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
             "orc_classify": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
             "orc_fresh": (_i, [_vp, _vp, _vp, _vp]),
             "orc_threads": (_i, []),
@@ -248,6 +249,23 @@ def laplace_weight(dt, dl, verts, src, point=None, face=None, c=340.3):
     if rc:
         raise RuntimeError("orc_laplace_weight failed")
     return out
+
+
+def pair_integral(dl, verts, src, k, point=None, face=None):
+    """Frequency-domain single / double layer integral of one pair at complex wave number k."""
+    lib = oracle_lib()
+    v = np.ascontiguousarray(verts, np.float32)
+    s = np.ascontiguousarray(src, np.int32)
+    out = np.zeros(4, np.float64)
+    if point is not None:
+        rc = lib.orc_pair_integral(float(dl), _p(v), _p(s), 1, None, _p(np.ascontiguousarray(point, np.float32)),
+                                   float(np.real(k)), float(np.imag(k)), _p(out))
+    else:
+        rc = lib.orc_pair_integral(float(dl), _p(v), _p(s), 0, _p(np.ascontiguousarray(face, np.int32)), None,
+                                   float(np.real(k)), float(np.imag(k)), _p(out))
+    if rc:
+        raise RuntimeError("orc_pair_integral failed")
+    return complex(out[0], out[1]), complex(out[2], out[3])
 
 
 def oracle_threads():

@@ -443,6 +443,37 @@ static void unpack(const rec72 *r, float *w32)
     }
 }
 
+/* Frequency-domain pair integral at an arbitrary complex wave number (the reference's
+ * TDBEM::helmholtz weights, bem.h:370-379): out4 = single (re, im), double (re, im). */
+int orc_pair_integral(float dl, const float *V, const int *src, int to_point, const int *dst_face,
+                      const float *dst_point, double k_re, double k_im, double *out4)
+{
+    v3 sv[3];
+    for (int k = 0; k < 3; k++)
+        sv[k] = V3(V[3 * src[k]], V[3 * src[k] + 1], V[3 * src[k] + 2]);
+    double complex kk = k_re + I * k_im, a, b;
+    if (to_point)
+    {
+        v3 p = V3(dst_point[0], dst_point[1], dst_point[2]);
+        double one = 1;
+        a = face_to_points(sv, &p, &one, 1, kk, 0);
+        b = face_to_points(sv, &p, &one, 1, kk, 1);
+    }
+    else
+    {
+        v3 tv[3];
+        for (int q = 0; q < 3; q++)
+            tv[q] = V3(V[3 * dst_face[q]], V[3 * dst_face[q] + 1], V[3 * dst_face[q] + 2]);
+        a = face_to_face(sv, src, tv, dst_face, kk, dl * 0.1, 0);
+        b = face_to_face(sv, src, tv, dst_face, kk, dl * 0.1, 1);
+    }
+    out4[0] = creal(a);
+    out4[1] = cimag(a);
+    out4[2] = creal(b);
+    out4[3] = cimag(b);
+    return 0;
+}
+
 int orc_laplace_weight(float dt, float dl, float c, const float *V, const int *src, int to_point, const int *dst_face,
                        const float *dst_point, double *out32)
 {

@@ -52,6 +52,9 @@ int orc_import_face_cache(orc_scene *s, const int *pairs, const void *records, i
 /* single pair weights (double): src triangle onto a point or a face */
 int orc_laplace_weight(float dt, float dl, float c, const float *V, const int *src, int to_point, const int *dst_face,
                        const float *dst_point, double *out32);
+/* frequency-domain pair integral at complex wave number k: single (re, im), double (re, im) */
+int orc_pair_integral(float dl, const float *V, const int *src, int to_point, const int *dst_face,
+                      const float *dst_point, double k_re, double k_im, double *out4);
 /* cell labels: type, nearest, ghost index, points (nearest xyz, reflect xyz, distance) */
 int orc_classify(orc_scene *s, int *type, int *nearest, int *ghost, float *points, int *ghost_count);
 int orc_fresh(orc_scene *s, const float *acc, const float *acc_old, int *fresh_count);
