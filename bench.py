@@ -258,12 +258,12 @@ def run_ours(args, ws, rank, local):
     s.step(acc_dev[a:b])
     us_st, us_face, us_near, nt_timed = s.kernel_times()
     s.enable_timing(False)
-    counts = s.dump("counts")
-    alg = algorithmic_bytes(counts, wl.res, len(wl.tris))
+    counts = [int(x) for x in s.dump("counts")]
+    alg = {k: int(v) for k, v in algorithmic_bytes(counts, wl.res, len(wl.tris)).items()}
     times = {"stencil": us_st, "face": us_face, "near": us_near}
     top = max(times, key=lambda k: times[k])
     peak, peak_kind = measured_peak()
-    achieved = alg[top] / (times[top] * 1e-6) / 1e9
+    achieved = float(alg[top] / (times[top] * 1e-6) / 1e9)
     traffic = load_traffic().get(top)
     # update_mesh share of a frame
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -180,6 +180,16 @@ int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, in
 int pppm_adjoint(pppm_handle *h, const float *acc, int nsteps, const float *dL_dsignal, int checkpoint_every,
                  float *dL_dacc);
 
+/* ------------------------------------------------------------ weight diagnostics ----- */
+/* TDBEM::init (bem.h:264-277) as this library evaluates it on the host: lambda and the 16
+ * complex wave numbers (wave[2k] real, wave[2k+1] imaginary).  No device is touched. */
+int pppm_tdbem_constants(float dt, float dl, float c, float *lambda, float *wave32);
+/* TDBEM::laplace_weight (bem.h:306-330) of one pair evaluated on device `device` with the
+ * FP32 weight arithmetic of the caches: src triangle (indices into verts) onto a point
+ * (to_point != 0) or onto dst_face.  out32: 16 single-layer then 16 double-layer taps. */
+int pppm_pair_weights(int device, float dt, float dl, float c, const float *verts, int nv, const int *src,
+                      int to_point, const int *dst_face, const float *dst_point, float *out32);
+
 /* ------------------------------------------------------------ diagnostics ------------ */
 const char *pppm_status_string(int status);
 const char *pppm_last_error_message(void);

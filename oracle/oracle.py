@@ -48,6 +48,7 @@ def oracle_lib():
             "orc_create": (_vp, [_i, _f, _f, _vp, _f, _f, _i, _i]),
             "orc_destroy": (None, [_vp]),
             "orc_set_mesh": (_i, [_vp, _vp, _i, _vp, _i]),
+            "orc_set_mesh_cells": (_i, [_vp, _vp, _i, _vp, _i, _vp]),
             "orc_update_mesh": (_i, [_vp, _vp]),
             "orc_step": (_i, [_vp, _vp, _i, _vp, _i, _vp]),
             "orc_time": (_i, [_vp]),
@@ -66,6 +67,7 @@ def oracle_lib():
             "orc_grid_records": (_i, [_vp, _vp]),
             "orc_face_records": (_i, [_vp, _vp]),
             "orc_import_grid_cache": (_i, [_vp, _vp]),
+            "orc_import_interp": (_i, [_vp, _vp]),
             "orc_import_face_cache": (_i, [_vp, _vp, _vp, _i]),
             "orc_laplace_weight": (_i, [_f, _f, _f, _vp, _vp, _i, _vp, _vp, _vp]),
             "orc_pair_integral": (_i, [_f, _vp, _vp, _i, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
@@ -110,6 +112,14 @@ class Oracle:
         v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
         f = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
         self._ok(self.lib.orc_set_mesh(self.s, _p(v), len(v), _p(f), len(f)), "set_mesh")
+        self.nv, self.nt = len(v), len(f)
+
+    def set_mesh_cells(self, verts, tris, cells):
+        """set_mesh with the triangles' grid / base cells given (n x 6)."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        c = np.ascontiguousarray(cells, np.int32).reshape(-1, 6)
+        self._ok(self.lib.orc_set_mesh_cells(self.s, _p(v), len(v), _p(f), len(f), _p(c)), "set_mesh_cells")
         self.nv, self.nt = len(v), len(f)
 
     def update_mesh(self, verts):
@@ -211,6 +221,9 @@ class Oracle:
     def import_grid_cache(self, records):
         r = np.ascontiguousarray(records)
         self._ok(self.lib.orc_import_grid_cache(self.s, _p(r)), "import_grid_cache")
+
+    def import_interp(self, w):
+        self._ok(self.lib.orc_import_interp(self.s, _p(np.ascontiguousarray(w, np.float32))), "import_interp")
 
     def import_face_cache(self, pairs, records):
         p = np.ascontiguousarray(pairs, np.int32)

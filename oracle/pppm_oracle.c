@@ -919,7 +919,22 @@ static void denominators(orc_scene *s)
     }
 }
 
+static int set_mesh_impl(orc_scene *s, const float *V, int nv, const int *F, int nt, const int *cells6);
+
 int orc_set_mesh(orc_scene *s, const float *V, int nv, const int *F, int nt)
+{
+    return set_mesh_impl(s, V, nv, F, nt, NULL);
+}
+
+/* Same as orc_set_mesh with the triangles' grid and base cells given (nt x 6), e.g. the
+ * reference's own assignment for centres that fall exactly on a cell face, where its
+ * approximate device division and the oracle's IEEE division can round to different cells. */
+int orc_set_mesh_cells(orc_scene *s, const float *V, int nv, const int *F, int nt, const int *cells6)
+{
+    return set_mesh_impl(s, V, nv, F, nt, cells6);
+}
+
+static int set_mesh_impl(orc_scene *s, const float *V, int nv, const int *F, int nt, const int *cells6)
 {
     if (!s || s->mesh_set || nv <= 0 || nt <= 0)
         return 1;
@@ -957,6 +972,17 @@ int orc_set_mesh(orc_scene *s, const float *V, int nv, const int *F, int nt)
     s->dirichlet = xcalloc((size_t)nt * RING, rs);
     if (geometry(s))
         return 1;
+    if (cells6)
+        for (int i = 0; i < nt; i++)
+        {
+            for (int q = 0; q < 3; q++)
+            {
+                s->cellc[3 * i + q] = cells6[6 * i + q];
+                s->basec[3 * i + q] = cells6[6 * i + 3 + q];
+            }
+            s->cell[i] = (int)lin(s->res, cells6[6 * i], cells6[6 * i + 1], cells6[6 * i + 2]);
+            s->base[i] = (int)lin(s->res, cells6[6 * i + 3], cells6[6 * i + 4], cells6[6 * i + 5]);
+        }
     lists(s);
     if (caches(s))
         return 3;
@@ -1427,6 +1453,19 @@ int orc_face_records(orc_scene *s, void *out)
     rec72 *o = (rec72 *)out;
     for (long long p = 0; p < s->pf; p++)
         o[p] = s->pool_r[s->face_slot[p]];
+    return 0;
+}
+
+/* trilinear face weights (nt x 8) taken from elsewhere, e.g. the reference's own */
+int orc_import_interp(orc_scene *s, const float *w)
+{
+    if (!s || !s->mesh_set)
+        return 5;
+    for (int i = 0; i < 8 * s->nt; i++)
+    {
+        s->interp[i] = w[i];
+        s->interp_d[i] = w[i];
+    }
     return 0;
 }
 

@@ -26,6 +26,7 @@ orc_scene *orc_create(int res, float dl, float dt, const float *min_pos, float r
                       int precision);
 void orc_destroy(orc_scene *s);
 int orc_set_mesh(orc_scene *s, const float *V, int nv, const int *F, int nt);
+int orc_set_mesh_cells(orc_scene *s, const float *V, int nv, const int *F, int nt, const int *cells6);
 int orc_update_mesh(orc_scene *s, const float *V);
 int orc_step(orc_scene *s, const float *acc, int nsteps, const int *listen_xyz, int nlisten, float *out);
 int orc_time(orc_scene *s);
@@ -48,6 +49,7 @@ int orc_face_weights(orc_scene *s, double *out);
 int orc_grid_records(orc_scene *s, void *out);
 int orc_face_records(orc_scene *s, void *out);
 int orc_import_grid_cache(orc_scene *s, const void *records);
+int orc_import_interp(orc_scene *s, const float *w);
 int orc_import_face_cache(orc_scene *s, const int *pairs, const void *records, int n);
 /* single pair weights (double): src triangle onto a point or a face */
 int orc_laplace_weight(float dt, float dl, float c, const float *V, const int *src, int to_point, const int *dst_face,

@@ -86,6 +86,9 @@ def _load():
         "pppm_enable_timing": [vp, i],
         "pppm_kernel_times": [vp, fp, fp, fp, ip],
     }
+    fl = ctypes.c_float
+    sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
+    sig["pppm_pair_weights"] = [i, fl, fl, fl, vp, i, vp, i, vp, vp, vp]
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -113,6 +116,34 @@ def _ptr(a):
             raise ValueError("tensor must be contiguous")
         return ctypes.c_void_p(a.data_ptr()), 1 if a.is_cuda else 0
     return a.ctypes.data_as(ctypes.c_void_p), 0
+
+
+def tdbem_constants(dt, dl, c=340.3):
+    """lambda and the 16 wave numbers (complex) the library derives from dt and h (host only)."""
+    lam = ctypes.c_float()
+    w = np.zeros(32, np.float32)
+    check(lib.pppm_tdbem_constants(float(dt), float(dl), float(c), ctypes.byref(lam),
+                                   w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "tdbem_constants")
+    return lam.value, w.reshape(16, 2)
+
+
+def pair_weights(dt, dl, verts, src, point=None, face=None, c=340.3, device=0):
+    """16 + 16 TDBEM taps of one pair computed on the device with the caches' FP32 arithmetic."""
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    s = np.ascontiguousarray(src, np.int32)
+    out = np.zeros(32, np.float32)
+    if point is not None:
+        pt = np.ascontiguousarray(point, np.float32)
+        rc = lib.pppm_pair_weights(device, float(dt), float(dl), float(c), v.ctypes.data_as(ctypes.c_void_p), len(v),
+                                   s.ctypes.data_as(ctypes.c_void_p), 1, None, pt.ctypes.data_as(ctypes.c_void_p),
+                                   out.ctypes.data_as(ctypes.c_void_p))
+    else:
+        fc = np.ascontiguousarray(face, np.int32)
+        rc = lib.pppm_pair_weights(device, float(dt), float(dl), float(c), v.ctypes.data_as(ctypes.c_void_p), len(v),
+                                   s.ctypes.data_as(ctypes.c_void_p), 0, fc.ctypes.data_as(ctypes.c_void_p), None,
+                                   out.ctypes.data_as(ctypes.c_void_p))
+    check(rc, "pair_weights")
+    return out
 
 
 class Solver:

@@ -196,5 +196,34 @@ def main(out):
     print("golden vectors written to", out)
 
 
+def noise_floor(out, repeats=3):
+    """The reference's own run-to-run spread: the same inputs run several times (its float
+    atomics sum in a different order each run).  noise.npz: series of each repeat for the
+    static sphere (2000 steps) and the small sphere (300 steps)."""
+    os.makedirs(out, exist_ok=True)
+    sc = scenes.StaticSphere()
+    big = []
+    for _ in range(repeats):
+        r = O.Reference(sc.res, sc.h, sc.dt, sc.min_pos)
+        r.set_mesh(sc.verts, sc.tris)
+        big.append(r.run(sc.acc(0, sc.steps), [sc.listener])[:, 0])
+        r.close()
+    v, fc, h, mn, dts = sphere_small_scene()
+    acc = np.repeat(np.sin(2 * np.pi * 1500.0 * np.arange(300) * float(dts)).astype(np.float32)[:, None], len(fc), 1)
+    small = []
+    for _ in range(repeats):
+        r = O.Reference(24, h, dts, mn)
+        r.set_mesh(v, fc)
+        small.append(r.run(acc, [(20, 20, 20)])[:, 0])
+        r.close()
+    np.savez_compressed(os.path.join(out, "noise.npz"), static_sphere=np.array(big), sphere_small=np.array(small))
+    print("noise floor written to", out)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    out = args[0] if args else os.path.join(ROOT, "gpurun_out", "golden")
+    if "--noise" in sys.argv:
+        noise_floor(out)
+    else:
+        main(out)

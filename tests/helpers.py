@@ -8,10 +8,18 @@ from pppm_b200 import scenes
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def sphere_small(res=24, sub=2, radius=0.1):
+# Grid offset (in cells) that keeps the symmetric icosphere's triangle centres off cell faces:
+# centred grids put many centres exactly on a face, where the device's approximate division
+# and the CPU oracle's IEEE division may round to neighbouring cells.
+OFFSET = np.array([0.137, 0.291, 0.0713])
+
+
+def sphere_small(res=24, sub=2, radius=0.1, offset=True):
     v, f = scenes.icosphere(sub)
     v = (v * radius).astype(np.float32)
     h, mn = scenes.grid_for_bbox(v.min(0), v.max(0), res, 2.0)
+    if offset:
+        mn = (mn + OFFSET * h).astype(np.float32)
     dt = np.float32(0.5 * h / (np.sqrt(3) * 340.3))
     return v, f, h, mn, dt
 

@@ -1,0 +1,222 @@
+"""libpppm_b200 on the B200 against golden vectors produced by the reference solver itself
+(tests/golden/, from tests/golden/make_golden.py).  Inputs are the reference runs' exact inputs,
+including its centred grids where triangle centres fall on cell faces; the library divides
+with the same approximate device division as the reference, so cells and lists must agree
+exactly.
+
+Measured agreement is also written to $PPPM_METRICS_DIR/golden_metrics.json when that variable
+is set (the figures quoted in the design notes).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import golden, moving_small_verts, per_cell_sets, records_to_taps, rel_l2, sine_acc
+from pppm_b200 import RECORD, Solver, pair_weights
+
+pytestmark = pytest.mark.gpu
+METRICS = {}
+
+
+def need(name):
+    g = golden(name)
+    if g is None:
+        pytest.skip("golden fixture %s missing" % name)
+    return g
+
+
+@pytest.fixture(scope="module", autouse=True)
+def write_metrics():
+    yield
+    d = os.environ.get("PPPM_METRICS_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "golden_metrics.json"), "w") as f:
+            json.dump(METRICS, f, indent=1, default=float)
+
+
+def test_pair_weights_match_reference(gpu):
+    g = need("pairs.npz")
+    worst = 0.0
+    exact = 0
+    for kind, src, dst, pt, w in zip(g["kinds"], g["src"], g["dst"], g["pts"], g["w"]):
+        if kind == "point":
+            got = pair_weights(g["dt"], g["h"], g["verts"], src, point=pt)
+        else:
+            got = pair_weights(g["dt"], g["h"], g["verts"], src, face=dst)
+        exact += int(np.array_equal(got, w))
+        for half in (slice(0, 16), slice(16, 32)):
+            sc = max(np.abs(w[half]).max(), 1e-30)
+            worst = max(worst, float(np.abs(got[half] - w[half]).max() / sc))
+    METRICS["pair_weights"] = {"pairs": len(g["w"]), "bit_exact": exact, "max_rel_diff": worst}
+    assert worst < 1e-5
+
+
+@pytest.mark.parametrize("name", ["fdtd.npz", "pml.npz"])
+def test_fdtd_matches_reference(gpu, name):
+    g = need(name)
+    s = Solver(int(g["res"]), float(g["dl"]), g["dt"], pml_width=int(g["pml"]))
+    s.t = 0
+    s.load("grid_t", g["init_t"])
+    s.load("grid_tm1", g["init_tm1"])
+    s.step(None, nsteps=int(g["t"]))
+    diffs = []
+    for rel, key in ((0, "grid_t"), (-1, "grid_tm1")):
+        scale = np.abs(g[key]).max()
+        d = float(np.abs(s.grid(rel) - g[key]).max() / scale)
+        diffs.append(d)
+        assert d <= 1e-5
+    METRICS[name] = {"max_abs_diff_over_scale": max(diffs),
+                     "bit_exact": bool(np.array_equal(s.grid(0), g["grid_t"]))}
+    s.close()
+
+
+def _small():
+    g = need("sphere_small.npz")
+    s = Solver(int(g["res"]), g["h"], g["dt"], g["min_pos"])
+    s.set_mesh(g["verts"], g["tris"])
+    return g, s
+
+
+def test_lists_and_cells_bit_exact_vs_reference(gpu):
+    g, s = _small()
+    assert np.array_equal(s.dump("tri_cells").reshape(-1, 6), g["cells"])
+    np.testing.assert_allclose(s.dump("tri_geom").reshape(-1, 7), g["geom"], rtol=1e-6, atol=1e-9)
+    assert np.array_equal(s.dump("cell_counts"), g["cell_counts"])
+    n3 = s.dump("n3_cells").reshape(-1, 4)
+    assert np.array_equal(n3, g["n3_cells"])
+    assert per_cell_sets(n3, s.dump("n3_tris")) == per_cell_sets(g["n3_cells"], g["n3_tris"])
+    b4 = s.dump("b4_cells").reshape(-1, 4)
+    assert np.array_equal(b4, g["b4_cells"])
+    ours4 = per_cell_sets(np.c_[b4[:, :3], g["n4_len"]], s.dump("n4_tris"))
+    assert ours4 == per_cell_sets(np.c_[g["b4_cells"][:, :3], g["n4_len"]], g["n4_tris"])
+    assert set(map(tuple, s.dump("face_pairs").reshape(-1, 2))) == set(map(tuple, g["face_pairs"]))
+    s.close()
+
+
+def test_cache_tables_vs_reference(gpu):
+    g, s = _small()
+    ref = g["grid_cache"].view(RECORD)
+    ours = s.dump("grid_cache")
+    same_gc = float(np.mean(ours.view(np.uint8).reshape(-1, 72) == ref.view(np.uint8).reshape(-1, 72)).__float__())
+    rec_exact_gc = float(np.mean(np.all(ours.view(np.uint8).reshape(-1, 72) == ref.view(np.uint8).reshape(-1, 72), 1)))
+    a, b = records_to_taps(ours), records_to_taps(ref)
+    worst = 0.0
+    for half in (slice(0, 16), slice(16, 32)):
+        sc = np.maximum(np.abs(b[:, half]).max(1), 1e-30)
+        worst = max(worst, float((np.abs(a[:, half] - b[:, half]).max(1) / sc).max()))
+    pairs = s.dump("face_pairs").reshape(-1, 2)
+    idx = {tuple(p): i for i, p in enumerate(pairs)}
+    order = np.array([idx[tuple(p)] for p in g["face_pairs"]])
+    fo = s.dump("face_cache")[order]
+    fr = g["face_cache"].view(RECORD)
+    rec_exact_fc = float(np.mean(np.all(fo.view(np.uint8).reshape(-1, 72) == fr.view(np.uint8).reshape(-1, 72), 1)))
+    a, b = records_to_taps(fo), records_to_taps(fr)
+    worst_fc = 0.0
+    for half in (slice(0, 16), slice(16, 32)):
+        sc = np.maximum(np.abs(b[:, half]).max(1), 1e-30)
+        worst_fc = max(worst_fc, float((np.abs(a[:, half] - b[:, half]).max(1) / sc).max()))
+    interp = float(np.abs(s.dump("interp").reshape(-1, 8) - g["interp"]).max())
+    METRICS["tables"] = {"grid_cache_records_bit_exact": rec_exact_gc, "grid_cache_bytes_equal": same_gc,
+                         "grid_cache_max_rel_diff": worst, "face_cache_records_bit_exact": rec_exact_fc,
+                         "face_cache_max_rel_diff": worst_fc, "interp_max_abs_diff": interp}
+    assert worst < 2e-3 and worst_fc < 2e-3
+    s.close()
+
+
+def _series(s, g):
+    steps = int(g["steps"])
+    acc = sine_acc(steps, len(g["tris"]), float(g["acc_freq"]), g["dt"])
+    for lx in g["listeners"]:
+        s.add_listener(*lx)
+    s.step(acc)
+    return s.listeners()
+
+
+def test_series_with_reference_tables(gpu):
+    g, s = _small()
+    s.import_grid_cache(g["grid_cache"].view(RECORD))
+    s.import_face_cache(g["face_pairs"], g["face_cache"].view(RECORD))
+    got = _series(s, g)
+    e50 = max(rel_l2(got[:50, l], g["series"][:50, l]) for l in range(got.shape[1]))
+    eall = max(rel_l2(got[:, l], g["series"][:, l]) for l in range(got.shape[1]))
+    METRICS["series_reference_tables"] = {"rel_l2_first50": e50, "rel_l2_300": eall,
+                                          "final_grid_rel_l2": rel_l2(s.grid(0), g["final_grid"])}
+    assert e50 < 1e-5
+    assert eall < 1e-3
+    s.close()
+
+
+def test_series_with_own_tables(gpu):
+    g, s = _small()
+    got = _series(s, g)
+    e50 = max(rel_l2(got[:50, l], g["series"][:50, l]) for l in range(got.shape[1]))
+    eall = max(rel_l2(got[:, l], g["series"][:, l]) for l in range(got.shape[1]))
+    METRICS["series_own_tables"] = {"rel_l2_first50": e50, "rel_l2_300": eall}
+    assert eall < 1e-2
+    s.close()
+
+
+def test_static_sphere_2000_steps(gpu):
+    from pppm_b200 import scenes
+
+    g = need("static_sphere.npz")
+    sc = scenes.StaticSphere()
+    s = Solver(sc.res, sc.h, sc.dt, sc.min_pos)
+    s.set_mesh(sc.verts, sc.tris)
+    assert np.array_equal(s.dump("n3_cells").reshape(-1, 4), g["n3_cells"])
+    assert np.array_equal(s.dump("cell_counts"), g["cell_counts"])
+    s.add_listener(*sc.listener)
+    s.step(sc.acc(0, sc.steps))
+    got = s.listeners()[:, 0]
+    ref = g["series"][:, 0]
+    METRICS["static_sphere"] = {"rel_l2_2000": rel_l2(got, ref), "rel_l2_first200": rel_l2(got[:200], ref[:200])}
+    assert rel_l2(got, ref) < 1e-2
+    s.close()
+
+
+def test_moving_small_vs_reference(gpu):
+    g = need("moving_small.npz")
+    s = Solver(int(g["res"]), g["h"], g["dt"], g["min_pos"])
+    v0, f, dt = g["v0"], g["tris"], g["dt"]
+    s.set_mesh(moving_small_verts(v0, 0, dt), f)
+    s.add_listener(20, 20, 20)
+    steps, every = int(g["steps"]), int(g["every"])
+    acc = sine_acc(steps, len(f), 1200.0, dt)
+    for s0 in range(0, steps, every):
+        if s0:
+            s.update_mesh(moving_small_verts(v0, s0, dt))
+        s.step(acc[s0: s0 + every])
+    got = s.listeners()[:, 0]
+    ref = g["series"][:, 0]
+    n3 = s.dump("n3_cells").reshape(-1, 4)
+    assert per_cell_sets(n3, s.dump("n3_tris")) == per_cell_sets(g["n3_cells"], g["n3_tris"])
+    METRICS["moving_small"] = {"rel_l2_200": rel_l2(got, ref), "rel_l2_first50": rel_l2(got[:50], ref[:50])}
+    assert rel_l2(got, ref) < 1e-2
+    s.close()
+
+
+def test_cell_labels_and_fresh_cells_vs_reference(gpu):
+    g = need("cells.npz")
+    res = int(g["res"])
+    s = Solver(res, g["h"], g["dt"], g["min_pos"])
+    s.set_mesh(g["v0"], g["tris"])
+    s.classify_cells()
+    assert np.array_equal(s.dump("cell_type"), g["type0"])
+    assert np.array_equal(s.dump("cell_ghost"), g["ghost0"])
+    s.load("grid_t", g["g_t"])
+    s.load("grid_tm1", g["g_tm1"])
+    s.update_mesh(g["v1"])
+    n = s.fill_fresh_cells(g["acc1"], g["acc0"])
+    assert np.array_equal(s.dump("cell_type"), g["type1"])
+    assert np.array_equal(s.dump("cell_ghost"), g["ghost1"])
+    near_same = float(np.mean(s.dump("cell_nearest") == g["nearest1"]))
+    d_t = float(np.abs(s.grid(0) - g["out_t"]).max())
+    d_tm1 = float(np.abs(s.grid(-1) - g["out_tm1"]).max())
+    METRICS["cells"] = {"fresh_cells": n, "nearest_equal_fraction": near_same, "fresh_max_abs_diff_t": d_t,
+                        "fresh_max_abs_diff_tm1": d_tm1}
+    assert n > 0
+    assert d_t < 1e-5 and d_tm1 < 1e-5
+    s.close()
