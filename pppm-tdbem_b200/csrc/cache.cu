@@ -64,7 +64,10 @@ struct DevConsts
     float c, dt, h;
     f3 mn;
     int res;
+    const double *tw;  // FFT twiddles, 8 x (cos, sin), filled on the device by twiddle_kernel
 };
+
+__global__ void twiddle_kernel(double *tw) { ref32::twiddle_fill(tw); }
 
 __device__ inline void load_tri(const float *verts, const int *tris, int t, f3 *v, int *idx)
 {
@@ -77,11 +80,11 @@ __device__ inline void load_tri(const float *verts, const int *tris, int t, f3 *
 }
 
 // spectrum k <= 8 -> full 16 with conjugates, FFT, scaling (bem.h:306-321)
-__device__ inline void spectrum_to_weights(cf *sp, float lambda, float *w)
+__device__ inline void spectrum_to_weights(cf *sp, float lambda, float *w, const double *tw)
 {
     for (int k = kTaps / 2 + 1; k < kTaps; k++)
         sp[k] = cf{sp[kTaps - k].re, -sp[kTaps - k].im};
-    ref32::scaled_fft(sp, lambda, w);
+    ref32::scaled_fft(sp, lambda, w, tw);
 }
 
 __device__ inline void spectrum_to_weights_d(cd *sp, double lambda, double *w)
@@ -148,12 +151,11 @@ __global__ void gc_compute_kernel(DevConsts dc, const float *verts, const int *t
     for (int k = 0; k <= kTaps / 2; k++)
     {
         cf kk{dc.wave_re[k], dc.wave_im[k]};
-        ss[k] = ref32::face_to_points(v, pts, sc, n, true, kk, false);
-        sd[k] = ref32::face_to_points(v, pts, sc, n, true, kk, true);
+        ref32::face_to_points2(v, pts, sc, n, true, kk, ss[k], sd[k]);
     }
     float ws[kTaps], wd[kTaps];
-    spectrum_to_weights(ss, dc.lambda, ws);
-    spectrum_to_weights(sd, dc.lambda, wd);
+    spectrum_to_weights(ss, dc.lambda, ws, dc.tw);
+    spectrum_to_weights(sd, dc.lambda, wd, dc.tw);
     // move(-1)
     for (int i = kTaps - 1; i >= 1; i--)
     {
@@ -171,11 +173,10 @@ __global__ void gc_compute_kernel(DevConsts dc, const float *verts, const int *t
         for (int k = 0; k <= kTaps / 2; k++)
         {
             cf kk{dc.wave_re[k], dc.wave_im[k]};
-            qs[k] = ref32::face_to_points(v, &p, nullptr, 1, false, kk, false);
-            qd[k] = ref32::face_to_points(v, &p, nullptr, 1, false, kk, true);
+            ref32::face_to_points2(v, &p, nullptr, 1, false, kk, qs[k], qd[k]);
         }
-        spectrum_to_weights(qs, dc.lambda, ps);
-        spectrum_to_weights(qd, dc.lambda, pd);
+        spectrum_to_weights(qs, dc.lambda, ps, dc.tw);
+        spectrum_to_weights(qd, dc.lambda, pd, dc.tw);
         for (int i = 2; i < kTaps; i++)
         {
             ws[i] += ps[i - 2] * -1.0f;
@@ -466,33 +467,37 @@ __device__ inline int centre_of(const int *face_start, int nt, int p)
     return lo;
 }
 
-// Phase A: face-to-face spectra, one thread per (recomputed pair, layer, k <= 8).
+// Phase A: face-to-face spectra, one thread per (recomputed pair, k <= 8) evaluating both
+// layers; spec[18 w + k] single layer, spec[18 w + 9 + k] double layer.
 // mode: 0 = ref32 throughout, 1 = FP64 for panels sharing vertices (stored as float)
 __global__ void fc_spectra_kernel(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
                                   const int *face_nbr, const int *work, int nwork, int mode, cf *spec)
 {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)nwork * 18)
+    if (gid >= (long long)nwork * 9)
         return;
-    int w = (int)(gid / 18), r = (int)(gid % 18);
-    int layer = r / 9, k = r % 9;
+    int w = (int)(gid / 9), k = (int)(gid % 9);
     int p = work[w];
     int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
     f3 sv[3], tv[3];
     int si[3], ti[3];
     load_tri(verts, tris, nbr, sv, si);
     load_tri(verts, tris, ctr, tv, ti);
-    cf out;
+    cf os, od;
     if (mode == 1 && ref32::common_vertices(si, ti) > 0)
     {
         using namespace f64;
         d3 s[3] = {dd(sv[0]), dd(sv[1]), dd(sv[2])}, t[3] = {dd(tv[0]), dd(tv[1]), dd(tv[2])};
-        cd v = face_to_face(s, si, t, ti, cd{dc.wave_re_d[k], dc.wave_im_d[k]}, dc.threshold, layer == 1);
-        out = cf{(float)v.re, (float)v.im};
+        cd kk{dc.wave_re_d[k], dc.wave_im_d[k]};
+        cd vs = face_to_face(s, si, t, ti, kk, dc.threshold, false);
+        cd vd = face_to_face(s, si, t, ti, kk, dc.threshold, true);
+        os = cf{(float)vs.re, (float)vs.im};
+        od = cf{(float)vd.re, (float)vd.im};
     }
     else
-        out = ref32::face_to_face(sv, si, tv, ti, cf{dc.wave_re[k], dc.wave_im[k]}, dc.threshold, layer == 1);
-    spec[(size_t)w * 18 + r] = out;
+        ref32::face_to_face2(sv, si, tv, ti, cf{dc.wave_re[k], dc.wave_im[k]}, dc.threshold, os, od);
+    spec[(size_t)w * 18 + k] = os;
+    spec[(size_t)w * 18 + 9 + k] = od;
 }
 
 __global__ void fc_spectra_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
@@ -552,14 +557,14 @@ __global__ void fc_finish_kernel(DevConsts dc, const float *verts, const int *tr
     {
         cf a = spec[(size_t)w * 18 + k], b = spec[(size_t)w * 18 + 9 + k];
         cf kk{dc.wave_re[k], dc.wave_im[k]};
-        cf ps = ref32::face_to_points(sv, pts, sc, n, true, kk, false);
-        cf pd = ref32::face_to_points(sv, pts, sc, n, true, kk, true);
+        cf ps, pd;
+        ref32::face_to_points2(sv, pts, sc, n, true, kk, ps, pd);
         ss[k] = cf{a.re + ps.re, a.im + ps.im};
         sd[k] = cf{b.re + pd.re, b.im + pd.im};
     }
     float ws[kTaps], wd[kTaps];
-    spectrum_to_weights(ss, dc.lambda, ws);
-    spectrum_to_weights(sd, dc.lambda, wd);
+    spectrum_to_weights(ss, dc.lambda, ws, dc.tw);
+    spectrum_to_weights(sd, dc.lambda, wd, dc.tw);
     int slot = face_pool[p];
     pack_half(ws, wd, pool_w + (size_t)slot * kTaps, pool_scale + slot);
 }
@@ -631,26 +636,41 @@ __global__ void gather_face_kernel(const int *face_pool, long long pf, const Rec
 
 // 0.5 * area - sum_j factor_j with factor_j = double-layer weight 0 of pair j, summed in
 // list order in the working precision (pppm.cu:172-193)
+// One warp per triangle: lanes fetch 32 factors at a time, every lane then adds them in list
+// order, so the sum rounds exactly like a sequential loop.
 __global__ void denom_kernel(const int *face_start, int nt, const float *area, const __half2 *face_w,
                              const float2 *face_scale, const double2 *face_wd, double *denom)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
     if (i >= nt)
         return;
-    if (face_wd)
+    int b = face_start[i], e = face_start[i + 1];
+    float sf = 0;
+    double sd = 0;
+    for (int base = b; base < e; base += 32)
     {
-        double s = 0;
-        for (int p = face_start[i]; p < face_start[i + 1]; p++)
-            s += face_wd[(size_t)p * kTaps].y;
-        denom[i] = 0.5 * (double)area[i] - s;
+        int p = base + lane;
+        float f = 0;
+        double fd = 0;
+        if (p < e)
+        {
+            if (face_wd)
+                fd = face_wd[(size_t)p * kTaps].y;
+            else
+                f = (float)__high2half(face_w[(size_t)p * kTaps]) * face_scale[p].y;
+        }
+        int cnt = min(32, e - base);
+        for (int j = 0; j < cnt; j++)
+        {
+            if (face_wd)
+                sd += __shfl_sync(0xffffffffu, fd, j);
+            else
+                sf += __shfl_sync(0xffffffffu, f, j);
+        }
     }
-    else
-    {
-        float s = 0;
-        for (int p = face_start[i]; p < face_start[i + 1]; p++)
-            s += (float)__high2half(face_w[(size_t)p * kTaps]) * face_scale[p].y;
-        denom[i] = 0.5 * area[i] - s;
-    }
+    if (lane == 0)
+        denom[i] = face_wd ? 0.5 * (double)area[i] - sd : 0.5 * area[i] - sf;
 }
 
 DevConsts make_consts(const Handle &h)
@@ -671,6 +691,7 @@ DevConsts make_consts(const Handle &h)
     dc.h = h.prm.dl;
     dc.mn = f3{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
     dc.res = h.res;
+    dc.tw = h.d_tw;
     return dc;
 }
 
@@ -700,6 +721,11 @@ int cache_refresh(Handle &h)
         if (h.fp64)
             PB_TRY(dalloc(&h.d_face_interp_d, (size_t)nt * 8));
         PB_TRY(dalloc(&h.d_face_denom, (size_t)nt));
+        PB_TRY(dalloc(&h.d_tw, (size_t)16));
+        twiddle_kernel<<<1, 1, 0, s>>>(h.d_tw);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+        dc.tw = h.d_tw;
         h.pool_used = 0;
         h.gc_empty = true;
     }
@@ -823,7 +849,7 @@ int cache_refresh(Handle &h)
             else
             {
                 int mode = h.prm.weights == PPPM_WEIGHTS_FP64 ? 1 : 0;
-                fc_spectra_kernel<<<div_up((long long)nwork * 18, 128), 128, 0, s>>>(
+                fc_spectra_kernel<<<div_up((long long)nwork * 9, 128), 128, 0, s>>>(
                     dc, h.d_verts, h.d_tris, h.d_face_start, nt, h.d_face_nbr, work, nwork, mode, (cf *)h.d_spec);
                 fc_finish_kernel<<<div_up(nwork, 128), 128, 0, s>>>(
                     dc, h.d_verts, h.d_tris, h.d_center, h.d_basec, h.d_face_interp, h.d_face_start, nt,
@@ -843,7 +869,7 @@ int cache_refresh(Handle &h)
         h.launches++;
         PB_CHECK_LAUNCH();
     }
-    denom_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_face_start, nt, h.d_area,
+    denom_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(h.d_face_start, nt, h.d_area,
                                               h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
                                               h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
     h.launches++;
@@ -855,7 +881,7 @@ int cache_free(Handle &h)
 {
     void *ptrs[] = {h.d_gc_w,      h.d_gc_scale,  h.d_gc_snap,   h.d_gc_flag,    h.d_fc_keys,
                     h.d_fc_slot,   h.d_pool_w,    h.d_pool_scale, h.d_pool_meta, h.d_pool_count,
-                    h.d_face_interp, h.d_face_interp_d, h.d_face_denom, h.d_spec};
+                    h.d_face_interp, h.d_face_interp_d, h.d_face_denom, h.d_spec, h.d_tw};
     for (void *p : ptrs)
         dev_free(p);
     h.d_gc_w = nullptr;
@@ -869,6 +895,7 @@ int cache_free(Handle &h)
     h.d_face_interp_d = nullptr;
     h.d_face_denom = nullptr;
     h.d_spec = nullptr;
+    h.d_tw = nullptr;
     h.pool_cap = h.pool_used = 0;
     h.spec_bytes = 0;
     return PPPM_OK;
@@ -946,7 +973,7 @@ int cache_regather(Handle &h)
                 h.d_face_scale);
         h.launches++;
     }
-    denom_kernel<<<div_up(h.nt, T), T, 0, s>>>(h.d_face_start, h.nt, h.d_area,
+    denom_kernel<<<div_up((long long)h.nt * 32, T), T, 0, s>>>(h.d_face_start, h.nt, h.d_area,
                                                 h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
                                                 h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
     h.launches++;

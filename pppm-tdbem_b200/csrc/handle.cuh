@@ -139,6 +139,7 @@ struct Handle
     int *d_status = nullptr;     // device-side status word (capacity / timeout)
     void *d_spec = nullptr;      // recompute scratch spectra
     size_t spec_bytes = 0;
+    double *d_tw = nullptr;      // 8 radix-2 FFT twiddles (cos, sin)
 
     // ---- histories
     void *d_neumann = nullptr, *d_dirichlet = nullptr;

@@ -174,26 +174,60 @@ __device__ inline R interior_cell(const R *cur, const R *prev, int res, int x, i
     return (R)p;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a, R *cur, const R *prev, R *next,
-                                                       const unsigned *corr_mask, R *neumann, R *series)
+// Work split of the stencil launch into three block ranges so no warp mixes the short
+// interior update with the long boundary solve:
+//   [0, nb_in)              interior cells [2, res-3]^3, consecutive threads along z
+//   [nb_in, nb_in + nb_bd)  boundary-layer cells (a coordinate equal to 1 or res-2)
+//   the rest                Neumann ring write, one thread per triangle
+struct StencilSplit
 {
-    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int res = a.res, m = res - 2;
-    if (gid < a.nt && a.acc)
-        neumann[(long long)gid * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[gid];
-    if (gid >= (long long)m * m * m)
+    int nb_in, nb_bd, nb_nt;
+};
+
+inline StencilSplit stencil_split(int res, int nt)
+{
+    long long mi = res - 4, m = res - 2;
+    long long n_in = mi * mi * mi;
+    long long n_bd = 2 * m * m + 2 * (m - 2) * m + 2 * (m - 2) * (m - 2);
+    return StencilSplit{div_up(n_in, 256), div_up(n_bd, 256), div_up(nt, 256)};
+}
+
+// i-th cell of the boundary layer of [1, res-2]^3: the two x faces, then the two y faces
+// without their x edges, then the two z faces without x and y edges
+__device__ inline void boundary_cell(int i, int res, int &x, int &y, int &z)
+{
+    const int m = res - 2, lo = 1, hi = res - 2;
+    int f = 2 * m * m;
+    if (i < f)
+    {
+        x = i < m * m ? lo : hi;
+        int r = i % (m * m);
+        y = lo + r / m;
+        z = lo + r % m;
         return;
-    int x = 1 + (int)(gid / ((long long)m * m));
-    int y = 1 + (int)((gid / m) % m);
-    int z = 1 + (int)(gid % m);
-    long long c = ((long long)x * res + y) * res + z;
-    bool inner = x >= 2 && y >= 2 && z >= 2 && x <= res - 3 && y <= res - 3 && z <= res - 3;
-    R v;
-    if (inner)
-        v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
-    else
-        v = abc_cell<R>(cur, prev, res, x, y, z, (R)a.c, (R)a.dt, (R)a.h);
+    }
+    i -= f;
+    f = 2 * (m - 2) * m;
+    if (i < f)
+    {
+        int half = (m - 2) * m;
+        y = i < half ? lo : hi;
+        int r = i % half;
+        x = lo + 1 + r / m;
+        z = lo + r % m;
+        return;
+    }
+    i -= f;
+    int half = (m - 2) * (m - 2);
+    z = i < half ? lo : hi;
+    int r = i % half;
+    x = lo + 1 + r / (m - 2);
+    y = lo + 1 + r % (m - 2);
+}
+
+template <typename R>
+__device__ inline void finish_cell(const StepArgs &a, long long c, R v, R *next, const unsigned *corr_mask, R *series)
+{
     if ((corr_mask[c >> 5] >> (c & 31)) & 1u)
     {
         R corr = next[c];
@@ -203,6 +237,43 @@ __global__ void __launch_bounds__(256) stencil_kernel(StepArgs a, R *cur, const 
     for (int l = 0; l < a.n_listen; l++)
         if (a.listen_cell[l] == (int)c && !a.listen_corr[l])
             series[a.step_row * a.n_listen + l] = v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a, StencilSplit sp, R *cur, const R *prev, R *next,
+                                                       const unsigned *corr_mask, R *neumann, R *series)
+{
+    const int res = a.res;
+    int b = blockIdx.x;
+    if (b < sp.nb_in)
+    {
+        const int mi = res - 4;
+        int i = b * 256 + threadIdx.x;
+        if (i >= mi * mi * mi)
+            return;
+        int x = 2 + i / (mi * mi), r = i % (mi * mi);
+        int y = 2 + r / mi, z = 2 + r % mi;
+        R v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
+        finish_cell<R>(a, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        return;
+    }
+    b -= sp.nb_in;
+    if (b < sp.nb_bd)
+    {
+        const int m = res - 2;
+        int i = b * 256 + threadIdx.x;
+        if (i >= 2 * m * m + 2 * (m - 2) * m + 2 * (m - 2) * (m - 2))
+            return;
+        int x, y, z;
+        boundary_cell(i, res, x, y, z);
+        R v = abc_cell<R>(cur, prev, res, x, y, z, (R)a.c, (R)a.dt, (R)a.h);
+        finish_cell<R>(a, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        return;
+    }
+    b -= sp.nb_bd;
+    int i = b * 256 + threadIdx.x;
+    if (i < a.nt && a.acc)
+        neumann[(long long)i * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[i];
 }
 
 // split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
@@ -322,14 +393,37 @@ __global__ void __launch_bounds__(256) face_kernel(StepArgs a, const R *next, co
     const int tslot = (a.tnew - k) & (kRing - 1);
     R acc = 0;
     int b = face_start[tri], e = face_start[tri + 1];
-    for (int p = b + half; p < e; p += 2)
+    // each half-warp takes every other pair; kUnroll pairs per iteration have their index,
+    // weight and history loads in flight together
+    constexpr int kUnroll = 4;
+    for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
     {
-        int nbr = face_nbr[p];
-        W w = face_w[(long long)p * kTaps + k];
-        float2 s = face_scale ? face_scale[p] : make_float2(1, 1);
-        R n = neumann[(long long)nbr * kRing + tslot];
-        R d = k == 0 ? (R)0 : dirichlet[(long long)nbr * kRing + tslot];
-        acc += conv_tap(w, s, n, d);
+        int nbr[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+        {
+            int p = p0 + 2 * u;
+            nbr[u] = p < e ? face_nbr[p] : -1;
+        }
+        W w[kUnroll];
+        float2 s[kUnroll];
+        R n[kUnroll], d[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+        {
+            int p = p0 + 2 * u;
+            if (nbr[u] >= 0)
+            {
+                w[u] = face_w[(long long)p * kTaps + k];
+                s[u] = face_scale ? face_scale[p] : make_float2(1, 1);
+                n[u] = neumann[(long long)nbr[u] * kRing + tslot];
+                d[u] = k == 0 ? (R)0 : dirichlet[(long long)nbr[u] * kRing + tslot];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+            if (nbr[u] >= 0)
+                acc += conv_tap(w[u], s[u], n[u], d[u]);
     }
     acc = warp_sum(acc);
     if (lane == 0)
@@ -361,20 +455,44 @@ __global__ void __launch_bounds__(256) near_kernel(StepArgs a, int n3, const int
     const int tslot = (a.tnew - k) & (kRing - 1);
     R acc_b = 0, acc_f = 0;
     int b = n3_start[ci], e = n3_start[ci + 1];
-    for (int p = b + half; p < e; p += 2)
+    constexpr int kUnroll = 4;
+    for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
     {
-        int tri = p3_tri[p];
-        R n = neumann[(long long)tri * kRing + tslot];
-        R d = dirichlet[(long long)tri * kRing + tslot];
-        W wf = k < kTaps - 1 ? w3[(long long)p * 2 * kTaps + k + 1] : WRec<R>::zero();
-        float2 sf = w3_scale ? w3_scale[2 * (long long)p] : make_float2(1, 1);
-        acc_f += conv_tap(wf, sf, n, d);
-        if (!prime)
+        int tri[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
         {
-            W wb = w3[((long long)p * 2 + 1) * kTaps + k];
-            float2 sb = w3_scale ? w3_scale[2 * (long long)p + 1] : make_float2(1, 1);
-            acc_b += conv_tap(wb, sb, n, d);
+            int p = p0 + 2 * u;
+            tri[u] = p < e ? p3_tri[p] : -1;
         }
+        R n[kUnroll], d[kUnroll];
+        W wf[kUnroll], wb[kUnroll];
+        float2 sf[kUnroll], sb[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+        {
+            long long p = p0 + 2 * u;
+            if (tri[u] >= 0)
+            {
+                n[u] = neumann[(long long)tri[u] * kRing + tslot];
+                d[u] = dirichlet[(long long)tri[u] * kRing + tslot];
+                wf[u] = k < kTaps - 1 ? w3[p * 2 * kTaps + k + 1] : WRec<R>::zero();
+                sf[u] = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
+                if (!prime)
+                {
+                    wb[u] = w3[(p * 2 + 1) * kTaps + k];
+                    sb[u] = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+            if (tri[u] >= 0)
+            {
+                acc_f += conv_tap(wf[u], sf[u], n[u], d[u]);
+                if (!prime)
+                    acc_b += conv_tap(wb[u], sb[u], n[u], d[u]);
+            }
     }
     acc_f = warp_sum(acc_f);
     if (!prime)
@@ -453,8 +571,11 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
                                                         (R *)h.pml_slot(h.t + 1), h.d_corr_mask, (R *)h.d_neumann,
                                                         series);
         else
-            stencil_kernel<R><<<div_up(n_st, T), T, 0, s>>>(a, cur, prev, next, h.d_corr_mask, (R *)h.d_neumann,
-                                                            series);
+        {
+            StencilSplit sp = stencil_split(h.res, a.nt);
+            stencil_kernel<R><<<sp.nb_in + sp.nb_bd + sp.nb_nt, T, 0, s>>>(a, sp, cur, prev, next, h.d_corr_mask,
+                                                                          (R *)h.d_neumann, series);
+        }
         h.launches++;
         if (h.timing)
             cudaEventRecord(h.ev[1], s);

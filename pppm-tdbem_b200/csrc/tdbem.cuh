@@ -130,6 +130,41 @@ __device__ inline void double_acc(cf &acc, f3 src, f3 trg, f3 n, cf k, float sca
     }
 }
 
+// Both layers of one source/target pair with one exponential: r^2 of (t - s) and (s - t) are
+// bitwise equal, so e^{ikr} is shared; each layer's own arithmetic is unchanged.
+__device__ inline void both_acc(cf &as, cf &ad, f3 src, f3 trg, f3 n, cf k, float scale, bool scaled)
+{
+    f3 d = src - trg;
+    float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    if (r2 != 0)
+    {
+        float r = sqrtf(r2);
+        cf ikr = ikr_of(r, k);
+        cf e = cexp(ikr.re, ikr.im);
+        double den1 = 4 * PB_PI * r;
+        double qre = e.re / den1, qim = e.im / den1;
+        double den = 4 * PB_PI * r2 * r;
+        double are = -e.re / den, aim = -e.im / den;
+        float bre = 1.0f - ikr.re, bim = -ikr.im;
+        double mre = are * bre - aim * bim;
+        double mim = are * bim + aim * bre;
+        float dn = dot3(d, n);
+        mre = mre * dn;
+        mim = mim * dn;
+        if (scaled)
+        {
+            qre = qre * scale;
+            qim = qim * scale;
+            mre = mre * scale;
+            mim = mim * scale;
+        }
+        as.re = (float)(as.re + qre);
+        as.im = (float)(as.im + qim);
+        ad.re = (float)(ad.re + mre);
+        ad.im = (float)(ad.im + mim);
+    }
+}
+
 __device__ inline cf layer_point(f3 src, f3 trg, f3 n, cf k, bool dbl)
 {
     cf acc{0.0f, 0.0f};
@@ -334,15 +369,193 @@ __device__ inline cf face_to_face(const f3 *src, const int *si, const f3 *trg, c
     return singular_face(src, trg, sj, tj, k, nn, dbl);
 }
 
+// ---- two-layer variants: single and double layer of the same integral in one pass (each
+// layer's arithmetic identical to the one-layer functions above)
+__device__ inline void face_to_points2(const f3 *src_v, const f3 *pts, const float *scales, int n, bool scaled, cf k,
+                                       cf &out_s, cf &out_d)
+{
+    float jac = jacobian(src_v);
+    f3 nrm = tri_normal(src_v);
+    const float gx = (float)PB_TRI_X;
+    f3 q = local_to_global(gx, gx, src_v);
+    cf ls{0.0f, 0.0f}, ld{0.0f, 0.0f};
+    for (int i = 0; i < n; i++)
+        both_acc(ls, ld, q, pts[i], nrm, k, scaled ? scales[i] : 1.0f, scaled);
+    double c = 0.5 * 1.0f * jac;
+    out_s = cf{(float)(0.0f + c * ls.re), (float)(0.0f + c * ls.im)};
+    out_d = cf{(float)(0.0f + c * ld.re), (float)(0.0f + c * ld.im)};
+}
+
+__device__ inline void add_both(cf &rs, cf &rd, f3 a, f3 b, f3 n, cf k, bool scaled, float s)
+{
+    cf ls{0.0f, 0.0f}, ld{0.0f, 0.0f};
+    both_acc(ls, ld, a, b, n, k, 1.0f, false);
+    if (scaled)
+    {
+        rs.re += ls.re * s;
+        rs.im += ls.im * s;
+        rd.re += ld.re * s;
+        rd.im += ld.im * s;
+    }
+    else
+    {
+        rs.re += ls.re;
+        rs.im += ls.im;
+        rd.re += ld.re;
+        rd.im += ld.im;
+    }
+}
+
+__device__ inline void singular_node2(float xsi, float e1, float e2, float e3, float weight, const f3 *tv,
+                                      const f3 *sv, f3 n, int nn, cf k, cf &os, cf &od)
+{
+    cf rs{0.0f, 0.0f}, rd{0.0f, 0.0f};
+    xsi = 0.5 * (xsi + 1);
+    e1 = 0.5 * (e1 + 1);
+    e2 = 0.5 * (e2 + 1);
+    e3 = 0.5 * (e3 + 1);
+    float w = 0;
+    if (nn == 3)
+    {
+        w = xsi * xsi * xsi * e1 * e1 * e2;
+        float e12 = e1 * e2;
+        float e123 = e1 * e2 * e3;
+        add_both(rs, rd, local_to_global2(xsi, xsi * (1.0 - e1 + e12), tv),
+                 local_to_global2(xsi * (1.0 - e123), xsi * (1.0 - e1), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e123), xsi * (1.0 - e1), tv),
+                 local_to_global2(xsi, xsi * (1.0 - e1 + e12), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi, xsi * (e1 - e12 + e123), tv),
+                 local_to_global2(xsi * (1.0 - e12), xsi * (e1 - e12), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e12), xsi * (e1 - e12), tv),
+                 local_to_global2(xsi, xsi * (e1 - e12 + e123), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e123), xsi * (e1 - e123), tv),
+                 local_to_global2(xsi, xsi * (e1 - e12), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi, xsi * (e1 - e12), tv),
+                 local_to_global2(xsi * (1.0 - e123), xsi * (e1 - e123), sv), n, k, false, 0);
+    }
+    else if (nn == 2)
+    {
+        w = xsi * xsi * xsi * e1 * e1;
+        float e12 = e1 * e2;
+        float e123 = e1 * e2 * e3;
+        add_both(rs, rd, local_to_global2(xsi, xsi * e1 * e3, tv),
+                 local_to_global2(xsi * (1.0 - e12), xsi * e1 * (1.0 - e2), sv), n, k, false, 0);
+        add_both(rs, rd, local_to_global2(xsi, xsi * e1, tv),
+                 local_to_global2(xsi * (1.0 - e123), xsi * e1 * e2 * (1 - e3), sv), n, k, true, e2);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e12), xsi * e1 * (1.0 - e2), tv),
+                 local_to_global2(xsi, xsi * e123, sv), n, k, true, e2);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e123), xsi * e12 * (1.0 - e3), tv),
+                 local_to_global2(xsi, xsi * e1, sv), n, k, true, e2);
+        add_both(rs, rd, local_to_global2(xsi * (1.0 - e123), xsi * e1 * (1.0 - e2 * e3), tv),
+                 local_to_global2(xsi, xsi * e12, sv), n, k, true, e2);
+    }
+    else if (nn == 1)
+    {
+        w = xsi * xsi * xsi * e2;
+        add_both(rs, rd, local_to_global2(xsi, xsi * e1, tv), local_to_global2(xsi * e2, xsi * e2 * e3, sv), n, k,
+                 false, 0);
+        add_both(rs, rd, local_to_global2(xsi * e2, xsi * e2 * e3, tv), local_to_global2(xsi, xsi * e1, sv), n, k,
+                 false, 0);
+    }
+    if (nn >= 1 && nn <= 3)
+    {
+        rs.re = rs.re * w;
+        rs.im = rs.im * w;
+        rs.re = rs.re * weight;
+        rs.im = rs.im * weight;
+        rd.re = rd.re * w;
+        rd.im = rd.im * w;
+        rd.re = rd.re * weight;
+        rd.im = rd.im * weight;
+    }
+    os = rs;
+    od = rd;
+}
+
+__device__ inline void face_to_face2(const f3 *src, const int *si, const f3 *trg, const int *ti, cf k, float threshold,
+                                     cf &out_s, cf &out_d)
+{
+    float sj = jacobian(src), tj = jacobian(trg);
+    int nn = common_vertices(si, ti);
+    f3 sc = (src[0] + src[1] + src[2]) / 3;
+    f3 tc = (trg[0] + trg[1] + trg[2]) / 3;
+    float dist = len3(sc - tc);
+    out_s = out_d = cf{0.0f, 0.0f};
+    if (dist < threshold && nn == 0)
+        return;
+    if (nn == 0)
+    {
+        f3 nrm = tri_normal(src);
+        const float gx = (float)PB_TRI_X;
+        f3 a = local_to_global(gx, gx, src);
+        f3 b = local_to_global(gx, gx, trg);
+        double c = 0.25 * 1.0f * 1.0f * sj * tj;
+        cf ls{0.0f, 0.0f}, ld{0.0f, 0.0f};
+        both_acc(ls, ld, a, b, nrm, k, 1.0f, false);
+        out_s = cf{(float)(0.0f + c * ls.re), (float)(0.0f + c * ls.im)};
+        out_d = cf{(float)(0.0f + c * ld.re), (float)(0.0f + c * ld.im)};
+        return;
+    }
+    const float gx[3] = {(float)PB_LINE_X0, 0.0f, (float)-PB_LINE_X0};
+    const float gw[3] = {(float)PB_LINE_W0, (float)PB_LINE_W1, (float)PB_LINE_W0};
+    f3 nrm = tri_normal(src);
+    cf as{0.0f, 0.0f}, ad{0.0f, 0.0f};
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++)
+                for (int d = 0; d < 3; d++)
+                {
+                    cf rs, rd;
+                    singular_node2(gx[a], gx[b], gx[c], gx[d], gw[a] * gw[b] * gw[c] * gw[d], src, trg, nrm, nn, k,
+                                   rs, rd);
+                    as.re += rs.re;
+                    as.im += rs.im;
+                    ad.re += rd.re;
+                    ad.im += rd.im;
+                }
+    out_s = cf{as.re * sj, as.im * sj};
+    out_s = cf{out_s.re * tj, out_s.im * tj};
+    out_s = cf{out_s.re / 16, out_s.im / 16};
+    out_d = cf{ad.re * sj, ad.im * sj};
+    out_d = cf{out_d.re * tj, out_d.im * tj};
+    out_d = cf{out_d.re / 16, out_d.im / 16};
+}
+
 // Recursive radix-2 transform of bem.h:12-38 (positive exponent), stage results rounded to
 // float, twiddles applied in double.  in/out/buf: 16 entries; STEP is the current stride.
+// Twiddle i of the transform, (cos, sin)(2 pi i / 16) with the reference's PI literal, from the
+// device's own cos/sin: either computed here or read from a table filled by twiddle_fill.
+__device__ inline void twiddle(int i, const double *tw, double &wr, double &wi)
+{
+    if (tw)
+    {
+        wr = tw[2 * i];
+        wi = tw[2 * i + 1];
+        return;
+    }
+    double ang = 2 * PB_PI * i / kTaps;
+    wr = cos(ang);
+    wi = sin(ang);
+    if (ang == 0.0)
+    {
+        wr = 1.0;
+        wi = 0.0;
+    }
+}
+
+__device__ inline void twiddle_fill(double *tw)
+{
+    for (int i = 0; i < kTaps / 2; i++)
+        twiddle(i, nullptr, tw[2 * i], tw[2 * i + 1]);
+}
+
 template <int STEP>
-__device__ inline void fft_rec(const cf *in, cf *out, cf *buf)
+__device__ inline void fft_rec(const cf *in, cf *out, cf *buf, const double *tw)
 {
     constexpr int N = kTaps;
     constexpr int NS = STEP * 2;
-    fft_rec<NS>(in, out, buf);
-    fft_rec<NS>(in + STEP, out + STEP, buf + STEP);
+    fft_rec<NS>(in, out, buf, tw);
+    fft_rec<NS>(in + STEP, out + STEP, buf + STEP, tw);
     for (int i = 0; i < N; i += NS)
     {
         buf[i / 2] = out[i];
@@ -350,13 +563,8 @@ __device__ inline void fft_rec(const cf *in, cf *out, cf *buf)
     }
     for (int i = 0; i < N / 2; i += STEP)
     {
-        double ang = 2 * PB_PI * i / N;
-        double wr = cos(ang), wi = sin(ang);
-        if (ang == 0.0)
-        {
-            wr = 1.0;
-            wi = 0.0;
-        }
+        double wr, wi;
+        twiddle(i, tw, wr, wi);
         cf b = buf[i + N / 2];
         double tre = wr * b.re - wi * b.im;
         double tim = wr * b.im + wi * b.re;
@@ -366,16 +574,16 @@ __device__ inline void fft_rec(const cf *in, cf *out, cf *buf)
     }
 }
 template <>
-__device__ inline void fft_rec<kTaps>(const cf *in, cf *out, cf *)
+__device__ inline void fft_rec<kTaps>(const cf *in, cf *out, cf *, const double *)
 {
     out[0] = in[0];
 }
 
 // spectrum (16 values, k > 8 already conjugated) -> 16 real time-domain weights
-__device__ inline void scaled_fft(const cf *spec, float lambda, float *out)
+__device__ inline void scaled_fft(const cf *spec, float lambda, float *out, const double *tw = nullptr)
 {
     cf b1[kTaps], b2[kTaps];
-    fft_rec<1>(spec, b1, b2);
+    fft_rec<1>(spec, b1, b2, tw);
     float temp = 1.0f;
     for (int i = 0; i < kTaps; i++)
     {
