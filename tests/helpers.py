@@ -66,3 +66,17 @@ def golden(name):
     if not os.path.exists(path):
         return None
     return dict(np.load(path, allow_pickle=False))
+
+
+def reference_noise_floor(name, steps=None):
+    """Largest relative L2 difference between the reference's own runs of one scene (the golden
+    series and the repeats in noise.npz, listener 0).  The reference accumulates its correction
+    sums with float atomics, so its repeats differ; the scheme amplifies that rounding step by
+    step, and agreement with it is only meaningful up to this floor."""
+    g, n = golden(name + ".npz"), golden("noise.npz")
+    if g is None or n is None or name not in n:
+        return None
+    runs = [g["series"][:, 0]] + list(n[name])
+    if steps is not None:
+        runs = [r[:steps] for r in runs]
+    return max(rel_l2(runs[i], runs[j]) for i in range(len(runs)) for j in range(i + 1, len(runs)))
