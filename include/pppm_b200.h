@@ -189,6 +189,21 @@ int pppm_tdbem_constants(float dt, float dl, float c, float *lambda, float *wave
  * (to_point != 0) or onto dst_face.  out32: 16 single-layer then 16 double-layer taps. */
 int pppm_pair_weights(int device, float dt, float dl, float c, const float *verts, int nv, const int *src,
                       int to_point, const int *dst_face, const float *dst_point, float *out32);
+/* No counterpart in the reference.  pppm_pair_weights without any device allocation, for
+ * callers that cannot allocate: a thread working beside a handle that is stepping on the same
+ * device (cudaMalloc / cudaFree may synchronise the whole device and stall that handle's stream)
+ * or a process whose device memory is already held by another allocator.  Same arguments and
+ * result as pppm_pair_weights, plus the stream the copies and the kernel run on (NULL: the
+ * default stream); returns after out32 is written.  The vertex rows are staged in a static
+ * device array of PPPM_STATIC_MAX_VERTS rows (768 KiB) inside the library; nv above that limit
+ * returns PPPM_ERR_CAPACITY.  Nothing in that array has to start at zero: each call copies its
+ * rows in and the kernel writes all 32 taps.  The first call on a device does one-time setup
+ * (it looks up the array's device address, which may load the library's device code); make that
+ * call before capturing any stream on the device.  All calls on one device share the array, so
+ * overlapping calls would race: calls from several host threads are serialised by a lock. */
+#define PPPM_STATIC_MAX_VERTS 65536
+int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float c, const float *verts, int nv,
+                             const int *src, int to_point, const int *dst_face, const float *dst_point, float *out32);
 
 /* ------------------------------------------------------------ diagnostics ------------ */
 const char *pppm_status_string(int status);

@@ -1,5 +1,6 @@
 // Weight diagnostics of the C ABI: host TDBEM constants and single-pair weights on the device,
 // used to pin the FP32 weight arithmetic against the reference's own values.
+#include <mutex>
 #include <vector>
 #include "handle.cuh"
 
@@ -79,6 +80,73 @@ int pppm_pair_weights(int device, float dt, float dl, float c, const float *vert
     PB_CUDA(cudaMemcpy(out32, dout, sizeof(float) * 2 * kTaps, cudaMemcpyDeviceToHost));
     dev_free(dv);
     dev_free(dout);
+    return PPPM_OK;
+}
+}
+
+// ---------------------------------------------------------------- no-allocation variant ---
+// pppm_pair_weights_static: the same kernel on scratch that lives in this library's own device
+// image instead of memory from cudaMalloc.  Callers that cannot allocate: a thread that runs
+// beside a stepping handle on the same device (cudaMalloc / cudaFree may synchronise the whole
+// device and stall that handle's stream for the length of its queued steps), and processes whose
+// device memory is fully held by another allocator (a framework's caching pool), where a fresh
+// cudaMalloc fails.  One scratch array per device and per process; calls that overlapped would
+// race on it, so they are serialised by a process-wide lock.
+
+namespace
+{
+constexpr int kStaticMaxVerts = PPPM_STATIC_MAX_VERTS;
+
+// vertex rows (3 floats each) followed by the 32 output taps
+static __device__ __align__(256) float g_pair_scratch[3 * kStaticMaxVerts + 2 * kTaps];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_lock;
+float *g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" {
+
+int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float c, const float *verts, int nv,
+                             const int *src, int to_point, const int *dst_face, const float *dst_point, float *out32)
+{
+    if (!verts || nv <= 0 || !src || !out32 || (to_point ? !dst_point : !dst_face))
+        return PPPM_ERR_ARG;
+    if (nv > kStaticMaxVerts)
+    {
+        pb::set_error("pppm_pair_weights_static: %d vertices exceed the static scratch limit of %d "
+                      "(PPPM_STATIC_MAX_VERTS); pass only the rows the pair uses or call pppm_pair_weights",
+                      nv, kStaticMaxVerts);
+        return PPPM_ERR_CAPACITY;
+    }
+    for (int k = 0; k < 3; k++)
+        if (src[k] < 0 || src[k] >= nv || (!to_point && (dst_face[k] < 0 || dst_face[k] >= nv)))
+            return PPPM_ERR_ARG;
+    if (device < 0 || device >= kMaxDevices)
+        return PPPM_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_static_lock);
+    PB_CUDA(cudaSetDevice(device));
+    if (!g_scratch_ptr[device])
+    {
+        // first call on this device: resolves the symbol (may load the module)
+        float *p = nullptr;
+        PB_CUDA(cudaGetSymbolAddress((void **)&p, g_pair_scratch));
+        g_scratch_ptr[device] = p;
+    }
+    float *dv = g_scratch_ptr[device];
+    float *dout = dv + 3 * kStaticMaxVerts;
+    cudaStream_t s = (cudaStream_t)stream;
+    TdbemConsts tc;
+    tdbem_init(tc, dt, dl, c);
+    // nothing has to start at zero: the rows are copied in and the kernel writes all 32 taps
+    PB_CUDA(cudaMemcpyAsync(dv, verts, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice, s));
+    int3 si = make_int3(src[0], src[1], src[2]);
+    int3 di = to_point ? make_int3(0, 0, 0) : make_int3(dst_face[0], dst_face[1], dst_face[2]);
+    f3 p = to_point ? f3{dst_point[0], dst_point[1], dst_point[2]} : f3{0, 0, 0};
+    pair_weight_kernel<<<1, 1, 0, s>>>(tc, dv, si, to_point, di, p, dout);
+    PB_CHECK_LAUNCH();
+    PB_CUDA(cudaMemcpyAsync(out32, dout, sizeof(float) * 2 * kTaps, cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
     return PPPM_OK;
 }
 }

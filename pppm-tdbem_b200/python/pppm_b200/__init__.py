@@ -89,6 +89,7 @@ def _load():
     fl = ctypes.c_float
     sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
     sig["pppm_pair_weights"] = [i, fl, fl, fl, vp, i, vp, i, vp, vp, vp]
+    sig["pppm_pair_weights_static"] = [i, vp, fl, fl, fl, vp, i, vp, i, vp, vp, vp]
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -144,6 +145,33 @@ def pair_weights(dt, dl, verts, src, point=None, face=None, c=340.3, device=0):
                                    out.ctypes.data_as(ctypes.c_void_p))
     check(rc, "pair_weights")
     return out
+
+
+def pair_weights_static(dt, dl, verts, src, point=None, face=None, c=340.3, device=0, stream=None):
+    """pair_weights without any device allocation: the library stages the vertex rows in its own
+    static device array (at most STATIC_MAX_VERTS rows).  stream: a raw cudaStream_t as an int
+    (None: the default stream)."""
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    s = np.ascontiguousarray(src, np.int32)
+    out = np.zeros(32, np.float32)
+    st = ctypes.c_void_p(stream) if stream else None
+    if point is not None:
+        pt = np.ascontiguousarray(point, np.float32)
+        rc = lib.pppm_pair_weights_static(device, st, float(dt), float(dl), float(c),
+                                          v.ctypes.data_as(ctypes.c_void_p), len(v), s.ctypes.data_as(ctypes.c_void_p),
+                                          1, None, pt.ctypes.data_as(ctypes.c_void_p),
+                                          out.ctypes.data_as(ctypes.c_void_p))
+    else:
+        fc = np.ascontiguousarray(face, np.int32)
+        rc = lib.pppm_pair_weights_static(device, st, float(dt), float(dl), float(c),
+                                          v.ctypes.data_as(ctypes.c_void_p), len(v), s.ctypes.data_as(ctypes.c_void_p),
+                                          0, fc.ctypes.data_as(ctypes.c_void_p), None,
+                                          out.ctypes.data_as(ctypes.c_void_p))
+    check(rc, "pair_weights_static")
+    return out
+
+
+STATIC_MAX_VERTS = 65536  # PPPM_STATIC_MAX_VERTS
 
 
 class Solver:
