@@ -211,8 +211,11 @@ def run_ours(args, ws, rank, local):
     W, K = args.warmup, args.steps
     wl = Workload(args.workload, W + K)
     sc = wl.scene
-    stream = torch.cuda.current_stream()
     dev = torch.device("cuda", local)
+    # one non-default stream for the solver, the L2 flush and every timing event (with the
+    # default stream the solver would create its own, which those events would not see)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     acc_dev = torch.from_numpy(wl.acc).to(dev)
     verts_dev = [torch.from_numpy(v).to(dev) for v in wl.verts]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
