@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--workload", default="moving", choices=["moving", "static"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--summarize-launches", metavar="CSV",
+                   help="print per-kernel launches / total time / share from an ncu "
+                        "gpu__time_duration.sum CSV log of this benchmark, and exit")
     return p.parse_args()
 
 
@@ -430,8 +433,33 @@ def run_reference(args, ws, rank, local):
                     "d2h_bytes_per_step": 0}}
 
 
+def summarize_launches(path):
+    """Per-kernel launch count, total and mean device time and share of an ncu launch list."""
+    import collections
+    import csv
+
+    with open(path) as f:
+        lines = [l for l in f if not l.startswith("==")]
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    scale = {"ns": 1e-3, "nsecond": 1e-3, "us": 1.0, "usecond": 1.0, "ms": 1e3, "msecond": 1e3}
+    for row in csv.DictReader(lines):
+        if row.get("Metric Name") != "gpu__time_duration.sum":
+            continue
+        name = row["Kernel Name"].split("(")[0].replace("pb::<unnamed>::", "").replace("void ", "")
+        agg[name][0] += 1
+        agg[name][1] += float(row["Metric Value"].replace(",", "")) * scale.get(row["Metric Unit"], 1.0)
+    total = sum(v[1] for v in agg.values())
+    print("| kernel | launches | total us | mean us | share |")
+    print("|---|---|---|---|---|")
+    for name, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+        print("| %s | %d | %.1f | %.2f | %.1f%% |" % (name, n, t, t / n, 100 * t / total))
+
+
 def main():
     args = parse()
+    if args.summarize_launches:
+        summarize_launches(args.summarize_launches)
+        return
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         line = run_reference(args, ws, rank, local)

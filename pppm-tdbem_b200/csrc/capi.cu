@@ -332,6 +332,7 @@ int pppm_destroy(pppm_handle *ph)
     Handle &h = ph->h;
     if (h.stream)
         cudaStreamSynchronize(h.stream);
+    step_free(h);
     free_mesh(h);
     void *ptrs[] = {h.grid[0],        h.grid[1],         h.grid[2],        h.pml[0],          h.pml[1],
                     h.pml[2],         h.d_verts,         h.d_tris,         h.d_center,        h.d_normal,

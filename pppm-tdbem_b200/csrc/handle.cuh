@@ -27,40 +27,26 @@
 namespace pb
 {
 
-// Device view of one scene used by the step kernels (POD, passed by value).
-template <typename Real>
-struct SceneView
+// The per-call values of a pppm_step call live in device memory (one StepState per handle,
+// written before the launches), so the kernels of a call can be recorded once as a CUDA graph
+// and replayed for every later call with the same number of steps: kernel k of a call derives
+// its time index, series row and acceleration row from the state and its own k (step.cu).
+struct StepState
 {
-    int res;
-    int n_cells;
-    Real *g0, *g1, *g2;  // grid slots for (t+1), t, t-1 after mapping by the launcher
-    const unsigned *corr_mask;
-    // 3^3 pairs
-    int n3;
-    const int *n3_cell;
-    const int *n3_start;
-    const int *p3_tri;
-    const void *w3;        // FP32: __half2[p3][2][16]; FP64: double[p3][2][32]
-    const float2 *w3_scale;  // FP32 only: [p3][2] (single scale, double scale)
-    // faces
-    int nt;
-    const int *face_start;
-    const int *face_nbr;
-    const void *face_w;        // FP32: __half2[pf][16]; FP64: double[pf][32]
-    const float2 *face_scale;  // FP32 only
-    const int *face_corner;    // nt x 8 linear cells
-    const float *face_interp;  // nt x 8 (FP32) ; FP64 uses face_interp_d
-    const double *face_interp_d;
-    const double *face_denom;  // nt
-    Real *neumann;             // nt x 32
-    Real *dirichlet;           // nt x 32
-    float reflect;
-    // listeners
-    int n_listen;
-    const int *listen_cell;  // linear cell
-    const int *listen_n3;    // compact index in the corrected-cell list or -1
-    Real *series;            // [step][listener]
+    int tnew0;         // time index produced by the call's first step
+    int n3;            // corrected cells
+    long long row0;    // listener-series row of the first step
+    const float *acc;  // nsteps rows of nt accelerations, or null
 };
+
+// a recorded pppm_step call
+struct StepGraph
+{
+    int nsteps = 0;
+    std::vector<unsigned char> sig;  // the launch set it was recorded with
+    cudaGraphExec_t exec = nullptr;
+};
+constexpr int kStepGraphs = 4;
 
 struct Handle
 {
@@ -164,6 +150,12 @@ struct Handle
     float us_stencil = 0, us_face = 0, us_near = 0;  // summed over timed_steps
     long long timed_steps = 0;
 
+    // ---- step launches
+    StepState *d_state = nullptr;  // per-call values the step kernels read
+    StepGraph graphs[kStepGraphs];
+    int graph_next = 0;
+    int near_blocks = 0;  // resident grid of the near kernel
+
     // ---- scratch for accelerations
     float *d_acc = nullptr;
     long long acc_cap = 0;
@@ -211,6 +203,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 // step.cu
 int step_prime(Handle &h);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
+int step_free(Handle &h);  // recorded graphs and the step state
 
 // cells.cu
 int cells_classify(Handle &h, int *ghost_count);

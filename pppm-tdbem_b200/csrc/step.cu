@@ -45,6 +45,23 @@ struct StepArgs
     int listen_corr[8];  // 1 if the listener cell is a corrected cell
 };
 
+__device__ inline void bind_step(StepArgs &a, const StepState *st, int k)
+{
+    a.tnew = st->tnew0 + k;
+    a.step_row = st->row0 + k;
+    a.acc = st->acc ? st->acc + (long long)k * a.nt : nullptr;
+}
+
+// the three grid time levels (and PML fields), by time index
+template <typename R>
+struct Ring
+{
+    R *g[3];
+    R *p[3];
+    __device__ R *slot(int time) const { return g[((time % 3) + 3) % 3]; }
+    __device__ R *pml(int time) const { return p[((time % 3) + 3) % 3]; }
+};
+
 template <typename Real>
 __device__ inline Real ld(const Real *g, int res, int x, int y, int z)
 {
@@ -240,9 +257,14 @@ __device__ inline void finish_cell(const StepArgs &a, long long c, R v, R *next,
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a, StencilSplit sp, R *cur, const R *prev, R *next,
-                                                       const unsigned *corr_mask, R *neumann, R *series)
+__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int k,
+                                                       StencilSplit sp, const unsigned *corr_mask, R *neumann,
+                                                       R *series)
 {
+    StepArgs a = a0;
+    bind_step(a, st, k);
+    R *cur = ring.slot(a.tnew - 1), *next = ring.slot(a.tnew);
+    const R *prev = ring.slot(a.tnew - 2);
     const int res = a.res;
     int b = blockIdx.x;
     if (b < sp.nb_in)
@@ -284,9 +306,15 @@ __device__ inline R pml_damp(int x, int y, int z, int res, int w, R damp)
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) pml_kernel(StepArgs a, const R *cur, const R *prev, R *next, const R *pcur,
-                                                   R *pnext, const unsigned *corr_mask, R *neumann, R *series)
+__global__ void __launch_bounds__(256) pml_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int k,
+                                                   const unsigned *corr_mask, R *neumann, R *series)
 {
+    StepArgs a = a0;
+    bind_step(a, st, k);
+    const R *cur = ring.slot(a.tnew - 1), *prev = ring.slot(a.tnew - 2);
+    R *next = ring.slot(a.tnew);
+    const R *pcur = ring.pml(a.tnew - 1);
+    R *pnext = ring.pml(a.tnew);
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int res = a.res, m = res - 2, w = a.pml_width;
     if (gid < a.nt && a.acc)
@@ -378,13 +406,17 @@ __device__ inline R warp_sum(R v)
 
 // face stage: one warp per centre triangle
 template <typename R>
-__global__ void __launch_bounds__(256) face_kernel(StepArgs a, const R *next, const int *face_start,
+__global__ void __launch_bounds__(256) face_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int kstep,
+                                                    const int *face_start,
                                                     const int *face_nbr, const typename WRec<R>::T *face_w,
                                                     const float2 *face_scale, const int *face_corner,
                                                     const float *interp, const double *interp_d,
                                                     const double *denom, const R *neumann, R *dirichlet, float reflect)
 {
     using W = typename WRec<R>::T;
+    StepArgs a = a0;
+    bind_step(a, st, kstep);
+    const R *next = ring.slot(a.tnew);
     int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     int lane = threadIdx.x & 31;
     if (tri >= a.nt)
@@ -441,73 +473,79 @@ __global__ void __launch_bounds__(256) face_kernel(StepArgs a, const R *next, co
 
 // near stage: one warp per corrected cell.  prime != 0: only the next step's FDTD-near sum.
 template <typename R>
-__global__ void __launch_bounds__(256) near_kernel(StepArgs a, int n3, const int *n3_cell, const int *n3_start,
-                                                    const int *p3_tri, const typename WRec<R>::T *w3,
-                                                    const float2 *w3_scale, const R *neumann, const R *dirichlet,
-                                                    R *cur, R *nextslot, R *series, int prime)
+__global__ void __launch_bounds__(256) near_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int kstep,
+                                                    const int *n3_cell, const int *n3_start, const int *p3_tri,
+                                                    const typename WRec<R>::T *w3, const float2 *w3_scale,
+                                                    const R *neumann, const R *dirichlet, R *series, int prime)
 {
     using W = typename WRec<R>::T;
-    int ci = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    int lane = threadIdx.x & 31;
-    if (ci >= n3)
-        return;
+    StepArgs a = a0;
+    bind_step(a, st, kstep);
+    R *cur = ring.slot(a.tnew), *nextslot = ring.slot(a.tnew + 1);
+    const int n3 = st->n3;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)(((long long)gridDim.x * blockDim.x) >> 5);
     const int k = lane & 15, half = lane >> 4;
     const int tslot = (a.tnew - k) & (kRing - 1);
-    R acc_b = 0, acc_f = 0;
-    int b = n3_start[ci], e = n3_start[ci + 1];
-    constexpr int kUnroll = 4;
-    for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
+    // a fixed grid of warps strides over the corrected cells (their number changes with the mesh)
+    for (int ci = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < n3; ci += nwarps)
     {
-        int tri[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++)
+        R acc_b = 0, acc_f = 0;
+        int b = n3_start[ci], e = n3_start[ci + 1];
+        constexpr int kUnroll = 4;
+        for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
         {
-            int p = p0 + 2 * u;
-            tri[u] = p < e ? p3_tri[p] : -1;
-        }
-        R n[kUnroll], d[kUnroll];
-        W wf[kUnroll], wb[kUnroll];
-        float2 sf[kUnroll], sb[kUnroll];
+            int tri[kUnroll];
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++)
-        {
-            long long p = p0 + 2 * u;
-            if (tri[u] >= 0)
+            for (int u = 0; u < kUnroll; u++)
             {
-                n[u] = neumann[(long long)tri[u] * kRing + tslot];
-                d[u] = dirichlet[(long long)tri[u] * kRing + tslot];
-                wf[u] = k < kTaps - 1 ? w3[p * 2 * kTaps + k + 1] : WRec<R>::zero();
-                sf[u] = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
-                if (!prime)
+                int p = p0 + 2 * u;
+                tri[u] = p < e ? p3_tri[p] : -1;
+            }
+            R n[kUnroll], d[kUnroll];
+            W wf[kUnroll], wb[kUnroll];
+            float2 sf[kUnroll], sb[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++)
+            {
+                long long p = p0 + 2 * u;
+                if (tri[u] >= 0)
                 {
-                    wb[u] = w3[(p * 2 + 1) * kTaps + k];
-                    sb[u] = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
+                    n[u] = neumann[(long long)tri[u] * kRing + tslot];
+                    d[u] = dirichlet[(long long)tri[u] * kRing + tslot];
+                    wf[u] = k < kTaps - 1 ? w3[p * 2 * kTaps + k + 1] : WRec<R>::zero();
+                    sf[u] = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
+                    if (!prime)
+                    {
+                        wb[u] = w3[(p * 2 + 1) * kTaps + k];
+                        sb[u] = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++)
-            if (tri[u] >= 0)
-            {
-                acc_f += conv_tap(wf[u], sf[u], n[u], d[u]);
-                if (!prime)
-                    acc_b += conv_tap(wb[u], sb[u], n[u], d[u]);
-            }
-    }
-    acc_f = warp_sum(acc_f);
-    if (!prime)
-        acc_b = warp_sum(acc_b);
-    if (lane == 0)
-    {
-        int c = n3_cell[ci];
-        nextslot[c] = acc_f;
+            for (int u = 0; u < kUnroll; u++)
+                if (tri[u] >= 0)
+                {
+                    acc_f += conv_tap(wf[u], sf[u], n[u], d[u]);
+                    if (!prime)
+                        acc_b += conv_tap(wb[u], sb[u], n[u], d[u]);
+                }
+        }
+        acc_f = warp_sum(acc_f);
         if (!prime)
+            acc_b = warp_sum(acc_b);
+        if (lane == 0)
         {
-            R v = (R)((double)cur[c] + (double)acc_b * 0.98);
-            cur[c] = v;
-            for (int l = 0; l < a.n_listen; l++)
-                if (a.listen_cell[l] == c)
-                    series[a.step_row * a.n_listen + l] = v;
+            int c = n3_cell[ci];
+            nextslot[c] = acc_f;
+            if (!prime)
+            {
+                R v = (R)((double)cur[c] + (double)acc_b * 0.98);
+                cur[c] = v;
+                for (int l = 0; l < a.n_listen; l++)
+                    if (a.listen_cell[l] == c)
+                        series[a.step_row * a.n_listen + l] = v;
+            }
         }
     }
 }
@@ -547,94 +585,219 @@ int fill_listeners(Handle &h, StepArgs &a)
     return PPPM_OK;
 }
 
+// Every argument the kernels of one step receive apart from the step index k.  Two calls with
+// equal launch sets (same arrays, counts and listeners) record identical graphs.
+template <typename R>
+struct StepLaunch
+{
+    using W = typename WRec<R>::T;
+    StepArgs a;  // the per-step fields stay zero: kernels bind them from the StepState
+    Ring<R> ring;
+    StencilSplit sp;
+    const StepState *st;
+    const unsigned *corr_mask;
+    R *neumann, *dirichlet, *series;
+    const int *face_start, *face_nbr, *face_corner, *n3_cell, *n3_start, *p3_tri;
+    const W *face_w, *w3;
+    const float2 *face_scale, *w3_scale;
+    const float *interp;
+    const double *interp_d, *denom;
+    float reflect;
+    int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
+};
+
+__global__ void set_state_kernel(StepState *dst, StepState v) { *dst = v; }
+
+template <typename R>
+int make_launch(Handle &h, StepLaunch<R> &L)
+{
+    using W = typename WRec<R>::T;
+    memset(&L, 0, sizeof(L));  // padding too: the launch set is compared byte by byte
+    L.a = make_args<R>(h);
+    PB_TRY(fill_listeners<R>(h, L.a));
+    for (int i = 0; i < 3; i++)
+    {
+        L.ring.g[i] = (R *)h.grid[i];
+        L.ring.p[i] = (R *)h.pml[i];
+    }
+    L.sp = stencil_split(h.res, L.a.nt);
+    L.st = h.d_state;
+    L.corr_mask = h.d_corr_mask;
+    L.neumann = (R *)h.d_neumann;
+    L.dirichlet = (R *)h.d_dirichlet;
+    L.series = (R *)h.d_series;
+    L.mesh = h.mesh_set ? 1 : 0;
+    L.pml = h.prm.pml_width > 0 ? 1 : 0;
+    const int m = h.res - 2, T = 256;
+    L.pml_blocks = (int)div_up(std::max<long long>((long long)m * m * m, L.a.nt), T);
+    L.stencil_blocks = L.sp.nb_in + L.sp.nb_bd + L.sp.nb_nt;
+    if (h.mesh_set)
+    {
+        L.face_start = h.d_face_start;
+        L.face_nbr = h.d_face_nbr;
+        L.face_corner = h.d_face_corner;
+        L.face_w = (const W *)h.d_face_w;
+        L.face_scale = h.fp64 ? nullptr : h.d_face_scale;
+        L.interp = h.d_face_interp;
+        L.interp_d = h.fp64 ? h.d_face_interp_d : nullptr;
+        L.denom = h.d_face_denom;
+        L.reflect = h.prm.reflect_coeff;
+        L.n3_cell = h.d_n3_cell;
+        L.n3_start = h.d_n3_start;
+        L.p3_tri = h.d_p3_tri;
+        L.w3 = (const W *)h.d_w3;
+        L.w3_scale = h.fp64 ? nullptr : h.d_w3_scale;
+        L.face_blocks = (int)div_up((long long)h.nt * 32, T);
+        if (h.near_blocks <= 0)
+        {
+            // as many warps as stay resident: they stride over the corrected cells
+            int per_sm = 0, sms = 0;
+            PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, near_kernel<R>, T, 0));
+            PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h.prm.device));
+            h.near_blocks = std::max(per_sm, 1) * std::max(sms, 1);
+        }
+        L.near_blocks = h.near_blocks;
+    }
+    return PPPM_OK;
+}
+
+// the kernels of step k of a call (no error check: may run under stream capture)
+template <typename R>
+void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
+{
+    const int T = 256;
+    if (timed)
+        cudaEventRecord(timed->ev[0], s);
+    if (L.pml)
+        pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask, L.neumann, L.series);
+    else
+        stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.neumann,
+                                                         L.series);
+    if (timed)
+        cudaEventRecord(timed->ev[1], s);
+    if (L.mesh)
+    {
+        face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.face_start, L.face_nbr, L.face_w,
+                                                   L.face_scale, L.face_corner, L.interp, L.interp_d, L.denom,
+                                                   L.neumann, L.dirichlet, L.reflect);
+        if (timed)
+            cudaEventRecord(timed->ev[2], s);
+        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
+                                                   L.w3_scale, L.neumann, L.dirichlet, L.series, 0);
+    }
+    if (timed)
+        cudaEventRecord(timed->ev[3], s);
+}
+
+// Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
+// first call with that step count and launch set (the graph removes the host launch cost and
+// most of the gap between dependent kernels); shorter calls, measurement mode and calls on a
+// stream that the caller is capturing launch the kernels directly.
+constexpr int kGraphSteps = 4;
+
+template <typename R>
+int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *out)
+{
+    const unsigned char *sig = (const unsigned char *)&L;
+    for (auto &g : h.graphs)
+        if (g.exec && g.nsteps == nsteps && g.sig.size() == sizeof(L) && memcmp(g.sig.data(), sig, sizeof(L)) == 0)
+        {
+            *out = g.exec;
+            return PPPM_OK;
+        }
+    StepGraph &g = h.graphs[h.graph_next];
+    h.graph_next = (h.graph_next + 1) % kStepGraphs;
+    if (g.exec)
+        cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    PB_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < nsteps; k++)
+        launch_step<R>(L, k, h.stream, nullptr);
+    cudaError_t e = cudaStreamEndCapture(h.stream, &graph);
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+    {
+        g.exec = nullptr;
+        set_error("recording the step graph failed: %s", cudaGetErrorString(e));
+        return PPPM_ERR_CUDA;
+    }
+    g.nsteps = nsteps;
+    g.sig.assign(sig, sig + sizeof(L));
+    *out = g.exec;
+    return PPPM_OK;
+}
+
 template <typename R>
 int run_steps(Handle &h, const float *acc_dev, int nsteps)
 {
-    using W = typename WRec<R>::T;
+    if (nsteps <= 0)
+        return PPPM_OK;
     cudaStream_t s = h.stream;
-    StepArgs a = make_args<R>(h);
-    PB_TRY(fill_listeners<R>(h, a));
-    const int m = h.res - 2;
-    long long n_st = std::max<long long>((long long)m * m * m, a.nt);
-    const int T = 256;
-    for (int st = 0; st < nsteps; st++)
+    if (!h.d_state)
+        PB_TRY(dalloc(&h.d_state, 1));
+    StepState stt{h.t + 1, h.mesh_set ? h.n3 : 0, h.series_count, acc_dev};
+    set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    StepLaunch<R> L;
+    PB_TRY(make_launch<R>(h, L));
+    const long long per_step = 1 + (h.mesh_set ? 2 : 0);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PB_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (!h.timing && cs == cudaStreamCaptureStatusNone && nsteps >= kGraphSteps)
     {
-        a.tnew = h.t + 1;
-        a.step_row = h.series_count;
-        a.acc = acc_dev ? acc_dev + (size_t)st * h.nt : nullptr;
-        R *cur = (R *)h.slot(h.t), *prev = (R *)h.slot(h.t - 1), *next = (R *)h.slot(h.t + 1);
-        R *series = (R *)h.d_series;
-        if (h.timing)
-            cudaEventRecord(h.ev[0], s);
-        if (h.prm.pml_width > 0)
-            pml_kernel<R><<<div_up(n_st, T), T, 0, s>>>(a, cur, prev, next, (const R *)h.pml_slot(h.t),
-                                                        (R *)h.pml_slot(h.t + 1), h.d_corr_mask, (R *)h.d_neumann,
-                                                        series);
-        else
-        {
-            StencilSplit sp = stencil_split(h.res, a.nt);
-            stencil_kernel<R><<<sp.nb_in + sp.nb_bd + sp.nb_nt, T, 0, s>>>(a, sp, cur, prev, next, h.d_corr_mask,
-                                                                          (R *)h.d_neumann, series);
-        }
-        h.launches++;
-        if (h.timing)
-            cudaEventRecord(h.ev[1], s);
-        if (h.mesh_set)
-        {
-            face_kernel<R><<<div_up((long long)h.nt * 32, T), T, 0, s>>>(
-                a, next, h.d_face_start, h.d_face_nbr, (const W *)h.d_face_w, h.fp64 ? nullptr : h.d_face_scale,
-                h.d_face_corner, h.d_face_interp, h.fp64 ? h.d_face_interp_d : nullptr, h.d_face_denom,
-                (const R *)h.d_neumann, (R *)h.d_dirichlet, h.prm.reflect_coeff);
-            h.launches++;
-            if (h.timing)
-                cudaEventRecord(h.ev[2], s);
-            if (h.n3 > 0)
-            {
-                near_kernel<R><<<div_up((long long)h.n3 * 32, T), T, 0, s>>>(
-                    a, h.n3, h.d_n3_cell, h.d_n3_start, h.d_p3_tri, (const W *)h.d_w3,
-                    h.fp64 ? nullptr : h.d_w3_scale, (const R *)h.d_neumann, (const R *)h.d_dirichlet, next,
-                    (R *)h.slot(h.t + 2), series, 0);
-                h.launches++;
-            }
-        }
-        if (h.timing)
-            cudaEventRecord(h.ev[3], s);
-        PB_CHECK_LAUNCH();
-        h.t++;
-        h.series_count++;
-        if (h.timing)
-        {
-            // per-kernel durations, accumulated over timed steps (measurement mode only)
-            PB_CUDA(cudaEventSynchronize(h.ev[3]));
-            float a = 0, b = 0, c = 0;
-            cudaEventElapsedTime(&a, h.ev[0], h.ev[1]);
-            if (h.mesh_set)
-            {
-                cudaEventElapsedTime(&b, h.ev[1], h.ev[2]);
-                cudaEventElapsedTime(&c, h.ev[2], h.ev[3]);
-            }
-            h.us_stencil += 1000 * a;
-            h.us_face += 1000 * b;
-            h.us_near += 1000 * c;
-            h.timed_steps++;
-        }
+        cudaGraphExec_t exec = nullptr;
+        PB_TRY(graph_for<R>(h, L, nsteps, &exec));
+        PB_CUDA(cudaGraphLaunch(exec, s));
     }
+    else
+        for (int k = 0; k < nsteps; k++)
+        {
+            launch_step<R>(L, k, s, h.timing ? &h : nullptr);
+            PB_CHECK_LAUNCH();
+            if (h.timing)
+            {
+                // per-kernel durations, accumulated over timed steps (measurement mode only)
+                PB_CUDA(cudaEventSynchronize(h.ev[3]));
+                float ta = 0, tb = 0, tc = 0;
+                cudaEventElapsedTime(&ta, h.ev[0], h.ev[1]);
+                if (h.mesh_set)
+                {
+                    cudaEventElapsedTime(&tb, h.ev[1], h.ev[2]);
+                    cudaEventElapsedTime(&tc, h.ev[2], h.ev[3]);
+                }
+                h.us_stencil += 1000 * ta;
+                h.us_face += 1000 * tb;
+                h.us_near += 1000 * tc;
+                h.timed_steps++;
+            }
+        }
+    h.launches += per_step * nsteps;
+    h.t += nsteps;
+    h.series_count += nsteps;
     return PPPM_OK;
 }
 
 template <typename R>
 int prime(Handle &h)
 {
-    using W = typename WRec<R>::T;
     if (!h.mesh_set || h.n3 == 0)
         return PPPM_OK;
-    StepArgs a = make_args<R>(h);
-    a.tnew = h.t;  // taps t-k of the current time
-    a.n_listen = 0;
-    near_kernel<R><<<div_up((long long)h.n3 * 32, 256), 256, 0, h.stream>>>(
-        a, h.n3, h.d_n3_cell, h.d_n3_start, h.d_p3_tri, (const W *)h.d_w3, h.fp64 ? nullptr : h.d_w3_scale,
-        (const R *)h.d_neumann, (const R *)h.d_dirichlet, (R *)h.slot(h.t), (R *)h.slot(h.t + 1), nullptr, 1);
-    h.launches++;
+    if (!h.d_state)
+        PB_TRY(dalloc(&h.d_state, 1));
+    // taps t-k of the current time: the FDTD-near sum of step t + 1 into its slot
+    StepState stt{h.t, h.n3, 0, nullptr};
+    set_state_kernel<<<1, 1, 0, h.stream>>>(h.d_state, stt);
+    StepLaunch<R> L;
+    PB_TRY(make_launch<R>(h, L));
+    L.a.n_listen = 0;
+    near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
+                                                        L.w3_scale, L.neumann, L.dirichlet, nullptr, 1);
+    h.launches += 2;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
 }
@@ -646,6 +809,20 @@ int step_prime(Handle &h) { return h.fp64 ? prime<double>(h) : prime<float>(h); 
 int step_run(Handle &h, const float *acc_dev, int nsteps)
 {
     return h.fp64 ? run_steps<double>(h, acc_dev, nsteps) : run_steps<float>(h, acc_dev, nsteps);
+}
+
+int step_free(Handle &h)
+{
+    for (auto &g : h.graphs)
+    {
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.sig.clear();
+    }
+    dev_free(h.d_state);
+    h.d_state = nullptr;
+    return PPPM_OK;
 }
 
 }  // namespace pb
