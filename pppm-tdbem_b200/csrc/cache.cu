@@ -312,7 +312,11 @@ __global__ void gather_w3_kernel(const int *p3_tri, const unsigned char *p3_woff
     long long pair = p / kTaps;
     int k = (int)(p % kTaps);
     size_t rec = (size_t)p3_tri[pair] * 54 + p3_woff[pair];
-    w3[(pair * 2) * kTaps + k] = gc_w[rec * kTaps + k];
+    // FDTD-near row shifted by one tap: the step pairs record tap k + 1 with history tap k (that
+    // sum belongs to the next step), so both rows of a pair read the same history window
+    Rec zero;
+    memset(&zero, 0, sizeof(zero));
+    w3[(pair * 2) * kTaps + k] = k < kTaps - 1 ? gc_w[rec * kTaps + k + 1] : zero;
     w3[(pair * 2 + 1) * kTaps + k] = gc_w[(rec + 27) * kTaps + k];
     if (k == 0 && gc_scale)
     {

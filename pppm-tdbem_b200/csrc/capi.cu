@@ -157,7 +157,8 @@ void free_mesh(Handle &h)
                      (void **)&h.d_b4_start,   (void **)&h.d_n4_tris,     (void **)&h.d_face_start,
                      (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
-                     (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet};
+                     (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
+                     (void **)&h.d_hist};
     for (void **q : ptrs)
     {
         dev_free(*q);
@@ -391,6 +392,8 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_TRY(dev_alloc(&h.d_dirichlet, (size_t)nt * kRing * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_neumann, 0, (size_t)nt * kRing * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)nt * kRing * h.real_size, h.stream));
+    PB_TRY(dev_alloc(&h.d_hist, (size_t)8 * nt * kRing * h.real_size));
+    PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
     if (rc == PPPM_OK)
         rc = cache_refresh(h);
@@ -582,6 +585,7 @@ int pppm_reset_fields(pppm_handle *ph)
     {
         PB_CUDA(cudaMemsetAsync(h.d_neumann, 0, (size_t)h.nt * kRing * h.real_size, h.stream));
         PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)h.nt * kRing * h.real_size, h.stream));
+        PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * h.nt * kRing * h.real_size, h.stream));
     }
     PB_TRY(step_prime(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
@@ -628,6 +632,7 @@ int pppm_save_state(pppm_handle *ph, void *dst, size_t bytes)
     if (h.mesh_set)
     {
         size_t hb = (size_t)h.nt * kRing * h.real_size;
+        PB_TRY(hist_export(h));
         PB_CUDA(cudaMemcpyAsync(p, h.d_neumann, hb, cudaMemcpyDeviceToHost, h.stream));
         p += hb;
         PB_CUDA(cudaMemcpyAsync(p, h.d_dirichlet, hb, cudaMemcpyDeviceToHost, h.stream));
@@ -664,6 +669,7 @@ int pppm_restore_state(pppm_handle *ph, const void *src, size_t bytes)
         PB_CUDA(cudaMemcpyAsync(h.d_neumann, p, hb, cudaMemcpyHostToDevice, h.stream));
         p += hb;
         PB_CUDA(cudaMemcpyAsync(h.d_dirichlet, p, hb, cudaMemcpyHostToDevice, h.stream));
+        PB_TRY(hist_import(h));
     }
     PB_TRY(step_prime(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
@@ -734,8 +740,8 @@ int pppm_dump(pppm_handle *ph, int what, void *dst, size_t bytes)
     case PPPM_DUMP_GRID_T: return copy(h.slot(h.t), need);
     case PPPM_DUMP_GRID_TM1: return copy(h.slot(h.t - 1), need);
     case PPPM_DUMP_GRID_TM2: return copy(h.slot(h.t - 2), need);
-    case PPPM_DUMP_NEUMANN: return copy(h.d_neumann, need);
-    case PPPM_DUMP_DIRICHLET: return copy(h.d_dirichlet, need);
+    case PPPM_DUMP_NEUMANN: PB_TRY(hist_export(h)); return copy(h.d_neumann, need);
+    case PPPM_DUMP_DIRICHLET: PB_TRY(hist_export(h)); return copy(h.d_dirichlet, need);
     case PPPM_DUMP_TRI_GEOM:
     {
         std::vector<float> c, nn, a;
@@ -912,7 +918,12 @@ int pppm_load(pppm_handle *ph, int what, const void *src, size_t bytes)
     }
     if (bytes < need)
         return PPPM_ERR_ARG;
+    const bool ring = what == PPPM_DUMP_NEUMANN || what == PPPM_DUMP_DIRICHLET;
+    if (ring)
+        PB_TRY(hist_export(h));  // the other ring keeps its current values
     PB_CUDA(cudaMemcpyAsync(dst, src, need, cudaMemcpyHostToDevice, h.stream));
+    if (ring)
+        PB_TRY(hist_import(h));
     PB_TRY(step_prime(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
     return PPPM_OK;

@@ -7,12 +7,15 @@
 //                  t+1 the dead slot t+1 carries, at corrected cells only, the FDTD-near
 //                  correction of step t+1 (see step.cu).
 //   pml[3]         res^3 x 6 real (PML only)
-//   neumann/dirichlet  nt x 32 real rings
+//   neumann/dirichlet  nt x 32 real rings in the reference layout (slot = t mod 32), for
+//                  read-out and loading; the step works on hist, four shifted copies of each
+//                  ring (copy c holds time tau at (c - tau) mod 32) so 4 taps are one aligned load
 //   cell CSR       cell_start[res^3 + 1] / cell_tris[nt] (sorted by triangle id per cell),
 //                  same for base cells
 //   3^3 pairs      n3 corrected cells: n3_cell, n3_start[n3 + 1]; p3 pairs: p3_tri,
 //                  p3_woff; dense weights w3_half[p3][2][32] + w3_scale[p3][2][2]
-//                  (FDTD-near then BEM-near, fp16 + per-row scale, the reference's format)
+//                  (FDTD-near then BEM-near, fp16 + per-row scale, the reference's format; the
+//                  FDTD-near row shifted by one tap: row[k] = record tap k + 1, row[15] = 0)
 //   face pairs     face_start[nt + 1] per centre triangle; pf pairs: face_nbr; dense
 //                  weights face_half[pf][32] + face_scale[pf][2]; per centre: 8 corner cells,
 //                  8 trilinear weights, denominator 0.5 * area - sum(factor)
@@ -128,7 +131,8 @@ struct Handle
     double *d_tw = nullptr;      // 8 radix-2 FFT twiddles (cos, sin)
 
     // ---- histories
-    void *d_neumann = nullptr, *d_dirichlet = nullptr;
+    void *d_neumann = nullptr, *d_dirichlet = nullptr;  // reference layout: read-out and loading
+    void *d_hist = nullptr;  // the step's copies: [Neumann, Dirichlet][4 copies][nt][kRing] (step.cu)
 
     // ---- listeners
     std::vector<int> listen_xyz;
@@ -204,6 +208,8 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 int step_prime(Handle &h);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state
+int hist_import(Handle &h);  // reference-layout rings -> the step's history copies
+int hist_export(Handle &h);  // the step's history copies -> reference-layout rings
 
 // cells.cu
 int cells_classify(Handle &h, int *ghost_count);

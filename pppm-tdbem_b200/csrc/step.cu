@@ -28,38 +28,68 @@ namespace pb
 namespace
 {
 
+// The values of a scene that every step kernel reads (the per-step ones come from StepState)
 struct StepArgs
 {
     int res;
-    int tnew;  // time index being produced (t + 1)
-    long long step_row;  // row of the listener series for this step
     double lap_coef;     // (c dt)^2 in double, reference arithmetic
     double hd;           // h in double
     float c, dt, h;
     int pml_width;
     float damp;
     int nt;
-    const float *acc;  // nt accelerations of this step (device) or null
     int n_listen;
     int listen_cell[8];
     int listen_corr[8];  // 1 if the listener cell is a corrected cell
 };
 
-__device__ inline void bind_step(StepArgs &a, const StepState *st, int k)
+// what step k of a call produces: its time index, listener-series row and acceleration row
+struct StepDyn
 {
-    a.tnew = st->tnew0 + k;
-    a.step_row = st->row0 + k;
-    a.acc = st->acc ? st->acc + (long long)k * a.nt : nullptr;
+    int tnew;
+    long long row;
+    const float *acc;
+};
+
+__device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
+{
+    StepDyn d;
+    d.tnew = st->tnew0 + k;
+    d.row = st->row0 + k;
+    d.acc = st->acc ? st->acc + (long long)k * nt : nullptr;
+    return d;
 }
 
-// the three grid time levels (and PML fields), by time index
+// History rings in the step.  The reference keeps per triangle a ring of 32 values indexed by
+// time mod 32 and reads the 16 taps t, t-1, ..., t-15 (bem.h:55).  The step keeps every ring in
+// four copies instead; copy c holds time tau at index (c - tau) mod 32, so taps 4q..4q+3 of time
+// t sit at indices (c - t + 4q) .. +3 of copy c, ascending with the tap, and for c = t mod 4
+// they start on a multiple of 4: one aligned 16-byte load (FP32) reads 4 taps.  A new value is
+// written into all four copies.  The reference-layout rings stay beside them for read-out and
+// loading (hist_export / hist_import).
+__host__ __device__ inline int hist_index(int copy, int time) { return (copy - time) & (kRing - 1); }
+
+// the three grid time levels (and PML fields) by time index, and the history copies
+// [field 0 = Neumann, 1 = Dirichlet][copy 0..3][nt][kRing]
 template <typename R>
 struct Ring
 {
     R *g[3];
     R *p[3];
+    R *hist;
+    int nt;
     __device__ R *slot(int time) const { return g[((time % 3) + 3) % 3]; }
     __device__ R *pml(int time) const { return p[((time % 3) + 3) % 3]; }
+    __device__ R *hrow(int field, int copy, int tri) const
+    {
+        return hist + ((long long)(field * 4 + copy) * nt + tri) * kRing;
+    }
+    __device__ void hwrite(int field, int tri, int time, R v) const
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            hrow(field, c, tri)[hist_index(c, time)] = v;
+    }
 };
 
 template <typename Real>
@@ -192,9 +222,10 @@ __device__ inline R interior_cell(const R *cur, const R *prev, int res, int x, i
 }
 
 // Work split of the stencil launch into three block ranges so no warp mixes the short
-// interior update with the long boundary solve:
-//   [0, nb_in)              interior cells [2, res-3]^3, consecutive threads along z
-//   [nb_in, nb_in + nb_bd)  boundary-layer cells (a coordinate equal to 1 or res-2)
+// interior update with the long boundary solve; the boundary blocks come first, so they are
+// scheduled first and their long solves overlap the interior blocks instead of trailing them:
+//   [0, nb_bd)              boundary-layer cells (a coordinate equal to 1 or res-2)
+//   [nb_bd, nb_bd + nb_in)  interior cells [2, res-3]^3, consecutive threads along z
 //   the rest                Neumann ring write, one thread per triangle
 struct StencilSplit
 {
@@ -243,7 +274,8 @@ __device__ inline void boundary_cell(int i, int res, int &x, int &y, int &z)
 }
 
 template <typename R>
-__device__ inline void finish_cell(const StepArgs &a, long long c, R v, R *next, const unsigned *corr_mask, R *series)
+__device__ inline void finish_cell(const StepArgs &a, long long row, long long c, R v, R *next,
+                                   const unsigned *corr_mask, R *series)
 {
     if ((corr_mask[c >> 5] >> (c & 31)) & 1u)
     {
@@ -253,33 +285,19 @@ __device__ inline void finish_cell(const StepArgs &a, long long c, R v, R *next,
     next[c] = v;
     for (int l = 0; l < a.n_listen; l++)
         if (a.listen_cell[l] == (int)c && !a.listen_corr[l])
-            series[a.step_row * a.n_listen + l] = v;
+            series[row * a.n_listen + l] = v;
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) stencil_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int k,
-                                                       StencilSplit sp, const unsigned *corr_mask, R *neumann,
-                                                       R *series)
+__global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int k,
+                                                       StencilSplit sp, const unsigned *corr_mask, R *series)
 {
-    StepArgs a = a0;
-    bind_step(a, st, k);
-    R *cur = ring.slot(a.tnew - 1), *next = ring.slot(a.tnew);
-    const R *prev = ring.slot(a.tnew - 2);
+    const StepArgs &a = a0;
+    const StepDyn dy = bind_step(st, k, a0.nt);
+    R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
+    const R *prev = ring.slot(dy.tnew - 2);
     const int res = a.res;
     int b = blockIdx.x;
-    if (b < sp.nb_in)
-    {
-        const int mi = res - 4;
-        int i = b * 256 + threadIdx.x;
-        if (i >= mi * mi * mi)
-            return;
-        int x = 2 + i / (mi * mi), r = i % (mi * mi);
-        int y = 2 + r / mi, z = 2 + r % mi;
-        R v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
-        finish_cell<R>(a, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
-        return;
-    }
-    b -= sp.nb_in;
     if (b < sp.nb_bd)
     {
         const int m = res - 2;
@@ -289,13 +307,26 @@ __global__ void __launch_bounds__(256) stencil_kernel(StepArgs a0, Ring<R> ring,
         int x, y, z;
         boundary_cell(i, res, x, y, z);
         R v = abc_cell<R>(cur, prev, res, x, y, z, (R)a.c, (R)a.dt, (R)a.h);
-        finish_cell<R>(a, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        finish_cell<R>(a, dy.row, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
         return;
     }
     b -= sp.nb_bd;
+    if (b < sp.nb_in)
+    {
+        const int mi = res - 4;
+        int i = b * 256 + threadIdx.x;
+        if (i >= mi * mi * mi)
+            return;
+        int x = 2 + i / (mi * mi), r = i % (mi * mi);
+        int y = 2 + r / mi, z = 2 + r % mi;
+        R v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
+        finish_cell<R>(a, dy.row, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        return;
+    }
+    b -= sp.nb_in;
     int i = b * 256 + threadIdx.x;
-    if (i < a.nt && a.acc)
-        neumann[(long long)i * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[i];
+    if (i < a.nt && dy.acc)
+        ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
 }
 
 // split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
@@ -306,19 +337,19 @@ __device__ inline R pml_damp(int x, int y, int z, int res, int w, R damp)
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) pml_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int k,
-                                                   const unsigned *corr_mask, R *neumann, R *series)
+__global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int k,
+                                                   const unsigned *corr_mask, R *series)
 {
-    StepArgs a = a0;
-    bind_step(a, st, k);
-    const R *cur = ring.slot(a.tnew - 1), *prev = ring.slot(a.tnew - 2);
-    R *next = ring.slot(a.tnew);
-    const R *pcur = ring.pml(a.tnew - 1);
-    R *pnext = ring.pml(a.tnew);
+    const StepArgs &a = a0;
+    const StepDyn dy = bind_step(st, k, a0.nt);
+    const R *cur = ring.slot(dy.tnew - 1), *prev = ring.slot(dy.tnew - 2);
+    R *next = ring.slot(dy.tnew);
+    const R *pcur = ring.pml(dy.tnew - 1);
+    R *pnext = ring.pml(dy.tnew);
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int res = a.res, m = res - 2, w = a.pml_width;
-    if (gid < a.nt && a.acc)
-        neumann[(long long)gid * kRing + (a.tnew & (kRing - 1))] = (R)a.acc[gid];
+    if (gid < a.nt && dy.acc)
+        ring.hwrite(0, (int)gid, dy.tnew, (R)dy.acc[gid]);
     if (gid >= (long long)m * m * m)
         return;
     int q[3] = {1 + (int)(gid / ((long long)m * m)), 1 + (int)((gid / m) % m), 1 + (int)(gid % m)};
@@ -370,15 +401,26 @@ __global__ void __launch_bounds__(256) pml_kernel(StepArgs a0, Ring<R> ring, con
     next[ci] = v;
     for (int l = 0; l < a.n_listen; l++)
         if (a.listen_cell[l] == (int)ci && !a.listen_corr[l])
-            series[a.step_row * a.n_listen + l] = v;
+            series[dy.row * a.n_listen + l] = v;
 }
 
-// ---- convolution helpers: lane k holds tap k of one pair
+// ---- convolution helpers
+// A pair is handled by a quad of 4 lanes: lane q takes taps 4q..4q+3 with one 16-byte load of
+// the pair's weights (4 fp16 (single, double) tap pairs) and one 16-byte load each of the
+// neighbour's Neumann and Dirichlet windows from the history copy whose taps 4q..4q+3 are
+// aligned at this time step; the 8 quads of a warp take pairs g, g + 8, ...  Each lane sums its
+// taps in increasing pair and tap order; the warp reduces once per triangle / cell.
 __device__ inline float conv_tap(__half2 w, float2 s, float n, float d)
 {
     return -__low2float(w) * s.x * n + __high2float(w) * s.y * d;
 }
 __device__ inline double conv_tap(double2 w, float2, double n, double d) { return -w.x * n + w.y * d; }
+
+template <typename T, int N>
+struct alignas(16) Vec
+{
+    T v[N];
+};
 
 template <typename R>
 struct WRec;
@@ -386,150 +428,123 @@ template <>
 struct WRec<float>
 {
     using T = __half2;
-    __device__ static T zero() { return __floats2half2_rn(0.f, 0.f); }
+    using W4 = Vec<__half2, 4>;
+    using H4 = Vec<float, 4>;
 };
 template <>
 struct WRec<double>
 {
     using T = double2;
-    __device__ static T zero() { return make_double2(0, 0); }
+    using W4 = Vec<double2, 4>;
+    using H4 = Vec<double, 4>;
 };
+
+constexpr unsigned kFull = 0xffffffffu;
 
 template <typename R>
 __device__ inline R warp_sum(R v)
 {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, off);
+        v += __shfl_xor_sync(kFull, v, off);
     return v;
 }
 
-// face stage: one warp per centre triangle
+// face stage: one warp per centre triangle.  The 8 far-field corner terms are fetched first
+// (lanes 0-7) so their latency overlaps the convolution.
 template <typename R>
-__global__ void __launch_bounds__(256) face_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int kstep,
-                                                    const int *face_start,
-                                                    const int *face_nbr, const typename WRec<R>::T *face_w,
-                                                    const float2 *face_scale, const int *face_corner,
-                                                    const float *interp, const double *interp_d,
-                                                    const double *denom, const R *neumann, R *dirichlet, float reflect)
+__global__ void __launch_bounds__(256) face_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
+                                                    const int *face_start, const int *face_nbr,
+                                                    const typename WRec<R>::T *face_w, const float2 *face_scale,
+                                                    const int *face_corner, const float *interp,
+                                                    const double *interp_d, const double *denom, float reflect)
 {
-    using W = typename WRec<R>::T;
-    StepArgs a = a0;
-    bind_step(a, st, kstep);
-    const R *next = ring.slot(a.tnew);
-    int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    int lane = threadIdx.x & 31;
+    using W4 = typename WRec<R>::W4;
+    using H4 = typename WRec<R>::H4;
+    const StepArgs &a = a0;
+    const StepDyn dy = bind_step(st, kstep, a0.nt);
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
     if (tri >= a.nt)
         return;
-    const int k = lane & 15, half = lane >> 4;
-    const int tslot = (a.tnew - k) & (kRing - 1);
-    R acc = 0;
-    int b = face_start[tri], e = face_start[tri + 1];
-    // each half-warp takes every other pair; kUnroll pairs per iteration have their index,
-    // weight and history loads in flight together
-    constexpr int kUnroll = 4;
-    for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
+    const R *next = ring.slot(dy.tnew);
+    const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
+    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
+    R iw = 0, pv = 0;
+    if (lane < 8)
     {
-        int nbr[kUnroll];
+        iw = interp_d ? (R)interp_d[8 * tri + lane] : (R)interp[8 * tri + lane];
+        pv = next[face_corner[8 * tri + lane]];
+    }
+    const int b = face_start[tri], e = face_start[tri + 1];
+    R acc = 0;
+    for (int p = b + g; p < e; p += 8)
+    {
+        const W4 w = *(const W4 *)(face_w + (long long)p * kTaps + 4 * q);
+        const float2 s = face_scale ? face_scale[p] : make_float2(1, 1);
+        const int nb = face_nbr[p];
+        const H4 hn = *(const H4 *)(nbase + (long long)nb * kRing);
+        const H4 hd = *(const H4 *)(dbase + (long long)nb * kRing);
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++)
+        for (int i = 0; i < 4; i++)
         {
-            int p = p0 + 2 * u;
-            nbr[u] = p < e ? face_nbr[p] : -1;
+            // tap 0 of the Dirichlet history is this step's unknown: left out
+            R di = (q == 0 && i == 0) ? (R)0 : hd.v[i];
+            acc += conv_tap(w.v[i], s, hn.v[i], di);
         }
-        W w[kUnroll];
-        float2 s[kUnroll];
-        R n[kUnroll], d[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++)
-        {
-            int p = p0 + 2 * u;
-            if (nbr[u] >= 0)
-            {
-                w[u] = face_w[(long long)p * kTaps + k];
-                s[u] = face_scale ? face_scale[p] : make_float2(1, 1);
-                n[u] = neumann[(long long)nbr[u] * kRing + tslot];
-                d[u] = k == 0 ? (R)0 : dirichlet[(long long)nbr[u] * kRing + tslot];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++)
-            if (nbr[u] >= 0)
-                acc += conv_tap(w[u], s[u], n[u], d[u]);
     }
     acc = warp_sum(acc);
-    if (lane == 0)
-    {
-        R far_sum = 0;
-        for (int wi = 0; wi < 8; wi++)
-        {
-            R iw = interp_d ? (R)interp_d[8 * tri + wi] : (R)interp[8 * tri + wi];
-            far_sum += iw * next[face_corner[8 * tri + wi]];
-        }
-        R num = far_sum * (R)reflect + acc;
-        dirichlet[(long long)tri * kRing + (a.tnew & (kRing - 1))] = (R)(num / denom[tri]);
-    }
+    R far_sum = 0;  // corners in order 0..7
+#pragma unroll
+    for (int wi = 0; wi < 8; wi++)
+        far_sum += __shfl_sync(kFull, iw, wi) * __shfl_sync(kFull, pv, wi);
+    R num = far_sum * (R)reflect + acc;
+    if (lane < 4)
+        ring.hrow(1, lane, tri)[hist_index(lane, dy.tnew)] = (R)(num / denom[tri]);  // lane c: copy c
 }
 
-// near stage: one warp per corrected cell.  prime != 0: only the next step's FDTD-near sum.
+// near stage: warps stride over the corrected cells (their number changes with the mesh, the
+// grid does not).  The FDTD-near rows are stored shifted by one tap (row[k] = record tap
+// k + 1, row[15] = 0), so both rows pair with the same history window.  prime != 0: only the
+// next step's FDTD-near sum.
 template <typename R>
-__global__ void __launch_bounds__(256) near_kernel(StepArgs a0, Ring<R> ring, const StepState *st, int kstep,
+__global__ void __launch_bounds__(256) near_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
                                                     const int *n3_cell, const int *n3_start, const int *p3_tri,
-                                                    const typename WRec<R>::T *w3, const float2 *w3_scale,
-                                                    const R *neumann, const R *dirichlet, R *series, int prime)
+                                                    const typename WRec<R>::T *w3, const float2 *w3_scale, R *series,
+                                                    int prime)
 {
-    using W = typename WRec<R>::T;
-    StepArgs a = a0;
-    bind_step(a, st, kstep);
-    R *cur = ring.slot(a.tnew), *nextslot = ring.slot(a.tnew + 1);
+    using W4 = typename WRec<R>::W4;
+    using H4 = typename WRec<R>::H4;
+    const StepArgs &a = a0;
+    const StepDyn dy = bind_step(st, kstep, a0.nt);
+    R *cur = ring.slot(dy.tnew), *nextslot = ring.slot(dy.tnew + 1);
     const int n3 = st->n3;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
     const int nwarps = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-    const int k = lane & 15, half = lane >> 4;
-    const int tslot = (a.tnew - k) & (kRing - 1);
-    // a fixed grid of warps strides over the corrected cells (their number changes with the mesh)
+    const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);
+    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
     for (int ci = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < n3; ci += nwarps)
     {
-        R acc_b = 0, acc_f = 0;
-        int b = n3_start[ci], e = n3_start[ci + 1];
-        constexpr int kUnroll = 4;
-        for (int p0 = b + half; p0 < e; p0 += 2 * kUnroll)
+        const int b = n3_start[ci], e = n3_start[ci + 1];
+        R acc_f = 0, acc_b = 0;
+        for (int p = b + g; p < e; p += 8)
         {
-            int tri[kUnroll];
+            const W4 wf = *(const W4 *)(w3 + (long long)p * 2 * kTaps + 4 * q);
+            const float2 sf = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
+            const int tr = p3_tri[p];
+            const H4 hn = *(const H4 *)(nbase + (long long)tr * kRing);
+            const H4 hd = *(const H4 *)(dbase + (long long)tr * kRing);
 #pragma unroll
-            for (int u = 0; u < kUnroll; u++)
+            for (int i = 0; i < 4; i++)
+                acc_f += conv_tap(wf.v[i], sf, hn.v[i], hd.v[i]);
+            if (!prime)
             {
-                int p = p0 + 2 * u;
-                tri[u] = p < e ? p3_tri[p] : -1;
-            }
-            R n[kUnroll], d[kUnroll];
-            W wf[kUnroll], wb[kUnroll];
-            float2 sf[kUnroll], sb[kUnroll];
+                const W4 wb = *(const W4 *)(w3 + (long long)p * 2 * kTaps + kTaps + 4 * q);
+                const float2 sb = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
 #pragma unroll
-            for (int u = 0; u < kUnroll; u++)
-            {
-                long long p = p0 + 2 * u;
-                if (tri[u] >= 0)
-                {
-                    n[u] = neumann[(long long)tri[u] * kRing + tslot];
-                    d[u] = dirichlet[(long long)tri[u] * kRing + tslot];
-                    wf[u] = k < kTaps - 1 ? w3[p * 2 * kTaps + k + 1] : WRec<R>::zero();
-                    sf[u] = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
-                    if (!prime)
-                    {
-                        wb[u] = w3[(p * 2 + 1) * kTaps + k];
-                        sb[u] = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
-                    }
-                }
+                for (int i = 0; i < 4; i++)
+                    acc_b += conv_tap(wb.v[i], sb, hn.v[i], hd.v[i]);
             }
-#pragma unroll
-            for (int u = 0; u < kUnroll; u++)
-                if (tri[u] >= 0)
-                {
-                    acc_f += conv_tap(wf[u], sf[u], n[u], d[u]);
-                    if (!prime)
-                        acc_b += conv_tap(wb[u], sb[u], n[u], d[u]);
-                }
         }
         acc_f = warp_sum(acc_f);
         if (!prime)
@@ -544,7 +559,7 @@ __global__ void __launch_bounds__(256) near_kernel(StepArgs a0, Ring<R> ring, co
                 cur[c] = v;
                 for (int l = 0; l < a.n_listen; l++)
                     if (a.listen_cell[l] == c)
-                        series[a.step_row * a.n_listen + l] = v;
+                        series[dy.row * a.n_listen + l] = v;
             }
         }
     }
@@ -555,7 +570,6 @@ StepArgs make_args(Handle &h)
 {
     StepArgs a{};
     a.res = h.res;
-    a.tnew = h.t + 1;
     a.c = h.prm.c;
     a.dt = h.prm.dt;
     a.h = h.prm.dl;
@@ -596,7 +610,7 @@ struct StepLaunch
     StencilSplit sp;
     const StepState *st;
     const unsigned *corr_mask;
-    R *neumann, *dirichlet, *series;
+    R *series;
     const int *face_start, *face_nbr, *face_corner, *n3_cell, *n3_start, *p3_tri;
     const W *face_w, *w3;
     const float2 *face_scale, *w3_scale;
@@ -623,8 +637,8 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.sp = stencil_split(h.res, L.a.nt);
     L.st = h.d_state;
     L.corr_mask = h.d_corr_mask;
-    L.neumann = (R *)h.d_neumann;
-    L.dirichlet = (R *)h.d_dirichlet;
+    L.ring.hist = (R *)h.d_hist;
+    L.ring.nt = h.mesh_set ? h.nt : 0;
     L.series = (R *)h.d_series;
     L.mesh = h.mesh_set ? 1 : 0;
     L.pml = h.prm.pml_width > 0 ? 1 : 0;
@@ -669,21 +683,20 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
     if (timed)
         cudaEventRecord(timed->ev[0], s);
     if (L.pml)
-        pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask, L.neumann, L.series);
+        pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask, L.series);
     else
-        stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.neumann,
-                                                         L.series);
+        stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
     if (timed)
         cudaEventRecord(timed->ev[1], s);
     if (L.mesh)
     {
         face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.face_start, L.face_nbr, L.face_w,
                                                    L.face_scale, L.face_corner, L.interp, L.interp_d, L.denom,
-                                                   L.neumann, L.dirichlet, L.reflect);
+                                                   L.reflect);
         if (timed)
             cudaEventRecord(timed->ev[2], s);
         near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
-                                                   L.w3_scale, L.neumann, L.dirichlet, L.series, 0);
+                                                   L.w3_scale, L.series, 0);
     }
     if (timed)
         cudaEventRecord(timed->ev[3], s);
@@ -796,13 +809,51 @@ int prime(Handle &h)
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
     near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
-                                                        L.w3_scale, L.neumann, L.dirichlet, nullptr, 1);
+                                                        L.w3_scale, nullptr, 1);
     h.launches += 2;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
 }
 
+// reference-layout rings (index = time mod 32) <-> the four history copies
+template <typename R>
+__global__ void hist_copy_kernel(R *canon_n, R *canon_d, R *hist, int nt, int to_copies)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per = (long long)nt * kRing;
+    if (i >= 2 * per)
+        return;
+    const int field = (int)(i / per);
+    const long long r = i % per;
+    const int tri = (int)(r / kRing), slot = (int)(r % kRing);
+    R *canon = field ? canon_d : canon_n;
+    if (to_copies)
+    {
+        const R v = canon[r];
+        for (int c = 0; c < 4; c++)
+            hist[((long long)(field * 4 + c) * nt + tri) * kRing + hist_index(c, slot)] = v;
+    }
+    else
+        canon[r] = hist[((long long)(field * 4) * nt + tri) * kRing + hist_index(0, slot)];
+}
+
+template <typename R>
+int hist_copy(Handle &h, int to_copies)
+{
+    if (!h.mesh_set || !h.d_hist)
+        return PPPM_OK;
+    const long long n = 2ll * h.nt * kRing;
+    hist_copy_kernel<R><<<div_up(n, 256), 256, 0, h.stream>>>((R *)h.d_neumann, (R *)h.d_dirichlet, (R *)h.d_hist,
+                                                               h.nt, to_copies);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
+
 }  // namespace
+
+int hist_import(Handle &h) { return h.fp64 ? hist_copy<double>(h, 1) : hist_copy<float>(h, 1); }
+int hist_export(Handle &h) { return h.fp64 ? hist_copy<double>(h, 0) : hist_copy<float>(h, 0); }
 
 int step_prime(Handle &h) { return h.fp64 ? prime<double>(h) : prime<float>(h); }
 
