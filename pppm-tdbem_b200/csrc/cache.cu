@@ -114,102 +114,152 @@ __global__ void gc_flag_kernel(const float *center, const float *normal, const f
     flag[i] = (len3(oc - c) > 0.01 * h || len3(on - n) > 0.01 || abs(oa - a) > 0.01 * a) ? 1 : 0;
 }
 
-// one thread per (triangle, weight index); FP32 records with the reference's arithmetic
-__global__ void gc_compute_kernel(DevConsts dc, const float *verts, const int *tris, const int *cellc,
-                                  const float *center, const float *normal, const float *area, const int *flag, int nt,
-                                  __half2 *gc_w, float2 *gc_scale, float *snap)
+// Grid-cache refresh, one block per flagged triangle.  The FDTD-near rows of a triangle's 27
+// records read the Green's function at the cell centres of 7-point stencils around its 27
+// neighbour cells, and the BEM-near rows at those 27 centres: 81 distinct cells (offsets in
+// [-2, 2]^3 with at most one coordinate of magnitude 2) instead of 243 point evaluations per
+// wave number.  The block evaluates each (cell, wave number) once into shared memory (the
+// unrounded terms of both_acc), then every (record, wave number) accumulates its points in the
+// reference's order, then one FFT per thread, then packing: the records are bit-identical to a
+// per-record evaluation.
+constexpr int kGcPoints = 81;
+
+// offset of distinct point p (0..80) from the triangle's cell
+__device__ inline void gc_point_offset(int p, int &dx, int &dy, int &dz)
 {
-    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)nt * 27)
+    if (p < 27)
+    {
+        dx = p % 3 - 1;
+        dy = p / 3 % 3 - 1;
+        dz = p / 9 - 1;
         return;
-    int tri = (int)(gid / 27), woff = (int)(gid % 27);
+    }
+    p -= 27;
+    const int axis = p / 18, side = (p / 9) & 1, a = p % 3 - 1, b = p / 3 % 3 - 1;
+    const int far = side ? 2 : -2;
+    dx = axis == 0 ? far : a;
+    dy = axis == 1 ? far : (axis == 0 ? a : b);
+    dz = axis == 2 ? far : b;
+}
+
+__global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float *verts, const int *tris,
+                                                       const int *cellc, const float *center, const float *normal,
+                                                       const float *area, const int *flag, __half2 *gc_w,
+                                                       float2 *gc_scale, float *snap)
+{
+    const int tri = blockIdx.x;
     if (!flag[tri])
         return;
+    __shared__ ref32::PointTerms terms[kGcPoints][kTaps / 2 + 1];
+    __shared__ short point_of[125];                  // 5^3 offset box -> distinct point
+    __shared__ cf spec[27][kTaps / 2 + 1][4];        // ss, sd, qs, qd per record and wave number
+    __shared__ float wts[27][4][kTaps];              // their 16-tap weights
+    const int tid = threadIdx.x;
     f3 v[3];
     int idx[3];
     load_tri(verts, tris, tri, v, idx);
-    int tx = cellc[3 * tri], ty = cellc[3 * tri + 1], tz = cellc[3 * tri + 2];
-    int nx = tx + woff % 3 - 1, ny = ty + woff / 3 % 3 - 1, nz = tz + woff / 9 - 1;
-    int dcx[8] = {nx, nx - 1, nx + 1, nx, nx, nx, nx, nx};
-    int dcy[8] = {ny, ny, ny, ny - 1, ny + 1, ny, ny, ny};
-    int dcz[8] = {nz, nz, nz, nz, nz, nz - 1, nz + 1, nz};
-    float scale = dc.c * dc.c * dc.dt * dc.dt / (dc.h * dc.h);
-    float dsc[8] = {2, scale, scale, scale, scale, scale, scale, -6 * scale};
-    f3 pts[8];
-    float sc[8];
-    int n = 0;
-    for (int i = 0; i < 8; i++)
+    const int tx = cellc[3 * tri], ty = cellc[3 * tri + 1], tz = cellc[3 * tri + 2];
+    const float jac = ref32::jacobian(v);
+    const f3 nrm = ref32::tri_normal(v);
+    const float gx = (float)PB_TRI_X;
+    const f3 q = ref32::local_to_global(gx, gx, v);
+    // 1. the Green's function terms of every distinct cell centre and wave number
+    for (int it = tid; it < kGcPoints * (kTaps / 2 + 1); it += blockDim.x)
     {
-        if (!(dcx[i] == tx && dcy[i] == ty && dcz[i] == tz))
+        const int p = it / (kTaps / 2 + 1), k = it % (kTaps / 2 + 1);
+        int dx, dy, dz;
+        gc_point_offset(p, dx, dy, dz);
+        if (k == 0)
+            point_of[(dx + 2) * 25 + (dy + 2) * 5 + (dz + 2)] = (short)p;
+        const f3 pt = cell_center(tx + dx, ty + dy, tz + dz, dc.h, dc.mn);
+        terms[p][k] = ref32::point_terms(q, pt, nrm, cf{dc.wave_re[k], dc.wave_im[k]});
+    }
+    __syncthreads();
+    // 2. spectra of each record: the 7-point stencil around its neighbour cell (FDTD-near) and
+    // its centre (BEM-near), accumulated in the reference's order
+    const float scale = dc.c * dc.c * dc.dt * dc.dt / (dc.h * dc.h);
+    const double c = 0.5 * 1.0f * jac;
+    for (int it = tid; it < 27 * (kTaps / 2 + 1); it += blockDim.x)
+    {
+        const int woff = it / (kTaps / 2 + 1), k = it % (kTaps / 2 + 1);
+        const int ox = woff % 3 - 1, oy = woff / 3 % 3 - 1, oz = woff / 9 - 1;
+        const int sx[8] = {0, -1, 1, 0, 0, 0, 0, 0}, sy[8] = {0, 0, 0, -1, 1, 0, 0, 0},
+                  sz[8] = {0, 0, 0, 0, 0, -1, 1, 0};
+        const float dsc[8] = {2, scale, scale, scale, scale, scale, scale, -6 * scale};
+        cf ls{0.0f, 0.0f}, ld{0.0f, 0.0f};
+        for (int i = 0; i < 8; i++)
         {
-            pts[n] = cell_center(dcx[i], dcy[i], dcz[i], dc.h, dc.mn);
-            sc[n] = dsc[i];
-            n++;
+            const int px = ox + sx[i], py = oy + sy[i], pz = oz + sz[i];
+            if (px == 0 && py == 0 && pz == 0)
+                continue;  // targets inside the triangle's own cell are skipped
+            ref32::acc_terms(ls, ld, terms[point_of[(px + 2) * 25 + (py + 2) * 5 + (pz + 2)]][k], dsc[i], true);
         }
+        spec[woff][k][0] = cf{(float)(0.0f + c * ls.re), (float)(0.0f + c * ls.im)};
+        spec[woff][k][1] = cf{(float)(0.0f + c * ld.re), (float)(0.0f + c * ld.im)};
+        cf bs{0.0f, 0.0f}, bd{0.0f, 0.0f};
+        if (!(ox == 0 && oy == 0 && oz == 0))
+            ref32::acc_terms(bs, bd, terms[point_of[(ox + 2) * 25 + (oy + 2) * 5 + (oz + 2)]][k], 1.0f, false);
+        spec[woff][k][2] = cf{(float)(0.0f + c * bs.re), (float)(0.0f + c * bs.im)};
+        spec[woff][k][3] = cf{(float)(0.0f + c * bd.re), (float)(0.0f + c * bd.im)};
     }
-    cf ss[kTaps], sd[kTaps];
-    for (int k = 0; k <= kTaps / 2; k++)
+    __syncthreads();
+    // 3. one 16-point transform per (record, layer row)
+    for (int it = tid; it < 27 * 4; it += blockDim.x)
     {
-        cf kk{dc.wave_re[k], dc.wave_im[k]};
-        ref32::face_to_points2(v, pts, sc, n, true, kk, ss[k], sd[k]);
-    }
-    float ws[kTaps], wd[kTaps];
-    spectrum_to_weights(ss, dc.lambda, ws, dc.tw);
-    spectrum_to_weights(sd, dc.lambda, wd, dc.tw);
-    // move(-1)
-    for (int i = kTaps - 1; i >= 1; i--)
-    {
-        ws[i] = ws[i - 1];
-        wd[i] = wd[i - 1];
-    }
-    ws[0] = 0;
-    wd[0] = 0;
-    bool inside = (nx == tx && ny == ty && nz == tz);
-    float ps[kTaps], pd[kTaps];
-    if (!inside)
-    {
-        f3 p = cell_center(nx, ny, nz, dc.h, dc.mn);
-        cf qs[kTaps], qd[kTaps];
+        const int woff = it / 4, which = it % 4;
+        cf sp[kTaps];
         for (int k = 0; k <= kTaps / 2; k++)
-        {
-            cf kk{dc.wave_re[k], dc.wave_im[k]};
-            ref32::face_to_points2(v, &p, nullptr, 1, false, kk, qs[k], qd[k]);
-        }
-        spectrum_to_weights(qs, dc.lambda, ps, dc.tw);
-        spectrum_to_weights(qd, dc.lambda, pd, dc.tw);
-        for (int i = 2; i < kTaps; i++)
-        {
-            ws[i] += ps[i - 2] * -1.0f;
-            wd[i] += pd[i - 2] * -1.0f;
-        }
+            sp[k] = spec[woff][k][which];
+        spectrum_to_weights(sp, dc.lambda, wts[woff][which], dc.tw);
     }
-    size_t rec = (size_t)tri * 54 + woff;
-    pack_half(ws, wd, gc_w + rec * kTaps, gc_scale + rec);
-    float bs[kTaps], bd[kTaps];
-    for (int i = 0; i < kTaps; i++)
+    __syncthreads();
+    // 4. move(-1), subtract the BEM-near weights two steps back, pack both records
+    for (int woff = tid; woff < 27; woff += blockDim.x)
     {
-        bs[i] = 0;
-        bd[i] = 0;
-    }
-    if (!inside)
+        const bool inside = woff == 13;  // the triangle's own cell
+        float ws[kTaps], wd[kTaps];
+        ws[0] = 0;
+        wd[0] = 0;
+        for (int i = 1; i < kTaps; i++)
+        {
+            ws[i] = wts[woff][0][i - 1];
+            wd[i] = wts[woff][1][i - 1];
+        }
+        if (!inside)
+            for (int i = 2; i < kTaps; i++)
+            {
+                ws[i] += wts[woff][2][i - 2] * -1.0f;
+                wd[i] += wts[woff][3][i - 2] * -1.0f;
+            }
+        const size_t rec = (size_t)tri * 54 + woff;
+        pack_half(ws, wd, gc_w + rec * kTaps, gc_scale + rec);
+        float bs[kTaps], bd[kTaps];
         for (int i = 0; i < kTaps; i++)
         {
-            bs[i] += ps[i] * 1.0f;
-            bd[i] += pd[i] * 1.0f;
+            bs[i] = 0;
+            bd[i] = 0;
         }
-    pack_half(bs, bd, gc_w + (rec + 27) * kTaps, gc_scale + rec + 27);
-    if (woff == 0)
+        if (!inside)
+            for (int i = 0; i < kTaps; i++)
+            {
+                bs[i] += wts[woff][2][i] * 1.0f;
+                bd[i] += wts[woff][3][i] * 1.0f;
+            }
+        pack_half(bs, bd, gc_w + (rec + 27) * kTaps, gc_scale + rec + 27);
+    }
+    if (tid == 0)
     {
-        f3 c = load3(center, tri), nn = load3(normal, tri);
-        snap[7 * tri] = c.x;
-        snap[7 * tri + 1] = c.y;
-        snap[7 * tri + 2] = c.z;
+        f3 cc = load3(center, tri), nn = load3(normal, tri);
+        snap[7 * tri] = cc.x;
+        snap[7 * tri + 1] = cc.y;
+        snap[7 * tri + 2] = cc.z;
         snap[7 * tri + 3] = nn.x;
         snap[7 * tri + 4] = nn.y;
         snap[7 * tri + 5] = nn.z;
         snap[7 * tri + 6] = area[tri];
     }
 }
+
 
 // FP64 scheme: the same records entirely in double, unquantised
 __global__ void gc_compute_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *cellc,
@@ -745,10 +795,8 @@ int cache_refresh(Handle &h)
                                                                              h.d_gc_flag, nt, (double2 *)h.d_gc_w,
                                                                              h.d_gc_snap);
     else
-        gc_compute_kernel<<<div_up((long long)nt * 27, 128), 128, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc,
-                                                                           h.d_center, h.d_normal, h.d_area,
-                                                                           h.d_gc_flag, nt, (__half2 *)h.d_gc_w,
-                                                                           h.d_gc_scale, h.d_gc_snap);
+        gc_block_kernel<<<nt, 256, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc, h.d_center, h.d_normal, h.d_area,
+                                           h.d_gc_flag, (__half2 *)h.d_gc_w, h.d_gc_scale, h.d_gc_snap);
     h.launches++;
     PB_CHECK_LAUNCH();
     h.gc_empty = false;

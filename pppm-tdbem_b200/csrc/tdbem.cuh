@@ -165,6 +165,59 @@ __device__ inline void both_acc(cf &as, cf &ad, f3 src, f3 trg, f3 n, cf k, floa
     }
 }
 
+// both_acc split in two: the unrounded double-precision terms of one point (valid = r != 0),
+// and their scaled accumulation.  point_terms + acc_terms perform exactly the operations of
+// both_acc, so a point's terms can be computed once and accumulated into several sums.
+struct PointTerms
+{
+    double qre, qim, mre, mim;
+    int valid;
+};
+
+__device__ inline PointTerms point_terms(f3 src, f3 trg, f3 n, cf k)
+{
+    PointTerms t{0, 0, 0, 0, 0};
+    f3 d = src - trg;
+    float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    if (r2 != 0)
+    {
+        float r = sqrtf(r2);
+        cf ikr = ikr_of(r, k);
+        cf e = cexp(ikr.re, ikr.im);
+        double den1 = 4 * PB_PI * r;
+        t.qre = e.re / den1;
+        t.qim = e.im / den1;
+        double den = 4 * PB_PI * r2 * r;
+        double are = -e.re / den, aim = -e.im / den;
+        float bre = 1.0f - ikr.re, bim = -ikr.im;
+        double mre = are * bre - aim * bim;
+        double mim = are * bim + aim * bre;
+        float dn = dot3(d, n);
+        t.mre = mre * dn;
+        t.mim = mim * dn;
+        t.valid = 1;
+    }
+    return t;
+}
+
+__device__ inline void acc_terms(cf &as, cf &ad, const PointTerms &t, float scale, bool scaled)
+{
+    if (!t.valid)
+        return;
+    double qre = t.qre, qim = t.qim, mre = t.mre, mim = t.mim;
+    if (scaled)
+    {
+        qre = qre * scale;
+        qim = qim * scale;
+        mre = mre * scale;
+        mim = mim * scale;
+    }
+    as.re = (float)(as.re + qre);
+    as.im = (float)(as.im + qim);
+    ad.re = (float)(ad.re + mre);
+    ad.im = (float)(ad.im + mim);
+}
+
 __device__ inline cf layer_point(f3 src, f3 trg, f3 n, cf k, bool dbl)
 {
     cf acc{0.0f, 0.0f};
