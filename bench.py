@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--steps", type=int, default=60, help="timed benchmark steps (motion frames)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="moving", choices=["moving", "static"])
+    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--summarize-launches", metavar="CSV",
@@ -343,6 +343,163 @@ def run_ours(args, ws, rank, local):
     return line
 
 
+# ---------------------------------------------------------------- batched scenes ------
+BATCH_SCENES = 64
+BATCH_SEED = 11
+BATCH_NAME = ("64 scenes from seed 11: res in {24,32,48,64}, perturbed icosphere subdivision 2-4 "
+              "(320-5120 tris), 1000-4000 steps each")
+
+
+def batch_listener(res):
+    return (res - 4, res // 2, res // 2)
+
+
+def batch_acc(spec, device):
+    """(steps, nt) float32 accelerations of one batch scene: a sine at the scene's frequency on
+    every triangle (device tensor, or pinned host tensor for device == "pinned")."""
+    import torch
+
+    t = torch.arange(spec["steps"], dtype=torch.float64) * float(spec["dt"])
+    a = torch.sin(2 * math.pi * spec["freq"] * t).to(torch.float32)
+    a = a[:, None].expand(spec["steps"], len(spec["tris"])).contiguous()
+    return a.pin_memory() if device == "pinned" else a.to(device)
+
+
+def run_batch(args, ws, rank, local):
+    """Scenes/s of the 64-scene batch: one benchmark step = every scene run through all of its
+    time steps, batched (pppm_batch_run) and, for comparison, scene by scene (pppm_step)."""
+    import torch
+
+    from pppm_b200 import Batch, Solver
+
+    W, K = args.warmup, args.steps
+    specs = scenes.batch_scenes(BATCH_SCENES, BATCH_SEED)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    solvers = []
+    for sp in specs:
+        s = Solver(sp["res"], sp["h"], sp["dt"], sp["min_pos"], device=local, stream=stream.cuda_stream)
+        s.set_mesh(sp["verts"], sp["tris"])
+        s.add_listener(*batch_listener(sp["res"]))
+        solvers.append(s)
+    accs = [batch_acc(sp, dev) for sp in specs]
+    t_start = [s.t for s in solvers]
+    batch = Batch(solvers)
+
+    def rewind():
+        for s, t0 in zip(solvers, t_start):
+            s.reset_fields()
+            s.rewind_listeners()
+            s.t = t0
+
+    def timed(run, reps, clocks=None):
+        for _ in range(W):
+            rewind()
+            run()
+        torch.cuda.synchronize()
+        launches0 = sum(s.launch_count() for s in solvers)
+        if clocks:
+            clocks.start()
+        barrier(ws)
+        ms = 0.0
+        for _ in range(reps):
+            rewind()
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        barrier(ws)
+        clk = clocks.stop() if clocks else None
+        return max_over_ranks(ws, ms), sum(s.launch_count() for s in solvers) - launches0, clk
+
+    def run_batched():
+        batch.run(accs)
+
+    def run_sequential():
+        for s, a in zip(solvers, accs):
+            s.step(a)
+
+    clocks = ClockSampler(local)
+    ms_b, launches, clk = timed(run_batched, K, clocks)
+    ms_s, launches_s, _ = timed(run_sequential, max(1, min(K, 2)))
+    reps_s = max(1, min(K, 2))
+    series_b = [s.listeners() for s in solvers]
+    rewind()
+    run_sequential()
+    same = all(np.array_equal(a, s.listeners()) for a, s in zip(series_b, solvers))
+    value = BATCH_SCENES * K * ws / (ms_b * 1e-3)
+    seq = BATCH_SCENES * reps_s * ws / (ms_s * 1e-3)
+    cell_steps = sum(float(sp["res"]) ** 3 * sp["steps"] for sp in specs)
+
+    e2e = None
+    if not args.no_e2e:
+        pinned = [batch_acc(sp, "pinned") for sp in specs]
+        h2d = sum(a.numel() * 4 for a in pinned)
+        d2h = 0
+        for _ in range(W):
+            rewind()
+            batch.run(pinned)
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(K):
+            rewind()
+            batch.run(pinned)
+            d2h = 0
+            for s in solvers:
+                d2h += s.listeners().nbytes
+        torch.cuda.synchronize()
+        te = max_over_ranks(ws, time.perf_counter() - t0)
+        e2e = {"value": round(BATCH_SCENES * K * ws / te, 3), "unit": "scenes/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+        del pinned
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_batch_baseline(specs)
+    batch.close()
+    for s in solvers:
+        s.close()
+    return {
+        "metric": "scenes/s, %s" % BATCH_NAME, "value": round(value, 3), "unit": "scenes/s", "n_gpus": ws,
+        "steps": K, "warmup": W, "ms_per_step": round(ms_b / K, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes and accelerations)",
+        "config": {"workload": BATCH_NAME, "scenes": BATCH_SCENES, "time_steps_per_bench_step":
+                   int(sum(sp["steps"] for sp in specs)), "gcell_steps_per_bench_step": round(cell_steps / 1e9, 3),
+                   "bench_step": "every scene through all of its time steps (one pppm_batch_run call)",
+                   "l2": "flushed (256 MiB write) between timed iterations", "parallelism": "replicas x%d" % ws},
+        "sequential": {"value": round(seq, 3), "unit": "scenes/s", "reps": reps_s, "ms_per_rep": round(ms_s / reps_s, 3),
+                       "gpu_launches_per_rep": int(launches_s // reps_s), "listeners_bit_identical": bool(same)},
+        "batched_over_sequential": round(value / seq, 3),
+        "gcell_steps_per_s": round(cell_steps * K * ws / (ms_b * 1e-3) / 1e9, 3),
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
+def cpu_batch_baseline(specs, sample=4, steps=20):
+    """The CPU restatement on the first `sample` batch scenes, `steps` time steps each (set_mesh
+    untimed), extrapolated to every step of those scenes: scenes/s on the host cores."""
+    from oracle.oracle import Oracle, oracle_threads
+
+    est = 0.0
+    for sp in specs[:sample]:
+        o = Oracle(sp["res"], sp["h"], sp["dt"], sp["min_pos"])
+        o.set_mesh(sp["verts"], sp["tris"])
+        acc = np.ones((steps, len(sp["tris"])), np.float32)
+        t0 = time.perf_counter()
+        o.step(acc, listeners=[batch_listener(sp["res"])])
+        est += (time.perf_counter() - t0) / steps * sp["steps"]
+        o.close()
+    return {"value": round(sample / est, 5), "unit": "scenes/s", "cores": oracle_threads(), "kind": "port",
+            "sample": "first %d scenes, %d time steps each, extrapolated to their full step counts (C restatement "
+                      "with OpenMP)" % (sample, steps)}
+
+
 def cpu_baseline(wl):
     """The CPU restatement (oracle/) on the host cores: one benchmark step of the same
     workload (set_mesh untimed)."""
@@ -370,6 +527,8 @@ def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
     W, K = args.warmup, args.steps
+    if args.workload == "batch":
+        return run_reference_batch(args)
     wl = Workload(args.workload, W + K)
     sc = wl.scene
     from oracle import oracle as O
@@ -434,6 +593,51 @@ def run_reference(args, ws, rank, local):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_reference_batch(args):
+    """The reference solver (oracle/_ref) run scene by scene over the 64-scene batch: one timed
+    pass (each scene's set_mesh untimed), after one warm-up scene."""
+    from oracle import oracle as O
+
+    line = {"impl": "reference", "metric": "scenes/s, %s" % BATCH_NAME, "unit": "scenes/s"}
+    if not O.reference_available():
+        line["unavailable"] = "reference solver not built (oracle/_ref)"
+        return line
+    import torch
+
+    specs = scenes.batch_scenes(BATCH_SCENES, BATCH_SEED)
+
+    def one(sp):
+        r = O.Reference(sp["res"], sp["h"], sp["dt"], sp["min_pos"])
+        try:
+            r.set_mesh(sp["verts"], sp["tris"])
+            acc = batch_acc(sp, torch.device("cuda"))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r.run_device(acc.data_ptr(), sp["steps"], batch_listener(sp["res"]))
+            torch.cuda.synchronize()
+            return time.perf_counter() - t0
+        finally:
+            r.close()
+
+    try:
+        one(specs[0])
+        total = sum(one(sp) for sp in specs)
+    except RuntimeError as e:
+        line["unavailable"] = "reference solver rejected a batch scene: %s" % e
+        return line
+    value = BATCH_SCENES / total
+    line.update({"value": round(value, 4), "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True,
+                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                 "data": "synthetic (seeded meshes and accelerations)",
+                 "config": {"workload": BATCH_NAME, "scenes": BATCH_SCENES},
+                 "cpu_baseline": {"value": round(value, 4), "unit": "scenes/s", "cores": 0, "kind": "reference",
+                                  "sample": "reference CUDA solver built from source, the 64 scenes one after another "
+                                            "(set_mesh untimed)"},
+                 "e2e": {"value": round(value, 4), "unit": "scenes/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    return line
+
+
 def summarize_launches(path):
     """Per-kernel launch count, total and mean device time and share of an ncu launch list."""
     import collections
@@ -464,6 +668,8 @@ def main():
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         line = run_reference(args, ws, rank, local)
+    elif args.workload == "batch":
+        line = run_batch(args, ws, rank, local)
     else:
         line = run_ours(args, ws, rank, local)
     if rank == 0 and line is not None:

@@ -868,13 +868,9 @@ int cache_refresh(Handle &h)
         h.pool_used = used;
 
         // compact the recompute list
-        int *pos = h.d_flags;  // res^3 scratch is free after mesh_build
-        int *work = h.d_flags + (h.pf + 1);
-        if (2 * (h.pf + 1) > 4 * (h.n_cells + 1))
-        {
-            set_error("face pair scratch too small");
-            return PPPM_ERR_CAPACITY;
-        }
+        PB_TRY(dgrow(&h.d_pair_work, h.pair_work_cap, 2 * (h.pf + 1), s));
+        int *pos = h.d_pair_work;
+        int *work = h.d_pair_work + (h.pf + 1);
         PB_TRY(exclusive_scan(h, h.d_pair_flag, pos, h.pf));
         int nwork = 0;
         PB_TRY(read_int(h, pos + h.pf, &nwork));

@@ -345,7 +345,7 @@ int pppm_destroy(pppm_handle *ph)
                     h.d_face_nbr,     h.d_face_pool,     h.d_face_w,       h.d_face_scale,    h.d_face_corner,
                     h.d_pair_flag,    h.d_status,        h.d_neumann,      h.d_dirichlet,     h.d_listen_cell,
                     h.d_listen_n3,    h.d_series,        h.d_cell_type,    h.d_cell_nearest,  h.d_cell_ghost,
-                    h.d_cell_points,  h.d_cell_type_old, h.d_acc};
+                    h.d_cell_points,  h.d_cell_type_old, h.d_acc,           h.d_pair_work};
     for (void *q : ptrs)
         dev_free(q);
     for (int i = 0; i < 4; i++)
@@ -462,6 +462,82 @@ int pppm_step(pppm_handle *ph, const float *acc, int acc_on_device, int nsteps)
     }
     PB_TRY(ensure_series(h, nsteps));
     return step_run(h, dacc, nsteps);
+}
+
+struct pppm_batch
+{
+    std::vector<pppm_handle *> scenes;
+    Batch *impl = nullptr;
+};
+
+int pppm_batch_create(pppm_handle **scenes, int nscenes, pppm_batch **out)
+{
+    if (!out)
+        return PPPM_ERR_ARG;
+    *out = nullptr;
+    if (!scenes || nscenes <= 0)
+        return PPPM_ERR_ARG;
+    std::vector<Handle *> hs(nscenes);
+    for (int i = 0; i < nscenes; i++)
+    {
+        PB_TRY(check_handle(scenes[i]));
+        hs[i] = &scenes[i]->h;
+    }
+    pppm_batch *b = new (std::nothrow) pppm_batch();
+    if (!b)
+        return PPPM_ERR_NOMEM;
+    b->scenes.assign(scenes, scenes + nscenes);
+    int rc = batch_create(hs.data(), nscenes, &b->impl);
+    if (rc)
+    {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return PPPM_OK;
+}
+
+int pppm_batch_destroy(pppm_batch *b)
+{
+    if (!b)
+        return PPPM_OK;
+    batch_destroy(b->impl);
+    delete b;
+    return PPPM_OK;
+}
+
+int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, int acc_on_device)
+{
+    if (!b || !b->impl || !acc || !nsteps)
+        return PPPM_ERR_ARG;
+    const int n = (int)b->scenes.size();
+    std::vector<const float *> dacc(n, nullptr);
+    for (int i = 0; i < n; i++)
+    {
+        Handle &h = b->scenes[i]->h;
+        if (nsteps[i] < 0 || (nsteps[i] > 0 && !acc[i]))
+            return PPPM_ERR_ARG;
+        if (nsteps[i] == 0)
+            continue;
+        cudaSetDevice(h.prm.device);
+        if (acc_on_device)
+            dacc[i] = acc[i];
+        else
+        {
+            long long need = (long long)nsteps[i] * h.nt;
+            if (need > h.acc_cap)
+            {
+                dev_free(h.d_acc);
+                h.d_acc = nullptr;
+                PB_TRY(dalloc(&h.d_acc, (size_t)need));
+                h.acc_cap = need;
+            }
+            PB_CUDA(cudaMemcpyAsync(h.d_acc, acc[i], sizeof(float) * need, cudaMemcpyHostToDevice, h.stream));
+            dacc[i] = h.d_acc;
+        }
+        PB_TRY(ensure_series(h, nsteps[i]));
+    }
+    return batch_run(b->impl, dacc.data(), nsteps);
 }
 
 int pppm_add_listener(pppm_handle *ph, int x, int y, int z)

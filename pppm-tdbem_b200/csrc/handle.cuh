@@ -81,6 +81,8 @@ struct Handle
     int *d_scan_tmp = nullptr;   // scan scratch
     size_t scan_tmp_elems = 0;
     int *d_flags = nullptr;      // res^3 scratch
+    int *d_pair_work = nullptr;  // face-pair recompute scan + list, 2 (pf + 1) ints, grown
+    long long pair_work_cap = 0;
 
     // ---- corrected cells and 3^3 pairs
     int n3 = 0;
@@ -208,6 +210,11 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 int step_prime(Handle &h);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state
+// batched scenes (step.cu): one set of stage launches advances every scene
+struct Batch;
+int batch_create(Handle **hs, int n, Batch **out);
+int batch_run(Batch *b, const float *const *dacc, const int *nsteps);  // dacc: device rows per scene
+void batch_destroy(Batch *b);
 int hist_import(Handle &h);  // reference-layout rings -> the step's history copies
 int hist_export(Handle &h);  // the step's history copies -> reference-layout rings
 

@@ -20,6 +20,7 @@
 // Inside a convolution a warp handles two pairs at a time, one lane per tap, so weights
 // (fp16 pairs) and history (16 consecutive ring slots) are read as coalesced 64-byte runs;
 // partial sums stay in registers and are reduced once per triangle / cell.  No atomics.
+#include <algorithm>
 #include "handle.cuh"
 
 namespace pb
@@ -288,16 +289,14 @@ __device__ inline void finish_cell(const StepArgs &a, long long row, long long c
             series[row * a.n_listen + l] = v;
 }
 
+// the stencil work of block b of one scene's stencil grid (256 threads)
 template <typename R>
-__global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int k,
-                                                       StencilSplit sp, const unsigned *corr_mask, R *series)
+__device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, int b, StencilSplit sp,
+                                    const unsigned *corr_mask, R *series)
 {
-    const StepArgs &a = a0;
-    const StepDyn dy = bind_step(st, k, a0.nt);
     R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
     const R *prev = ring.slot(dy.tnew - 2);
     const int res = a.res;
-    int b = blockIdx.x;
     if (b < sp.nb_bd)
     {
         const int m = res - 2;
@@ -327,6 +326,14 @@ __global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ St
     int i = b * 256 + threadIdx.x;
     if (i < a.nt && dy.acc)
         ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ StepArgs a0,
+                                                       const __grid_constant__ Ring<R> ring, const StepState *st, int k,
+                                                       StencilSplit sp, const unsigned *corr_mask, R *series)
+{
+    stencil_body<R>(a0, ring, bind_step(st, k, a0.nt), blockIdx.x, sp, corr_mask, series);
 }
 
 // split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
@@ -452,21 +459,31 @@ __device__ inline R warp_sum(R v)
 
 // face stage: one warp per centre triangle.  The 8 far-field corner terms are fetched first
 // (lanes 0-7) so their latency overlaps the convolution.
+// the face-stage work of one scene's centre triangle tri (whole warp)
 template <typename R>
-__global__ void __launch_bounds__(256) face_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
-                                                    const int *face_start, const int *face_nbr,
-                                                    const typename WRec<R>::T *face_w, const float2 *face_scale,
-                                                    const int *face_corner, const float *interp,
-                                                    const double *interp_d, const double *denom, float reflect)
+struct FaceArgs
+{
+    const int *face_start, *face_nbr, *face_corner;
+    const typename WRec<R>::T *face_w;
+    const float2 *face_scale;
+    const float *interp;
+    const double *interp_d, *denom;
+    float reflect;
+};
+
+template <typename R>
+__device__ inline void face_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, const FaceArgs<R> &f,
+                                 int tri, int lane)
 {
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
-    const StepArgs &a = a0;
-    const StepDyn dy = bind_step(st, kstep, a0.nt);
-    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    if (tri >= a.nt)
-        return;
+    const int *face_start = f.face_start, *face_nbr = f.face_nbr, *face_corner = f.face_corner;
+    const typename WRec<R>::T *face_w = f.face_w;
+    const float2 *face_scale = f.face_scale;
+    const float *interp = f.interp;
+    const double *interp_d = f.interp_d, *denom = f.denom;
+    const float reflect = f.reflect;
+    const int g = lane >> 2, q = lane & 3;
     const R *next = ring.slot(dy.tnew);
     const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
     const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
@@ -503,27 +520,45 @@ __global__ void __launch_bounds__(256) face_kernel(const __grid_constant__ StepA
         ring.hrow(1, lane, tri)[hist_index(lane, dy.tnew)] = (R)(num / denom[tri]);  // lane c: copy c
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) face_kernel(const __grid_constant__ StepArgs a0,
+                                                    const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
+                                                    const __grid_constant__ FaceArgs<R> f)
+{
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (tri < a0.nt)
+        face_body<R>(a0, ring, bind_step(st, kstep, a0.nt), f, tri, threadIdx.x & 31);
+}
+
 // near stage: warps stride over the corrected cells (their number changes with the mesh, the
 // grid does not).  The FDTD-near rows are stored shifted by one tap (row[k] = record tap
 // k + 1, row[15] = 0), so both rows pair with the same history window.  prime != 0: only the
 // next step's FDTD-near sum.
 template <typename R>
-__global__ void __launch_bounds__(256) near_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
-                                                    const int *n3_cell, const int *n3_start, const int *p3_tri,
-                                                    const typename WRec<R>::T *w3, const float2 *w3_scale, R *series,
-                                                    int prime)
+struct NearArgs
+{
+    const int *n3_cell, *n3_start, *p3_tri;
+    const typename WRec<R>::T *w3;
+    const float2 *w3_scale;
+    R *series;
+};
+
+// the near-stage work of corrected cells warp0, warp0 + nwarps, ... < n3 of one scene
+template <typename R>
+__device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, const NearArgs<R> &na,
+                                 int n3, int warp0, int nwarps, int lane, int prime)
 {
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
-    const StepArgs &a = a0;
-    const StepDyn dy = bind_step(st, kstep, a0.nt);
+    const int *n3_cell = na.n3_cell, *n3_start = na.n3_start, *p3_tri = na.p3_tri;
+    const typename WRec<R>::T *w3 = na.w3;
+    const float2 *w3_scale = na.w3_scale;
+    R *series = na.series;
     R *cur = ring.slot(dy.tnew), *nextslot = ring.slot(dy.tnew + 1);
-    const int n3 = st->n3;
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    const int nwarps = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    const int g = lane >> 2, q = lane & 3;
     const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);
     const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
-    for (int ci = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < n3; ci += nwarps)
+    for (int ci = warp0; ci < n3; ci += nwarps)
     {
         const int b = n3_start[ci], e = n3_start[ci + 1];
         R acc_f = 0, acc_b = 0;
@@ -563,6 +598,16 @@ __global__ void __launch_bounds__(256) near_kernel(const __grid_constant__ StepA
             }
         }
     }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) near_kernel(const __grid_constant__ StepArgs a0,
+                                                    const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
+                                                    const __grid_constant__ NearArgs<R> na, int prime)
+{
+    near_body<R>(a0, ring, bind_step(st, kstep, a0.nt), na, st->n3,
+                 (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5),
+                 (int)(((long long)gridDim.x * blockDim.x) >> 5), threadIdx.x & 31, prime);
 }
 
 template <typename R>
@@ -611,12 +656,8 @@ struct StepLaunch
     const StepState *st;
     const unsigned *corr_mask;
     R *series;
-    const int *face_start, *face_nbr, *face_corner, *n3_cell, *n3_start, *p3_tri;
-    const W *face_w, *w3;
-    const float2 *face_scale, *w3_scale;
-    const float *interp;
-    const double *interp_d, *denom;
-    float reflect;
+    FaceArgs<R> fa;
+    NearArgs<R> na;
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
 };
 
@@ -640,6 +681,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.ring.hist = (R *)h.d_hist;
     L.ring.nt = h.mesh_set ? h.nt : 0;
     L.series = (R *)h.d_series;
+    L.na.series = L.series;
     L.mesh = h.mesh_set ? 1 : 0;
     L.pml = h.prm.pml_width > 0 ? 1 : 0;
     const int m = h.res - 2, T = 256;
@@ -647,20 +689,20 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.stencil_blocks = L.sp.nb_in + L.sp.nb_bd + L.sp.nb_nt;
     if (h.mesh_set)
     {
-        L.face_start = h.d_face_start;
-        L.face_nbr = h.d_face_nbr;
-        L.face_corner = h.d_face_corner;
-        L.face_w = (const W *)h.d_face_w;
-        L.face_scale = h.fp64 ? nullptr : h.d_face_scale;
-        L.interp = h.d_face_interp;
-        L.interp_d = h.fp64 ? h.d_face_interp_d : nullptr;
-        L.denom = h.d_face_denom;
-        L.reflect = h.prm.reflect_coeff;
-        L.n3_cell = h.d_n3_cell;
-        L.n3_start = h.d_n3_start;
-        L.p3_tri = h.d_p3_tri;
-        L.w3 = (const W *)h.d_w3;
-        L.w3_scale = h.fp64 ? nullptr : h.d_w3_scale;
+        L.fa.face_start = h.d_face_start;
+        L.fa.face_nbr = h.d_face_nbr;
+        L.fa.face_corner = h.d_face_corner;
+        L.fa.face_w = (const W *)h.d_face_w;
+        L.fa.face_scale = h.fp64 ? nullptr : h.d_face_scale;
+        L.fa.interp = h.d_face_interp;
+        L.fa.interp_d = h.fp64 ? h.d_face_interp_d : nullptr;
+        L.fa.denom = h.d_face_denom;
+        L.fa.reflect = h.prm.reflect_coeff;
+        L.na.n3_cell = h.d_n3_cell;
+        L.na.n3_start = h.d_n3_start;
+        L.na.p3_tri = h.d_p3_tri;
+        L.na.w3 = (const W *)h.d_w3;
+        L.na.w3_scale = h.fp64 ? nullptr : h.d_w3_scale;
         L.face_blocks = (int)div_up((long long)h.nt * 32, T);
         if (h.near_blocks <= 0)
         {
@@ -690,13 +732,10 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
         cudaEventRecord(timed->ev[1], s);
     if (L.mesh)
     {
-        face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.face_start, L.face_nbr, L.face_w,
-                                                   L.face_scale, L.face_corner, L.interp, L.interp_d, L.denom,
-                                                   L.reflect);
+        face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.fa);
         if (timed)
             cudaEventRecord(timed->ev[2], s);
-        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
-                                                   L.w3_scale, L.series, 0);
+        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
     }
     if (timed)
         cudaEventRecord(timed->ev[3], s);
@@ -808,8 +847,8 @@ int prime(Handle &h)
     StepLaunch<R> L;
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
-    near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.n3_cell, L.n3_start, L.p3_tri, L.w3,
-                                                        L.w3_scale, nullptr, 1);
+    L.na.series = nullptr;
+    near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.na, 1);
     h.launches += 2;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
@@ -874,6 +913,363 @@ int step_free(Handle &h)
     dev_free(h.d_state);
     h.d_state = nullptr;
     return PPPM_OK;
+}
+
+}  // namespace pb
+
+// ---------------------------------------------------------------- batched scenes -------
+//
+// Many scenes advance together: one launch of each stage kernel covers every active scene.
+// A block finds its scene and its place in that scene's grid in a per-stage block map, then
+// runs the same stage code as a single-scene launch on that scene's descriptor, so every
+// scene's results are bit-identical to running it alone.  Scenes with fewer steps drop out:
+// the run is split into phases with a fixed active set, and each phase replays a recorded
+// CUDA graph of G steps (plus a kernel that advances every active scene's step state by G).
+namespace pb
+{
+namespace
+{
+
+template <typename R>
+struct BatchScene
+{
+    StepArgs a;
+    Ring<R> ring;
+    StencilSplit sp;
+    const unsigned *corr_mask;
+    R *series;
+    FaceArgs<R> fa;
+    NearArgs<R> na;
+    StepState *st;
+    int near_warps;  // warps of this scene's near grid
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) batch_stencil_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    stencil_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), m.y, S.sp, S.corr_mask, S.series);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) batch_face_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    const int tri = m.y * 8 + (threadIdx.x >> 5);
+    if (tri < S.a.nt)
+        face_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), S.fa, tri, threadIdx.x & 31);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) batch_near_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    near_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), S.na, S.st->n3, m.y * 8 + (threadIdx.x >> 5), S.near_warps,
+                 threadIdx.x & 31, 0);
+}
+
+// after G steps: every active scene's state moves on by G steps
+__global__ void batch_advance_kernel(StepState *const *states, const int *nt, int n, int g)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    StepState *st = states[i];
+    st->tnew0 += g;
+    st->row0 += g;
+    if (st->acc)
+        st->acc += (long long)g * nt[i];
+}
+
+}  // namespace
+}  // namespace pb
+
+namespace pb
+{
+
+struct BatchGraph
+{
+    std::vector<unsigned char> sig;
+    cudaGraphExec_t exec = nullptr;
+};
+
+constexpr int kBatchGraphSteps = 16;  // steps per replayed graph
+constexpr int kBatchGraphs = 16;      // recorded graphs kept per batch
+
+struct Batch
+{
+    std::vector<Handle *> hs;
+    bool fp64 = false;
+    cudaStream_t stream = nullptr;  // the first scene's stream
+    cudaEvent_t ev = nullptr;
+    std::vector<unsigned char> host_scenes;
+    std::vector<int2> host_map[3];
+    std::vector<StepState *> host_states;
+    std::vector<int> host_nt;
+    void *d_scenes = nullptr;
+    size_t scenes_cap = 0;
+    int2 *d_map[3] = {nullptr, nullptr, nullptr};
+    size_t map_cap[3] = {0, 0, 0};
+    StepState **d_states = nullptr;
+    int *d_nt = nullptr;
+    size_t states_cap = 0, nt_cap = 0;
+    BatchGraph graphs[kBatchGraphs];
+    int graph_next = 0;
+    long long launches = 0;
+};
+
+namespace
+{
+
+template <typename T>
+int grow(T **p, size_t &cap, size_t need)
+{
+    if (need <= cap)
+        return PPPM_OK;
+    dev_free(*p);
+    *p = nullptr;
+    size_t nc = need + need / 2 + 16;
+    PB_TRY(dev_alloc((void **)p, nc * sizeof(T)));
+    cap = nc;
+    return PPPM_OK;
+}
+
+// descriptors, block maps and state pointers of the active scenes, uploaded on b.stream
+template <typename R>
+int batch_tables(Batch &b, const std::vector<int> &active)
+{
+    const int T = 256;
+    const size_t na = active.size();
+    b.host_scenes.assign(na * sizeof(BatchScene<R>), 0);
+    for (auto &m : b.host_map)
+        m.clear();
+    b.host_states.resize(na);
+    b.host_nt.resize(na);
+    for (size_t ai = 0; ai < na; ai++)
+    {
+        Handle &h = *b.hs[active[ai]];
+        StepLaunch<R> L;
+        PB_TRY(make_launch<R>(h, L));
+        BatchScene<R> S;
+        memset(&S, 0, sizeof(S));
+        S.a = L.a;
+        S.ring = L.ring;
+        S.sp = L.sp;
+        S.corr_mask = L.corr_mask;
+        S.series = L.series;
+        S.fa = L.fa;
+        S.na = L.na;
+        S.st = h.d_state;
+        const int near_blocks = std::max(1, div_up((long long)h.n3 * 32, T));
+        S.near_warps = near_blocks * (T / 32);
+        memcpy(b.host_scenes.data() + ai * sizeof(S), &S, sizeof(S));
+        for (int k = 0; k < L.stencil_blocks; k++)
+            b.host_map[0].push_back(make_int2((int)ai, k));
+        for (int k = 0; k < div_up(h.nt, T / 32); k++)
+            b.host_map[1].push_back(make_int2((int)ai, k));
+        for (int k = 0; k < near_blocks; k++)
+            b.host_map[2].push_back(make_int2((int)ai, k));
+        b.host_states[ai] = h.d_state;
+        b.host_nt[ai] = h.nt;
+    }
+    void *ds = b.d_scenes;
+    PB_TRY(grow((unsigned char **)&ds, b.scenes_cap, b.host_scenes.size()));
+    b.d_scenes = ds;
+    PB_CUDA(cudaMemcpyAsync(b.d_scenes, b.host_scenes.data(), b.host_scenes.size(), cudaMemcpyHostToDevice, b.stream));
+    for (int i = 0; i < 3; i++)
+    {
+        PB_TRY(grow(&b.d_map[i], b.map_cap[i], b.host_map[i].size()));
+        PB_CUDA(cudaMemcpyAsync(b.d_map[i], b.host_map[i].data(), b.host_map[i].size() * sizeof(int2),
+                                cudaMemcpyHostToDevice, b.stream));
+    }
+    PB_TRY(grow(&b.d_states, b.states_cap, na));
+    PB_TRY(grow(&b.d_nt, b.nt_cap, na));
+    PB_CUDA(cudaMemcpyAsync(b.d_states, b.host_states.data(), na * sizeof(StepState *), cudaMemcpyHostToDevice,
+                            b.stream));
+    PB_CUDA(cudaMemcpyAsync(b.d_nt, b.host_nt.data(), na * sizeof(int), cudaMemcpyHostToDevice, b.stream));
+    return PPPM_OK;
+}
+
+// the graph of g steps of the active set described by the current tables
+template <typename R>
+int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
+{
+    std::vector<unsigned char> sig(b.host_scenes);
+    const void *ptrs[] = {b.d_scenes, b.d_map[0], b.d_map[1], b.d_map[2], b.d_states, b.d_nt};
+    const size_t sizes[] = {b.host_map[0].size(), b.host_map[1].size(), b.host_map[2].size(), (size_t)g,
+                            (size_t)nactive};
+    sig.insert(sig.end(), (const unsigned char *)ptrs, (const unsigned char *)ptrs + sizeof(ptrs));
+    sig.insert(sig.end(), (const unsigned char *)sizes, (const unsigned char *)sizes + sizeof(sizes));
+    for (auto &gr : b.graphs)
+        if (gr.exec && gr.sig == sig)
+        {
+            *out = gr.exec;
+            return PPPM_OK;
+        }
+    BatchGraph &gr = b.graphs[b.graph_next];
+    b.graph_next = (b.graph_next + 1) % kBatchGraphs;
+    if (gr.exec)
+        cudaGraphExecDestroy(gr.exec);
+    gr.exec = nullptr;
+    const BatchScene<R> *sc = (const BatchScene<R> *)b.d_scenes;
+    const int n0 = (int)b.host_map[0].size(), n1 = (int)b.host_map[1].size(), n2 = (int)b.host_map[2].size();
+    cudaGraph_t graph = nullptr;
+    PB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < g; k++)
+    {
+        batch_stencil_kernel<R><<<n0, 256, 0, b.stream>>>(sc, b.d_map[0], k);
+        if (n1 > 0)
+            batch_face_kernel<R><<<n1, 256, 0, b.stream>>>(sc, b.d_map[1], k);
+        if (n2 > 0)
+            batch_near_kernel<R><<<n2, 256, 0, b.stream>>>(sc, b.d_map[2], k);
+    }
+    batch_advance_kernel<<<div_up(nactive, 128), 128, 0, b.stream>>>(b.d_states, b.d_nt, nactive, g);
+    cudaError_t e = cudaStreamEndCapture(b.stream, &graph);
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+    {
+        gr.exec = nullptr;
+        set_error("recording the batch graph failed: %s", cudaGetErrorString(e));
+        return PPPM_ERR_CUDA;
+    }
+    gr.sig.swap(sig);
+    *out = gr.exec;
+    return PPPM_OK;
+}
+
+template <typename R>
+int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
+{
+    const int n = (int)b.hs.size();
+    // work queued on the scenes' own streams comes first
+    for (Handle *h : b.hs)
+        if (h->stream != b.stream)
+        {
+            PB_CUDA(cudaEventRecord(b.ev, h->stream));
+            PB_CUDA(cudaStreamWaitEvent(b.stream, b.ev, 0));
+        }
+    for (int i = 0; i < n; i++)
+    {
+        Handle &h = *b.hs[i];
+        if (!h.d_state)
+            PB_TRY(dalloc(&h.d_state, 1));
+        StepState stt{h.t + 1, h.n3, h.series_count, dacc[i]};
+        set_state_kernel<<<1, 1, 0, b.stream>>>(h.d_state, stt);
+        b.launches++;
+    }
+    PB_CHECK_LAUNCH();
+    std::vector<int> ends;
+    for (int i = 0; i < n; i++)
+        if (nsteps[i] > 0)
+            ends.push_back(nsteps[i]);
+    std::sort(ends.begin(), ends.end());
+    ends.erase(std::unique(ends.begin(), ends.end()), ends.end());
+    int done = 0;
+    for (int end : ends)
+    {
+        std::vector<int> active;
+        for (int i = 0; i < n; i++)
+            if (nsteps[i] > done)
+                active.push_back(i);
+        PB_TRY(batch_tables<R>(b, active));
+        int left = end - done;
+        while (left > 0)
+        {
+            const int g = std::min(left, kBatchGraphSteps);
+            cudaGraphExec_t exec = nullptr;
+            PB_TRY(batch_graph<R>(b, g, (int)active.size(), &exec));
+            PB_CUDA(cudaGraphLaunch(exec, b.stream));
+            b.launches += 3ll * g + 1;
+            left -= g;
+        }
+        done = end;
+    }
+    for (int i = 0; i < n; i++)
+    {
+        Handle &h = *b.hs[i];
+        h.t += nsteps[i];
+        h.series_count += nsteps[i];
+        h.launches += 3ll * nsteps[i];
+    }
+    // later work on the scenes' streams waits for the batch
+    PB_CUDA(cudaEventRecord(b.ev, b.stream));
+    for (Handle *h : b.hs)
+        if (h->stream != b.stream)
+            PB_CUDA(cudaStreamWaitEvent(h->stream, b.ev, 0));
+    return PPPM_OK;
+}
+
+}  // namespace
+
+int batch_create(Handle **hs, int n, Batch **out)
+{
+    *out = nullptr;
+    if (!hs || n <= 0)
+        return PPPM_ERR_ARG;
+    for (int i = 0; i < n; i++)
+    {
+        if (!hs[i] || !hs[i]->mesh_set)
+        {
+            set_error("batch scene %d has no mesh", i);
+            return PPPM_ERR_STATE;
+        }
+        if (hs[i]->prm.pml_width > 0 || hs[i]->fp64 != hs[0]->fp64 || hs[i]->prm.device != hs[0]->prm.device)
+        {
+            set_error("batch scenes must share device and precision and use the absorbing boundary (scene %d)", i);
+            return PPPM_ERR_ARG;
+        }
+        for (int j = 0; j < i; j++)
+            if (hs[j] == hs[i])
+            {
+                set_error("scene %d appears twice in the batch", i);
+                return PPPM_ERR_ARG;
+            }
+    }
+    Batch *b = new (std::nothrow) Batch();
+    if (!b)
+        return PPPM_ERR_NOMEM;
+    b->hs.assign(hs, hs + n);
+    b->fp64 = hs[0]->fp64;
+    b->stream = hs[0]->stream;
+    if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess)
+    {
+        delete b;
+        set_error("cudaEventCreate failed");
+        return PPPM_ERR_CUDA;
+    }
+    *out = b;
+    return PPPM_OK;
+}
+
+int batch_run(Batch *b, const float *const *dacc, const int *nsteps)
+{
+    cudaSetDevice(b->hs[0]->prm.device);
+    return b->fp64 ? batch_run_t<double>(*b, dacc, nsteps) : batch_run_t<float>(*b, dacc, nsteps);
+}
+
+void batch_destroy(Batch *b)
+{
+    if (!b)
+        return;
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    for (auto &g : b->graphs)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
+    dev_free(b->d_scenes);
+    for (auto *m : b->d_map)
+        dev_free(m);
+    dev_free(b->d_states);
+    dev_free(b->d_nt);
+    if (b->ev)
+        cudaEventDestroy(b->ev);
+    delete b;
 }
 
 }  // namespace pb

@@ -355,3 +355,57 @@ class Solver:
         check(lib.pppm_kernel_times(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(n)),
               "kernel_times")
         return a.value, b.value, c.value, n.value
+
+
+class Batch:
+    """Scenes advanced together: one set of stage launches per step covers every scene
+    (pppm_batch_*).  Each scene keeps its own state, listeners and series; results equal
+    those of stepping each Solver alone."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
+        self.h = ctypes.c_void_p()
+        check(lib.pppm_batch_create(arr, len(self.solvers), ctypes.byref(self.h)), "batch_create")
+
+    def run(self, accs):
+        """accs[i]: (nsteps_i, nt_i) float32 host arrays or CUDA tensors (all of one kind)."""
+        n = len(self.solvers)
+        if len(accs) != n:
+            raise ValueError("one acceleration block per scene")
+        def on_device(a):
+            return bool(getattr(a, "is_cuda", False))
+
+        on_dev = on_device(accs[0])
+        keep = []
+        ptrs = (ctypes.c_void_p * n)()
+        steps = (ctypes.c_int * n)()
+        for i, a in enumerate(accs):
+            if on_device(a) != on_dev:
+                raise ValueError("acceleration blocks must all be on the device or all on the host")
+            if hasattr(a, "data_ptr"):  # torch tensor (CUDA, or host memory such as pinned buffers)
+                if not a.is_contiguous() or a.dtype.itemsize != 4:
+                    raise ValueError("tensor must be contiguous float32")
+                if a.dim() == 2 and a.shape[0] and a.shape[1] != self.solvers[i].nt:
+                    raise ValueError("scene %d: acceleration rows need %d values" % (i, self.solvers[i].nt))
+                ptrs[i] = a.data_ptr()
+                steps[i] = a.shape[0]
+            else:
+                a = np.ascontiguousarray(a, dtype=np.float32)
+                if a.ndim != 2 or (a.shape[0] and a.shape[1] != self.solvers[i].nt):
+                    raise ValueError("scene %d: accelerations must be (nsteps, %d)" % (i, self.solvers[i].nt))
+                keep.append(a)
+                ptrs[i] = a.ctypes.data
+                steps[i] = a.shape[0]
+        check(lib.pppm_batch_run(self.h, ptrs, steps, 1 if on_dev else 0), "batch_run")
+
+    def close(self):
+        if self.h:
+            lib.pppm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
