@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--steps", type=int, default=60, help="timed benchmark steps (motion frames)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch"])
+    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--summarize-launches", metavar="CSV",
@@ -435,6 +435,11 @@ def run_batch(args, ws, rank, local):
     value = BATCH_SCENES * K * ws / (ms_b * 1e-3)
     seq = BATCH_SCENES * reps_s * ws / (ms_s * 1e-3)
     cell_steps = sum(float(sp["res"]) ** 3 * sp["steps"] for sp in specs)
+    # compulsory bytes of the whole job (per-step kernel bytes of each scene x its steps)
+    job_bytes = 0.0
+    for sp, s in zip(specs, solvers):
+        counts = [int(x) for x in s.dump("counts")]
+        job_bytes += sum(algorithmic_bytes(counts, sp["res"], len(sp["tris"])).values()) * sp["steps"]
 
     e2e = None
     if not args.no_e2e:
@@ -476,8 +481,102 @@ def run_batch(args, ws, rank, local):
         "sequential": {"value": round(seq, 3), "unit": "scenes/s", "reps": reps_s, "ms_per_rep": round(ms_s / reps_s, 3),
                        "gpu_launches_per_rep": int(launches_s // reps_s), "listeners_bit_identical": bool(same)},
         "batched_over_sequential": round(value / seq, 3),
+        "roofline": {"bound": "hbm", "kernel": "all step kernels of the job", "traffic": None,
+                     "algorithmic_bytes_per_bench_step": int(job_bytes),
+                     "achieved": round(job_bytes * K / (ms_b * 1e-3) / 1e9, 1),
+                     "achieved_sequential": round(job_bytes * reps_s / (ms_s * 1e-3) / 1e9, 1),
+                     "peak": measured_peak()[0], "unit": "GB/s", "peak_kind": measured_peak()[1],
+                     "frac": round(job_bytes * K / (ms_b * 1e-3) / 1e9 / measured_peak()[0], 4)},
         "gcell_steps_per_s": round(cell_steps * K * ws / (ms_b * 1e-3) / 1e9, 3),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
+# ---------------------------------------------------------------- adjoint -------------
+ADJ_NAME = ("moving-scene geometry held static at res 48 (5120-tri perturbed sphere + 1280-tri plate), "
+            "4000 steps, loss ||s - s_target||^2, gradient w.r.t. every acceleration (FP32)")
+
+
+def run_adjoint(args, ws, rank, local):
+    """Cost of the gradient against the forward run: one benchmark step = the 4000-step forward
+    run (pppm_step, device-resident accelerations) and the adjoint sweep over the same steps
+    (pppm_adjoint from dL/dsignal on the device)."""
+    import torch
+
+    from pppm_b200 import Solver
+
+    W, K = args.warmup, args.steps
+    sc = scenes.MovingScene(res=48)
+    nsteps = 4000
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    s = Solver(sc.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+    s.set_mesh(sc.frame_verts(0), sc.tris)
+    s.add_listener(*sc.listener)
+    acc = torch.from_numpy(sc.acc(0, nsteps)).to(dev)
+    target = torch.zeros((nsteps, 1), dtype=torch.float32, device=dev)
+    sig = torch.empty((nsteps, 1), dtype=torch.float32, device=dev)
+    t0 = s.t
+
+    def forward():
+        s.reset_fields()
+        s.rewind_listeners()
+        s.t = t0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record(stream)
+        s.step(acc)
+        e1.record(stream)
+        s.series(0, nsteps, out=sig)
+        return e0, e1
+
+    def backward():
+        g = 2 * (sig - target)
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        grad = s.adjoint(g, fresh=True)
+        e1.record(stream)
+        return e0, e1, grad
+
+    for _ in range(W):
+        forward()
+        backward()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    launches0 = s.launch_count()
+    f_ms = b_ms = 0.0
+    for _ in range(K):
+        f0, f1 = forward()
+        b0, b1, grad = backward()
+        b1.synchronize()
+        f_ms += f0.elapsed_time(f1)
+        b_ms += b0.elapsed_time(b1)
+    barrier(ws)
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    f_ms, b_ms = max_over_ranks(ws, f_ms), max_over_ranks(ws, b_ms)
+    finite = bool(torch.isfinite(grad).all().item())
+    s.close()
+    ratio = b_ms / f_ms
+    cells = float(sc.res) ** 3
+    return {
+        "metric": "adjoint / forward cost, %s" % ADJ_NAME, "value": round(ratio, 4), "unit": "x forward",
+        "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": round((f_ms + b_ms) / K, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded mesh and accelerations)",
+        "config": {"workload": ADJ_NAME, "res": sc.res, "triangles": int(len(sc.tris)), "time_steps": nsteps,
+                   "bench_step": "forward run + adjoint sweep", "l2": "flushed (256 MiB write) before each timed run",
+                   "parallelism": "replicas x%d" % ws},
+        "forward_us_per_step": round(f_ms * 1e3 / (K * nsteps), 3),
+        "adjoint_us_per_step": round(b_ms * 1e3 / (K * nsteps), 3),
+        "forward_gcell_steps_per_s": round(cells * nsteps * K * ws / (f_ms * 1e-3) / 1e9, 3),
+        "adjoint_gcell_steps_per_s": round(cells * nsteps * K * ws / (b_ms * 1e-3) / 1e9, 3),
+        "gradient_finite": finite, "cpu_baseline": None, "e2e": None, "gpu_launches": int(launches), "clocks": clk,
     }
 
 
@@ -529,6 +628,9 @@ def run_reference(args, ws, rank, local):
     W, K = args.warmup, args.steps
     if args.workload == "batch":
         return run_reference_batch(args)
+    if args.workload == "adjoint":
+        return {"impl": "reference", "metric": "adjoint / forward cost, %s" % ADJ_NAME,
+                "unavailable": "the reference has no adjoint"}
     wl = Workload(args.workload, W + K)
     sc = wl.scene
     from oracle import oracle as O
@@ -670,6 +772,8 @@ def main():
         line = run_reference(args, ws, rank, local)
     elif args.workload == "batch":
         line = run_batch(args, ws, rank, local)
+    elif args.workload == "adjoint":
+        line = run_adjoint(args, ws, rank, local)
     else:
         line = run_ours(args, ws, rank, local)
     if rank == 0 and line is not None:

@@ -94,7 +94,15 @@ int pppm_clear_listeners(pppm_handle *h);
 int pppm_listener_count(pppm_handle *h, int *nsteps, int *nlisteners);
 /* Copy recorded samples [first, first + count) x nlisteners into out (host). */
 int pppm_read_listeners(pppm_handle *h, int first, int count, float *out);
+/* No counterpart in the reference.  The same samples in the handle's element type (float for
+ * FP32 handles, double for FP64), into a device buffer on the handle's stream (on_device != 0,
+ * returns once queued) or a host buffer; non-finite samples are not checked. */
+int pppm_read_listeners_raw(pppm_handle *h, int first, int count, void *out, int on_device);
 int pppm_rewind_listeners(pppm_handle *h);
+
+/* No counterpart in the reference.  The CUDA stream every call of the handle queues its work on
+ * (the one given in pppm_params, or the handle's own), for ordering other work against it. */
+int pppm_get_stream(pppm_handle *h, void **stream);
 
 /* Current time index t (fdtd.t). */
 int pppm_get_time(pppm_handle *h, int *t);
@@ -105,7 +113,7 @@ int pppm_set_time(pppm_handle *h, int t);
 int pppm_reset_fields(pppm_handle *h);
 
 /* Whole solver state (grids, histories, PML fields, t) into / from a caller-owned host
- * buffer: cross-fade restart (demo/main.cu:215-244) and adjoint checkpoints. */
+ * buffer: cross-fade restart (demo/main.cu:215-244). */
 int pppm_state_size(pppm_handle *h, size_t *bytes);
 int pppm_save_state(pppm_handle *h, void *dst, size_t bytes);
 int pppm_restore_state(pppm_handle *h, const void *src, size_t bytes);
@@ -172,13 +180,21 @@ int pppm_batch_destroy(pppm_batch *b);
 int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, int acc_on_device);
 
 /* ------------------------------------------------------------ adjoint ---------------- */
-/* Gradient of L = sum_s sum_l g[s][l] * p_l(s) over the next nsteps forward steps from the
- * current state, with geometry and labels held fixed: dL/dacc[s][tri].  No reference
- * counterpart.  acc: nsteps x nt forward inputs (host); dL_dsignal: nsteps x nlisteners
- * (host); dL_dacc out: nsteps x nt (host).  Checkpoints every `checkpoint_every` steps; the
- * forward state is advanced by nsteps on return. */
-int pppm_adjoint(pppm_handle *h, const float *acc, int nsteps, const float *dL_dsignal, int checkpoint_every,
-                 float *dL_dacc);
+/* No counterpart in the reference.  Gradient of L = sum_s sum_l dL_dsignal[s][l] * p_l(s)
+ * over nsteps consecutive forward steps with respect to those steps' accelerations,
+ * dL_dacc[s][tri], with the geometry, the labels and so every weight table held as they are
+ * now (the absorbing boundary; PML handles return PPPM_ERR_ARG).  The listener samples are
+ * linear in the accelerations, so the gradient does not depend on the forward state and no
+ * forward state is stored: the transposed step runs backwards in time on adjoint state of the
+ * forward state's size.  fresh != 0 starts a new reverse sweep (the nsteps steps are the last
+ * ones of the differentiated run); fresh == 0 continues the sweep the previous call left,
+ * for the nsteps steps just before the ones that call covered (a long run differentiated in
+ * chunks, latest chunk first).  Element type: float for FP32 handles, double for FP64
+ * handles.  dL_dsignal: nsteps x nlisteners; dL_dacc: nsteps x nt; both device pointers on
+ * the handle's stream when on_device != 0 (the call returns once the work is queued), else
+ * host buffers (the call returns with dL_dacc written).  Listeners must lie in
+ * [1, res-2]^3.  Changing the geometry between chunks of one sweep returns PPPM_ERR_STATE. */
+int pppm_adjoint(pppm_handle *h, const void *dL_dsignal, int nsteps, int on_device, int fresh, void *dL_dacc);
 
 /* ------------------------------------------------------------ weight diagnostics ----- */
 /* TDBEM::init (bem.h:264-277) as this library evaluates it on the host: lambda and the 16

@@ -145,6 +145,8 @@ int refresh_listeners(Handle &h)
 void free_mesh(Handle &h)
 {
     cudaStreamSynchronize(h.stream);
+    adjoint_free(h);
+    h.mesh_version++;
     cache_free(h);
     void **ptrs[] = {(void **)&h.d_verts,      (void **)&h.d_tris,        (void **)&h.d_center,
                      (void **)&h.d_normal,     (void **)&h.d_area,        (void **)&h.d_cellc,
@@ -403,6 +405,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
         return rc;
     }
     h.mesh_set = true;
+    h.mesh_version++;
     PB_TRY(step_prime(h));
     PB_TRY(refresh_listeners(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
@@ -420,6 +423,7 @@ int pppm_update_mesh(pppm_handle *ph, const float *verts, int verts_on_device)
     cudaSetDevice(h.prm.device);
     PB_CUDA(cudaMemcpyAsync(h.d_verts, verts, sizeof(float) * 3 * h.nv,
                             verts_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h.stream));
+    h.mesh_version++;
     PB_TRY(mesh_build(h));
     PB_TRY(cache_refresh(h));
     PB_TRY(step_prime(h));
@@ -540,6 +544,45 @@ int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, in
     return batch_run(b->impl, dacc.data(), nsteps);
 }
 
+int pppm_adjoint(pppm_handle *ph, const void *dL_dsignal, int nsteps, int on_device, int fresh, void *dL_dacc)
+{
+    PB_TRY(check_handle(ph));
+    Handle &h = ph->h;
+    if (!h.mesh_set)
+    {
+        set_error("adjoint needs a mesh");
+        return PPPM_ERR_STATE;
+    }
+    if (h.prm.pml_width > 0)
+    {
+        set_error("the adjoint covers the absorbing boundary; this handle uses the PML");
+        return PPPM_ERR_ARG;
+    }
+    const int nl = (int)h.listen_xyz.size() / 3;
+    for (int k = 0; k < 3 * nl; k++)
+        if (h.listen_xyz[k] < 1 || h.listen_xyz[k] > h.res - 2)
+        {
+            set_error("adjoint: listener %d lies on the outer ghost layer", k / 3);
+            return PPPM_ERR_ARG;
+        }
+    if (nsteps < 0 || (nsteps > 0 && ((!dL_dsignal && nl > 0) || !dL_dacc)))
+        return PPPM_ERR_ARG;
+    if (nsteps == 0)
+        return PPPM_OK;
+    cudaSetDevice(h.prm.device);
+    const size_t gb = (size_t)nsteps * nl * h.real_size, ob = (size_t)nsteps * h.nt * h.real_size;
+    if (on_device)
+        return adjoint_run(h, dL_dsignal, nsteps, dL_dacc, fresh);
+    void *dg = nullptr, *dout = nullptr;
+    PB_TRY(adjoint_stage(h, std::max<size_t>(gb, 16), ob, &dg, &dout));
+    if (gb)
+        PB_CUDA(cudaMemcpyAsync(dg, dL_dsignal, gb, cudaMemcpyHostToDevice, h.stream));
+    PB_TRY(adjoint_run(h, dg, nsteps, dout, fresh));
+    PB_CUDA(cudaMemcpyAsync(dL_dacc, dout, ob, cudaMemcpyDeviceToHost, h.stream));
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    return PPPM_OK;
+}
+
 int pppm_add_listener(pppm_handle *ph, int x, int y, int z)
 {
     PB_TRY(check_handle(ph));
@@ -619,6 +662,32 @@ int pppm_read_listeners(pppm_handle *ph, int first, int count, float *out)
             set_error("non-finite listener sample at step %lld", (long long)first + (long long)(i / nl));
             return PPPM_ERR_NAN;
         }
+    return PPPM_OK;
+}
+
+int pppm_read_listeners_raw(pppm_handle *ph, int first, int count, void *out, int on_device)
+{
+    PB_TRY(check_handle(ph));
+    Handle &h = ph->h;
+    const int nl = (int)h.listen_xyz.size() / 3;
+    if (!out || first < 0 || count < 0 || first + (long long)count > h.series_count)
+        return PPPM_ERR_ARG;
+    if (count == 0 || nl == 0)
+        return PPPM_OK;
+    const size_t n = (size_t)count * nl * h.real_size;
+    PB_CUDA(cudaMemcpyAsync(out, (const char *)h.d_series + (size_t)first * nl * h.real_size, n,
+                            on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h.stream));
+    if (!on_device)
+        PB_CUDA(cudaStreamSynchronize(h.stream));
+    return PPPM_OK;
+}
+
+int pppm_get_stream(pppm_handle *ph, void **stream)
+{
+    PB_TRY(check_handle(ph));
+    if (!stream)
+        return PPPM_ERR_ARG;
+    *stream = (void *)ph->h.stream;
     return PPPM_OK;
 }
 
@@ -1013,6 +1082,7 @@ int pppm_import_grid_cache(pppm_handle *ph, const void *records, size_t bytes)
         return PPPM_ERR_STATE;
     if (!records || bytes < (size_t)h.nt * 54 * 72)
         return PPPM_ERR_ARG;
+    h.mesh_version++;
     PB_TRY(cache_import_grid(h, records));
     PB_TRY(step_prime(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
@@ -1027,6 +1097,7 @@ int pppm_import_face_cache(pppm_handle *ph, const int *face_pairs, const void *r
         return PPPM_ERR_STATE;
     if (!face_pairs || !records || npairs < 0)
         return PPPM_ERR_ARG;
+    h.mesh_version++;
     PB_TRY(cache_import_face(h, face_pairs, records, npairs));
     PB_TRY(step_prime(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));

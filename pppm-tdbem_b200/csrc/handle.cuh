@@ -162,6 +162,10 @@ struct Handle
     int graph_next = 0;
     int near_blocks = 0;  // resident grid of the near kernel
 
+    // ---- adjoint (adjoint.cu): transposed tables and adjoint state, built on first use
+    long long mesh_version = 0;  // bumped whenever the lists or weight tables change
+    struct Adjoint *adj = nullptr;
+
     // ---- scratch for accelerations
     float *d_acc = nullptr;
     long long acc_cap = 0;
@@ -198,6 +202,12 @@ int dgrow(T **p, long long &cap, long long need, cudaStream_t s)
 int mesh_build(Handle &h);                      // geometry + all lists from d_verts/d_tris
 int exclusive_scan(Handle &h, const int *in, int *out, long long n);  // out[n] = total
 int read_int(Handle &h, const int *d, int *out);
+
+// adjoint.cu
+struct Adjoint;
+int adjoint_run(Handle &h, const void *g, int nsteps, void *out, int fresh);  // device buffers
+int adjoint_stage(Handle &h, size_t g_bytes, size_t out_bytes, void **g, void **out);
+void adjoint_free(Handle &h);
 
 // cache.cu
 int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators

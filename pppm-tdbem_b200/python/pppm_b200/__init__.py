@@ -81,7 +81,9 @@ def _load():
         "pppm_batch_create": [ctypes.POINTER(vp), i, ctypes.POINTER(vp)],
         "pppm_batch_destroy": [vp],
         "pppm_batch_run": [vp, ctypes.POINTER(vp), ip, i],
-        "pppm_adjoint": [vp, vp, i, vp, i, vp],
+        "pppm_adjoint": [vp, vp, i, i, i, vp],
+        "pppm_read_listeners_raw": [vp, i, i, vp, i],
+        "pppm_get_stream": [vp, ctypes.POINTER(vp)],
         "pppm_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "pppm_enable_timing": [vp, i],
         "pppm_kernel_times": [vp, fp, fp, fp, ip],
@@ -266,6 +268,69 @@ class Solver:
             check(lib.pppm_read_listeners(self.h, first, count, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
                   "read_listeners")
         return out
+
+    @property
+    def stream(self):
+        """cudaStream_t (int) the solver queues its work on."""
+        v = ctypes.c_void_p()
+        check(lib.pppm_get_stream(self.h, ctypes.byref(v)), "get_stream")
+        return v.value or 0
+
+    @property
+    def series_count(self):
+        n, nl = ctypes.c_int(), ctypes.c_int()
+        check(lib.pppm_listener_count(self.h, ctypes.byref(n), ctypes.byref(nl)), "listener_count")
+        return n.value
+
+    @property
+    def n_listeners(self):
+        n, nl = ctypes.c_int(), ctypes.c_int()
+        check(lib.pppm_listener_count(self.h, ctypes.byref(n), ctypes.byref(nl)), "listener_count")
+        return nl.value
+
+    def series(self, first=0, count=None, out=None):
+        """Listener samples [first, first + count) in the handle's precision: a host array, or
+        written into `out` (a contiguous CUDA tensor of that dtype, queued on the solver's
+        stream)."""
+        if count is None:
+            count = self.series_count - first
+        nl = self.n_listeners
+        if out is not None:
+            if not out.is_contiguous() or out.numel() != count * nl or out.element_size() != np.dtype(self.real).itemsize:
+                raise ValueError("out must be a contiguous (%d, %d) tensor of the handle's precision" % (count, nl))
+            check(lib.pppm_read_listeners_raw(self.h, first, count, ctypes.c_void_p(out.data_ptr()), 1 if out.is_cuda else 0),
+                  "read_listeners_raw")
+            return out
+        a = np.zeros((count, nl), self.real)
+        if count and nl:
+            check(lib.pppm_read_listeners_raw(self.h, first, count, a.ctypes.data_as(ctypes.c_void_p), 0),
+                  "read_listeners_raw")
+        return a
+
+    def adjoint(self, dL_dsignal, fresh=True, out=None):
+        """dL/dacc (nsteps, nt) for L = sum dL_dsignal * listener samples over the last nsteps
+        steps differentiated (pppm_adjoint).  fresh=False continues the previous call's reverse
+        sweep with the steps just before it.  Host arrays in, host array out; CUDA tensors in,
+        CUDA tensor out (queued on the solver's stream)."""
+        nl = self.n_listeners
+        if hasattr(dL_dsignal, "data_ptr") and getattr(dL_dsignal, "is_cuda", False):
+            import torch
+
+            g = dL_dsignal.contiguous()
+            if g.element_size() != np.dtype(self.real).itemsize:
+                raise ValueError("gradient dtype must match the handle's precision")
+            n = g.shape[0]
+            if out is None:
+                out = torch.empty((n, self.nt), dtype=g.dtype, device=g.device)
+            check(lib.pppm_adjoint(self.h, ctypes.c_void_p(g.data_ptr()), n, 1, 1 if fresh else 0,
+                                   ctypes.c_void_p(out.data_ptr())), "adjoint")
+            return out
+        g = np.ascontiguousarray(dL_dsignal, dtype=self.real).reshape(-1, nl)
+        n = g.shape[0]
+        res = np.zeros((n, self.nt), self.real)
+        check(lib.pppm_adjoint(self.h, g.ctypes.data_as(ctypes.c_void_p), n, 0, 1 if fresh else 0,
+                               res.ctypes.data_as(ctypes.c_void_p)), "adjoint")
+        return res
 
     def rewind_listeners(self):
         check(lib.pppm_rewind_listeners(self.h), "rewind_listeners")
