@@ -175,9 +175,13 @@ def algorithmic_bytes(counts, res, nt):
     m = res - 2
     n3, p3, pf = counts[0], counts[1], counts[4]
     abc = 6 * m * m
-    stencil = 12 * m ** 3 + 16 * abc + 4 * n3 + 8 * nt  # p^t, p^{t-1}, p^{t+1}; ghost writes; corrections; acc->ring
-    face = pf * (64 + 8 + 4) + nt * (8 * 4 + 8 * 4 + 8 * 4 + 8 + 8 + 4) + nt * 2 * 64
-    near = p3 * (2 * 64 + 2 * 8 + 4) + n3 * (4 + 4 + 4 + 4 + 4) + nt * 2 * 64
+    stencil = 12 * m ** 3 + 16 * abc + 4 * n3 + 16 * nt  # p^t, p^{t-1}, p^{t+1}; ghosts; corrections; acc -> 4 ring copies
+    # face pairs (weights 64, scale 8, neighbour index 4); per triangle: corners, interpolation
+    # weights, far-field values, start, denominator, 4 Dirichlet copies, its own history windows;
+    # the near-field terms: 54 grid-cache records (64 + scale 8) read, 54 terms written
+    face = pf * (64 + 8 + 4) + nt * (8 * 4 + 8 * 4 + 8 * 4 + 8 + 8 + 16 + 2 * 64) + nt * 54 * (64 + 8 + 4)
+    # per pair: triangle index 4, record offset 1, two terms 8; per cell: index, start, p read/write, next
+    near = p3 * (4 + 1 + 8) + n3 * (4 + 8 + 4 + 4 + 4)
     return {"stencil": stencil, "face": face, "near": near}
 
 

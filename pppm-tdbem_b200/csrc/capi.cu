@@ -160,13 +160,14 @@ void free_mesh(Handle &h)
                      (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
                      (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
-                     (void **)&h.d_hist};
+                     (void **)&h.d_hist,       (void **)&h.d_terms};
     for (void **q : ptrs)
     {
         dev_free(*q);
         *q = nullptr;
     }
     h.p3_cap = h.n4_cap = h.pf_cap = 0;
+    h.n3_cells_cap = h.b4_cells_cap = 0;
     h.n3 = h.b4 = 0;
     h.p3 = h.p4 = h.pf = 0;
     h.nv = h.nt = 0;
@@ -395,6 +396,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_CUDA(cudaMemsetAsync(h.d_neumann, 0, (size_t)nt * kRing * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)nt * kRing * h.real_size, h.stream));
     PB_TRY(dev_alloc(&h.d_hist, (size_t)8 * nt * kRing * h.real_size));
+    PB_TRY(dev_alloc(&h.d_terms, (size_t)54 * nt * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
     if (rc == PPPM_OK)

@@ -93,6 +93,7 @@ struct Handle
     void *d_w3 = nullptr;
     float2 *d_w3_scale = nullptr;
     long long p3_cap = 0;
+    long long n3_cells_cap = 0, b4_cells_cap = 0;  // n3_cell / n3_start, b4_cell / b4_start
     unsigned *d_corr_mask = nullptr;
 
     // ---- base cells and 4^3 lists
@@ -135,6 +136,7 @@ struct Handle
     // ---- histories
     void *d_neumann = nullptr, *d_dirichlet = nullptr;  // reference layout: read-out and loading
     void *d_hist = nullptr;  // the step's copies: [Neumann, Dirichlet][4 copies][nt][kRing] (step.cu)
+    void *d_terms = nullptr;  // nt x 54 near-field terms of the current step (step.cu: near_terms)
 
     // ---- listeners
     std::vector<int> listen_xyz;

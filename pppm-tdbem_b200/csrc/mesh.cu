@@ -440,20 +440,24 @@ int mesh_build(Handle &h)
 
     h.n3 = n3;
     h.b4 = b4;
+    // compact arrays grow only: stable addresses keep the recorded step graphs valid across
+    // updates, and no cudaFree (a device-wide synchronisation) runs per motion frame
+    if (n3 + 1 > h.n3_cells_cap)
     {
-        long long cap3 = 0;
-        (void)cap3;
+        long long cap = 0;
+        PB_TRY(dgrow(&h.d_n3_cell, cap, n3 + 1, s));
+        cap = 0;
+        PB_TRY(dgrow(&h.d_n3_start, cap, n3 + 1, s));
+        h.n3_cells_cap = cap;
     }
-    // (re)allocate compact arrays
-    dev_free(h.d_n3_cell);
-    dev_free(h.d_n3_start);
-    dev_free(h.d_b4_cell);
-    dev_free(h.d_b4_start);
-    h.d_n3_cell = h.d_n3_start = h.d_b4_cell = h.d_b4_start = nullptr;
-    PB_TRY(dalloc(&h.d_n3_cell, (size_t)n3 + 1));
-    PB_TRY(dalloc(&h.d_n3_start, (size_t)n3 + 1));
-    PB_TRY(dalloc(&h.d_b4_cell, (size_t)b4 + 1));
-    PB_TRY(dalloc(&h.d_b4_start, (size_t)b4 + 1));
+    if (b4 + 1 > h.b4_cells_cap)
+    {
+        long long cap = 0;
+        PB_TRY(dgrow(&h.d_b4_cell, cap, b4 + 1, s));
+        cap = 0;
+        PB_TRY(dgrow(&h.d_b4_start, cap, b4 + 1, s));
+        h.b4_cells_cap = cap;
+    }
     int *n3_len = h.d_base_count;  // scratch (nc entries available)
     compact_kernel<<<div_up(nc, T), T, 0, s>>>(flag3, pos3, len3, nc, h.d_n3_cell, n3_len);
     h.launches++;

@@ -392,7 +392,71 @@ struct FaceArgs
     const float *interp;
     const double *interp_d, *denom;
     float reflect;
+    // near-field terms of every triangle (see near_terms): its 54 grid-cache records
+    const typename WRec<R>::T *gc_w;
+    const float2 *gc_scale;
+    R *terms;  // [nt][54]
 };
+
+constexpr int kGcRecords = 54;  // per triangle: 27 FDTD-near then 27 BEM-near records (offsets in 3^3)
+
+// The near-field terms of one triangle at time t (whole warp): for each of its 54 grid-cache
+// records (27 offsets x {FDTD-near, BEM-near}) the record's convolution with the triangle's OWN
+// history window, terms[tri][r].  A corrected cell's two sums are then plain sums of these terms
+// over its 3^3 list (near_gather_body): each triangle's history is read once per step instead of
+// once per corrected cell around it, and the records stream contiguously.  The FDTD-near terms
+// belong to the next step: record tap k + 1 pairs with history tap k (taps t..t-14).  Lane q of
+// quad g takes taps 4q..4q+3 of records g, g + 8, ...; d0 != 0 replaces Dirichlet tap 0 (time t)
+// with dnew, the value this warp has just computed.
+template <typename R>
+__device__ inline void near_terms(const Ring<R> &ring, int t, const FaceArgs<R> &f, int tri, int lane, bool d0,
+                                  R dnew)
+{
+    using W4 = typename WRec<R>::W4;
+    using H4 = typename WRec<R>::H4;
+    const int g = lane >> 2, q = lane & 3;
+    const int copy = t & 3, off = (hist_index(copy, t) + 4 * q) & (kRing - 1);
+    const H4 hn = *(const H4 *)(ring.hrow(0, copy, tri) + off);
+    H4 hd = *(const H4 *)(ring.hrow(1, copy, tri) + off);
+    if (d0 && q == 0)
+        hd.v[0] = dnew;
+    // history taps 4q-1 .. 4q+2 for the shifted FDTD-near records (tap -1 does not exist: 0)
+    H4 sn, sd;
+    const R pn = __shfl_up_sync(kFull, hn.v[3], 1), pd = __shfl_up_sync(kFull, hd.v[3], 1);
+    sn.v[0] = q ? pn : (R)0;
+    sd.v[0] = q ? pd : (R)0;
+#pragma unroll
+    for (int i = 1; i < 4; i++)
+    {
+        sn.v[i] = hn.v[i - 1];
+        sd.v[i] = hd.v[i - 1];
+    }
+    const unsigned quad = 0xfu << (lane & ~3);
+    const typename WRec<R>::T *rec = f.gc_w + (long long)tri * kGcRecords * kTaps;
+    R *out = f.terms + (long long)tri * kGcRecords;
+    for (int r = g; r < kGcRecords; r += 8)
+    {
+        const W4 w = *(const W4 *)(rec + (long long)r * kTaps + 4 * q);
+        const float2 s = f.gc_scale ? f.gc_scale[(long long)tri * kGcRecords + r] : make_float2(1, 1);
+        R v = 0;
+        if (r < kGcRecords / 2)
+        {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                v += conv_tap(w.v[i], s, sn.v[i], sd.v[i]);
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                v += conv_tap(w.v[i], s, hn.v[i], hd.v[i]);
+        }
+        v += __shfl_xor_sync(quad, v, 1);
+        v += __shfl_xor_sync(quad, v, 2);
+        if (q == 0)
+            out[r] = v;
+    }
+}
 
 template <typename R>
 __device__ inline void face_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, const FaceArgs<R> &f,
@@ -439,8 +503,20 @@ __device__ inline void face_body(const StepArgs &a, const Ring<R> &ring, const S
     for (int wi = 0; wi < 8; wi++)
         far_sum += __shfl_sync(kFull, iw, wi) * __shfl_sync(kFull, pv, wi);
     R num = far_sum * (R)reflect + acc;
+    const R dnew = (R)(num / denom[tri]);
     if (lane < 4)
-        ring.hrow(1, lane, tri)[hist_index(lane, dy.tnew)] = (R)(num / denom[tri]);  // lane c: copy c
+        ring.hrow(1, lane, tri)[hist_index(lane, dy.tnew)] = dnew;  // lane c: copy c
+    near_terms<R>(ring, dy.tnew, f, tri, lane, true, dnew);
+}
+
+// the near-field terms of time t for every triangle without a face step (priming)
+template <typename R>
+__global__ void __launch_bounds__(256) terms_kernel(const __grid_constant__ Ring<R> ring, int nt, int t,
+                                                     const __grid_constant__ FaceArgs<R> f)
+{
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (tri < nt)
+        near_terms<R>(ring, t, f, tri, threadIdx.x & 31, false, (R)0);
 }
 
 template <typename R>
@@ -454,15 +530,15 @@ __global__ void __launch_bounds__(256) face_kernel(const __grid_constant__ StepA
 }
 
 // near stage: warps stride over the corrected cells (their number changes with the mesh, the
-// grid does not).  The FDTD-near rows are stored shifted by one tap (row[k] = record tap
-// k + 1, row[15] = 0), so both rows pair with the same history window.  prime != 0: only the
+// grid does not).  A corrected cell's FDTD-near sum (for the next step) and BEM-near sum are the
+// sums of its pairs' terms (near_terms), lanes striding over the pair list.  prime != 0: only the
 // next step's FDTD-near sum.
 template <typename R>
 struct NearArgs
 {
     const int *n3_cell, *n3_start, *p3_tri;
-    const typename WRec<R>::T *w3;
-    const float2 *w3_scale;
+    const unsigned char *p3_woff;  // the pair's record offset in 3^3
+    const R *terms;
     R *series;
 };
 
@@ -471,45 +547,24 @@ template <typename R>
 __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, const NearArgs<R> &na,
                                  int n3, int warp0, int nwarps, int lane, int prime)
 {
-    using W4 = typename WRec<R>::W4;
-    using H4 = typename WRec<R>::H4;
-    const int *n3_cell = na.n3_cell, *n3_start = na.n3_start, *p3_tri = na.p3_tri;
-    const typename WRec<R>::T *w3 = na.w3;
-    const float2 *w3_scale = na.w3_scale;
-    R *series = na.series;
     R *cur = ring.slot(dy.tnew), *nextslot = ring.slot(dy.tnew + 1);
-    const int g = lane >> 2, q = lane & 3;
-    const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);
-    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
     for (int ci = warp0; ci < n3; ci += nwarps)
     {
-        const int b = n3_start[ci], e = n3_start[ci + 1];
+        const int b = na.n3_start[ci], e = na.n3_start[ci + 1];
         R acc_f = 0, acc_b = 0;
-        for (int p = b + g; p < e; p += 8)
+        for (int p = b + lane; p < e; p += 32)
         {
-            const W4 wf = *(const W4 *)(w3 + (long long)p * 2 * kTaps + 4 * q);
-            const float2 sf = w3_scale ? w3_scale[2 * p] : make_float2(1, 1);
-            const int tr = p3_tri[p];
-            const H4 hn = *(const H4 *)(nbase + (long long)tr * kRing);
-            const H4 hd = *(const H4 *)(dbase + (long long)tr * kRing);
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-                acc_f += conv_tap(wf.v[i], sf, hn.v[i], hd.v[i]);
+            const R *t = na.terms + (long long)na.p3_tri[p] * kGcRecords + na.p3_woff[p];
+            acc_f += t[0];
             if (!prime)
-            {
-                const W4 wb = *(const W4 *)(w3 + (long long)p * 2 * kTaps + kTaps + 4 * q);
-                const float2 sb = w3_scale ? w3_scale[2 * p + 1] : make_float2(1, 1);
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    acc_b += conv_tap(wb.v[i], sb, hn.v[i], hd.v[i]);
-            }
+                acc_b += t[kGcRecords / 2];
         }
         acc_f = warp_sum(acc_f);
         if (!prime)
             acc_b = warp_sum(acc_b);
         if (lane == 0)
         {
-            int c = n3_cell[ci];
+            int c = na.n3_cell[ci];
             nextslot[c] = acc_f;
             if (!prime)
             {
@@ -517,7 +572,7 @@ __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const S
                 cur[c] = v;
                 for (int l = 0; l < a.n_listen; l++)
                     if (a.listen_cell[l] == c)
-                        series[dy.row * a.n_listen + l] = v;
+                        na.series[dy.row * a.n_listen + l] = v;
             }
         }
     }
@@ -621,11 +676,14 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.fa.interp_d = h.fp64 ? h.d_face_interp_d : nullptr;
         L.fa.denom = h.d_face_denom;
         L.fa.reflect = h.prm.reflect_coeff;
+        L.fa.gc_w = (const W *)h.d_gc_w;
+        L.fa.gc_scale = h.fp64 ? nullptr : h.d_gc_scale;
+        L.fa.terms = (R *)h.d_terms;
         L.na.n3_cell = h.d_n3_cell;
         L.na.n3_start = h.d_n3_start;
         L.na.p3_tri = h.d_p3_tri;
-        L.na.w3 = (const W *)h.d_w3;
-        L.na.w3_scale = h.fp64 ? nullptr : h.d_w3_scale;
+        L.na.p3_woff = h.d_p3_woff;
+        L.na.terms = (const R *)h.d_terms;
         L.face_blocks = (int)div_up((long long)h.nt * 32, T);
         if (h.near_blocks <= 0)
         {
@@ -771,8 +829,9 @@ int prime(Handle &h)
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
     L.na.series = nullptr;
+    terms_kernel<R><<<div_up((long long)h.nt * 32, 256), 256, 0, h.stream>>>(L.ring, h.nt, h.t, L.fa);
     near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.na, 1);
-    h.launches += 2;
+    h.launches += 3;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
 }
