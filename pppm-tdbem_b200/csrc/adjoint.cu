@@ -113,8 +113,9 @@ struct AdjArgs
     using W = typename AdjWRec<R>::T;
     int res, nt, n3, nl, ncorner;
     long long ncells;
-    int listen_cell[8], listen_corr[8];
+    int listen_cell[8];
     const int *n3_cell;
+    const unsigned *corr_mask;  // corrected-cell bits
     const int *fT_start, *fT_src;
     const W *fT_w;
     const float2 *fT_scale;
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(256) adj_cells_kernel(const __grid_constant__ 
         const int c = a.n3_cell[i];
         R v = cur[c];
         for (int l = 0; l < a.nl; l++)
-            if (a.listen_corr[l] && a.listen_cell[l] == c)
+            if (a.listen_cell[l] == c)
                 v += g[l];
         cur[c] = v;
         ring_put<R>(a.ring_p, a.n3, i, sigma, (R)0.98 * v);
@@ -171,8 +172,11 @@ __global__ void __launch_bounds__(256) adj_cells_kernel(const __grid_constant__ 
     }
     else if (i == a.n3)
         for (int l = 0; l < a.nl; l++)
-            if (!a.listen_corr[l])
-                cur[a.listen_cell[l]] += g[l];
+        {
+            const int c = a.listen_cell[l];
+            if (!((a.corr_mask[c >> 5] >> (c & 31)) & 1u))  // corrected cells: done above
+                cur[c] += g[l];
+        }
 }
 
 template <typename R>
@@ -621,10 +625,10 @@ AdjArgs<R> make_adj_args(Handle &h, Adjoint &A)
     for (int l = 0; l < a.nl; l++)
     {
         a.listen_cell[l] = (h.listen_xyz[3 * l] * h.res + h.listen_xyz[3 * l + 1]) * h.res + h.listen_xyz[3 * l + 2];
-        a.listen_corr[l] = l < (int)h.listen_corr.size() ? h.listen_corr[l] : 0;
     }
     a.ncorner = A.ncorner;
     a.n3_cell = h.d_n3_cell;
+    a.corr_mask = h.d_corr_mask;
     a.fT_start = A.fT_start;
     a.fT_src = A.fT_src;
     a.fT_w = (const W *)A.fT_w;

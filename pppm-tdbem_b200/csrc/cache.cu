@@ -856,24 +856,22 @@ int cache_refresh(Handle &h)
             h.pool_cap, h.d_pool_meta, h.d_face_pool, h.d_pair_flag, h.d_status);
         h.launches++;
         PB_CHECK_LAUNCH();
-        int st = 0;
-        PB_TRY(read_int(h, h.d_status, &st));
-        if (st)
-        {
-            set_error("face cache: more than %d distinct neighbours seen by one face", kFaceCacheSlots);
-            return st;
-        }
-        int used = 0;
-        PB_TRY(read_int(h, h.d_pool_count, &used));
-        h.pool_used = used;
-
-        // compact the recompute list
+        // compact the recompute list; one synchronisation reads the lookup status, the pool
+        // size and the number of pairs to recompute
         PB_TRY(dgrow(&h.d_pair_work, h.pair_work_cap, 2 * (h.pf + 1), s));
         int *pos = h.d_pair_work;
         int *work = h.d_pair_work + (h.pf + 1);
         PB_TRY(exclusive_scan(h, h.d_pair_flag, pos, h.pf));
-        int nwork = 0;
-        PB_TRY(read_int(h, pos + h.pf, &nwork));
+        int v[3];
+        const int *src[3] = {h.d_status, h.d_pool_count, pos + h.pf};
+        PB_TRY(read_ints(h, src, 3, v));
+        if (v[0])
+        {
+            set_error("face cache: more than %d distinct neighbours seen by one face", kFaceCacheSlots);
+            return v[0];
+        }
+        h.pool_used = v[1];
+        const int nwork = v[2];
         if (nwork > 0)
         {
             compact_pairs_kernel<<<div_up(h.pf, T), T, 0, s>>>(h.d_pair_flag, pos, h.pf, work);

@@ -121,26 +121,6 @@ int check_handle(pppm_handle *p)
     return PPPM_OK;
 }
 
-int refresh_listeners(Handle &h)
-{
-    int n = (int)h.listen_xyz.size() / 3;
-    h.listen_corr.assign(n, 0);
-    if (n > 0 && h.mesh_set && h.n3 > 0)
-    {
-        std::vector<unsigned> mask((h.n_cells + 31) / 32);
-        PB_CUDA(cudaMemcpyAsync(mask.data(), h.d_corr_mask, mask.size() * sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                h.stream));
-        PB_CUDA(cudaStreamSynchronize(h.stream));
-        for (int l = 0; l < n; l++)
-        {
-            long long c = ((long long)h.listen_xyz[3 * l] * h.res + h.listen_xyz[3 * l + 1]) * h.res +
-                          h.listen_xyz[3 * l + 2];
-            h.listen_corr[l] = (mask[c >> 5] >> (c & 31)) & 1u;
-        }
-    }
-    return PPPM_OK;
-}
-
 // release every array sized by the mesh (a failed set_mesh leaves the handle mesh-free)
 void free_mesh(Handle &h)
 {
@@ -167,7 +147,6 @@ void free_mesh(Handle &h)
         *q = nullptr;
     }
     h.p3_cap = h.n4_cap = h.pf_cap = 0;
-    h.n3_cells_cap = h.b4_cells_cap = 0;
     h.n3 = h.b4 = 0;
     h.p3 = h.p4 = h.pf = 0;
     h.nv = h.nt = 0;
@@ -319,6 +298,12 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
     }
     for (int i = 0; i < 4; i++)
         cudaEventCreate(&h.ev[i]);
+    if (cudaMallocHost((void **)&h.h_pin, kPinnedInts * sizeof(int)) != cudaSuccess)
+    {
+        h.h_pin = nullptr;
+        set_error("cudaMallocHost failed");
+        return fail(PPPM_ERR_NOMEM);
+    }
     tdbem_init(h.tc, p->dt, p->dl, p->c);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess)
     {
@@ -354,6 +339,8 @@ int pppm_destroy(pppm_handle *ph)
     for (int i = 0; i < 4; i++)
         if (h.ev[i])
             cudaEventDestroy(h.ev[i]);
+    if (h.h_pin)
+        cudaFreeHost(h.h_pin);
     if (h.own_stream && h.stream)
         cudaStreamDestroy(h.stream);
     delete ph;
@@ -409,7 +396,6 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     h.mesh_set = true;
     h.mesh_version++;
     PB_TRY(step_prime(h));
-    PB_TRY(refresh_listeners(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
     return PPPM_OK;
 }
@@ -429,7 +415,6 @@ int pppm_update_mesh(pppm_handle *ph, const float *verts, int verts_on_device)
     PB_TRY(mesh_build(h));
     PB_TRY(cache_refresh(h));
     PB_TRY(step_prime(h));
-    PB_TRY(refresh_listeners(h));
     return PPPM_OK;
 }
 
@@ -607,7 +592,7 @@ int pppm_add_listener(pppm_handle *ph, int x, int y, int z)
     dev_free(h.d_series);
     h.d_series = nullptr;
     h.series_cap = 0;
-    return refresh_listeners(h);
+    return PPPM_OK;
 }
 
 int pppm_clear_listeners(pppm_handle *ph)
@@ -615,7 +600,6 @@ int pppm_clear_listeners(pppm_handle *ph)
     PB_TRY(check_handle(ph));
     Handle &h = ph->h;
     h.listen_xyz.clear();
-    h.listen_corr.clear();
     dev_free(h.d_series);
     h.d_series = nullptr;
     h.series_cap = 0;

@@ -93,7 +93,6 @@ struct Handle
     void *d_w3 = nullptr;
     float2 *d_w3_scale = nullptr;
     long long p3_cap = 0;
-    long long n3_cells_cap = 0, b4_cells_cap = 0;  // n3_cell / n3_start, b4_cell / b4_start
     unsigned *d_corr_mask = nullptr;
 
     // ---- base cells and 4^3 lists
@@ -140,7 +139,6 @@ struct Handle
 
     // ---- listeners
     std::vector<int> listen_xyz;
-    std::vector<int> listen_corr;  // 1 if the listener cell is a corrected cell
     int *d_listen_cell = nullptr, *d_listen_n3 = nullptr;
     void *d_series = nullptr;
     long long series_cap = 0;  // steps
@@ -161,12 +159,16 @@ struct Handle
     // ---- step launches
     StepState *d_state = nullptr;  // per-call values the step kernels read
     StepGraph graphs[kStepGraphs];
+    StepGraph timing_graph;  // one step with event records between its kernels (measurement mode)
     int graph_next = 0;
     int near_blocks = 0;  // resident grid of the near kernel
 
     // ---- adjoint (adjoint.cu): transposed tables and adjoint state, built on first use
     long long mesh_version = 0;  // bumped whenever the lists or weight tables change
     struct Adjoint *adj = nullptr;
+
+    // ---- pinned host words for batched reads of device counts (read_ints)
+    int *h_pin = nullptr;
 
     // ---- scratch for accelerations
     float *d_acc = nullptr;
@@ -204,6 +206,8 @@ int dgrow(T **p, long long &cap, long long need, cudaStream_t s)
 int mesh_build(Handle &h);                      // geometry + all lists from d_verts/d_tris
 int exclusive_scan(Handle &h, const int *in, int *out, long long n);  // out[n] = total
 int read_int(Handle &h, const int *d, int *out);
+constexpr int kPinnedInts = 16;
+int read_ints(Handle &h, const int *const *src, int n, int *out);  // n device words, one synchronisation
 
 // adjoint.cu
 struct Adjoint;

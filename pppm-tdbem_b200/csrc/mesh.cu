@@ -207,13 +207,19 @@ __global__ void block_counts_kernel(const int *cell_start, const int *base_start
     len4[i] = s4;
 }
 
-__global__ void compact_kernel(const int *flag, const int *pos, const int *len, long long n, int *out_cell, int *out_len)
+// flagged cells i < n -> out_cell[pos[i]] = i, out_start[pos[i]] = start[i]; out_start[pos[n]] =
+// start[n] closes the list (pos and start: exclusive scans over the n cells of the flags and of
+// the list lengths, which are 0 for cells that are not flagged)
+__global__ void compact_kernel(const int *flag, const int *pos, const int *start, long long n, int *out_cell,
+                               int *out_start)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == n)
+        out_start[pos[n]] = start[n];
     if (i >= n || !flag[i])
         return;
     out_cell[pos[i]] = (int)i;
-    out_len[pos[i]] = len[i];
+    out_start[pos[i]] = start[i];
 }
 
 // 3^3 pairs of each corrected cell, sub-cells x fastest (particle_grid.cu:164-182);
@@ -311,6 +317,18 @@ int read_int(Handle &h, const int *d, int *out)
     return PPPM_OK;
 }
 
+int read_ints(Handle &h, const int *const *src, int n, int *out)
+{
+    if (n > kPinnedInts)
+        return PPPM_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        PB_CUDA(cudaMemcpyAsync(h.h_pin + i, src[i], sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    for (int i = 0; i < n; i++)
+        out[i] = h.h_pin[i];
+    return PPPM_OK;
+}
+
 // out[0..n] exclusive prefix sums of in[0..n), out[n] = total.  Scratch: h.d_scan_tmp.
 static int scan_level(Handle &h, const int *in, int *out, long long n_in, int *scratch, long long scratch_left)
 {
@@ -379,7 +397,14 @@ int mesh_build(Handle &h)
         PB_TRY(dalloc(&h.d_cell_start, (size_t)nc + 1));
         PB_TRY(dalloc(&h.d_base_start, (size_t)nc + 1));
         PB_TRY(dalloc(&h.d_cursor, (size_t)nc + 1));
-        PB_TRY(dalloc(&h.d_flags, 4 * ((size_t)nc + 1)));
+        PB_TRY(dalloc(&h.d_flags, 6 * ((size_t)nc + 1)));
+        // compact cell lists at their upper bounds: every corrected cell is within one cell of a
+        // triangle's cell, every base cell holds a centre, so n3 <= 27 nt and b4 <= nt
+        const long long n3_max = std::min<long long>(nc, 27ll * nt) + 1, b4_max = std::min<long long>(nc, nt) + 1;
+        PB_TRY(dalloc(&h.d_n3_cell, (size_t)n3_max));
+        PB_TRY(dalloc(&h.d_n3_start, (size_t)n3_max));
+        PB_TRY(dalloc(&h.d_b4_cell, (size_t)b4_max));
+        PB_TRY(dalloc(&h.d_b4_start, (size_t)b4_max));
         PB_TRY(dalloc(&h.d_face_start, (size_t)nt + 1));
         PB_TRY(dalloc(&h.d_face_corner, 8 * (size_t)nt));
         PB_TRY(dalloc(&h.d_status, 4));
@@ -390,13 +415,8 @@ int mesh_build(Handle &h)
                                                  h.d_area, h.d_cellc, h.d_basec, h.d_cell, h.d_base, h.d_status);
     h.launches++;
     PB_CHECK_LAUNCH();
-    int st = 0;
-    PB_TRY(read_int(h, h.d_status, &st));
-    if (st)
-    {
-        set_error("mesh leaves the grid interior: every triangle must lie at least two cells inside the grid");
-        return st;
-    }
+    // (the status is read with the list sizes below: triangles outside the interior get no cell,
+    // so the list builds in between stay in bounds)
 
     // ---- per-cell and per-base-cell CSR, ids ascending inside a cell
     for (int pass = 0; pass < 2; pass++)
@@ -424,59 +444,42 @@ int mesh_build(Handle &h)
     block_counts_kernel<<<div_up(nc, T), T, 0, s>>>(h.d_cell_start, h.d_base_start, res, flag3, len3, flag4, len4);
     h.launches++;
     PB_CHECK_LAUNCH();
-    // positions of corrected cells -> d_cursor; positions of base cells -> d_count of bases
-    // (the counts were consumed by the CSR build above)
-    int *pos3 = h.d_cursor, *pos4 = h.d_base_count;
+    // Positions and list offsets of corrected cells and base cells from scans over the whole
+    // grid, so no count is needed on the host before the compaction; one synchronisation then
+    // reads the status and every size the host needs.
+    int *pos3 = h.d_cursor;                           // nc + 1
+    int *st3 = h.d_flags + 4 * (nc + 1);              // nc + 1
+    int *st4 = h.d_flags + 5 * (nc + 1);              // nc + 1
+    int *b4_pos = h.d_cell_count;                     // nc (flags of the last cell are 0: never inner)
     PB_TRY(exclusive_scan(h, flag3, pos3, nc));
-    int n3 = 0;
-    PB_TRY(read_int(h, pos3 + nc, &n3));
-    // base-cell positions need nc + 1 entries: the base_count array has only nc, so use the
-    // cell_count array (also consumed) for the last entry via a separate scan target
-    PB_TRY(exclusive_scan(h, flag4, h.d_cell_count, nc - 1));
-    (void)pos4;
-    int *b4_pos = h.d_cell_count;  // b4_pos[c] valid for flagged c < nc - 1 (the last cell is never inner)
-    int b4 = 0;
-    PB_TRY(read_int(h, b4_pos + (nc - 1), &b4));
-
+    PB_TRY(exclusive_scan(h, len3, st3, nc));
+    PB_TRY(exclusive_scan(h, flag4, b4_pos, nc - 1));
+    PB_TRY(exclusive_scan(h, len4, st4, nc));
+    compact_kernel<<<div_up(nc + 1, T), T, 0, s>>>(flag3, pos3, st3, nc, h.d_n3_cell, h.d_n3_start);
+    h.launches++;
+    compact_kernel<<<div_up(nc, T), T, 0, s>>>(flag4, b4_pos, st4, nc - 1, h.d_b4_cell, h.d_b4_start);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    // face pairs per centre triangle: length of its base cell's 4^3 list
+    int *face_len = len3;  // len3 was consumed by its scan
+    face_len_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, nt, b4_pos, flag4, h.d_b4_start, face_len);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    PB_TRY(exclusive_scan(h, face_len, h.d_face_start, nt));
+    int v[6];
+    const int *src[6] = {h.d_status, pos3 + nc, b4_pos + (nc - 1), st3 + nc, st4 + nc, h.d_face_start + nt};
+    PB_TRY(read_ints(h, src, 6, v));
+    if (v[0])
+    {
+        set_error("mesh leaves the grid interior: every triangle must lie at least two cells inside the grid");
+        return v[0];
+    }
+    const int n3 = v[1], b4 = v[2], p3 = v[3], p4 = v[4], pf = v[5];
     h.n3 = n3;
     h.b4 = b4;
-    // compact arrays grow only: stable addresses keep the recorded step graphs valid across
-    // updates, and no cudaFree (a device-wide synchronisation) runs per motion frame
-    if (n3 + 1 > h.n3_cells_cap)
-    {
-        long long cap = 0;
-        PB_TRY(dgrow(&h.d_n3_cell, cap, n3 + 1, s));
-        cap = 0;
-        PB_TRY(dgrow(&h.d_n3_start, cap, n3 + 1, s));
-        h.n3_cells_cap = cap;
-    }
-    if (b4 + 1 > h.b4_cells_cap)
-    {
-        long long cap = 0;
-        PB_TRY(dgrow(&h.d_b4_cell, cap, b4 + 1, s));
-        cap = 0;
-        PB_TRY(dgrow(&h.d_b4_start, cap, b4 + 1, s));
-        h.b4_cells_cap = cap;
-    }
-    int *n3_len = h.d_base_count;  // scratch (nc entries available)
-    compact_kernel<<<div_up(nc, T), T, 0, s>>>(flag3, pos3, len3, nc, h.d_n3_cell, n3_len);
-    h.launches++;
-    PB_CHECK_LAUNCH();
-    PB_TRY(exclusive_scan(h, n3_len, h.d_n3_start, n3));
-    int p3 = 0;
-    PB_TRY(read_int(h, h.d_n3_start + n3, &p3));
     h.p3 = p3;
-
-    // b4: compact into b4_cell with lengths in a scratch then scan.  The 3^3 scratch (len3)
-    // is free again after n3_len was written.
-    int *b4_len = len3;
-    compact_kernel<<<div_up(nc - 1, T), T, 0, s>>>(flag4, b4_pos, len4, nc - 1, h.d_b4_cell, b4_len);
-    h.launches++;
-    PB_CHECK_LAUNCH();
-    PB_TRY(exclusive_scan(h, b4_len, h.d_b4_start, b4));
-    int p4 = 0;
-    PB_TRY(read_int(h, h.d_b4_start + b4, &p4));
     h.p4 = p4;
+    h.pf = pf;
 
     // ---- 3^3 pairs and corrected-cell mask
     if (p3 > h.p3_cap)
@@ -517,14 +520,6 @@ int mesh_build(Handle &h)
     PB_CHECK_LAUNCH();
 
     // ---- face pairs per centre triangle
-    int *face_len = len3;  // scratch again (b4_len consumed by the scan)
-    face_len_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, nt, b4_pos, flag4, h.d_b4_start, face_len);
-    h.launches++;
-    PB_CHECK_LAUNCH();
-    PB_TRY(exclusive_scan(h, face_len, h.d_face_start, nt));
-    int pf = 0;
-    PB_TRY(read_int(h, h.d_face_start + nt, &pf));
-    h.pf = pf;
     if (pf > h.pf_cap)
     {
         dev_free(h.d_face_nbr);

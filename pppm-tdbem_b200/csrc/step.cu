@@ -42,7 +42,6 @@ struct StepArgs
     int nt;
     int n_listen;
     int listen_cell[8];
-    int listen_corr[8];  // 1 if the listener cell is a corrected cell
 };
 
 // what step k of a call produces: its time index, listener-series row and acceleration row
@@ -201,15 +200,18 @@ template <typename R>
 __device__ inline void finish_cell(const StepArgs &a, long long row, long long c, R v, R *next,
                                    const unsigned *corr_mask, R *series)
 {
-    if ((corr_mask[c >> 5] >> (c & 31)) & 1u)
+    const bool corrected = (corr_mask[c >> 5] >> (c & 31)) & 1u;
+    if (corrected)
     {
         R corr = next[c];
         v = v - corr;
     }
     next[c] = v;
-    for (int l = 0; l < a.n_listen; l++)
-        if (a.listen_cell[l] == (int)c && !a.listen_corr[l])
-            series[row * a.n_listen + l] = v;
+    // a listener at a corrected cell is recorded by the near stage, after its correction
+    if (!corrected)
+        for (int l = 0; l < a.n_listen; l++)
+            if (a.listen_cell[l] == (int)c)
+                series[row * a.n_listen + l] = v;
 }
 
 // the stencil work of block b of one scene's stencil grid (256 threads)
@@ -326,12 +328,14 @@ __global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepAr
             pnext[6 * ci + 3 + d] = pcur[6 * ci + 3 + d] + c * dt * r2;
         }
     }
-    if ((corr_mask[ci >> 5] >> (ci & 31)) & 1u)
+    const bool corrected = (corr_mask[ci >> 5] >> (ci & 31)) & 1u;
+    if (corrected)
         v = v - next[ci];
     next[ci] = v;
-    for (int l = 0; l < a.n_listen; l++)
-        if (a.listen_cell[l] == (int)ci && !a.listen_corr[l])
-            series[dy.row * a.n_listen + l] = v;
+    if (!corrected)
+        for (int l = 0; l < a.n_listen; l++)
+            if (a.listen_cell[l] == (int)ci)
+                series[dy.row * a.n_listen + l] = v;
 }
 
 // ---- convolution helpers
@@ -617,7 +621,6 @@ int fill_listeners(Handle &h, StepArgs &a)
     for (int l = 0; l < a.n_listen; l++)
     {
         a.listen_cell[l] = (h.listen_xyz[3 * l] * h.res + h.listen_xyz[3 * l + 1]) * h.res + h.listen_xyz[3 * l + 2];
-        a.listen_corr[l] = l < (int)h.listen_corr.size() ? h.listen_corr[l] : 0;
     }
     return PPPM_OK;
 }
@@ -703,23 +706,24 @@ template <typename R>
 void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
 {
     const int T = 256;
-    if (timed)
-        cudaEventRecord(timed->ev[0], s);
+    // timed: event records between the kernels (graph nodes when captured, see run_steps)
+    auto mark = [&](int i) {
+        if (timed)
+            cudaEventRecordWithFlags(timed->ev[i], s, cudaEventRecordExternal);
+    };
+    mark(0);
     if (L.pml)
         pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask, L.series);
     else
         stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
-    if (timed)
-        cudaEventRecord(timed->ev[1], s);
+    mark(1);
     if (L.mesh)
     {
         face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.fa);
-        if (timed)
-            cudaEventRecord(timed->ev[2], s);
+        mark(2);
         near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
     }
-    if (timed)
-        cudaEventRecord(timed->ev[3], s);
+    mark(3);
 }
 
 // Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
@@ -729,24 +733,30 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
 constexpr int kGraphSteps = 4;
 
 template <typename R>
-int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *out)
+int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *out, bool timed = false)
 {
     const unsigned char *sig = (const unsigned char *)&L;
-    for (auto &g : h.graphs)
+    StepGraph *slots = timed ? &h.timing_graph : h.graphs;
+    const int nslots = timed ? 1 : kStepGraphs;
+    for (int i = 0; i < nslots; i++)
+    {
+        StepGraph &g = slots[i];
         if (g.exec && g.nsteps == nsteps && g.sig.size() == sizeof(L) && memcmp(g.sig.data(), sig, sizeof(L)) == 0)
         {
             *out = g.exec;
             return PPPM_OK;
         }
-    StepGraph &g = h.graphs[h.graph_next];
-    h.graph_next = (h.graph_next + 1) % kStepGraphs;
+    }
+    StepGraph &g = timed ? h.timing_graph : h.graphs[h.graph_next];
+    if (!timed)
+        h.graph_next = (h.graph_next + 1) % kStepGraphs;
     if (g.exec)
         cudaGraphExecDestroy(g.exec);
     g.exec = nullptr;
     cudaGraph_t graph = nullptr;
     PB_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < nsteps; k++)
-        launch_step<R>(L, k, h.stream, nullptr);
+        launch_step<R>(L, k, h.stream, timed ? &h : nullptr);
     cudaError_t e = cudaStreamEndCapture(h.stream, &graph);
     if (e == cudaSuccess)
         e = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -781,7 +791,35 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     const long long per_step = 1 + (h.mesh_set ? 2 : 0);
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     PB_CUDA(cudaStreamIsCapturing(s, &cs));
-    if (!h.timing && cs == cudaStreamCaptureStatusNone && nsteps >= kGraphSteps)
+    if (h.timing && cs == cudaStreamCaptureStatusNone)
+    {
+        // Measurement mode: every step replays a one-step graph whose event-record nodes sit
+        // between its kernels, so each kernel's duration is measured the way it runs inside the
+        // recorded step graphs (no host launch gaps); the step state is rewritten per step.
+        cudaGraphExec_t exec = nullptr;
+        PB_TRY(graph_for<R>(h, L, 1, &exec, true));
+        for (int k = 0; k < nsteps; k++)
+        {
+            StepState sk{stt.tnew0 + k, stt.n3, stt.row0 + k,
+                         acc_dev ? acc_dev + (long long)k * (h.mesh_set ? h.nt : 0) : nullptr};
+            set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sk);
+            PB_CHECK_LAUNCH();
+            PB_CUDA(cudaGraphLaunch(exec, s));
+            PB_CUDA(cudaEventSynchronize(h.ev[3]));
+            float ta = 0, tb = 0, tc = 0;
+            cudaEventElapsedTime(&ta, h.ev[0], h.ev[1]);
+            if (h.mesh_set)
+            {
+                cudaEventElapsedTime(&tb, h.ev[1], h.ev[2]);
+                cudaEventElapsedTime(&tc, h.ev[2], h.ev[3]);
+            }
+            h.us_stencil += 1000 * ta;
+            h.us_face += 1000 * tb;
+            h.us_near += 1000 * tc;
+            h.timed_steps++;
+        }
+    }
+    else if (cs == cudaStreamCaptureStatusNone && nsteps >= kGraphSteps)
     {
         cudaGraphExec_t exec = nullptr;
         PB_TRY(graph_for<R>(h, L, nsteps, &exec));
@@ -790,24 +828,8 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     else
         for (int k = 0; k < nsteps; k++)
         {
-            launch_step<R>(L, k, s, h.timing ? &h : nullptr);
+            launch_step<R>(L, k, s, nullptr);
             PB_CHECK_LAUNCH();
-            if (h.timing)
-            {
-                // per-kernel durations, accumulated over timed steps (measurement mode only)
-                PB_CUDA(cudaEventSynchronize(h.ev[3]));
-                float ta = 0, tb = 0, tc = 0;
-                cudaEventElapsedTime(&ta, h.ev[0], h.ev[1]);
-                if (h.mesh_set)
-                {
-                    cudaEventElapsedTime(&tb, h.ev[1], h.ev[2]);
-                    cudaEventElapsedTime(&tc, h.ev[2], h.ev[3]);
-                }
-                h.us_stencil += 1000 * ta;
-                h.us_face += 1000 * tb;
-                h.us_near += 1000 * tc;
-                h.timed_steps++;
-            }
         }
     h.launches += per_step * nsteps;
     h.t += nsteps;
@@ -885,12 +907,12 @@ int step_run(Handle &h, const float *acc_dev, int nsteps)
 
 int step_free(Handle &h)
 {
-    for (auto &g : h.graphs)
+    for (auto *g : {&h.graphs[0], &h.graphs[1], &h.graphs[2], &h.graphs[3], &h.timing_graph})
     {
-        if (g.exec)
-            cudaGraphExecDestroy(g.exec);
-        g.exec = nullptr;
-        g.sig.clear();
+        if (g->exec)
+            cudaGraphExecDestroy(g->exec);
+        g->exec = nullptr;
+        g->sig.clear();
     }
     dev_free(h.d_state);
     h.d_state = nullptr;
