@@ -59,6 +59,8 @@ struct Adjoint
     void *fT_w = nullptr;                         // [pfT][16] (a_m, b_{m+1}) weight pairs
     float2 *fT_scale = nullptr;                   // [pfT] (single, double) scales (FP32 weights)
     int *nT_start = nullptr, *nT_cell = nullptr, *nT_pair = nullptr;  // per triangle: (corrected index, pair)
+    void *nT_w = nullptr;        // [p3T][2][16]: the pair's FDTD-near (shifted) and BEM-near records
+    float2 *nT_scale = nullptr;  // [p3T][2] (FP32 weights)
     int *cT_cell = nullptr, *cT_start = nullptr, *cT_ref = nullptr;    // corner cells: (tri * 8 + k)
     // adjoint state
     void *lam[3] = {nullptr, nullptr, nullptr};
@@ -120,8 +122,8 @@ struct AdjArgs
     const W *fT_w;
     const float2 *fT_scale;
     const int *nT_start, *nT_cell, *nT_pair;
-    const W *w3;
-    const float2 *w3_scale;
+    const W *nT_w;
+    const float2 *nT_scale;
     const int *cT_cell, *cT_start, *cT_ref;
     const float *interp;
     const double *interp_d, *denom;
@@ -218,16 +220,15 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ A
     R near_n = 0, near_d = 0;
     if (!flush)
     {
-        // near pairs: lamP / lamC windows sigma .. sigma + 15, the forward records in place
+        // near pairs: lamP / lamC windows sigma .. sigma + 15
         const R *wp = ring_window<R>(a.ring_p, a.n3, sigma, q), *wc = ring_window<R>(a.ring_c, a.n3, sigma, q);
         for (int p = a.nT_start[j] + g; p < a.nT_start[j + 1]; p += 8)
         {
             const int ci = a.nT_cell[p];
-            const long long pp = a.nT_pair[p];
-            const W4 rf = *(const W4 *)(a.w3 + pp * 2 * kTaps + 4 * q);
-            const W4 rb = *(const W4 *)(a.w3 + pp * 2 * kTaps + kTaps + 4 * q);
-            const float2 sf = a.w3_scale ? a.w3_scale[2 * pp] : make_float2(1, 1);
-            const float2 sb = a.w3_scale ? a.w3_scale[2 * pp + 1] : make_float2(1, 1);
+            const W4 rf = *(const W4 *)(a.nT_w + (long long)p * 2 * kTaps + 4 * q);
+            const W4 rb = *(const W4 *)(a.nT_w + (long long)p * 2 * kTaps + kTaps + 4 * q);
+            const float2 sf = a.nT_scale ? a.nT_scale[2 * p] : make_float2(1, 1);
+            const float2 sb = a.nT_scale ? a.nT_scale[2 * p + 1] : make_float2(1, 1);
             const H4 hp = *(const H4 *)(wp + (long long)ci * kRing);
             const H4 hc = *(const H4 *)(wc + (long long)ci * kRing);
 #pragma unroll
@@ -436,6 +437,33 @@ __global__ void shift_face_kernel(const typename AdjWRec<R>::T *w, const float2 
         wt[t] = make_double2(src[m].x, m + 1 < kTaps ? src[m + 1].y : 0.0);
 }
 
+// near records of the transposed pairs: pair p2 (forward pair pair[p2] of triangle p3_tri and
+// record offset p3_woff) gets its FDTD-near record shifted by one tap (row[k] = tap k + 1, the
+// step pairs it with the next step's history) and its BEM-near record
+template <typename R>
+__global__ void near_records_kernel(const typename AdjWRec<R>::T *gc_w, const float2 *gc_scale, const int *p3_tri,
+                                    const unsigned char *p3_woff, const int *pair, long long n,
+                                    typename AdjWRec<R>::T *wt, float2 *scale_t)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * kTaps)
+        return;
+    const long long p2 = t / kTaps;
+    const int k = (int)(t % kTaps);
+    const long long pp = pair[p2];
+    const long long rec = (long long)p3_tri[pp] * 54 + p3_woff[pp];
+    const auto *f = gc_w + rec * kTaps, *b = gc_w + (rec + 27) * kTaps;
+    typename AdjWRec<R>::T zero;
+    memset(&zero, 0, sizeof(zero));
+    wt[p2 * 2 * kTaps + k] = k + 1 < kTaps ? f[k + 1] : zero;
+    wt[p2 * 2 * kTaps + kTaps + k] = b[k];
+    if (k == 0 && gc_scale)
+    {
+        scale_t[2 * p2] = gc_scale[rec];
+        scale_t[2 * p2 + 1] = gc_scale[rec + 27];
+    }
+}
+
 template <typename T>
 int upload(Handle &h, T **d, const std::vector<T> &v)
 {
@@ -472,9 +500,9 @@ void transpose_csr(int nkeys, const std::vector<int> &keys, std::vector<int> &st
 
 void adj_free_tables(Adjoint &A)
 {
-    void **ptrs[] = {(void **)&A.fT_start, (void **)&A.fT_src,  &A.fT_w,  (void **)&A.fT_scale, (void **)&A.nT_start,
-                     (void **)&A.nT_cell,  (void **)&A.nT_pair, (void **)&A.cT_cell, (void **)&A.cT_start,
-                     (void **)&A.cT_ref};
+    void **ptrs[] = {(void **)&A.fT_start, (void **)&A.fT_src,   &A.fT_w,  (void **)&A.fT_scale,
+                     (void **)&A.nT_start, (void **)&A.nT_cell,  (void **)&A.nT_pair, &A.nT_w,
+                     (void **)&A.nT_scale, (void **)&A.cT_cell,  (void **)&A.cT_start, (void **)&A.cT_ref};
     for (void **p : ptrs)
     {
         dev_free(*p);
@@ -554,6 +582,14 @@ int build_tables(Handle &h, Adjoint &A)
     PB_TRY(upload(h, &A.nT_start, start));
     PB_TRY(upload(h, &A.nT_cell, cell));
     PB_TRY(upload(h, &A.nT_pair, order));
+    PB_TRY(dev_alloc(&A.nT_w, (size_t)std::max<long long>(p3, 1) * 2 * kTaps * sizeof(W)));
+    if (!h.fp64)
+        PB_TRY(dalloc(&A.nT_scale, (size_t)std::max<long long>(p3, 1) * 2));
+    if (p3 > 0)
+        near_records_kernel<R><<<div_up(p3 * kTaps, 256), 256, 0, h.stream>>>(
+            (const W *)h.d_gc_w, h.fp64 ? nullptr : h.d_gc_scale, h.d_p3_tri, h.d_p3_woff, A.nT_pair, p3,
+            (W *)A.nT_w, A.nT_scale);
+    h.launches++;
     A.p3T = p3;
 
     // corner cells
@@ -636,8 +672,8 @@ AdjArgs<R> make_adj_args(Handle &h, Adjoint &A)
     a.nT_start = A.nT_start;
     a.nT_cell = A.nT_cell;
     a.nT_pair = A.nT_pair;
-    a.w3 = (const W *)h.d_w3;
-    a.w3_scale = h.fp64 ? nullptr : h.d_w3_scale;
+    a.nT_w = (const W *)A.nT_w;
+    a.nT_scale = h.fp64 ? nullptr : A.nT_scale;
     a.cT_cell = A.cT_cell;
     a.cT_start = A.cT_start;
     a.cT_ref = A.cT_ref;

@@ -352,28 +352,6 @@ __global__ void gc_compute_kernel_d(DevConsts dc, const float *verts, const int 
 }
 
 // dense copy of the 3^3 pair records in hot-path order
-template <typename Rec>
-__global__ void gather_w3_kernel(const int *p3_tri, const unsigned char *p3_woff, long long p3, const Rec *gc_w,
-                                 const float2 *gc_scale, Rec *w3, float2 *w3_scale)
-{
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= p3 * kTaps)
-        return;
-    long long pair = p / kTaps;
-    int k = (int)(p % kTaps);
-    size_t rec = (size_t)p3_tri[pair] * 54 + p3_woff[pair];
-    // FDTD-near row shifted by one tap: the step pairs record tap k + 1 with history tap k (that
-    // sum belongs to the next step), so both rows of a pair read the same history window
-    Rec zero;
-    memset(&zero, 0, sizeof(zero));
-    w3[(pair * 2) * kTaps + k] = k < kTaps - 1 ? gc_w[rec * kTaps + k + 1] : zero;
-    w3[(pair * 2 + 1) * kTaps + k] = gc_w[(rec + 27) * kTaps + k];
-    if (k == 0 && gc_scale)
-    {
-        w3_scale[pair * 2] = gc_scale[rec];
-        w3_scale[pair * 2 + 1] = gc_scale[rec + 27];
-    }
-}
 
 // ---------------------------------------------------------------- face cache ---------
 // trilinear weights of the 2x2x2 corner cells at the face's 1-point Gauss node
@@ -800,18 +778,6 @@ int cache_refresh(Handle &h)
     h.launches++;
     PB_CHECK_LAUNCH();
     h.gc_empty = false;
-    if (h.p3 > 0)
-    {
-        if (h.fp64)
-            gather_w3_kernel<double2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(
-                h.d_p3_tri, h.d_p3_woff, h.p3, (const double2 *)h.d_gc_w, nullptr, (double2 *)h.d_w3, nullptr);
-        else
-            gather_w3_kernel<__half2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(h.d_p3_tri, h.d_p3_woff, h.p3,
-                                                                            (const __half2 *)h.d_gc_w, h.d_gc_scale,
-                                                                            (__half2 *)h.d_w3, h.d_w3_scale);
-        h.launches++;
-        PB_CHECK_LAUNCH();
-    }
 
     // ---- face cache
     const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
@@ -997,17 +963,6 @@ int cache_regather(Handle &h)
 {
     cudaStream_t s = h.stream;
     const int T = 256;
-    if (h.p3 > 0)
-    {
-        if (h.fp64)
-            gather_w3_kernel<double2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(
-                h.d_p3_tri, h.d_p3_woff, h.p3, (const double2 *)h.d_gc_w, nullptr, (double2 *)h.d_w3, nullptr);
-        else
-            gather_w3_kernel<__half2><<<div_up(h.p3 * kTaps, T), T, 0, s>>>(h.d_p3_tri, h.d_p3_woff, h.p3,
-                                                                            (const __half2 *)h.d_gc_w, h.d_gc_scale,
-                                                                            (__half2 *)h.d_w3, h.d_w3_scale);
-        h.launches++;
-    }
     if (h.pf > 0)
     {
         if (h.fp64)

@@ -135,7 +135,7 @@ void free_mesh(Handle &h)
                      (void **)&h.d_base_count, (void **)&h.d_base_start,  (void **)&h.d_base_tris,
                      (void **)&h.d_cursor,     (void **)&h.d_flags,       (void **)&h.d_n3_cell,
                      (void **)&h.d_n3_start,   (void **)&h.d_p3_tri,      (void **)&h.d_p3_woff,
-                     (void **)&h.d_w3,         (void **)&h.d_w3_scale,    (void **)&h.d_b4_cell,
+                     (void **)&h.d_b4_cell,
                      (void **)&h.d_b4_start,   (void **)&h.d_n4_tris,     (void **)&h.d_face_start,
                      (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
@@ -328,7 +328,7 @@ int pppm_destroy(pppm_handle *ph)
                     h.d_area,         h.d_cellc,         h.d_basec,        h.d_cell,          h.d_base,
                     h.d_cell_count,   h.d_cell_start,    h.d_cell_tris,    h.d_base_count,    h.d_base_start,
                     h.d_base_tris,    h.d_cursor,        h.d_scan_tmp,     h.d_flags,         h.d_n3_cell,
-                    h.d_n3_start,     h.d_p3_tri,        h.d_p3_woff,      h.d_w3,            h.d_w3_scale,
+                    h.d_n3_start,     h.d_p3_tri,        h.d_p3_woff,
                     h.d_corr_mask,    h.d_b4_cell,       h.d_b4_start,     h.d_n4_tris,       h.d_face_start,
                     h.d_face_nbr,     h.d_face_pool,     h.d_face_w,       h.d_face_scale,    h.d_face_corner,
                     h.d_pair_flag,    h.d_status,        h.d_neumann,      h.d_dirichlet,     h.d_listen_cell,

@@ -12,10 +12,10 @@
 //                  ring (copy c holds time tau at (c - tau) mod 32) so 4 taps are one aligned load
 //   cell CSR       cell_start[res^3 + 1] / cell_tris[nt] (sorted by triangle id per cell),
 //                  same for base cells
-//   3^3 pairs      n3 corrected cells: n3_cell, n3_start[n3 + 1]; p3 pairs: p3_tri,
-//                  p3_woff; dense weights w3_half[p3][2][32] + w3_scale[p3][2][2]
-//                  (FDTD-near then BEM-near, fp16 + per-row scale, the reference's format; the
-//                  FDTD-near row shifted by one tap: row[k] = record tap k + 1, row[15] = 0)
+//   3^3 pairs      n3 corrected cells: n3_cell, n3_start[n3 + 1]; p3 pairs: p3_tri, p3_woff
+//                  (the pair's record offset in the triangle's grid-cache records)
+//   near terms     terms[nt][54]: each triangle's 54 grid-cache records convolved with its own
+//                  history in the current step (step.cu); a corrected cell sums its pairs' terms
 //   face pairs     face_start[nt + 1] per centre triangle; pf pairs: face_nbr; dense
 //                  weights face_half[pf][32] + face_scale[pf][2]; per centre: 8 corner cells,
 //                  8 trilinear weights, denominator 0.5 * area - sum(factor)
@@ -90,8 +90,6 @@ struct Handle
     int *d_n3_cell = nullptr, *d_n3_start = nullptr;
     int *d_p3_tri = nullptr;
     unsigned char *d_p3_woff = nullptr;
-    void *d_w3 = nullptr;
-    float2 *d_w3_scale = nullptr;
     long long p3_cap = 0;
     unsigned *d_corr_mask = nullptr;
 
@@ -205,6 +203,8 @@ int dgrow(T **p, long long &cap, long long need, cudaStream_t s)
 // mesh.cu
 int mesh_build(Handle &h);                      // geometry + all lists from d_verts/d_tris
 int exclusive_scan(Handle &h, const int *in, int *out, long long n);  // out[n] = total
+// up to 4 independent exclusive scans in one set of launches
+int exclusive_scan_set(Handle &h, const int *const *in, int *const *out, const long long *n, int count);
 int read_int(Handle &h, const int *d, int *out);
 constexpr int kPinnedInts = 16;
 int read_ints(Handle &h, const int *const *src, int n, int *out);  // n device words, one synchronisation

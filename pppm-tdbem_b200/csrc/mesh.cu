@@ -25,8 +25,24 @@ constexpr int kScanThreads = 512;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void scan_tiles_kernel(const int *in, int *out, int *tile_sums, long long n_in, long long n_out)
+// up to kScanBatch independent scans in one launch (blockIdx.y selects the array)
+constexpr int kScanBatch = 4;
+struct ScanSet
 {
+    const int *in[kScanBatch];
+    int *out[kScanBatch];
+    int *sums[kScanBatch];  // per-tile totals, or null for single-tile arrays
+    long long n_in[kScanBatch], n_out[kScanBatch];
+};
+
+__global__ void scan_tiles_kernel(const __grid_constant__ ScanSet set)
+{
+    const int a = blockIdx.y;
+    const long long n_in = set.n_in[a], n_out = set.n_out[a];
+    if ((long long)blockIdx.x * kScanTile >= n_out)
+        return;  // block-uniform: this array has fewer tiles
+    const int *in = set.in[a];
+    int *out = set.out[a], *tile_sums = set.sums[a];
     __shared__ int warp_tot[kScanThreads / 32];
     long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -78,10 +94,15 @@ __global__ void scan_tiles_kernel(const int *in, int *out, int *tile_sums, long 
     }
 }
 
-__global__ void scan_add_kernel(int *out, const int *tile_offsets, long long n_out)
+__global__ void scan_add_kernel(const __grid_constant__ ScanSet set)
 {
+    const int a = blockIdx.y;
+    const long long n_out = set.n_out[a];
+    if ((long long)blockIdx.x * kScanTile >= n_out || !set.sums[a])
+        return;
+    int *out = set.out[a];
     long long base = (long long)blockIdx.x * kScanTile;
-    int add = tile_offsets[blockIdx.x];
+    int add = set.in[a][blockIdx.x];  // scanned tile totals
     for (int i = threadIdx.x; i < kScanTile; i += blockDim.x)
     {
         long long idx = base + i;
@@ -227,45 +248,86 @@ __global__ void compact_kernel(const int *flag, const int *pos, const int *start
 __global__ void fill_pairs3_kernel(const int *n3_cell, const int *n3_start, int n3, int res, const int *cell_start,
                                    const int *cell_tris, int *p3_tri, unsigned char *p3_woff, unsigned *mask)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n3)
+    // one warp per corrected cell: lane l < 27 copies sub-cell l's list to its offset in the
+    // cell's list (a warp prefix sum over the 27 lengths keeps the sub-cell order)
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= n3)
         return;
-    int c = n3_cell[i];
-    int x = c / (res * res), y = (c / res) % res, z = c % res;
-    int o = n3_start[i];
-    for (int idx = 0; idx < 27; idx++)
+    const int i = (int)gw;
+    const int c = n3_cell[i];
+    const int x = c / (res * res), y = (c / res) % res, z = c % res;
+    int b = 0, len = 0;
+    unsigned char woff = 0;
+    if (lane < 27)
     {
-        int dx = idx % 3 - 1, dy = idx / 3 % 3 - 1, dz = idx / 9 - 1;
-        int sc = ((x + dx) * res + (y + dy)) * res + (z + dz);
-        unsigned char woff = (unsigned char)((1 - dx) + 3 * (1 - dy) + 9 * (1 - dz));
-        for (int j = cell_start[sc]; j < cell_start[sc + 1]; j++)
-        {
-            p3_tri[o] = cell_tris[j];
-            p3_woff[o] = woff;
-            o++;
-        }
+        const int dx = lane % 3 - 1, dy = lane / 3 % 3 - 1, dz = lane / 9 - 1;
+        const int sc = ((x + dx) * res + (y + dy)) * res + (z + dz);
+        woff = (unsigned char)((1 - dx) + 3 * (1 - dy) + 9 * (1 - dz));
+        b = cell_start[sc];
+        len = cell_start[sc + 1] - b;
     }
-    atomicOr(&mask[c >> 5], 1u << (c & 31));
+    int incl = len;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        const int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off)
+            incl += v;
+    }
+    const int o = n3_start[i] + incl - len;
+    for (int j = 0; j < len; j++)
+    {
+        p3_tri[o + j] = cell_tris[b + j];
+        p3_woff[o + j] = woff;
+    }
+    if (lane == 0)
+        atomicOr(&mask[c >> 5], 1u << (c & 31));
 }
 
 // 4^3 lists of the non-empty base cells (particle_grid.cu:198-223)
 __global__ void fill_n4_kernel(const int *b4_cell, const int *b4_start, int b4, int res, const int *cell_start,
                                const int *cell_tris, int *n4_tris)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b4)
+    // one warp per base cell: lane l copies sub-cells l and l + 32 (x fastest, then y, then z)
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= b4)
         return;
-    int c = b4_cell[i];
-    int x = c / (res * res), y = (c / res) % res, z = c % res;
-    int o = b4_start[i];
-    for (int idx = 0; idx < 64; idx++)
+    const int i = (int)gw;
+    const int c = b4_cell[i];
+    const int x = c / (res * res), y = (c / res) % res, z = c % res;
+    int b[2], len[2];
+#pragma unroll
+    for (int half = 0; half < 2; half++)
     {
-        int sx = x + idx % 4 - 1, sy = y + idx / 4 % 4 - 1, sz = z + idx / 16 - 1;
-        if (sx < 0 || sy < 0 || sz < 0 || sx >= res || sy >= res || sz >= res)
-            continue;
-        int sc = (sx * res + sy) * res + sz;
-        for (int j = cell_start[sc]; j < cell_start[sc + 1]; j++)
-            n4_tris[o++] = cell_tris[j];
+        const int idx = lane + 32 * half;
+        const int sx = x + idx % 4 - 1, sy = y + idx / 4 % 4 - 1, sz = z + idx / 16 - 1;
+        b[half] = 0;
+        len[half] = 0;
+        if (sx >= 0 && sy >= 0 && sz >= 0 && sx < res && sy < res && sz < res)
+        {
+            const int sc = (sx * res + sy) * res + sz;
+            b[half] = cell_start[sc];
+            len[half] = cell_start[sc + 1] - b[half];
+        }
+    }
+    int o = b4_start[i];
+#pragma unroll
+    for (int half = 0; half < 2; half++)
+    {
+        int incl = len[half];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off)
+                incl += v;
+        }
+        const int mine = o + incl - len[half];
+        for (int j = 0; j < len[half]; j++)
+            n4_tris[mine + j] = cell_tris[b[half] + j];
+        o += __shfl_sync(0xffffffffu, incl, 31);
     }
 }
 
@@ -290,22 +352,26 @@ __global__ void face_fill_kernel(const int *base, const int *basec, int nt, int 
                                  const int *b4_flag, const int *b4_start, const int *n4_tris, const int *face_start,
                                  int *face_nbr, int *face_corner)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nt)
+    // one warp per centre triangle: its 8 trilinear corner cells and a copy of its base cell's
+    // 4^3 list (lanes stride over the list)
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= nt)
         return;
-    int b = base[i];
-    int bx = basec[3 * i], by = basec[3 * i + 1], bz = basec[3 * i + 2];
-    for (int w = 0; w < 8; w++)
+    const int i = (int)gw;
+    const int b = base[i];
+    if (lane < 8)
     {
-        int dx = w >> 2, dy = (w >> 1) & 1, dz = w & 1;
-        face_corner[8 * i + w] = ((bx + dx) * res + (by + dy)) * res + (bz + dz);
+        const int bx = basec[3 * i], by = basec[3 * i + 1], bz = basec[3 * i + 2];
+        const int dx = lane >> 2, dy = (lane >> 1) & 1, dz = lane & 1;
+        face_corner[8 * i + lane] = ((bx + dx) * res + (by + dy)) * res + (bz + dz);
     }
     if (b < 0 || !b4_flag[b])
         return;
-    int k = b4_pos[b];
-    int o = face_start[i];
-    for (int j = b4_start[k]; j < b4_start[k + 1]; j++)
-        face_nbr[o++] = n4_tris[j];
+    const int k = b4_pos[b];
+    const int o = face_start[i], s0 = b4_start[k], n = b4_start[k + 1] - s0;
+    for (int j = lane; j < n; j += 32)
+        face_nbr[o + j] = n4_tris[s0 + j];
 }
 
 }  // namespace
@@ -329,39 +395,73 @@ int read_ints(Handle &h, const int *const *src, int n, int *out)
     return PPPM_OK;
 }
 
-// out[0..n] exclusive prefix sums of in[0..n), out[n] = total.  Scratch: h.d_scan_tmp.
-static int scan_level(Handle &h, const int *in, int *out, long long n_in, int *scratch, long long scratch_left)
+// Exclusive prefix sums of up to kScanBatch arrays at once: out_i[0..n_i] = scan of in_i[0..n_i),
+// out_i[n_i] = total.  Three launches per level for the whole set (tiles, the tile totals
+// recursively, tile offsets added).  Scratch: h.d_scan_tmp.
+static int scan_level(Handle &h, ScanSet set, int count, int *scratch, long long scratch_left)
 {
-    long long n_out = n_in + 1;
-    long long nb = (n_out + kScanTile - 1) / kScanTile;
-    if (nb > 1)
+    ScanSet up{};  // the tile totals of every multi-tile array
+    ScanSet add{};
+    long long nb_max = 0;
+    int multi = 0;
+    for (int i = 0; i < count; i++)
     {
-        if (scratch_left < 2 * (nb + 1))
+        const long long nb = (set.n_out[i] + kScanTile - 1) / kScanTile;
+        nb_max = std::max(nb_max, nb);
+        if (nb > 1)
         {
-            set_error("scan scratch exhausted");
-            return PPPM_ERR_CAPACITY;
+            if (scratch_left < 2 * (nb + 1))
+            {
+                set_error("scan scratch exhausted");
+                return PPPM_ERR_CAPACITY;
+            }
+            int *sums = scratch, *offs = scratch + nb + 1;
+            scratch += 2 * (nb + 1);
+            scratch_left -= 2 * (nb + 1);
+            set.sums[i] = sums;
+            up.in[multi] = sums;
+            up.out[multi] = offs;
+            up.n_in[multi] = nb;
+            up.n_out[multi] = nb + 1;
+            add.in[multi] = offs;
+            add.out[multi] = set.out[i];
+            add.sums[multi] = sums;
+            add.n_out[multi] = set.n_out[i];
+            multi++;
         }
-        int *sums = scratch, *offs = scratch + nb + 1;
-        scan_tiles_kernel<<<(unsigned)nb, kScanThreads, 0, h.stream>>>(in, out, sums, n_in, n_out);
-        h.launches++;
-        PB_CHECK_LAUNCH();
-        PB_TRY(scan_level(h, sums, offs, nb, scratch + 2 * (nb + 1), scratch_left - 2 * (nb + 1)));
-        scan_add_kernel<<<(unsigned)nb, 256, 0, h.stream>>>(out, offs, n_out);
-        h.launches++;
-        PB_CHECK_LAUNCH();
+        else
+            set.sums[i] = nullptr;
     }
-    else
+    scan_tiles_kernel<<<dim3((unsigned)nb_max, count), kScanThreads, 0, h.stream>>>(set);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    if (multi > 0)
     {
-        scan_tiles_kernel<<<1, kScanThreads, 0, h.stream>>>(in, out, nullptr, n_in, n_out);
+        PB_TRY(scan_level(h, up, multi, scratch, scratch_left));
+        long long nb_add = 0;
+        for (int i = 0; i < multi; i++)
+            nb_add = std::max(nb_add, (add.n_out[i] + kScanTile - 1) / kScanTile);
+        scan_add_kernel<<<dim3((unsigned)nb_add, multi), 256, 0, h.stream>>>(add);
         h.launches++;
         PB_CHECK_LAUNCH();
     }
     return PPPM_OK;
 }
 
-int exclusive_scan(Handle &h, const int *in, int *out, long long n)
+int exclusive_scan_set(Handle &h, const int *const *in, int *const *out, const long long *n, int count)
 {
-    long long need = 4 * (n / kScanTile + 8) + 64;
+    if (count < 1 || count > kScanBatch)
+        return PPPM_ERR_ARG;
+    ScanSet set{};
+    long long need = 64;
+    for (int i = 0; i < count; i++)
+    {
+        set.in[i] = in[i];
+        set.out[i] = out[i];
+        set.n_in[i] = n[i];
+        set.n_out[i] = n[i] + 1;
+        need += 4 * (n[i] / kScanTile + 8);
+    }
     if ((long long)h.scan_tmp_elems < need)
     {
         dev_free(h.d_scan_tmp);
@@ -369,7 +469,12 @@ int exclusive_scan(Handle &h, const int *in, int *out, long long n)
         PB_TRY(dalloc(&h.d_scan_tmp, (size_t)need));
         h.scan_tmp_elems = (size_t)need;
     }
-    return scan_level(h, in, out, n, h.d_scan_tmp, (long long)h.scan_tmp_elems);
+    return scan_level(h, set, count, h.d_scan_tmp, (long long)h.scan_tmp_elems);
+}
+
+int exclusive_scan(Handle &h, const int *in, int *out, long long n)
+{
+    return exclusive_scan_set(h, &in, &out, &n, 1);
 }
 
 int mesh_build(Handle &h)
@@ -419,18 +524,24 @@ int mesh_build(Handle &h)
     // so the list builds in between stay in bounds)
 
     // ---- per-cell and per-base-cell CSR, ids ascending inside a cell
+    PB_CUDA(cudaMemsetAsync(h.d_cell_count, 0, sizeof(int) * nc, s));
+    PB_CUDA(cudaMemsetAsync(h.d_base_count, 0, sizeof(int) * nc, s));
+    count_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_cell, nt, h.d_cell_count);
+    count_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, nt, h.d_base_count);
+    h.launches += 2;
+    PB_CHECK_LAUNCH();
+    {
+        const int *in[2] = {h.d_cell_count, h.d_base_count};
+        int *out[2] = {h.d_cell_start, h.d_base_start};
+        const long long n[2] = {nc, nc};
+        PB_TRY(exclusive_scan_set(h, in, out, n, 2));
+    }
     for (int pass = 0; pass < 2; pass++)
     {
         const int *key = pass == 0 ? h.d_cell : h.d_base;
-        int *count = pass == 0 ? h.d_cell_count : h.d_base_count;
         int *start = pass == 0 ? h.d_cell_start : h.d_base_start;
         int *list = pass == 0 ? h.d_cell_tris : h.d_base_tris;
-        PB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * nc, s));
         PB_CUDA(cudaMemsetAsync(h.d_cursor, 0, sizeof(int) * nc, s));
-        count_kernel<<<div_up(nt, T), T, 0, s>>>(key, nt, count);
-        h.launches++;
-        PB_CHECK_LAUNCH();
-        PB_TRY(exclusive_scan(h, count, start, nc));
         fill_kernel<<<div_up(nt, T), T, 0, s>>>(key, nt, start, h.d_cursor, list);
         h.launches++;
         sort_segments_kernel<<<div_up(nc, T), T, 0, s>>>(start, nc, list);
@@ -451,10 +562,12 @@ int mesh_build(Handle &h)
     int *st3 = h.d_flags + 4 * (nc + 1);              // nc + 1
     int *st4 = h.d_flags + 5 * (nc + 1);              // nc + 1
     int *b4_pos = h.d_cell_count;                     // nc (flags of the last cell are 0: never inner)
-    PB_TRY(exclusive_scan(h, flag3, pos3, nc));
-    PB_TRY(exclusive_scan(h, len3, st3, nc));
-    PB_TRY(exclusive_scan(h, flag4, b4_pos, nc - 1));
-    PB_TRY(exclusive_scan(h, len4, st4, nc));
+    {
+        const int *in[4] = {flag3, len3, flag4, len4};
+        int *out[4] = {pos3, st3, b4_pos, st4};
+        const long long n[4] = {nc, nc, nc - 1, nc};
+        PB_TRY(exclusive_scan_set(h, in, out, n, 4));
+    }
     compact_kernel<<<div_up(nc + 1, T), T, 0, s>>>(flag3, pos3, st3, nc, h.d_n3_cell, h.d_n3_start);
     h.launches++;
     compact_kernel<<<div_up(nc, T), T, 0, s>>>(flag4, b4_pos, st4, nc - 1, h.d_b4_cell, h.d_b4_start);
@@ -486,21 +599,15 @@ int mesh_build(Handle &h)
     {
         dev_free(h.d_p3_tri);
         dev_free(h.d_p3_woff);
-        dev_free(h.d_w3);
-        dev_free(h.d_w3_scale);
         h.d_p3_tri = nullptr;
         h.d_p3_woff = nullptr;
-        h.d_w3 = nullptr;
-        h.d_w3_scale = nullptr;
         long long cap = p3 + p3 / 4 + 256;
         PB_TRY(dalloc(&h.d_p3_tri, (size_t)cap));
         PB_TRY(dalloc(&h.d_p3_woff, (size_t)cap));
-        PB_TRY(dev_alloc(&h.d_w3, (size_t)cap * 2 * (h.fp64 ? 16 * sizeof(double2) : 16 * sizeof(__half2))));
-        PB_TRY(dalloc(&h.d_w3_scale, (size_t)cap * 2));
         h.p3_cap = cap;
     }
     PB_CUDA(cudaMemsetAsync(h.d_corr_mask, 0, sizeof(unsigned) * ((nc + 31) / 32), s));
-    fill_pairs3_kernel<<<div_up(n3, T), T, 0, s>>>(h.d_n3_cell, h.d_n3_start, n3, res, h.d_cell_start, h.d_cell_tris,
+    fill_pairs3_kernel<<<div_up((long long)n3 * 32, T), T, 0, s>>>(h.d_n3_cell, h.d_n3_start, n3, res, h.d_cell_start, h.d_cell_tris,
                                                    h.d_p3_tri, h.d_p3_woff, h.d_corr_mask);
     h.launches++;
     PB_CHECK_LAUNCH();
@@ -514,7 +621,7 @@ int mesh_build(Handle &h)
         PB_TRY(dalloc(&h.d_n4_tris, (size_t)cap));
         h.n4_cap = cap;
     }
-    fill_n4_kernel<<<div_up(b4, T), T, 0, s>>>(h.d_b4_cell, h.d_b4_start, b4, res, h.d_cell_start, h.d_cell_tris,
+    fill_n4_kernel<<<div_up((long long)b4 * 32, T), T, 0, s>>>(h.d_b4_cell, h.d_b4_start, b4, res, h.d_cell_start, h.d_cell_tris,
                                                h.d_n4_tris);
     h.launches++;
     PB_CHECK_LAUNCH();
@@ -538,7 +645,7 @@ int mesh_build(Handle &h)
         PB_TRY(dalloc(&h.d_face_scale, (size_t)cap));
         h.pf_cap = cap;
     }
-    face_fill_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_base, h.d_basec, nt, res, b4_pos, flag4, h.d_b4_start,
+    face_fill_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(h.d_base, h.d_basec, nt, res, b4_pos, flag4, h.d_b4_start,
                                                  h.d_n4_tris, h.d_face_start, h.d_face_nbr, h.d_face_corner);
     h.launches++;
     PB_CHECK_LAUNCH();
