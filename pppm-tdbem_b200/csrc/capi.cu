@@ -140,7 +140,7 @@ void free_mesh(Handle &h)
                      (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
                      (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
-                     (void **)&h.d_hist,       (void **)&h.d_terms};
+                     (void **)&h.d_hist,       (void **)&h.d_terms,       (void **)&h.d_conv};
     for (void **q : ptrs)
     {
         dev_free(*q);
@@ -298,6 +298,13 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
     }
     for (int i = 0; i < 4; i++)
         cudaEventCreate(&h.ev[i]);
+    if (cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_fin, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_conv, cudaEventDisableTiming) != cudaSuccess)
+    {
+        set_error("cudaStreamCreate / cudaEventCreate failed");
+        return fail(PPPM_ERR_CUDA);
+    }
     if (cudaMallocHost((void **)&h.h_pin, kPinnedInts * sizeof(int)) != cudaSuccess)
     {
         h.h_pin = nullptr;
@@ -341,6 +348,12 @@ int pppm_destroy(pppm_handle *ph)
             cudaEventDestroy(h.ev[i]);
     if (h.h_pin)
         cudaFreeHost(h.h_pin);
+    if (h.ev_fin)
+        cudaEventDestroy(h.ev_fin);
+    if (h.ev_conv)
+        cudaEventDestroy(h.ev_conv);
+    if (h.side)
+        cudaStreamDestroy(h.side);
     if (h.own_stream && h.stream)
         cudaStreamDestroy(h.stream);
     delete ph;
@@ -384,6 +397,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)nt * kRing * h.real_size, h.stream));
     PB_TRY(dev_alloc(&h.d_hist, (size_t)8 * nt * kRing * h.real_size));
     PB_TRY(dev_alloc(&h.d_terms, (size_t)54 * nt * h.real_size));
+    PB_TRY(dev_alloc(&h.d_conv, (size_t)nt * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
     if (rc == PPPM_OK)

@@ -58,6 +58,8 @@ struct Handle
     size_t real_size = 4;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr;                         // second branch of the recorded step graphs
+    cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;     // fork / join points while recording
     int res = 0;
     long long n_cells = 0;
     int t = -1;
@@ -134,6 +136,7 @@ struct Handle
     void *d_neumann = nullptr, *d_dirichlet = nullptr;  // reference layout: read-out and loading
     void *d_hist = nullptr;  // the step's copies: [Neumann, Dirichlet][4 copies][nt][kRing] (step.cu)
     void *d_terms = nullptr;  // nt x 54 near-field terms of the current step (step.cu: near_terms)
+    void *d_conv = nullptr;   // nt face-pair convolution sums of the pipelined step (step.cu)
 
     // ---- listeners
     std::vector<int> listen_xyz;

@@ -462,35 +462,27 @@ __device__ inline void near_terms(const Ring<R> &ring, int t, const FaceArgs<R> 
     }
 }
 
+// The face stage of centre triangle tri (whole warp) in two parts.  face_conv: the face-pair
+// convolution over the triangle's 4^3 list -> its warp sum.  It reads only history that is final
+// before the step begins (Neumann taps t..t-15 with N[t] = acc[t] already in the ring, Dirichlet
+// taps t-1..t-15), so the pipelined step graph runs it beside the stencil.  face_finish: the far
+// field at the 8 trilinear corners (from this step's stencil output), the Dirichlet update and the
+// triangle's near-field terms.  Fused or split, the arithmetic and its order are the same.
 template <typename R>
-__device__ inline void face_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, const FaceArgs<R> &f,
-                                 int tri, int lane)
+__device__ inline R face_conv(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane)
 {
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
-    const int *face_start = f.face_start, *face_nbr = f.face_nbr, *face_corner = f.face_corner;
-    const typename WRec<R>::T *face_w = f.face_w;
-    const float2 *face_scale = f.face_scale;
-    const float *interp = f.interp;
-    const double *interp_d = f.interp_d, *denom = f.denom;
-    const float reflect = f.reflect;
     const int g = lane >> 2, q = lane & 3;
-    const R *next = ring.slot(dy.tnew);
-    const int copy = dy.tnew & 3, off = (hist_index(copy, dy.tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
+    const int copy = tnew & 3, off = (hist_index(copy, tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
     const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
-    R iw = 0, pv = 0;
-    if (lane < 8)
-    {
-        iw = interp_d ? (R)interp_d[8 * tri + lane] : (R)interp[8 * tri + lane];
-        pv = next[face_corner[8 * tri + lane]];
-    }
-    const int b = face_start[tri], e = face_start[tri + 1];
+    const int b = f.face_start[tri], e = f.face_start[tri + 1];
     R acc = 0;
     for (int p = b + g; p < e; p += 8)
     {
-        const W4 w = *(const W4 *)(face_w + (long long)p * kTaps + 4 * q);
-        const float2 s = face_scale ? face_scale[p] : make_float2(1, 1);
-        const int nb = face_nbr[p];
+        const W4 w = *(const W4 *)(f.face_w + (long long)p * kTaps + 4 * q);
+        const float2 s = f.face_scale ? f.face_scale[p] : make_float2(1, 1);
+        const int nb = f.face_nbr[p];
         const H4 hn = *(const H4 *)(nbase + (long long)nb * kRing);
         const H4 hd = *(const H4 *)(dbase + (long long)nb * kRing);
 #pragma unroll
@@ -501,16 +493,94 @@ __device__ inline void face_body(const StepArgs &a, const Ring<R> &ring, const S
             acc += conv_tap(w.v[i], s, hn.v[i], di);
         }
     }
-    acc = warp_sum(acc);
+    return warp_sum(acc);
+}
+
+// far-field corner values of triangle tri (lanes 0-7; the others 0)
+template <typename R>
+__device__ inline void face_corners(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane, R &iw,
+                                    R &pv)
+{
+    iw = 0;
+    pv = 0;
+    if (lane < 8)
+    {
+        iw = f.interp_d ? (R)f.interp_d[8 * tri + lane] : (R)f.interp[8 * tri + lane];
+        pv = ring.slot(tnew)[f.face_corner[8 * tri + lane]];
+    }
+}
+
+template <typename R>
+__device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane, R iw, R pv,
+                                   R conv)
+{
     R far_sum = 0;  // corners in order 0..7
 #pragma unroll
     for (int wi = 0; wi < 8; wi++)
         far_sum += __shfl_sync(kFull, iw, wi) * __shfl_sync(kFull, pv, wi);
-    R num = far_sum * (R)reflect + acc;
-    const R dnew = (R)(num / denom[tri]);
+    R num = far_sum * (R)f.reflect + conv;
+    const R dnew = (R)(num / f.denom[tri]);
     if (lane < 4)
-        ring.hrow(1, lane, tri)[hist_index(lane, dy.tnew)] = dnew;  // lane c: copy c
-    near_terms<R>(ring, dy.tnew, f, tri, lane, true, dnew);
+        ring.hrow(1, lane, tri)[hist_index(lane, tnew)] = dnew;  // lane c: copy c
+    near_terms<R>(ring, tnew, f, tri, lane, true, dnew);
+}
+
+// the fused face stage (corner loads issued first so their latency overlaps the convolution)
+template <typename R>
+__device__ inline void face_body(const StepArgs &, const Ring<R> &ring, const StepDyn &dy, const FaceArgs<R> &f,
+                                 int tri, int lane)
+{
+    R iw, pv;
+    face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
+    const R conv = face_conv<R>(ring, dy.tnew, f, tri, lane);
+    face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv);
+}
+
+// pipelined step: the face-pair convolution of step kstep into conv[tri]
+template <typename R>
+__global__ void __launch_bounds__(256) conv_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                    int kstep, int nt, const __grid_constant__ FaceArgs<R> f, R *conv)
+{
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (tri >= nt)
+        return;
+    const R v = face_conv<R>(ring, st->tnew0 + kstep, f, tri, threadIdx.x & 31);
+    if ((threadIdx.x & 31) == 0)
+        conv[tri] = v;
+}
+
+// pipelined step: the rest of the face stage of step kstep; next != 0: also the Neumann value of
+// step kstep + 1 into the history (its slot is outside every window of this step), so the next
+// step's convolution can start before that step's stencil
+template <typename R>
+__global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                      int kstep, int nt, const __grid_constant__ FaceArgs<R> f,
+                                                      const R *conv, int next)
+{
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (tri >= nt)
+        return;
+    const int lane = threadIdx.x & 31;
+    const StepDyn dy = bind_step(st, kstep, nt);
+    R iw, pv;
+    face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
+    face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri]);
+    if (next && lane == 0)
+    {
+        const StepDyn dn = bind_step(st, kstep + 1, nt);
+        if (dn.acc)
+            ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
+    }
+}
+
+// the Neumann value of step kstep into the history (first step of a pipelined call)
+template <typename R>
+__global__ void nwrite_kernel(const __grid_constant__ Ring<R> ring, const StepState *st, int kstep, int nt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const StepDyn dy = bind_step(st, kstep, nt);
+    if (i < nt && dy.acc)
+        ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
 }
 
 // the near-field terms of time t for every triangle without a face step (priming)
@@ -639,6 +709,7 @@ struct StepLaunch
     R *series;
     FaceArgs<R> fa;
     NearArgs<R> na;
+    R *conv;  // per-triangle convolution sums of the pipelined step
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
 };
 
@@ -682,6 +753,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.fa.gc_w = (const W *)h.d_gc_w;
         L.fa.gc_scale = h.fp64 ? nullptr : h.d_gc_scale;
         L.fa.terms = (R *)h.d_terms;
+        L.conv = (R *)h.d_conv;
         L.na.n3_cell = h.d_n3_cell;
         L.na.n3_start = h.d_n3_start;
         L.na.p3_tri = h.d_p3_tri;
@@ -726,6 +798,35 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
     mark(3);
 }
 
+// The kernels of nsteps steps as a two-branch graph (absorbing boundary with a mesh).  Per step:
+//   side   conv(k)                       after finish(k-1): needs D[t-1] and N[t]
+//   main   stencil(k) -> finish(k) -> near(k)   finish waits for conv(k) too
+// so each step's face-pair convolution (the heavy part of the face stage) runs beside the
+// previous step's near stage and this step's stencil; finish(k) also writes N[t+1] for conv(k+1).
+// Only used under stream capture: main = h.stream, side = h.side, joined back before the end.
+template <typename R>
+void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps)
+{
+    const int T = 256;
+    const int nt = L.a.nt;
+    const int wblocks = div_up((long long)nt * 32, T);
+    cudaStream_t s = h.stream, side = h.side;
+    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
+    cudaEventRecord(h.ev_fin, s);
+    for (int k = 0; k < nsteps; k++)
+    {
+        cudaStreamWaitEvent(side, h.ev_fin, 0);
+        conv_kernel<R><<<wblocks, T, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv);
+        cudaEventRecord(h.ev_conv, side);
+        // the stencil without its Neumann block range (finish / nwrite wrote N[t])
+        stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
+        cudaStreamWaitEvent(s, h.ev_conv, 0);
+        finish_kernel<R><<<wblocks, T, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, k + 1 < nsteps ? 1 : 0);
+        cudaEventRecord(h.ev_fin, s);
+        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
+    }
+}
+
 // Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
 // first call with that step count and launch set (the graph removes the host launch cost and
 // most of the gap between dependent kernels); shorter calls, measurement mode and calls on a
@@ -755,8 +856,11 @@ int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *ou
     g.exec = nullptr;
     cudaGraph_t graph = nullptr;
     PB_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < nsteps; k++)
-        launch_step<R>(L, k, h.stream, timed ? &h : nullptr);
+    if (!timed && L.mesh && !L.pml && h.side)
+        capture_pipelined<R>(h, L, nsteps);
+    else
+        for (int k = 0; k < nsteps; k++)
+            launch_step<R>(L, k, h.stream, timed ? &h : nullptr);
     cudaError_t e = cudaStreamEndCapture(h.stream, &graph);
     if (e == cudaSuccess)
         e = cudaGraphInstantiate(&g.exec, graph, 0);
