@@ -45,6 +45,10 @@ extern "C" {
 #define PPPM_WEIGHTS_REF32 0 /* TDBEM weights in FP32 with the reference's arithmetic       */
 #define PPPM_WEIGHTS_FP64 1  /* singular and near-singular face integrals in FP64           */
 
+#define PPPM_METHOD_PPPM 0  /* FDTD + TDBEM near-field correction (PPPMSolver)              */
+#define PPPM_METHOD_GHOST 1 /* FDTD + ghost cells (GhostCellSolver, ghost_cell.h:72-152);
+                               FP32 handles, absorbing boundary                             */
+
 typedef struct pppm_params {
     int res;               /* grid resolution (cells per axis), >= 8                      */
     float dl;              /* cell size h                                                 */
@@ -58,6 +62,10 @@ typedef struct pppm_params {
     int weights;           /* PPPM_WEIGHTS_*                                              */
     int device;            /* CUDA device ordinal                                         */
     void *stream;          /* cudaStream_t to use, or NULL to create one                  */
+    int method;            /* PPPM_METHOD_*                                               */
+    float ghost_threshold; /* ghost-cell method: condition number above which a ghost cell
+                              falls back to first order (reference 25); 0 = first order
+                              everywhere with thin-shell labels (ghost_cell.h:77, :95)     */
 } pppm_params;
 
 typedef struct pppm_handle pppm_handle;
@@ -141,6 +149,10 @@ int pppm_restore_state(pppm_handle *h, const void *src, size_t bytes);
 #define PPPM_DUMP_CELL_GHOST 19   /* int res^3 ghost index (-1 if not GHOST)             */
 #define PPPM_DUMP_CELL_POINTS 20  /* float res^3 x 7: nearest xyz, reflect xyz, distance */
 #define PPPM_DUMP_COUNTS 21       /* int[8]: n3, p3, b4, p4(pairs per centre), pf, nt, nv, ghost count */
+#define PPPM_DUMP_GHOST_CELLS 22  /* ghost-cell method: int ghosts: linear cell index of each ghost */
+#define PPPM_DUMP_GHOST_ORDER 23  /* int ghosts: 1 = first order, 0 = second order             */
+#define PPPM_DUMP_GHOST_WEIGHTS 24 /* float ghosts x 8: reflection-point interpolation weights */
+#define PPPM_DUMP_GHOST_ITERS 25  /* int: BiCGSTAB iterations of the last step's solve         */
 
 int pppm_dump_size(pppm_handle *h, int what, size_t *bytes);
 int pppm_dump(pppm_handle *h, int what, void *dst, size_t bytes);

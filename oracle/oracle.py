@@ -342,9 +342,69 @@ def reference_lib(ndebug=False):
             "ref_cells_write_grid": (_i, [_vp, _i, _vp]),
             "ref_cells_read_grid": (_i, [_vp, _i, _vp]),
             "ref_cells_fresh_error": (_i, [_vp]),
+            "ref_ghost_create": (_vp, [_i, _f, _f, _vp, _f]),
+            "ref_ghost_set_mesh": (_i, [_vp, _vp, _i, _vp, _i]),
+            "ref_ghost_update_mesh": (_i, [_vp, _vp]),
+            "ref_ghost_run": (_i, [_vp, _vp, _i, _vp, _i, _vp]),
+            "ref_ghost_count": (_i, [_vp]),
+            "ref_ghost_read": (_i, [_vp, _vp, _vp, _vp]),
         })
         _rlibs[path] = lib
     return _rlibs[path]
+
+
+class ReferenceGhost:
+    """The reference GhostCellSolver (compiled from source): labels, the ghost system from an
+    8 x 8 SVD per ghost cell (cuSOLVER), BiCGSTAB-ILU0 per step (cuSPARSE)."""
+
+    def __init__(self, res, dl, dt, min_pos=(0, 0, 0), threshold=25.0):
+        self.lib = reference_lib()
+        mn = np.asarray(min_pos, np.float32)
+        self.h = self.lib.ref_ghost_create(int(res), float(dl), float(dt), _p(mn), float(threshold))
+        if not self.h:
+            raise RuntimeError("ref_ghost_create failed")
+        self.res, self.nt = int(res), 0
+
+    def close(self):
+        if self.h:
+            self.lib.ref_cells_destroy(self.h)
+            self.h = None
+
+    def _ok(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("reference %s failed (%d)" % (what, rc))
+
+    def set_mesh(self, verts, tris):
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        self._ok(self.lib.ref_ghost_set_mesh(self.h, _p(v), len(v), _p(f), len(f)), "ghost set_mesh")
+        self.nt = len(f)
+
+    def update_mesh(self, verts):
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        self._ok(self.lib.ref_ghost_update_mesh(self.h, _p(v)), "ghost update_mesh")
+
+    def run(self, acc, listeners):
+        a = np.ascontiguousarray(acc, np.float32).reshape(-1, self.nt)
+        lx = np.ascontiguousarray(np.asarray(listeners, np.int32).reshape(-1, 3))
+        out = np.zeros((a.shape[0], len(lx)), np.float32)
+        self._ok(self.lib.ref_ghost_run(self.h, _p(a), a.shape[0], _p(lx), len(lx), _p(out)), "ghost run")
+        return out
+
+    def ghosts(self):
+        """(cells (g, 3), second_order (g,), weights (g, 8))"""
+        g = self.lib.ref_ghost_count(self.h)
+        c = np.zeros((max(g, 0), 3), np.int32)
+        o = np.zeros(max(g, 0), np.int32)
+        w = np.zeros((max(g, 0), 8), np.float32)
+        if g > 0:
+            self._ok(self.lib.ref_ghost_read(self.h, _p(c), _p(o), _p(w)), "ghost read")
+        return c, o, w
+
+    def grid(self, rel=0):
+        out = np.zeros(self.res ** 3, np.float32)
+        self._ok(self.lib.ref_cells_read_grid(self.h, rel, _p(out)), "read_grid")
+        return out.reshape((self.res,) * 3)
 
 
 class Reference:

@@ -1014,4 +1014,110 @@ int ref_cells_fresh_error(void *p)
     return e[0];
 }
 
+// ---- the reference GhostCellSolver as a whole (ghost_cell.h:72-152): set_mesh builds labels and
+// the ghost system, each step is update(acc) (FDTD step, boundary condition, ghost solve, SOLID
+// cells zeroed).  Handles share RefCells; threshold as set_condition_number_threshold.
+void *ref_ghost_create(int res, float dl, float dt, const float *min_pos, float threshold)
+{
+    RefCells *h = (RefCells *)ref_cells_create(res, dl, dt, min_pos);
+    if (h)
+        h->solver->set_condition_number_threshold(threshold);
+    return h;
+}
+
+int ref_ghost_set_mesh(void *p, const float *V, int nv, const int *F, int nt)
+{
+    RefCells *h = (RefCells *)p;
+    if (!h || nv <= 0 || nt <= 0)
+        return REF_ERR_ARG;
+    int rc = h->cap.check(V, nv, F, nt, false);
+    if (rc)
+        return rc;
+    h->nv = nv;
+    h->nt = nt;
+    return guarded([&] {
+        CArr<float3> verts = to_float3(V, nv);
+        CArr<int3> tris = to_int3(F, nt);
+        h->solver->set_mesh(verts, tris);
+        return last_cuda_status();
+    });
+}
+
+int ref_ghost_update_mesh(void *p, const float *V)
+{
+    RefCells *h = (RefCells *)p;
+    if (!h || h->nt == 0)
+        return REF_ERR_STATE;
+    return guarded([&] {
+        CArr<float3> verts = to_float3(V, h->nv);
+        h->solver->update_mesh(verts);
+        return last_cuda_status();
+    });
+}
+
+// nsteps steps with acc (nsteps x nt, host); the listener cells read after every step
+int ref_ghost_run(void *p, const float *acc, int nsteps, const int *listen_xyz, int nlisten, float *out)
+{
+    RefCells *h = (RefCells *)p;
+    if (!h || h->nt == 0 || nsteps < 0)
+        return REF_ERR_ARG;
+    return guarded([&] {
+        auto &s = *h->solver;
+        CArr<float> a(h->nt);
+        for (int k = 0; k < nsteps; k++)
+        {
+            for (int i = 0; i < h->nt; i++)
+                a[i] = acc[(size_t)k * h->nt + i];
+            GArr<float> ga(a);
+            s.update(ga);
+            ga.clear();
+            auto g = s.get_grid().cpu();
+            const int n = s.res();
+            for (int l = 0; l < nlisten; l++)
+                out[(size_t)k * nlisten + l] =
+                    g.data[((size_t)listen_xyz[3 * l] * n + listen_xyz[3 * l + 1]) * n + listen_xyz[3 * l + 2]];
+        }
+        return last_cuda_status();
+    });
+}
+
+// ghost count, then per ghost: cell coordinates (3 ints), order (0 first, 1 second), 8 weights
+int ref_ghost_count(void *p)
+{
+    RefCells *h = (RefCells *)p;
+    return h ? h->solver->ghost_cell_num : -1;
+}
+
+int ref_ghost_read(void *p, int *coords, int *order, float *weights)
+{
+    RefCells *h = (RefCells *)p;
+    if (!h)
+        return REF_ERR_ARG;
+    return guarded([&] {
+        auto &s = *h->solver;
+        const int g = s.ghost_cell_num;
+        if (g <= 0)
+            return 0;
+        auto cells = s.ghost_cells.cpu();
+        auto ord = s.ghost_order.cpu();
+        for (int i = 0; i < g; i++)
+        {
+            coords[3 * i] = cells[i].x;
+            coords[3 * i + 1] = cells[i].y;
+            coords[3 * i + 2] = cells[i].z;
+            order[i] = ord[i] == AccuracyOrder::SECOND_ORDER ? 1 : 0;
+        }
+        if (s.condition_number_threshold > 0)
+        {
+            auto w = s.p_weight.cpu();
+            for (size_t i = 0; i < (size_t)g * GHOST_CELL_NEIGHBOR_NUM; i++)
+                weights[i] = w.data[i];
+        }
+        else
+            for (size_t i = 0; i < (size_t)g * GHOST_CELL_NEIGHBOR_NUM; i++)
+                weights[i] = 0;
+        return last_cuda_status();
+    });
+}
+
 }  // extern "C"

@@ -126,6 +126,7 @@ void free_mesh(Handle &h)
 {
     cudaStreamSynchronize(h.stream);
     adjoint_free(h);
+    ghost_free(h);
     h.mesh_version++;
     cache_free(h);
     void **ptrs[] = {(void **)&h.d_verts,      (void **)&h.d_tris,        (void **)&h.d_center,
@@ -140,7 +141,8 @@ void free_mesh(Handle &h)
                      (void **)&h.d_face_nbr,   (void **)&h.d_face_pool,   (void **)&h.d_face_w,
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
                      (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
-                     (void **)&h.d_hist,       (void **)&h.d_terms,       (void **)&h.d_conv};
+                     (void **)&h.d_hist,       (void **)&h.d_terms,       (void **)&h.d_conv,
+                     (void **)&h.d_gneu,       (void **)&h.d_gneu_old};
     for (void **q : ptrs)
     {
         dev_free(*q);
@@ -229,6 +231,8 @@ int pppm_params_default(pppm_params *p)
     p->weights = PPPM_WEIGHTS_REF32;
     p->device = 0;
     p->stream = nullptr;
+    p->method = PPPM_METHOD_PPPM;
+    p->ghost_threshold = 25.0f;
     return PPPM_OK;
 }
 
@@ -239,9 +243,15 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
     *out = nullptr;
     if (p->res < 8 || p->res > 1024 || !(p->dl > 0) || !(p->dt > 0) || !(p->c > 0) || p->pml_width < 0 ||
         p->pml_width * 2 >= p->res || (p->precision != PPPM_PRECISION_FP32 && p->precision != PPPM_PRECISION_FP64) ||
-        (p->weights != PPPM_WEIGHTS_REF32 && p->weights != PPPM_WEIGHTS_FP64))
+        (p->weights != PPPM_WEIGHTS_REF32 && p->weights != PPPM_WEIGHTS_FP64) ||
+        (p->method != PPPM_METHOD_PPPM && p->method != PPPM_METHOD_GHOST) || !(p->ghost_threshold >= 0))
     {
         set_error("invalid parameters");
+        return PPPM_ERR_ARG;
+    }
+    if (p->method == PPPM_METHOD_GHOST && (p->precision != PPPM_PRECISION_FP32 || p->pml_width > 0))
+    {
+        set_error("the ghost-cell method runs on FP32 handles with the absorbing boundary");
         return PPPM_ERR_ARG;
     }
     pppm_handle *ph = new (std::nothrow) pppm_handle();
@@ -400,6 +410,31 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_TRY(dev_alloc(&h.d_conv, (size_t)nt * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
+    if (rc == PPPM_OK && h.prm.method == PPPM_METHOD_GHOST)
+    {
+        // GhostCellSolver::set_mesh (ghost_cell.h:84-99): labels, ghost system, zero accelerations
+        rc = dalloc(&h.d_gneu, (size_t)nt);
+        if (rc == PPPM_OK)
+            rc = dalloc(&h.d_gneu_old, (size_t)nt);
+        if (rc == PPPM_OK)
+        {
+            cudaMemsetAsync(h.d_gneu, 0, sizeof(float) * nt, h.stream);
+            cudaMemsetAsync(h.d_gneu_old, 0, sizeof(float) * nt, h.stream);
+            h.mesh_set = true;
+            rc = cells_classify(h, nullptr);
+            if (rc == PPPM_OK)
+                rc = ghost_build(h);
+        }
+        if (rc != PPPM_OK)
+        {
+            h.mesh_set = false;
+            free_mesh(h);
+            return rc;
+        }
+        h.mesh_version++;
+        PB_CUDA(cudaStreamSynchronize(h.stream));
+        return PPPM_OK;
+    }
     if (rc == PPPM_OK)
         rc = cache_refresh(h);
     if (rc != PPPM_OK)
@@ -427,6 +462,15 @@ int pppm_update_mesh(pppm_handle *ph, const float *verts, int verts_on_device)
                             verts_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h.stream));
     h.mesh_version++;
     PB_TRY(mesh_build(h));
+    if (h.prm.method == PPPM_METHOD_GHOST)
+    {
+        // GhostCellSolver::update_mesh (ghost_cell.h:101-117): new labels, fresh cells filled from
+        // this and the previous step's accelerations, new ghost system
+        PB_TRY(cells_classify(h, nullptr));
+        PB_TRY(cells_fresh_dev(h, h.d_gneu, h.d_gneu_old, nullptr));
+        PB_TRY(ghost_build(h));
+        return PPPM_OK;
+    }
     PB_TRY(cache_refresh(h));
     PB_TRY(step_prime(h));
     return PPPM_OK;
@@ -858,6 +902,10 @@ int pppm_dump_size(pppm_handle *ph, int what, size_t *bytes)
     case PPPM_DUMP_CELL_GHOST: *bytes = n * sizeof(int); break;
     case PPPM_DUMP_CELL_POINTS: *bytes = n * 7 * sizeof(float); break;
     case PPPM_DUMP_COUNTS: *bytes = 8 * sizeof(int); break;
+    case PPPM_DUMP_GHOST_CELLS:
+    case PPPM_DUMP_GHOST_ORDER: *bytes = h.ghost ? (size_t)h.ghost_count * sizeof(int) : 0; break;
+    case PPPM_DUMP_GHOST_WEIGHTS: *bytes = h.ghost ? (size_t)h.ghost_count * 8 * sizeof(float) : 0; break;
+    case PPPM_DUMP_GHOST_ITERS: *bytes = h.ghost ? sizeof(int) : 0; break;
     default: return PPPM_ERR_ARG;
     }
     return PPPM_OK;
@@ -1035,6 +1083,10 @@ int pppm_dump(pppm_handle *ph, int what, void *dst, size_t bytes)
         o[7] = h.ghost_count;
         return PPPM_OK;
     }
+    case PPPM_DUMP_GHOST_CELLS: return ghost_read(h, 0, dst, bytes);
+    case PPPM_DUMP_GHOST_ORDER: return ghost_read(h, 1, dst, bytes);
+    case PPPM_DUMP_GHOST_WEIGHTS: return ghost_read(h, 2, dst, bytes);
+    case PPPM_DUMP_GHOST_ITERS: return ghost_read(h, 3, dst, bytes);
     default: return PPPM_ERR_ARG;
     }
 }

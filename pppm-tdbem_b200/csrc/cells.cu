@@ -202,7 +202,7 @@ __device__ inline f3 vertex_normal(int v, const float *verts, const int *tris, c
 
 __global__ void nearest_kernel(int res, float h, f3 mn, const float *verts, const int *tris, const float *normal,
                                const int *cell_start, const int *cell_tris, const int *vf_start, const int *vf_list,
-                               int *type, int *nearest, float *points)
+                               int thin, int *type, int *nearest, float *points)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)res * res * res;
@@ -248,7 +248,11 @@ __global__ void nearest_kernel(int res, float h, f3 mn, const float *verts, cons
             nv[k] = vertex_normal(tris[3 * bi + k], verts, tris, normal, vf_start, vf_list);
         f3 nn = bco.x * nv[0] + bco.y * nv[1] + bco.z * nv[2];
         float dir = dot3(nn, gc - bp);
-        ty = dir <= 0 ? SOLID : AIR;
+        // thin shell (first-order ghost cells): a centre within half a cell of its nearest point
+        // on every axis is SOLID too (ghost_cell_util.cu:101-103)
+        const f3 dv = bp - gc;
+        const bool shell = thin && fabsf(dv.x) < h / 2 && fabsf(dv.y) < h / 2 && fabsf(dv.z) < h / 2;
+        ty = (dir <= 0 || shell) ? SOLID : AIR;
     }
     type[i] = ty;
     nearest[i] = bi;
@@ -471,8 +475,9 @@ int cells_classify(Handle &h, int *ghost_count)
     const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
     int *raw = h.d_flags, *flag = h.d_flags + (n + 1), *excl = h.d_flags + 2 * (n + 1);
     nearest_kernel<<<div_up(n, T), T, 0, s>>>(h.res, h.prm.dl, mn, h.d_verts, h.d_tris, h.d_normal, h.d_cell_start,
-                                              h.d_cell_tris, vf_start, vf_list, raw, h.d_cell_nearest,
-                                              h.d_cell_points);
+                                              h.d_cell_tris, vf_start, vf_list,
+                                              h.prm.method == PPPM_METHOD_GHOST && h.prm.ghost_threshold <= 0, raw,
+                                              h.d_cell_nearest, h.d_cell_points);
     ghost_kernel<<<div_up(n, T), T, 0, s>>>(h.res, raw, h.d_cell_type, flag);
     sweep_kernel<<<div_up((long long)h.res * h.res, T), T, 0, s>>>(h.res, h.d_cell_type);
     h.launches += 3;
@@ -495,14 +500,24 @@ int cells_fresh(Handle &h, const float *acc, const float *acc_old, int *fresh_co
 {
     if (!h.mesh_set || !h.d_cell_type)
         return PPPM_ERR_STATE;
-    cudaStream_t s = h.stream;
-    const long long n = h.n_cells;
-    int *list = h.d_flags, *count = h.d_flags + (n + 1);
     float *dacc = nullptr, *dold = nullptr;
     PB_TRY(dalloc(&dacc, (size_t)h.nt));
     PB_TRY(dalloc(&dold, (size_t)h.nt));
-    PB_CUDA(cudaMemcpyAsync(dacc, acc, sizeof(float) * h.nt, cudaMemcpyHostToDevice, s));
-    PB_CUDA(cudaMemcpyAsync(dold, acc_old, sizeof(float) * h.nt, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(dacc, acc, sizeof(float) * h.nt, cudaMemcpyHostToDevice, h.stream));
+    PB_CUDA(cudaMemcpyAsync(dold, acc_old, sizeof(float) * h.nt, cudaMemcpyHostToDevice, h.stream));
+    const int rc = cells_fresh_dev(h, dacc, dold, fresh_count);
+    dev_free(dacc);
+    dev_free(dold);
+    return rc;
+}
+
+int cells_fresh_dev(Handle &h, const float *dacc, const float *dold, int *fresh_count)
+{
+    if (!h.mesh_set || !h.d_cell_type)
+        return PPPM_ERR_STATE;
+    cudaStream_t s = h.stream;
+    const long long n = h.n_cells;
+    int *list = h.d_flags, *count = h.d_flags + (n + 1);
     PB_CUDA(cudaMemsetAsync(count, 0, sizeof(int), s));
     fresh_list_kernel<<<div_up(n, 256), 256, 0, s>>>(n, h.d_cell_type_old, h.d_cell_type, list, count);
     const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
@@ -515,8 +530,6 @@ int cells_fresh(Handle &h, const float *acc, const float *acc_old, int *fresh_co
     PB_TRY(read_int(h, count, &cnt));
     if (fresh_count)
         *fresh_count = cnt;
-    dev_free(dacc);
-    dev_free(dold);
     return PPPM_OK;
 }
 

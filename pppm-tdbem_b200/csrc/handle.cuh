@@ -42,6 +42,23 @@ struct StepState
     const float *acc;  // nsteps rows of nt accelerations, or null
 };
 
+// what step k of a call produces: its time index, listener-series row and acceleration row
+struct StepDyn
+{
+    int tnew;
+    long long row;
+    const float *acc;
+};
+
+__device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
+{
+    StepDyn d;
+    d.tnew = st->tnew0 + k;
+    d.row = st->row0 + k;
+    d.acc = st->acc ? st->acc + (long long)k * nt : nullptr;
+    return d;
+}
+
 // a recorded pppm_step call
 struct StepGraph
 {
@@ -164,6 +181,10 @@ struct Handle
     int graph_next = 0;
     int near_blocks = 0;  // resident grid of the near kernel
 
+    // ---- ghost-cell method (ghost.cu)
+    struct Ghost *ghost = nullptr;
+    float *d_gneu = nullptr, *d_gneu_old = nullptr;  // this and the previous step's accelerations
+
     // ---- adjoint (adjoint.cu): transposed tables and adjoint state, built on first use
     long long mesh_version = 0;  // bumped whenever the lists or weight tables change
     struct Adjoint *adj = nullptr;
@@ -218,6 +239,12 @@ int adjoint_run(Handle &h, const void *g, int nsteps, void *out, int fresh);  //
 int adjoint_stage(Handle &h, size_t g_bytes, size_t out_bytes, void **g, void **out);
 void adjoint_free(Handle &h);
 
+// ghost.cu
+struct Ghost;
+int ghost_build(Handle &h);  // ghost list, interpolation weights, sparse rows, SOLID list
+int ghost_read(Handle &h, int what, void *dst, size_t bytes);
+void ghost_free(Handle &h);
+
 // cache.cu
 int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators
 int cache_free(Handle &h);
@@ -239,6 +266,7 @@ int hist_export(Handle &h);  // the step's history copies -> reference-layout ri
 
 // cells.cu
 int cells_classify(Handle &h, int *ghost_count);
-int cells_fresh(Handle &h, const float *acc, const float *acc_old, int *fresh_count);
+int cells_fresh(Handle &h, const float *acc, const float *acc_old, int *fresh_count);  // host arrays
+int cells_fresh_dev(Handle &h, const float *acc, const float *acc_old, int *fresh_count);  // device arrays
 
 }  // namespace pb

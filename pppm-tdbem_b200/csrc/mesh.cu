@@ -549,6 +549,21 @@ int mesh_build(Handle &h)
         PB_CHECK_LAUNCH();
     }
 
+    if (h.prm.method == PPPM_METHOD_GHOST)
+    {
+        // the ghost-cell method labels cells from the per-cell lists; no correction lists
+        int st = 0;
+        PB_TRY(read_int(h, h.d_status, &st));
+        if (st)
+        {
+            set_error("mesh leaves the grid interior: every triangle must lie at least two cells inside the grid");
+            return st;
+        }
+        h.n3 = h.b4 = 0;
+        h.p3 = h.p4 = h.pf = 0;
+        return PPPM_OK;
+    }
+
     // ---- corrected cells (3^3) and base cells (4^3)
     int *flag3 = h.d_flags, *len3 = h.d_flags + (nc + 1), *flag4 = h.d_flags + 2 * (nc + 1),
         *len4 = h.d_flags + 3 * (nc + 1);

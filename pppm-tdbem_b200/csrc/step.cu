@@ -22,6 +22,7 @@
 // partial sums stay in registers and are reduced once per triangle / cell.  No atomics.
 #include <algorithm>
 #include "fdtd.cuh"
+#include "ghost.cuh"
 #include "handle.cuh"
 
 namespace pb
@@ -44,22 +45,6 @@ struct StepArgs
     int listen_cell[8];
 };
 
-// what step k of a call produces: its time index, listener-series row and acceleration row
-struct StepDyn
-{
-    int tnew;
-    long long row;
-    const float *acc;
-};
-
-__device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
-{
-    StepDyn d;
-    d.tnew = st->tnew0 + k;
-    d.row = st->row0 + k;
-    d.acc = st->acc ? st->acc + (long long)k * nt : nullptr;
-    return d;
-}
 
 // History rings in the step.  The reference keeps per triangle a ring of 32 values indexed by
 // time mod 32 and reads the 16 taps t, t-1, ..., t-15 (bem.h:55).  The step keeps every ring in
@@ -711,6 +696,8 @@ struct StepLaunch
     NearArgs<R> na;
     R *conv;  // per-triangle convolution sums of the pipelined step
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
+    int ghost;     // ghost-cell method: the ghost kernel after the stencil instead of face / near
+    GhostStep gs;  // its arguments
 };
 
 __global__ void set_state_kernel(StepState *dst, StepState v) { *dst = v; }
@@ -734,11 +721,20 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.ring.nt = h.mesh_set ? h.nt : 0;
     L.series = (R *)h.d_series;
     L.na.series = L.series;
-    L.mesh = h.mesh_set ? 1 : 0;
+    L.mesh = h.mesh_set && h.prm.method == PPPM_METHOD_PPPM ? 1 : 0;
     L.pml = h.prm.pml_width > 0 ? 1 : 0;
     const int m = h.res - 2, T = 256;
     L.pml_blocks = (int)div_up(std::max<long long>((long long)m * m * m, L.a.nt), T);
     L.stencil_blocks = L.sp.nb_in + L.sp.nb_bd + L.sp.nb_nt;
+    if (h.mesh_set && h.prm.method == PPPM_METHOD_GHOST)
+    {
+        if constexpr (sizeof(R) == 4)
+        {
+            L.ghost = 1;
+            L.gs = ghost_args(h, L.a.n_listen, L.a.listen_cell);
+        }
+        return PPPM_OK;
+    }
     if (h.mesh_set)
     {
         L.fa.face_start = h.d_face_start;
@@ -789,6 +785,12 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
     else
         stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
     mark(1);
+    if constexpr (sizeof(R) == 4)
+        if (L.ghost)
+        {
+            ghost_launch(L.gs, L.st, k, L.a.nt, L.series, s);
+            mark(2);
+        }
     if (L.mesh)
     {
         face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.fa);
@@ -936,6 +938,22 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
             PB_CHECK_LAUNCH();
         }
     h.launches += per_step * nsteps;
+    if (L.ghost)
+    {
+        // this and the previous step's accelerations, for the fresh cells of the next update
+        h.launches += nsteps;
+        const size_t row = sizeof(float) * h.nt;
+        if (nsteps >= 2 && acc_dev)
+            PB_CUDA(cudaMemcpyAsync(h.d_gneu_old, acc_dev + (long long)(nsteps - 2) * h.nt, row,
+                                    cudaMemcpyDeviceToDevice, s));
+        else
+            PB_CUDA(cudaMemcpyAsync(h.d_gneu_old, h.d_gneu, row, cudaMemcpyDeviceToDevice, s));
+        if (acc_dev)
+            PB_CUDA(cudaMemcpyAsync(h.d_gneu, acc_dev + (long long)(nsteps - 1) * h.nt, row,
+                                    cudaMemcpyDeviceToDevice, s));
+        else
+            PB_CUDA(cudaMemsetAsync(h.d_gneu, 0, row, s));
+    }
     h.t += nsteps;
     h.series_count += nsteps;
     return PPPM_OK;

@@ -21,14 +21,16 @@ WEIGHTS = {"ref32": 0, "fp64": 1}
 
 DUMP = dict(grid_t=0, grid_tm1=1, grid_tm2=2, neumann=3, dirichlet=4, tri_geom=5, tri_cells=6, cell_counts=7,
             n3_cells=8, n3_tris=9, b4_cells=10, b4_tris=11, n4_tris=12, grid_cache=13, face_pairs=14,
-            face_cache=15, interp=16, cell_type=17, cell_nearest=18, cell_ghost=19, cell_points=20, counts=21)
+            face_cache=15, interp=16, cell_type=17, cell_nearest=18, cell_ghost=19, cell_points=20, counts=21,
+            ghost_cells=22, ghost_order=23, ghost_weights=24, ghost_iters=25)
 
 # dtype of each dump (None: follows the handle precision; "rec": 72-byte weight records)
 _DUMP_DTYPE = dict(grid_t=None, grid_tm1=None, grid_tm2=None, neumann=None, dirichlet=None, tri_geom=np.float32,
                    tri_cells=np.int32, cell_counts=np.int32, n3_cells=np.int32, n3_tris=np.int32,
                    b4_cells=np.int32, b4_tris=np.int32, n4_tris=np.int32, grid_cache="rec", face_pairs=np.int32,
                    face_cache="rec", interp=np.float32, cell_type=np.int32, cell_nearest=np.int32,
-                   cell_ghost=np.int32, cell_points=np.float32, counts=np.int32)
+                   cell_ghost=np.int32, cell_points=np.float32, counts=np.int32, ghost_cells=np.int32,
+                   ghost_order=np.int32, ghost_weights=np.float32, ghost_iters=np.int32)
 
 # the reference's LayerWeightHalf record (bem.h:163-169)
 RECORD = np.dtype([("s", "<f2", 16), ("ms", "<f4"), ("d", "<f2", 16), ("md", "<f4")])
@@ -45,7 +47,11 @@ class _Params(ctypes.Structure):
     _fields_ = [("res", ctypes.c_int), ("dl", ctypes.c_float), ("dt", ctypes.c_float),
                 ("min_pos", ctypes.c_float * 3), ("pml_width", ctypes.c_int), ("reflect_coeff", ctypes.c_float),
                 ("c", ctypes.c_float), ("rho", ctypes.c_float), ("precision", ctypes.c_int),
-                ("weights", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+                ("weights", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
+                ("method", ctypes.c_int), ("ghost_threshold", ctypes.c_float)]
+
+
+METHOD = dict(pppm=0, ghost=1)
 
 
 def _load():
@@ -180,7 +186,10 @@ class Solver:
     """One scene: FDTD grid + TDBEM near-field correction (reference PPPMSolver)."""
 
     def __init__(self, res, dl, dt, min_pos=(0.0, 0.0, 0.0), pml_width=0, reflect_coeff=0.83, c=340.3,
-                 rho=1.225, precision="fp32", weights="ref32", device=0, stream=None):
+                 rho=1.225, precision="fp32", weights="ref32", device=0, stream=None, method="pppm",
+                 ghost_threshold=25.0):
+        """method "pppm": FDTD + TDBEM near-field correction (PPPMSolver); "ghost": FDTD + ghost
+        cells (GhostCellSolver) with the given condition-number threshold (0: first order)."""
         p = _Params()
         check(lib.pppm_params_default(ctypes.byref(p)), "params_default")
         p.res, p.dl, p.dt = int(res), float(dl), float(dt)
@@ -189,6 +198,7 @@ class Solver:
         p.pml_width, p.reflect_coeff, p.c, p.rho = int(pml_width), float(reflect_coeff), float(c), float(rho)
         p.precision, p.weights, p.device = PRECISION[precision], WEIGHTS[weights], int(device)
         p.stream = stream
+        p.method, p.ghost_threshold = METHOD[method], float(ghost_threshold)
         self.h = ctypes.c_void_p()
         check(lib.pppm_create(ctypes.byref(p), ctypes.byref(self.h)), "pppm_create")
         self.res, self.dl, self.dt = int(res), float(dl), float(dt)
