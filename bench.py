@@ -377,7 +377,11 @@ def run_batch(args, ws, rank, local):
     from pppm_b200 import Batch, Solver
 
     W, K = args.warmup, args.steps
-    specs = scenes.batch_scenes(BATCH_SCENES, BATCH_SEED)
+    all_specs = scenes.batch_scenes(BATCH_SCENES, BATCH_SEED)
+    # N ranks: a static partition of the scenes by estimated cost, no exchange while stepping,
+    # one gather of the listener series at the end (strong scaling: the 64-scene job is fixed)
+    mine = scenes.shard_by_cost(all_specs, ws)[rank]
+    specs = [all_specs[i] for i in mine]
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
@@ -436,14 +440,29 @@ def run_batch(args, ws, rank, local):
     rewind()
     run_sequential()
     same = all(np.array_equal(a, s.listeners()) for a, s in zip(series_b, solvers))
-    value = BATCH_SCENES * K * ws / (ms_b * 1e-3)
-    seq = BATCH_SCENES * reps_s * ws / (ms_s * 1e-3)
-    cell_steps = sum(float(sp["res"]) ** 3 * sp["steps"] for sp in specs)
+    value = BATCH_SCENES * K / (ms_b * 1e-3)
+    seq = BATCH_SCENES * reps_s / (ms_s * 1e-3)
+    cell_steps = sum(float(sp["res"]) ** 3 * sp["steps"] for sp in all_specs)
     # compulsory bytes of the whole job (per-step kernel bytes of each scene x its steps)
     job_bytes = 0.0
     for sp, s in zip(specs, solvers):
         counts = [int(x) for x in s.dump("counts")]
         job_bytes += sum(algorithmic_bytes(counts, sp["res"], len(sp["tris"])).values()) * sp["steps"]
+    gather_ms, gathered = 0.0, len(specs)
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([job_bytes], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        job_bytes = float(t.item())
+        # the job's result: every scene's listener series on every rank
+        barrier(ws)
+        t0 = time.perf_counter()
+        parts = [None] * ws
+        dist.all_gather_object(parts, [(i, s.listeners()) for i, s in zip(mine, solvers)])
+        gather_ms = max_over_ranks(ws, (time.perf_counter() - t0) * 1e3)
+        gathered = len({i for part in parts for i, _ in part})
+        same = bool(int(max_over_ranks(ws, 0.0 if same else 1.0)) == 0)
 
     e2e = None
     if not args.no_e2e:
@@ -464,7 +483,7 @@ def run_batch(args, ws, rank, local):
                 d2h += s.listeners().nbytes
         torch.cuda.synchronize()
         te = max_over_ranks(ws, time.perf_counter() - t0)
-        e2e = {"value": round(BATCH_SCENES * K * ws / te, 3), "unit": "scenes/s", "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": round(BATCH_SCENES * K / te, 3), "unit": "scenes/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
         del pinned
 
@@ -476,12 +495,16 @@ def run_batch(args, ws, rank, local):
         s.close()
     return {
         "metric": "scenes/s, %s" % BATCH_NAME, "value": round(value, 3), "unit": "scenes/s", "n_gpus": ws,
-        "steps": K, "warmup": W, "ms_per_step": round(ms_b / K, 3), "higher_is_better": True, "scaling": "weak",
+        "steps": K, "warmup": W, "ms_per_step": round(ms_b / K, 3), "higher_is_better": True,
+        "scaling": "strong" if ws > 1 else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes and accelerations)",
         "config": {"workload": BATCH_NAME, "scenes": BATCH_SCENES, "time_steps_per_bench_step":
-                   int(sum(sp["steps"] for sp in specs)), "gcell_steps_per_bench_step": round(cell_steps / 1e9, 3),
+                   int(sum(sp["steps"] for sp in all_specs)), "gcell_steps_per_bench_step": round(cell_steps / 1e9, 3),
                    "bench_step": "every scene through all of its time steps (one pppm_batch_run call)",
-                   "l2": "flushed (256 MiB write) between timed iterations", "parallelism": "replicas x%d" % ws},
+                   "l2": "flushed (256 MiB write) between timed iterations",
+                   "parallelism": "scenes sharded by estimated cost over %d ranks, no exchange while stepping" % ws
+                   if ws > 1 else "one GPU", "scenes_on_rank0": len(specs), "series_gathered": gathered,
+                   "gather_ms": round(gather_ms, 3)},
         "sequential": {"value": round(seq, 3), "unit": "scenes/s", "reps": reps_s, "ms_per_rep": round(ms_s / reps_s, 3),
                        "gpu_launches_per_rep": int(launches_s // reps_s), "listeners_bit_identical": bool(same)},
         "batched_over_sequential": round(value / seq, 3),
@@ -491,7 +514,7 @@ def run_batch(args, ws, rank, local):
                      "achieved_sequential": round(job_bytes * reps_s / (ms_s * 1e-3) / 1e9, 1),
                      "peak": measured_peak()[0], "unit": "GB/s", "peak_kind": measured_peak()[1],
                      "frac": round(job_bytes * K / (ms_b * 1e-3) / 1e9 / measured_peak()[0], 4)},
-        "gcell_steps_per_s": round(cell_steps * K * ws / (ms_b * 1e-3) / 1e9, 3),
+        "gcell_steps_per_s": round(cell_steps * K / (ms_b * 1e-3) / 1e9, 3),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
     }
 

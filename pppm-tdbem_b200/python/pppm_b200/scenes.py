@@ -203,3 +203,27 @@ def batch_scenes(n=64, seed=11, c=C_REF):
         steps = int(rng.integers(1000, 4001))
         out.append(dict(res=res, verts=v, tris=f, h=h, min_pos=mn, dt=dt, steps=steps, freq=float(rng.uniform(500, 2000))))
     return out
+
+
+def scene_cost(spec):
+    """Estimated device work of one batch scene for sharding: steps x (grid cells + face-pair
+    bytes in cell units).  The face pairs of a closed surface of T triangles spanning about half
+    the grid: each centre sees the triangles of the ~16 surface cells of its 4^3 block, and the
+    surface covers ~4 pi (res / 4)^2 cells, so P4 ~ 16 T^2 / (pi res^2 / 4); a face pair moves
+    76 bytes against 12 per grid cell."""
+    res, nt = spec["res"], len(spec["tris"])
+    p4 = 16.0 * nt * nt / (math.pi * res * res / 4.0)
+    return float(spec["steps"]) * (res ** 3 + p4 * 76.0 / 12.0)
+
+
+def shard_by_cost(specs, world):
+    """Static partition of batch scenes over `world` ranks: longest-processing-time-first by
+    scene_cost (ties by index).  Returns one ascending index list per rank."""
+    order = sorted(range(len(specs)), key=lambda i: (-scene_cost(specs[i]), i))
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        shards[r].append(i)
+        load[r] += scene_cost(specs[i])
+    return [sorted(s) for s in shards]
