@@ -1067,6 +1067,7 @@ struct BatchScene
     FaceArgs<R> fa;
     NearArgs<R> na;
     StepState *st;
+    R *conv;         // the scene's per-triangle convolution sums (pipelined graphs)
     int near_warps;  // warps of this scene's near grid
 };
 
@@ -1095,6 +1096,52 @@ __global__ void __launch_bounds__(256) batch_near_kernel(const BatchScene<R> *sc
     const BatchScene<R> &S = sc[m.x];
     near_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), S.na, S.st->n3, m.y * 8 + (threadIdx.x >> 5), S.near_warps,
                  threadIdx.x & 31, 0);
+}
+
+// the pipelined batch step (see capture_pipelined): face-pair convolutions, the rest of the face
+// stage, and the first step's Neumann values, over the same per-scene block maps
+template <typename R>
+__global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    const int tri = m.y * 8 + (threadIdx.x >> 5);
+    if (tri >= S.a.nt)
+        return;
+    const R v = face_conv<R>(S.ring, S.st->tnew0 + k, S.fa, tri, threadIdx.x & 31);
+    if ((threadIdx.x & 31) == 0)
+        S.conv[tri] = v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) batch_finish_kernel(const BatchScene<R> *sc, const int2 *map, int k, int next)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    const int tri = m.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (tri >= S.a.nt)
+        return;
+    const StepDyn dy = bind_step(S.st, k, S.a.nt);
+    R iw, pv;
+    face_corners<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv);
+    face_finish<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv, S.conv[tri]);
+    if (next && lane == 0)
+    {
+        const StepDyn dn = bind_step(S.st, k + 1, S.a.nt);
+        if (dn.acc)
+            S.ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
+    }
+}
+
+template <typename R>
+__global__ void batch_nwrite_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    const int i = m.y * blockDim.x + threadIdx.x;
+    const StepDyn dy = bind_step(S.st, k, S.a.nt);
+    if (i < S.a.nt && dy.acc)
+        S.ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
 }
 
 // after G steps: every active scene's state moves on by G steps
@@ -1132,13 +1179,17 @@ struct Batch
     cudaStream_t stream = nullptr;  // the first scene's stream
     cudaEvent_t ev = nullptr;
     std::vector<unsigned char> host_scenes;
-    std::vector<int2> host_map[3];
+    // block maps: 0 stencil (with the Neumann range), 1 face (8 triangles per block), 2 near,
+    // 3 stencil without the Neumann range, 4 Neumann values (256 triangles per block)
+    std::vector<int2> host_map[5];
     std::vector<StepState *> host_states;
     std::vector<int> host_nt;
     void *d_scenes = nullptr;
     size_t scenes_cap = 0;
-    int2 *d_map[3] = {nullptr, nullptr, nullptr};
-    size_t map_cap[3] = {0, 0, 0};
+    int2 *d_map[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t map_cap[5] = {0, 0, 0, 0, 0};
+    cudaStream_t side = nullptr;                      // second branch while recording
+    cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;  // fork / join points while recording
     StepState **d_states = nullptr;
     int *d_nt = nullptr;
     size_t states_cap = 0, nt_cap = 0;
@@ -1189,6 +1240,7 @@ int batch_tables(Batch &b, const std::vector<int> &active)
         S.fa = L.fa;
         S.na = L.na;
         S.st = h.d_state;
+        S.conv = L.conv;
         const int near_blocks = std::max(1, div_up((long long)h.n3 * 32, T));
         S.near_warps = near_blocks * (T / 32);
         memcpy(b.host_scenes.data() + ai * sizeof(S), &S, sizeof(S));
@@ -1198,6 +1250,10 @@ int batch_tables(Batch &b, const std::vector<int> &active)
             b.host_map[1].push_back(make_int2((int)ai, k));
         for (int k = 0; k < near_blocks; k++)
             b.host_map[2].push_back(make_int2((int)ai, k));
+        for (int k = 0; k < L.sp.nb_bd + L.sp.nb_in; k++)
+            b.host_map[3].push_back(make_int2((int)ai, k));
+        for (int k = 0; k < div_up(h.nt, T); k++)
+            b.host_map[4].push_back(make_int2((int)ai, k));
         b.host_states[ai] = h.d_state;
         b.host_nt[ai] = h.nt;
     }
@@ -1205,7 +1261,7 @@ int batch_tables(Batch &b, const std::vector<int> &active)
     PB_TRY(grow((unsigned char **)&ds, b.scenes_cap, b.host_scenes.size()));
     b.d_scenes = ds;
     PB_CUDA(cudaMemcpyAsync(b.d_scenes, b.host_scenes.data(), b.host_scenes.size(), cudaMemcpyHostToDevice, b.stream));
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 5; i++)
     {
         PB_TRY(grow(&b.d_map[i], b.map_cap[i], b.host_map[i].size()));
         PB_CUDA(cudaMemcpyAsync(b.d_map[i], b.host_map[i].data(), b.host_map[i].size() * sizeof(int2),
@@ -1224,9 +1280,9 @@ template <typename R>
 int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
 {
     std::vector<unsigned char> sig(b.host_scenes);
-    const void *ptrs[] = {b.d_scenes, b.d_map[0], b.d_map[1], b.d_map[2], b.d_states, b.d_nt};
-    const size_t sizes[] = {b.host_map[0].size(), b.host_map[1].size(), b.host_map[2].size(), (size_t)g,
-                            (size_t)nactive};
+    const void *ptrs[] = {b.d_scenes, b.d_map[0], b.d_map[1], b.d_map[2], b.d_map[3], b.d_map[4], b.d_states, b.d_nt};
+    const size_t sizes[] = {b.host_map[0].size(), b.host_map[1].size(), b.host_map[2].size(), b.host_map[3].size(),
+                            b.host_map[4].size(), (size_t)g, (size_t)nactive};
     sig.insert(sig.end(), (const unsigned char *)ptrs, (const unsigned char *)ptrs + sizeof(ptrs));
     sig.insert(sig.end(), (const unsigned char *)sizes, (const unsigned char *)sizes + sizeof(sizes));
     for (auto &gr : b.graphs)
@@ -1243,15 +1299,37 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
     const BatchScene<R> *sc = (const BatchScene<R> *)b.d_scenes;
     const int n0 = (int)b.host_map[0].size(), n1 = (int)b.host_map[1].size(), n2 = (int)b.host_map[2].size();
     cudaGraph_t graph = nullptr;
+    const int n3 = (int)b.host_map[3].size(), n4 = (int)b.host_map[4].size();
     PB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < g; k++)
+    if (n1 > 0 && n4 > 0 && b.side)
     {
-        batch_stencil_kernel<R><<<n0, 256, 0, b.stream>>>(sc, b.d_map[0], k);
-        if (n1 > 0)
-            batch_face_kernel<R><<<n1, 256, 0, b.stream>>>(sc, b.d_map[1], k);
-        if (n2 > 0)
-            batch_near_kernel<R><<<n2, 256, 0, b.stream>>>(sc, b.d_map[2], k);
+        // two branches as for one scene (capture_pipelined): each step's face-pair convolutions
+        // beside the previous near stage and this step's stencil
+        cudaStream_t s = b.stream;
+        batch_nwrite_kernel<R><<<n4, 256, 0, s>>>(sc, b.d_map[4], 0);
+        cudaEventRecord(b.ev_fin, s);
+        for (int k = 0; k < g; k++)
+        {
+            cudaStreamWaitEvent(b.side, b.ev_fin, 0);
+            batch_conv_kernel<R><<<n1, 256, 0, b.side>>>(sc, b.d_map[1], k);
+            cudaEventRecord(b.ev_conv, b.side);
+            batch_stencil_kernel<R><<<n3, 256, 0, s>>>(sc, b.d_map[3], k);
+            cudaStreamWaitEvent(s, b.ev_conv, 0);
+            batch_finish_kernel<R><<<n1, 256, 0, s>>>(sc, b.d_map[1], k, k + 1 < g ? 1 : 0);
+            cudaEventRecord(b.ev_fin, s);
+            if (n2 > 0)
+                batch_near_kernel<R><<<n2, 256, 0, s>>>(sc, b.d_map[2], k);
+        }
     }
+    else
+        for (int k = 0; k < g; k++)
+        {
+            batch_stencil_kernel<R><<<n0, 256, 0, b.stream>>>(sc, b.d_map[0], k);
+            if (n1 > 0)
+                batch_face_kernel<R><<<n1, 256, 0, b.stream>>>(sc, b.d_map[1], k);
+            if (n2 > 0)
+                batch_near_kernel<R><<<n2, 256, 0, b.stream>>>(sc, b.d_map[2], k);
+        }
     batch_advance_kernel<<<div_up(nactive, 128), 128, 0, b.stream>>>(b.d_states, b.d_nt, nactive, g);
     cudaError_t e = cudaStreamEndCapture(b.stream, &graph);
     if (e == cudaSuccess)
@@ -1345,9 +1423,11 @@ int batch_create(Handle **hs, int n, Batch **out)
             set_error("batch scene %d has no mesh", i);
             return PPPM_ERR_STATE;
         }
-        if (hs[i]->prm.pml_width > 0 || hs[i]->fp64 != hs[0]->fp64 || hs[i]->prm.device != hs[0]->prm.device)
+        if (hs[i]->prm.pml_width > 0 || hs[i]->fp64 != hs[0]->fp64 || hs[i]->prm.device != hs[0]->prm.device ||
+            hs[i]->prm.method != PPPM_METHOD_PPPM)
         {
-            set_error("batch scenes must share device and precision and use the absorbing boundary (scene %d)", i);
+            set_error("batch scenes must share device and precision and use the absorbing boundary and the "
+                      "PPPM method (scene %d)", i);
             return PPPM_ERR_ARG;
         }
         for (int j = 0; j < i; j++)
@@ -1363,7 +1443,10 @@ int batch_create(Handle **hs, int n, Batch **out)
     b->hs.assign(hs, hs + n);
     b->fp64 = hs[0]->fp64;
     b->stream = hs[0]->stream;
-    if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess)
+    if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fin, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_conv, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess)
     {
         delete b;
         set_error("cudaEventCreate failed");
@@ -1395,6 +1478,12 @@ void batch_destroy(Batch *b)
     dev_free(b->d_nt);
     if (b->ev)
         cudaEventDestroy(b->ev);
+    if (b->ev_fin)
+        cudaEventDestroy(b->ev_fin);
+    if (b->ev_conv)
+        cudaEventDestroy(b->ev_conv);
+    if (b->side)
+        cudaStreamDestroy(b->side);
     delete b;
 }
 
