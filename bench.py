@@ -8,7 +8,10 @@ frame).  One benchmark step = one motion frame: update_mesh (lists + cache refre
 69 time steps of that frame.  `value` is device-resident (inputs uploaded before timing);
 `e2e` drives the same frames through the public API from pinned host buffers and reads the
 listener samples back every frame.  --workload static runs the 1280-triangle sphere at
-res 32 without motion (benchmark step = 100 time steps).
+res 32 without motion (benchmark step = 100 time steps).  --workload large runs two moving
+20480-triangle icospheres at res 128 (2.1 M cells, ~6.2 M face pairs; one benchmark step = one
+1 kHz motion frame of 82 time steps).  --workload batch: 64 independent scenes in one batched
+run (scenes/s); --workload adjoint: the transposed step against the forward step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -36,6 +39,7 @@ sys.path.insert(0, os.path.join(ROOT, "pppm-tdbem_b200", "python"))
 from pppm_b200 import scenes  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20
+CPU_SAMPLE_STEPS = 10
 
 
 def parse():
@@ -44,7 +48,7 @@ def parse():
     p.add_argument("--steps", type=int, default=60, help="timed benchmark steps (motion frames)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint"])
+    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint", "large"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--summarize-launches", metavar="CSV",
@@ -145,17 +149,15 @@ class Workload:
 
     def __init__(self, kind, nframes):
         self.kind = kind
-        if kind == "moving":
-            sc = scenes.MovingScene()
+        self.moving = kind in ("moving", "large")
+        if self.moving:
+            sc = scenes.MovingScene() if kind == "moving" else scenes.LargeScene()
             self.scene = sc
-            steps_needed = int(math.ceil((nframes + 1) / sc.frame_hz / float(sc.dt))) + 2
-            frame = [sc.frame_of_step(s) for s in range(steps_needed)]
-            self.ranges = []
-            for f in range(nframes + 1):
-                idx = [s for s in range(steps_needed) if frame[s] == f]
-                self.ranges.append((idx[0], idx[-1] + 1))
+            self.ranges = scenes.frame_ranges(sc, nframes)
             self.verts = [sc.frame_verts(f) for f in range(nframes + 1)]
-            self.name = "moving icosphere (5120 tris) + static plate (1280 tris), res 64, 1 kHz motion frames"
+            self.name = ("moving icosphere (5120 tris) + static plate (1280 tris), res 64, 1 kHz motion frames"
+                         if kind == "moving" else
+                         "two moving icospheres (2 x 20480 tris), res 128, 1 kHz motion frames")
         else:
             sc = scenes.StaticSphere()
             self.scene = sc
@@ -185,15 +187,32 @@ def algorithmic_bytes(counts, res, nt):
     return {"stencil": stencil, "face": face, "near": near}
 
 
-def load_traffic():
+def conv_bytes(counts, nt, pairs):
+    """Compulsory bytes of one launch of the face-pair convolution: per pair its weights (64),
+    scale (8) and neighbour index (4); per triangle its list start, its own two history windows
+    (2 x 64) and its output sum(s); the two-step pass also reads the next acceleration row."""
+    pf = counts[4]
+    return pf * (64 + 8 + 4) + nt * (4 + 2 * 64 + (8 + 4 if pairs else 4))
+
+
+def fix_bytes(counts, nt):
+    """Compulsory bytes of the completion of a two-step pass: per pair its tap-1 factor and
+    neighbour index; per triangle its list start, the neighbour value it gathers, the partial sum
+    read and the sum written."""
+    return counts[4] * (4 + 4) + nt * (4 + 4 + 4 + 4)
+
+
+def load_traffic(workload):
+    """ncu DRAM bytes (read + write) per launch by kernel for one workload, from
+    profiles/traffic.txt (lines: workload kernel bytes)."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     out = {}
     if os.path.exists(path):
         for line in open(path):
             f = line.split()
-            if len(f) >= 2 and not line.startswith("#"):
+            if len(f) >= 3 and not line.startswith("#") and f[0] == workload:
                 try:
-                    out[f[0]] = float(f[1])
+                    out[f[1]] = float(f[2])
                 except ValueError:
                     pass
     return out
@@ -230,10 +249,13 @@ def run_ours(args, ws, rank, local):
     s = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
     s.set_mesh(wl.verts[0], wl.tris)
     s.add_listener(*wl.listener)
+    # face-stage autotuner on the first frame's mesh (setup, untimed): picks one or two steps per
+    # pass over the face pairs and the block size of the face kernels
+    tune = s.autotune(reps=20)
 
     def frame(f, timed_events=None):
         a, b = wl.ranges[f]
-        if f > 0 and wl.kind == "moving":
+        if f > 0 and wl.moving:
             s.update_mesh(verts_dev[f])
         s.step(acc_dev[a:b])
 
@@ -252,7 +274,7 @@ def run_ours(args, ws, rank, local):
         e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         a, b = wl.ranges[f]
         e0.record(stream)
-        if wl.kind == "moving":
+        if wl.moving:
             s.update_mesh(verts_dev[f])
         em.record(stream)
         s.step(acc_dev[a:b])
@@ -277,10 +299,17 @@ def run_ours(args, ws, rank, local):
     counts = [int(x) for x in s.dump("counts")]
     alg = {k: int(v) for k, v in algorithmic_bytes(counts, wl.res, len(wl.tris)).items()}
     times = {"stencil": us_st, "face": us_face, "near": us_near}
-    top = max(times, key=lambda k: times[k])
+    # the dominant kernel of the recorded steps: the tuned face-pair convolution (its launch time
+    # from the autotuner's events on the solver's stream, last frame's mesh: re-tuned here)
+    tune = s.autotune(reps=20)
+    pairs, threads = tune["best"]
+    nt = len(wl.tris)
+    top = "conv2" if pairs else "conv"
+    top_us = tune["launch_us"][tune["best"]][0]
+    top_bytes = conv_bytes(counts, nt, pairs)
     peak, peak_kind = measured_peak()
-    achieved = float(alg[top] / (times[top] * 1e-6) / 1e9)
-    traffic = load_traffic().get(top)
+    achieved = float(top_bytes / (top_us * 1e-6) / 1e9)
+    traffic = load_traffic(args.workload).get(top)
     # split of a timed frame: update_mesh, then the frame's time steps (one recorded graph)
     us_update = (total_ms - step_ms) * 1e3 / K
     us_per_step = step_ms * 1e3 / steps
@@ -289,6 +318,8 @@ def run_ours(args, ws, rank, local):
     e2e = None
     if not args.no_e2e:
         s2 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+        s2.set_option("conv_pairs", pairs)
+        s2.set_option("face_threads", threads)
         s2.set_mesh(wl.verts[0], wl.tris)
         s2.add_listener(*wl.listener)
         acc_pin = torch.from_numpy(wl.acc).pin_memory()
@@ -297,7 +328,7 @@ def run_ours(args, ws, rank, local):
         h2d = d2h = 0
         for f in range(0, W + 1):
             a, b = wl.ranges[f]
-            if f > 0 and wl.kind == "moving":
+            if f > 0 and wl.moving:
                 s2.update_mesh(verts_pin[f])
             s2.step(acc_pin[a:b])
         barrier(ws)
@@ -305,7 +336,7 @@ def run_ours(args, ws, rank, local):
         steps2 = 0
         for f in range(W + 1, W + K + 1):
             a, b = wl.ranges[f]
-            if wl.kind == "moving":
+            if wl.moving:
                 s2.update_mesh(verts_pin[f])
                 h2d += verts_pin[f].numel() * 4
             s2.step(acc_pin[a:b])
@@ -332,14 +363,19 @@ def run_ours(args, ws, rank, local):
         "dtype": "f32", "data": "synthetic (seeded meshes, trajectories and accelerations)",
         "config": {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris)),
                    "time_steps_per_bench_step": round(steps / K, 2), "time_steps_timed": steps,
-                   "bench_step": "one motion frame: update_mesh + its time steps" if wl.kind == "moving"
+                   "bench_step": "one motion frame: update_mesh + its time steps" if wl.moving
                    else "100 time steps", "l2": "flushed (256 MiB write) between timed iterations",
                    "parallelism": "replicas x%d" % ws, "precision": "fp32 grids, fp16+scale weights",
                    "n3_cells": int(counts[0]), "pairs_3x3x3": int(counts[1]), "face_pairs": int(counts[4])},
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes": alg[top],
-                     "kernel_us": {k: round(v, 3) for k, v in times.items()},
+                     "traffic": traffic, "algorithmic_bytes": int(top_bytes), "kernel_launch_us": round(top_us, 3),
+                     "autotune": {"best": {"two_steps_per_pass": bool(pairs), "threads": threads},
+                                  "us_per_two_steps": {"%s/%d" % ("pairs" if p else "single", t): round(u, 2)
+                                                       for (p, t), u in tune["us"].items()}},
+                     "fix_us": round(tune["launch_us"][tune["best"]][1], 3) if pairs else None,
+                     "fix_bytes": int(fix_bytes(counts, nt)) if pairs else None,
+                     "kernel_us_measurement_mode": {k: round(v, 3) for k, v in times.items()},
                      "update_mesh_us": round(us_update, 1), "time_step_us": round(us_per_step, 2),
                      "gb_per_s_all_kernels": round(sum(alg.values()) / (sum(times.values()) * 1e-6) / 1e9, 1)},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
@@ -636,16 +672,23 @@ def cpu_baseline(wl):
     o.set_mesh(wl.verts[0], wl.tris)
     f = 1
     a, b = wl.ranges[f]
+    # the large scene's frame takes about a minute on the host: time update_mesh and the first
+    # CPU_SAMPLE_STEPS of its steps, and extrapolate the steps to the whole frame
+    n = b - a if wl.kind != "large" else min(b - a, CPU_SAMPLE_STEPS)
     t0 = time.perf_counter()
-    if wl.kind == "moving":
+    if wl.moving:
         o.update_mesh(wl.verts[f])
-    o.step(wl.acc[a:b], listeners=[wl.listener])
-    dt = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    o.step(wl.acc[a:a + n], listeners=[wl.listener])
+    t2 = time.perf_counter()
     o.close()
+    dt = (t1 - t0) + (t2 - t1) * (b - a) / n
+    sample = "one benchmark step (%d time steps%s) of the same workload, C restatement with OpenMP" % (
+        b - a, " + update_mesh" if wl.moving else "")
+    if n < b - a:
+        sample += "; update_mesh and the first %d time steps timed, the steps extrapolated to %d" % (n, b - a)
     return {"value": round(float(wl.res) ** 3 * (b - a) / dt / 1e9, 5), "unit": "Gcell-steps/s",
-            "cores": oracle_threads(), "kind": "port",
-            "sample": "one benchmark step (%d time steps%s) of the same workload, C restatement with OpenMP"
-                      % (b - a, " + update_mesh" if wl.kind == "moving" else "")}
+            "cores": oracle_threads(), "kind": "port", "sample": sample}
 
 
 # ---------------------------------------------------------------- reference arm -------
@@ -667,7 +710,7 @@ def run_reference(args, ws, rank, local):
 
         r = O.Reference(wl.res, sc.h, sc.dt, sc.min_pos)
         r.set_mesh(wl.verts[0], wl.tris)
-        if wl.kind == "moving":
+        if wl.moving:
             for v in wl.verts[1:]:
                 r.check_mesh(v)  # validate the whole trajectory against the reference capacities
             r.set_checks(False)
@@ -677,7 +720,7 @@ def run_reference(args, ws, rank, local):
 
         def frame(f):
             a, b = wl.ranges[f]
-            if f > 0 and wl.kind == "moving":
+            if f > 0 and wl.moving:
                 r.update_mesh(wl.verts[f])
             r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
 
@@ -704,7 +747,7 @@ def run_reference(args, ws, rank, local):
         steps = 0
         for f in range(1, min(W + K, 3) + 1):
             a, b = wl.ranges[f]
-            if wl.kind == "moving":
+            if wl.moving:
                 o.update_mesh(wl.verts[f])
             o.step(wl.acc[a:b], listeners=[wl.listener])
             steps += b - a

@@ -233,6 +233,26 @@ int pppm_pair_weights(int device, float dt, float dl, float c, const float *vert
 int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float c, const float *verts, int nv,
                              const int *src, int to_point, const int *dst_face, const float *dst_point, float *out32);
 
+/* ------------------------------------------------------------ tuning ----------------- */
+/* No counterpart in the reference.  Launch options of the recorded step graphs (pppm_step calls
+ * of 4 or more steps with the absorbing boundary).  A change takes effect at the next such call,
+ * which records new graphs. */
+#define PPPM_OPT_CONV_PAIRS 0   /* 1 (default): the face-pair convolution streams the pairs' weights
+                                   once for two consecutive steps; 0: once per step             */
+#define PPPM_OPT_FACE_THREADS 1 /* threads per block of the face-stage kernels: 64, 128, 256    */
+int pppm_set_option(pppm_handle *h, int option, int value);
+int pppm_get_option(pppm_handle *h, int option, int *value);
+/* No counterpart in the reference.  Autotuner of the face stage: on the current mesh and state,
+ * times the face-pair convolution of two steps in each of PPPM_TUNE_CANDIDATES configurations
+ * (candidate i: pairs = i / 3, threads = {64, 128, 256}[i % 3]), reps launches of each of its two
+ * kernels, and sets the options to the fastest.  us_out (may be NULL; 2 * PPPM_TUNE_CANDIDATES
+ * floats): microseconds per launch of candidate i's first kernel (us_out[2 i]: the convolution,
+ * or the two-step convolution) and second kernel (us_out[2 i + 1]: the next step's convolution,
+ * or the two-step pass's completion); *best (may be NULL): the index chosen.  Changes no field
+ * or history.  Needs a mesh and the PPPM method. */
+#define PPPM_TUNE_CANDIDATES 6
+int pppm_autotune(pppm_handle *h, int reps, float *us_out, int *best);
+
 /* ------------------------------------------------------------ diagnostics ------------ */
 const char *pppm_status_string(int status);
 const char *pppm_last_error_message(void);

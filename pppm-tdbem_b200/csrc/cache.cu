@@ -669,9 +669,12 @@ __global__ void gather_face_kernel(const int *face_pool, long long pf, const Rec
 // 0.5 * area - sum_j factor_j with factor_j = double-layer weight 0 of pair j, summed in
 // list order in the working precision (pppm.cu:172-193)
 // One warp per triangle: lanes fetch 32 factors at a time, every lane then adds them in list
-// order, so the sum rounds exactly like a sequential loop.
+// order, so the sum rounds exactly like a sequential loop.  Also writes each pair's
+// double-layer tap 1 with its scale applied (the factor of D[t-1] in the convolution, as the
+// step evaluates it) into d1 (float for FP32 handles, double for FP64), which the two-step
+// convolution of the step reads (step.cu: fix_kernel).
 __global__ void denom_kernel(const int *face_start, int nt, const float *area, const __half2 *face_w,
-                             const float2 *face_scale, const double2 *face_wd, double *denom)
+                             const float2 *face_scale, const double2 *face_wd, double *denom, void *d1)
 {
     int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     int lane = threadIdx.x & 31;
@@ -688,9 +691,17 @@ __global__ void denom_kernel(const int *face_start, int nt, const float *area, c
         if (p < e)
         {
             if (face_wd)
+            {
                 fd = face_wd[(size_t)p * kTaps].y;
+                if (d1)
+                    ((double *)d1)[p] = face_wd[(size_t)p * kTaps + 1].y;
+            }
             else
+            {
                 f = (float)__high2half(face_w[(size_t)p * kTaps]) * face_scale[p].y;
+                if (d1)
+                    ((float *)d1)[p] = __high2float(face_w[(size_t)p * kTaps + 1]) * face_scale[p].y;
+            }
         }
         int cnt = min(32, e - base);
         for (int j = 0; j < cnt; j++)
@@ -883,7 +894,8 @@ int cache_refresh(Handle &h)
     }
     denom_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(h.d_face_start, nt, h.d_area,
                                               h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
-                                              h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
+                                              h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom,
+                                              h.d_face_d1);
     h.launches++;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
@@ -976,7 +988,8 @@ int cache_regather(Handle &h)
     }
     denom_kernel<<<div_up((long long)h.nt * 32, T), T, 0, s>>>(h.d_face_start, h.nt, h.d_area,
                                                 h.fp64 ? nullptr : (const __half2 *)h.d_face_w, h.d_face_scale,
-                                                h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom);
+                                                h.fp64 ? (const double2 *)h.d_face_w : nullptr, h.d_face_denom,
+                                              h.d_face_d1);
     h.launches++;
     PB_CHECK_LAUNCH();
     return PPPM_OK;

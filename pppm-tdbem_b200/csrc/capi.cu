@@ -142,7 +142,8 @@ void free_mesh(Handle &h)
                      (void **)&h.d_face_scale, (void **)&h.d_face_corner, (void **)&h.d_pair_flag,
                      (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
                      (void **)&h.d_hist,       (void **)&h.d_terms,       (void **)&h.d_conv,
-                     (void **)&h.d_gneu,       (void **)&h.d_gneu_old};
+                     (void **)&h.d_gneu,       (void **)&h.d_gneu_old,    (void **)&h.d_face_d1,
+                     (void **)&h.d_conv1,      (void **)&h.d_dlast};
     for (void **q : ptrs)
     {
         dev_free(*q);
@@ -408,6 +409,9 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_TRY(dev_alloc(&h.d_hist, (size_t)8 * nt * kRing * h.real_size));
     PB_TRY(dev_alloc(&h.d_terms, (size_t)54 * nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_conv, (size_t)nt * h.real_size));
+    PB_TRY(dev_alloc(&h.d_conv1, (size_t)nt * h.real_size));
+    PB_TRY(dev_alloc(&h.d_dlast, (size_t)nt * h.real_size));
+    PB_CUDA(cudaMemsetAsync(h.d_dlast, 0, (size_t)nt * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
     if (rc == PPPM_OK && h.prm.method == PPPM_METHOD_GHOST)
@@ -1199,6 +1203,68 @@ int pppm_launch_count(pppm_handle *ph, long long *count)
     if (!count)
         return PPPM_ERR_ARG;
     *count = ph->h.launches;
+    return PPPM_OK;
+}
+
+int pppm_set_option(pppm_handle *ph, int option, int value)
+{
+    PB_TRY(check_handle(ph));
+    Handle &h = ph->h;
+    switch (option)
+    {
+    case PPPM_OPT_CONV_PAIRS:
+        if (value != 0 && value != 1)
+            break;
+        h.conv_pairs = value != 0;
+        return PPPM_OK;
+    case PPPM_OPT_FACE_THREADS:
+        if (value != 64 && value != 128 && value != 256)
+            break;
+        h.face_threads = value;
+        return PPPM_OK;
+    default:
+        set_error("unknown option %d", option);
+        return PPPM_ERR_ARG;
+    }
+    set_error("option %d: value %d out of range", option, value);
+    return PPPM_ERR_ARG;
+}
+
+int pppm_get_option(pppm_handle *ph, int option, int *value)
+{
+    PB_TRY(check_handle(ph));
+    if (!value)
+        return PPPM_ERR_ARG;
+    Handle &h = ph->h;
+    if (option == PPPM_OPT_CONV_PAIRS)
+        *value = h.conv_pairs ? 1 : 0;
+    else if (option == PPPM_OPT_FACE_THREADS)
+        *value = h.face_threads;
+    else
+    {
+        set_error("unknown option %d", option);
+        return PPPM_ERR_ARG;
+    }
+    return PPPM_OK;
+}
+
+int pppm_autotune(pppm_handle *ph, int reps, float *us_out, int *best)
+{
+    PB_TRY(check_handle(ph));
+    if (reps < 1 || reps > 10000)
+    {
+        set_error("autotune: reps must lie in [1, 10000]");
+        return PPPM_ERR_ARG;
+    }
+    Handle &h = ph->h;
+    cudaSetDevice(h.prm.device);
+    float us[2 * PPPM_TUNE_CANDIDATES] = {0};
+    int b = 0;
+    PB_TRY(step_autotune(h, reps, us, &b));
+    if (us_out)
+        memcpy(us_out, us, sizeof(us));
+    if (best)
+        *best = b;
     return PPPM_OK;
 }
 

@@ -40,6 +40,9 @@ struct StepState
     int n3;            // corrected cells
     long long row0;    // listener-series row of the first step
     const float *acc;  // nsteps rows of nt accelerations, or null
+    // batched runs: steps of time pair0, pair0 + 2, ... start a two-step pass over the face pairs
+    // when their partner (the next time) is at most pair_end; pair_end < pair0: one pass per step
+    int pair0 = 0, pair_end = -1;
 };
 
 // what step k of a call produces: its time index, listener-series row and acceleration row
@@ -123,6 +126,7 @@ struct Handle
     int *d_face_start = nullptr, *d_face_nbr = nullptr, *d_face_pool = nullptr;
     void *d_face_w = nullptr;
     float2 *d_face_scale = nullptr;
+    void *d_face_d1 = nullptr;  // pf: double-layer tap 1 of each pair, scale applied (step.cu: fix_kernel)
     long long pf_cap = 0;
     int *d_face_corner = nullptr;
     float *d_face_interp = nullptr;
@@ -154,6 +158,10 @@ struct Handle
     void *d_hist = nullptr;  // the step's copies: [Neumann, Dirichlet][4 copies][nt][kRing] (step.cu)
     void *d_terms = nullptr;  // nt x 54 near-field terms of the current step (step.cu: near_terms)
     void *d_conv = nullptr;   // nt face-pair convolution sums of the pipelined step (step.cu)
+    void *d_conv1 = nullptr;  // nt partial sums of the following step (step.cu: conv2_kernel)
+    void *d_dlast = nullptr;  // nt Dirichlet values of the last finished step (step.cu: fix_kernel)
+    bool conv_pairs = true;   // recorded step graphs convolve the face pairs two steps per pass
+    int face_threads = 256;   // threads per block of their face-stage kernels (step_autotune)
 
     // ---- listeners
     std::vector<int> listen_xyz;
@@ -254,6 +262,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 
 // step.cu
 int step_prime(Handle &h);
+int step_autotune(Handle &h, int reps, float *us, int *best);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state
 // batched scenes (step.cu): one set of stage launches advances every scene

@@ -649,15 +649,18 @@ int mesh_build(Handle &h)
         dev_free(h.d_face_w);
         dev_free(h.d_face_scale);
         dev_free(h.d_pair_flag);
+        dev_free(h.d_face_d1);
         h.d_face_nbr = h.d_face_pool = h.d_pair_flag = nullptr;
         h.d_face_w = nullptr;
         h.d_face_scale = nullptr;
+        h.d_face_d1 = nullptr;
         long long cap = pf + pf / 4 + 256;
         PB_TRY(dalloc(&h.d_face_nbr, (size_t)cap));
         PB_TRY(dalloc(&h.d_face_pool, (size_t)cap));
         PB_TRY(dalloc(&h.d_pair_flag, (size_t)cap + 1));
         PB_TRY(dev_alloc(&h.d_face_w, (size_t)cap * (h.fp64 ? 16 * sizeof(double2) : 16 * sizeof(__half2))));
         PB_TRY(dalloc(&h.d_face_scale, (size_t)cap));
+        PB_TRY(dev_alloc(&h.d_face_d1, (size_t)cap * h.real_size));
         h.pf_cap = cap;
     }
     face_fill_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(h.d_base, h.d_basec, nt, res, b4_pos, flag4, h.d_b4_start,

@@ -378,6 +378,9 @@ struct FaceArgs
     const int *face_start, *face_nbr, *face_corner;
     const typename WRec<R>::T *face_w;
     const float2 *face_scale;
+    const R *face_d1;  // per pair: double-layer tap 1 with its scale (fix_kernel)
+    const int *order;  // centre triangles in base-cell order (the convolution kernels' warp order)
+    R *dlast;          // per triangle: the Dirichlet value of the last finished step
     const float *interp;
     const double *interp_d, *denom;
     float reflect;
@@ -481,6 +484,62 @@ __device__ inline R face_conv(const Ring<R> &ring, int tnew, const FaceArgs<R> &
     return warp_sum(acc);
 }
 
+// Two steps from one pass over the face pairs.  c0: step k's convolution, exactly as face_conv
+// (same loads, same per-lane order).  c1: step k+1's convolution without its one term that needs
+// a value of step k: Dirichlet tap 1 of time t+1 is D[t], which finish(k) computes; fix_kernel
+// adds that term, sum_j d1_j D_j[t].  Everything else of step k+1 is final before step k:
+// Neumann taps t+1..t-14 (N[t+1] = acc[k+1], read from the acceleration row since the ring
+// receives it only in finish(k)) and Dirichlet taps t-1..t-14.  Tap 4q+i of time t+1 is tap
+// 4q+i-1 of time t, so lane q's shifted window is its own taps 4q..4q+2 plus tap 4q-1 from the
+// lane before it in the quad (tap -1: N[t+1]; for D, taps 0 and 1 of time t+1 are left out).
+// The face weights, scales and neighbour indices are read once for both steps.
+template <typename R>
+__device__ inline void face_conv2(const Ring<R> &ring, int tnew, const float *acc_next, const FaceArgs<R> &f, int tri,
+                                  int lane, R &c0, R &c1)
+{
+    using W4 = typename WRec<R>::W4;
+    using H4 = typename WRec<R>::H4;
+    const int g = lane >> 2, q = lane & 3;
+    const int copy = tnew & 3, off = (hist_index(copy, tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
+    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
+    const int nslot = hist_index(0, tnew + 1);  // N[t+1] in copy 0 (used when no acceleration row)
+    const unsigned quad = 0xfu << (lane & ~3);
+    const int b = f.face_start[tri], e = f.face_start[tri + 1];
+    R a0 = 0, a1 = 0;
+    for (int p = b + g; p < e; p += 8)
+    {
+        const W4 w = *(const W4 *)(f.face_w + (long long)p * kTaps + 4 * q);
+        const float2 s = f.face_scale ? f.face_scale[p] : make_float2(1, 1);
+        const int nb = f.face_nbr[p];
+        const H4 hn = *(const H4 *)(nbase + (long long)nb * kRing);
+        const H4 hd = *(const H4 *)(dbase + (long long)nb * kRing);
+        R nnew = 0;
+        if (q == 0)
+            nnew = acc_next ? (R)acc_next[nb] : ring.hrow(0, 0, nb)[nslot];
+        const R un = __shfl_up_sync(quad, hn.v[3], 1, 4), ud = __shfl_up_sync(quad, hd.v[3], 1, 4);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+        {
+            R di = (q == 0 && i == 0) ? (R)0 : hd.v[i];
+            a0 += conv_tap(w.v[i], s, hn.v[i], di);
+        }
+        H4 sn, sd;
+        sn.v[0] = q ? un : nnew;
+        sd.v[0] = q ? ud : (R)0;
+        sd.v[1] = q ? hd.v[0] : (R)0;
+#pragma unroll
+        for (int i = 1; i < 4; i++)
+            sn.v[i] = hn.v[i - 1];
+        sd.v[2] = hd.v[1];
+        sd.v[3] = hd.v[2];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            a1 += conv_tap(w.v[i], s, sn.v[i], sd.v[i]);
+    }
+    c0 = warp_sum(a0);
+    c1 = warp_sum(a1);
+}
+
 // far-field corner values of triangle tri (lanes 0-7; the others 0)
 template <typename R>
 __device__ inline void face_corners(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane, R &iw,
@@ -507,6 +566,8 @@ __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs
     const R dnew = (R)(num / f.denom[tri]);
     if (lane < 4)
         ring.hrow(1, lane, tri)[hist_index(lane, tnew)] = dnew;  // lane c: copy c
+    else if (lane == 4 && f.dlast)
+        f.dlast[tri] = dnew;
     near_terms<R>(ring, tnew, f, tri, lane, true, dnew);
 }
 
@@ -522,16 +583,71 @@ __device__ inline void face_body(const StepArgs &, const Ring<R> &ring, const St
 }
 
 // pipelined step: the face-pair convolution of step kstep into conv[tri]
+// Warps take the centre triangles in base-cell order: centres that share a base cell have the
+// same 4^3 neighbour list, so the warps of one block gather the same neighbours' history windows
+// and mostly hit L1.  Each centre's sum is the same whatever warp computes it.
+template <typename R>
+__device__ inline int centre_of(const FaceArgs<R> &f, int w)
+{
+    return f.order ? f.order[w] : w;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) conv_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
                                                     int kstep, int nt, const __grid_constant__ FaceArgs<R> f, R *conv)
 {
-    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (tri >= nt)
+    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= nt)
         return;
+    const int tri = centre_of(f, w);
     const R v = face_conv<R>(ring, st->tnew0 + kstep, f, tri, threadIdx.x & 31);
     if ((threadIdx.x & 31) == 0)
         conv[tri] = v;
+}
+
+// pipelined step pair: the face-pair convolution of step kstep into conv[tri] and the partial
+// convolution of step kstep + 1 into conv1[tri] (face_conv2)
+template <typename R>
+__global__ void __launch_bounds__(256) conv2_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                     int kstep, int nt, const __grid_constant__ FaceArgs<R> f, R *conv,
+                                                     R *conv1)
+{
+    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= nt)
+        return;
+    const int tri = centre_of(f, w);
+    const StepDyn dn = bind_step(st, kstep + 1, nt);
+    R c0, c1;
+    face_conv2<R>(ring, st->tnew0 + kstep, dn.acc, f, tri, threadIdx.x & 31, c0, c1);
+    if ((threadIdx.x & 31) == 0)
+    {
+        conv[tri] = c0;
+        conv1[tri] = c1;
+    }
+}
+
+// second step of a pipelined pair: conv[tri] = conv1[tri] + sum_j d1_j D_j[t-1], with D[t-1] the
+// Dirichlet values that finish of the step before has just written (compact per-triangle copy,
+// small enough to stay in L1), lanes striding over the pairs
+template <typename R>
+__device__ inline void face_fix(const FaceArgs<R> &f, const R *conv1, R *conv, int tri, int lane)
+{
+    const int b = f.face_start[tri], e = f.face_start[tri + 1];
+    R a = 0;
+    for (int p = b + lane; p < e; p += 32)
+        a += f.face_d1[p] * f.dlast[f.face_nbr[p]];
+    a = warp_sum(a);
+    if (lane == 0)
+        conv[tri] = conv1[tri] + a;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) fix_kernel(int nt, const __grid_constant__ FaceArgs<R> f, const R *conv1, R *conv)
+{
+    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= nt)
+        return;
+    face_fix<R>(f, conv1, conv, centre_of(f, w), threadIdx.x & 31);
 }
 
 // pipelined step: the rest of the face stage of step kstep; next != 0: also the Neumann value of
@@ -694,7 +810,10 @@ struct StepLaunch
     R *series;
     FaceArgs<R> fa;
     NearArgs<R> na;
-    R *conv;  // per-triangle convolution sums of the pipelined step
+    R *conv;   // per-triangle convolution sums of the pipelined step
+    R *conv1;  // partial sums of the second step of a pipelined pair
+    int pairs;         // pipelined graphs convolve the face pairs for two steps per pass (conv2 + fix)
+    int face_threads;  // threads per block of the pipelined face-stage kernels
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
     int ghost;     // ghost-cell method: the ghost kernel after the stencil instead of face / near
     GhostStep gs;  // its arguments
@@ -750,6 +869,12 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.fa.gc_scale = h.fp64 ? nullptr : h.d_gc_scale;
         L.fa.terms = (R *)h.d_terms;
         L.conv = (R *)h.d_conv;
+        L.conv1 = (R *)h.d_conv1;
+        L.pairs = h.conv_pairs ? 1 : 0;
+        L.face_threads = h.face_threads;
+        L.fa.face_d1 = (const R *)h.d_face_d1;
+        L.fa.order = h.d_base_tris;
+        L.fa.dlast = (R *)h.d_dlast;
         L.na.n3_cell = h.d_n3_cell;
         L.na.n3_start = h.d_n3_start;
         L.na.p3_tri = h.d_p3_tri;
@@ -805,28 +930,104 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
 //   main   stencil(k) -> finish(k) -> near(k)   finish waits for conv(k) too
 // so each step's face-pair convolution (the heavy part of the face stage) runs beside the
 // previous step's near stage and this step's stencil; finish(k) also writes N[t+1] for conv(k+1).
+// With pair set, steps go in pairs (k, k+1): conv2(k) streams the face pairs once for both steps
+// and fix(k+1), after finish(k), adds the one term of step k+1 that needs D of step k.
 // Only used under stream capture: main = h.stream, side = h.side, joined back before the end.
 template <typename R>
-void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps)
+void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
 {
-    const int T = 256;
+    const int T = 256, FT = L.face_threads;
     const int nt = L.a.nt;
-    const int wblocks = div_up((long long)nt * 32, T);
+    const int wblocks = div_up((long long)nt * 32, FT);
     cudaStream_t s = h.stream, side = h.side;
     nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
     cudaEventRecord(h.ev_fin, s);
     for (int k = 0; k < nsteps; k++)
     {
         cudaStreamWaitEvent(side, h.ev_fin, 0);
-        conv_kernel<R><<<wblocks, T, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv);
+        if (pair && (k & 1))
+            fix_kernel<R><<<wblocks, FT, 0, side>>>(nt, L.fa, L.conv1, L.conv);
+        else if (pair && k + 1 < nsteps)
+            conv2_kernel<R><<<wblocks, FT, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv, L.conv1);
+        else
+            conv_kernel<R><<<wblocks, FT, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv);
         cudaEventRecord(h.ev_conv, side);
         // the stencil without its Neumann block range (finish / nwrite wrote N[t])
         stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
         cudaStreamWaitEvent(s, h.ev_conv, 0);
-        finish_kernel<R><<<wblocks, T, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, k + 1 < nsteps ? 1 : 0);
+        finish_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, k + 1 < nsteps ? 1 : 0);
         cudaEventRecord(h.ev_fin, s);
         near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
     }
+}
+
+// Autotuner of the face stage: on the handle's current mesh and state, time the face-pair
+// convolution of two consecutive steps in every candidate configuration - one pass per step
+// (conv, conv) or one pass for both (conv2, fix) - at 64, 128 and 256 threads per block, each of
+// the two launches reps times back to back on the handle's stream between CUDA events, and keep
+// the fastest for the recorded step graphs.  The kernels write only the convolution scratch
+// sums, so no state of the scene changes.  us[2 i], us[2 i + 1]: microseconds per launch of the
+// first and second kernel of candidate i, in the order (pairs 0, 64), (pairs 0, 128),
+// (pairs 0, 256), (pairs 1, 64), ...
+constexpr int kTuneThreads[3] = {64, 128, 256};
+
+template <typename R>
+int autotune(Handle &h, int reps, float *us, int *best)
+{
+    if (!h.mesh_set || h.prm.method != PPPM_METHOD_PPPM || h.nt == 0)
+    {
+        set_error("autotune needs a mesh (PPPM method)");
+        return PPPM_ERR_STATE;
+    }
+    if (!h.d_state)
+        PB_TRY(dalloc(&h.d_state, 1));
+    cudaStream_t s = h.stream;
+    StepState stt{h.t + 1, h.n3, 0, nullptr};
+    set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
+    StepLaunch<R> L;
+    PB_TRY(make_launch<R>(h, L));
+    const int nt = h.nt;
+    auto run = [&](int c, int which) {
+        const int FT = kTuneThreads[c % 3], nb = div_up((long long)nt * 32, FT);
+        if (c < 3)
+            conv_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, which, nt, L.fa, L.conv);
+        else if (which == 0)
+            conv2_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, L.conv1);
+        else
+            fix_kernel<R><<<nb, FT, 0, s>>>(nt, L.fa, L.conv1, L.conv);
+    };
+    for (int c = 0; c < 6; c++)
+    {
+        run(c, 0);
+        run(c, 1);
+    }
+    PB_CHECK_LAUNCH();
+    int bi = 0;
+    float tot[6];
+    for (int c = 0; c < 6; c++)
+    {
+        PB_CUDA(cudaEventRecord(h.ev[0], s));
+        for (int r = 0; r < reps; r++)
+            run(c, 0);
+        PB_CUDA(cudaEventRecord(h.ev[1], s));
+        for (int r = 0; r < reps; r++)
+            run(c, 1);
+        PB_CUDA(cudaEventRecord(h.ev[2], s));
+        PB_CUDA(cudaEventSynchronize(h.ev[2]));
+        float ma = 0, mb = 0;
+        PB_CUDA(cudaEventElapsedTime(&ma, h.ev[0], h.ev[1]));
+        PB_CUDA(cudaEventElapsedTime(&mb, h.ev[1], h.ev[2]));
+        us[2 * c] = 1000.0f * ma / reps;
+        us[2 * c + 1] = 1000.0f * mb / reps;
+        tot[c] = us[2 * c] + us[2 * c + 1];
+        if (tot[c] < tot[bi])
+            bi = c;
+    }
+    h.launches += 2LL * reps * 6 + 13;
+    h.conv_pairs = bi >= 3;
+    h.face_threads = kTuneThreads[bi % 3];
+    *best = bi;
+    return PPPM_OK;
 }
 
 // Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
@@ -859,7 +1060,7 @@ int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *ou
     cudaGraph_t graph = nullptr;
     PB_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
     if (!timed && L.mesh && !L.pml && h.side)
-        capture_pipelined<R>(h, L, nsteps);
+        capture_pipelined<R>(h, L, nsteps, L.pairs != 0);
     else
         for (int k = 0; k < nsteps; k++)
             launch_step<R>(L, k, h.stream, timed ? &h : nullptr);
@@ -1022,6 +1223,11 @@ int hist_export(Handle &h) { return h.fp64 ? hist_copy<double>(h, 0) : hist_copy
 
 int step_prime(Handle &h) { return h.fp64 ? prime<double>(h) : prime<float>(h); }
 
+int step_autotune(Handle &h, int reps, float *us, int *best)
+{
+    return h.fp64 ? autotune<double>(h, reps, us, best) : autotune<float>(h, reps, us, best);
+}
+
 int step_run(Handle &h, const float *acc_dev, int nsteps)
 {
     return h.fp64 ? run_steps<double>(h, acc_dev, nsteps) : run_steps<float>(h, acc_dev, nsteps);
@@ -1068,6 +1274,7 @@ struct BatchScene
     NearArgs<R> na;
     StepState *st;
     R *conv;         // the scene's per-triangle convolution sums (pipelined graphs)
+    R *conv1;        // partial sums of the second step of a pair (two steps per pass)
     int near_warps;  // warps of this scene's near grid
 };
 
@@ -1100,17 +1307,40 @@ __global__ void __launch_bounds__(256) batch_near_kernel(const BatchScene<R> *sc
 
 // the pipelined batch step (see capture_pipelined): face-pair convolutions, the rest of the face
 // stage, and the first step's Neumann values, over the same per-scene block maps
+// The face-pair convolution of step k of every scene, one pass per step or two steps per pass
+// (conv2_kernel / fix_kernel) as the scene's state says: a scene's steps pair up from the first
+// step of its batched run (pair0), so the pairs, and the results, are those of the same steps
+// run alone in one pppm_step call, wherever the batch's graphs and phases begin and end.
 template <typename R>
 __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc, const int2 *map, int k)
 {
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    const int tri = m.y * 8 + (threadIdx.x >> 5);
-    if (tri >= S.a.nt)
+    const int w = m.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (w >= S.a.nt)
         return;
-    const R v = face_conv<R>(S.ring, S.st->tnew0 + k, S.fa, tri, threadIdx.x & 31);
-    if ((threadIdx.x & 31) == 0)
-        S.conv[tri] = v;
+    const int tri = centre_of(S.fa, w);
+    const int tnew = S.st->tnew0 + k, p0 = S.st->pair0, pe = S.st->pair_end;
+    const bool paired = pe >= p0;
+    if (paired && ((tnew - p0) & 1))
+        face_fix<R>(S.fa, S.conv1, S.conv, tri, lane);  // second step of a pair
+    else if (paired && tnew + 1 <= pe)
+    {
+        const StepDyn dn = bind_step(S.st, k + 1, S.a.nt);
+        R c0, c1;
+        face_conv2<R>(S.ring, tnew, dn.acc, S.fa, tri, lane, c0, c1);
+        if (lane == 0)
+        {
+            S.conv[tri] = c0;
+            S.conv1[tri] = c1;
+        }
+    }
+    else
+    {
+        const R v = face_conv<R>(S.ring, tnew, S.fa, tri, lane);
+        if (lane == 0)
+            S.conv[tri] = v;
+    }
 }
 
 template <typename R>
@@ -1241,6 +1471,7 @@ int batch_tables(Batch &b, const std::vector<int> &active)
         S.na = L.na;
         S.st = h.d_state;
         S.conv = L.conv;
+        S.conv1 = L.conv1;
         const int near_blocks = std::max(1, div_up((long long)h.n3 * 32, T));
         S.near_warps = near_blocks * (T / 32);
         memcpy(b.host_scenes.data() + ai * sizeof(S), &S, sizeof(S));
@@ -1364,6 +1595,10 @@ int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
         if (!h.d_state)
             PB_TRY(dalloc(&h.d_state, 1));
         StepState stt{h.t + 1, h.n3, h.series_count, dacc[i]};
+        // the scene's steps pair up as in one pppm_step call of nsteps[i] steps (recorded graphs:
+        // at least kGraphSteps steps)
+        stt.pair0 = h.t + 1;
+        stt.pair_end = h.conv_pairs && nsteps[i] >= kGraphSteps ? h.t + nsteps[i] : h.t;
         set_state_kernel<<<1, 1, 0, b.stream>>>(h.d_state, stt);
         b.launches++;
     }

@@ -92,6 +92,9 @@ def _load():
         "pppm_get_stream": [vp, ctypes.POINTER(vp)],
         "pppm_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "pppm_enable_timing": [vp, i],
+        "pppm_set_option": [vp, i, i],
+        "pppm_get_option": [vp, i, ip],
+        "pppm_autotune": [vp, i, fp, ip],
         "pppm_kernel_times": [vp, fp, fp, fp, ip],
     }
     fl = ctypes.c_float
@@ -421,6 +424,31 @@ class Solver:
         v = ctypes.c_longlong()
         check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
         return v.value
+
+    OPTIONS = {"conv_pairs": 0, "face_threads": 1}
+    TUNE_CANDIDATES = [(pairs, threads) for pairs in (0, 1) for threads in (64, 128, 256)]
+
+    def set_option(self, name, value):
+        """Launch option of the recorded step graphs (pppm_set_option): conv_pairs (0/1),
+        face_threads (64/128/256)."""
+        check(lib.pppm_set_option(self.h, self.OPTIONS[name], int(value)), "set_option")
+
+    def get_option(self, name):
+        v = ctypes.c_int()
+        check(lib.pppm_get_option(self.h, self.OPTIONS[name], ctypes.byref(v)), "get_option")
+        return v.value
+
+    def autotune(self, reps=20):
+        """Time the face-stage candidates on the current mesh (pppm_autotune) and keep the
+        fastest.  Returns {"us": {(pairs, threads): us per two steps}, "launch_us":
+        {(pairs, threads): (first kernel, second kernel) us per launch}, "best": (pairs, threads)}."""
+        n = len(self.TUNE_CANDIDATES)
+        us = (ctypes.c_float * (2 * n))()
+        best = ctypes.c_int()
+        check(lib.pppm_autotune(self.h, int(reps), us, ctypes.byref(best)), "autotune")
+        per = [(float(us[2 * i]), float(us[2 * i + 1])) for i in range(n)]
+        return {"us": {c: a + b for c, (a, b) in zip(self.TUNE_CANDIDATES, per)},
+                "launch_us": dict(zip(self.TUNE_CANDIDATES, per)), "best": self.TUNE_CANDIDATES[best.value]}
 
     def enable_timing(self, on=True):
         check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")

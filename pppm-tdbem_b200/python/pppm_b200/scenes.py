@@ -189,6 +189,135 @@ class MovingScene:
         return out
 
 
+def _bandpass_sos(lo_hz, hi_hz, fs, order=4):
+    from scipy.signal import butter
+
+    return butter(order, [lo_hz, hi_hz], btype="bandpass", fs=fs, output="sos")
+
+
+class StreamedNoise:
+    """Band-limited Gaussian noise for many series, generated in time order without holding the
+    whole run: white noise in seeded blocks through a Butterworth band-pass whose state carries
+    over between blocks, scaled to unit RMS by the filter's noise gain.  Any step range can be
+    asked for; a range before the last one restarts from step 0 (same values)."""
+
+    BLOCK = 512
+
+    def __init__(self, n_series, dt, lo_hz, hi_hz, seed):
+        from scipy.signal import sosfilt, sosfilt_zi  # noqa: F401
+
+        self.n, self.seed = n_series, seed
+        self.sos = _bandpass_sos(lo_hz, hi_hz, 1.0 / float(dt))
+        imp = np.zeros(1 << 17)
+        imp[0] = 1.0
+        from scipy.signal import sosfilt
+
+        self.gain = float(np.sqrt((sosfilt(self.sos, imp) ** 2).sum()))
+        self._reset()
+
+    def _reset(self):
+        self.zi = np.zeros((self.sos.shape[0], self.n, 2))
+        self.pos = 0
+        self.buf = np.zeros((self.n, 0), np.float32)
+        self.buf0 = 0
+
+    def _block(self, b):
+        from scipy.signal import sosfilt
+
+        x = np.random.default_rng([self.seed, b]).standard_normal((self.n, self.BLOCK))
+        y, self.zi = sosfilt(self.sos, x, axis=1, zi=self.zi)
+        return (y / self.gain).astype(np.float32)
+
+    def get(self, first, count):
+        """(n_series, count) noise for steps [first, first + count)."""
+        if first < self.buf0:
+            self._reset()
+        while self.pos < first + count:
+            blk = self._block(self.pos // self.BLOCK)
+            keep0 = min(max(self.buf0, first), self.pos)  # drop what lies before the request
+            self.buf = np.concatenate([self.buf[:, keep0 - self.buf0:], blk], 1)
+            self.buf0 = keep0
+            self.pos += self.BLOCK
+        return self.buf[:, first - self.buf0: first - self.buf0 + count]
+
+
+class LargeScene:
+    """Two moving perturbed icospheres (subdivision 5, 20480 triangles each) at res 128.
+
+    Each sphere (radius 0.1 m, seeded +-10% radial noise) sits at x = -+0.17 m and follows its
+    own seeded rigid trajectory: translation a sin(2 pi f t + phase) along a random direction
+    (a in [0.02, 0.04] m, f in [1, 4] Hz) and rotation at omega in [1, 3] rad/s about a random
+    axis.  The spheres stay more than 4 cells apart, so no face pair joins them.  The grid is
+    centred on the box the motion can reach, length 1.5 x its longest side (h ~ 7.5 mm), which
+    keeps every 3^3 list below 256 and every 4^3 list below 512 triangles (the reference's
+    fixed capacities, particle_grid.h:9-11).  Both spheres carry per-vertex band-limited
+    (100 Hz - 8 kHz) unit-RMS Gaussian accelerations averaged to triangles; motion frames at
+    1 kHz; dt as in the demo driver; 20000 steps."""
+
+    def __init__(self, res=128, seed=23, subdivisions=5, radius=0.1, noise=0.1, sep=0.17, factor=1.5, steps=20000,
+                 frame_hz=1000.0, c=C_REF):
+        rng = np.random.default_rng(seed)
+        self.bodies = []
+        verts, tris = [], []
+        nv = 0
+        for k, cx in enumerate((-sep, sep)):
+            v, f = perturbed_sphere(subdivisions, radius, noise, rng)
+            d = rng.standard_normal(3)
+            ax = rng.standard_normal(3)
+            body = dict(verts=v, centre=np.array([cx, 0.0, 0.0]), dir=d / np.linalg.norm(d),
+                        axis=ax / np.linalg.norm(ax), amp=float(rng.uniform(0.02, 0.04)),
+                        freq=float(rng.uniform(1.0, 4.0)), phase=float(rng.uniform(0, 2 * math.pi)),
+                        omega=float(rng.uniform(1.0, 3.0)))
+            self.bodies.append(body)
+            verts.append(v)
+            tris.append(f + nv)
+            nv += len(v)
+        self.tris = np.concatenate(tris).astype(np.int32)
+        self.nv = nv
+        rmax = radius * (1 + noise)
+        lo = np.min([b["centre"] - b["amp"] - rmax for b in self.bodies], 0)
+        hi = np.max([b["centre"] + b["amp"] + rmax for b in self.bodies], 0)
+        self.res = res
+        self.h, self.min_pos = grid_for_bbox(lo, hi, res, factor)
+        self.dt, self.frame_rate = demo_dt(self.h, c)
+        self.steps = steps
+        self.frame_hz = frame_hz
+        self.listener = (int(0.875 * res),) * 3
+        self.seed = seed
+        self._noise = StreamedNoise(nv, float(self.dt), 100.0, 8000.0, seed + 1)
+
+    def verts_at(self, time):
+        out = []
+        for b in self.bodies:
+            R = rotation_matrix(b["axis"], b["omega"] * time)
+            v = b["verts"] @ R.T
+            v += b["centre"] + b["dir"] * (b["amp"] * math.sin(2 * math.pi * b["freq"] * time + b["phase"]))
+            out.append(v)
+        return np.concatenate(out).astype(np.float32)
+
+    def frame_of_step(self, step):
+        return int(math.floor(step * float(self.dt) * self.frame_hz + 1e-9))
+
+    def frame_verts(self, frame):
+        return self.verts_at(frame / self.frame_hz)
+
+    def acc(self, first, count):
+        vn = self._noise.get(first, count)
+        f = self.tris
+        return ((vn[f[:, 0]] + vn[f[:, 1]] + vn[f[:, 2]]) / np.float32(3)).T.copy()
+
+
+def frame_ranges(scene, nframes):
+    """Step range [a, b) of each of the first nframes + 1 motion frames of a moving scene."""
+    need = int(math.ceil((nframes + 1) / scene.frame_hz / float(scene.dt))) + 2
+    start = [None] * (nframes + 2)
+    for s in range(need):
+        fr = scene.frame_of_step(s)
+        if fr <= nframes + 1 and start[fr] is None:
+            start[fr] = s
+    return [(start[fr], start[fr + 1]) for fr in range(nframes + 1)]
+
+
 def batch_scenes(n=64, seed=11, c=C_REF):
     """Independent scenes drawn from one seed: (res, verts, tris, h, min_pos, dt, steps)."""
     rng = np.random.default_rng(seed)

@@ -1,0 +1,112 @@
+"""Launch options of the recorded step graphs and the face-stage autotuner, on the B200.
+
+The two-step face-pair convolution (conv2 + fix: one pass over the pairs' weights for two
+consecutive steps) sums the same products as one pass per step, with the term of D[t] added after
+the rest instead of among it.  Tolerances: FP64 series of the two variants within 1e-12 relative
+L2 over 300 steps (the algebra is the same); FP32 within 1e-6 over the first 50 steps and 1e-4
+over 300 (reassociation only: the scheme amplifies rounding differences step after step, and
+summing the same pairs in reverse order already moves a 300-step FP32 series by ~3e-5); both
+within the oracle bounds of the parity tests (1e-5 over the first 50 steps with shared tables)."""
+import numpy as np
+import pytest
+
+from helpers import moving_small_verts, rel_l2, sine_acc, sphere_small
+from oracle.oracle import Oracle
+from pppm_b200 import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False):
+    v0, f, h, mn, dt = sphere_small()
+    res = 24
+    s = Solver(res, h, dt, mn, precision=precision)
+    s.set_option("conv_pairs", pairs)
+    s.set_option("face_threads", threads)
+    s.set_mesh(moving_small_verts(v0, 0, dt) if moving else v0, f)
+    s.add_listener(20, 20, 20)
+    acc = sine_acc(steps, len(f), 1500.0, dt)
+    chunk = chunk or steps
+    for s0 in range(0, steps, chunk):
+        if moving and s0:
+            s.update_mesh(moving_small_verts(v0, s0, dt))
+        s.step(acc[s0: s0 + chunk])
+    out = s.listeners()[:, 0].astype(np.float64)
+    s.close()
+    return out
+
+
+def test_pairs_match_single_pass_fp64(gpu):
+    a = _series("fp64", 0)
+    b = _series("fp64", 1)
+    assert np.all(np.isfinite(b))
+    assert rel_l2(b, a) < 1e-12
+
+
+def test_pairs_match_single_pass_fp32(gpu):
+    a = _series("fp32", 0)
+    b = _series("fp32", 1)
+    assert np.all(np.isfinite(b))
+    assert rel_l2(b[:50], a[:50]) < 1e-6
+    assert rel_l2(b, a) < 1e-4
+
+
+@pytest.mark.parametrize("chunk", [5, 7, 13])
+def test_pairs_odd_calls_and_motion(gpu, chunk):
+    # odd step counts end a call on a single pass; motion frames change the pair lists between
+    # calls (the tap-1 factors are rebuilt with the weights)
+    a = _series("fp64", 0, steps=120, chunk=chunk, moving=True)
+    b = _series("fp64", 1, steps=120, chunk=chunk, moving=True)
+    assert rel_l2(b, a) < 1e-12
+
+
+@pytest.mark.parametrize("threads", [64, 128])
+def test_face_threads(gpu, threads):
+    a = _series("fp32", 1)
+    b = _series("fp32", 1, threads=threads)
+    assert np.array_equal(a, b)  # same arithmetic, other block shape
+
+
+def test_autotune_keeps_results(gpu):
+    v, f, h, mn, dt = sphere_small()
+    res = 24
+    s = Solver(res, h, dt, mn)
+    s.set_mesh(v, f)
+    s.add_listener(20, 20, 20)
+    acc = sine_acc(200, len(f), 1500.0, dt)
+    s.step(acc[:100])
+    t_before = s.t
+    g_before = s.grid(0).copy()
+    tune = s.autotune(reps=5)
+    assert len(tune["us"]) == 6 and all(u > 0 for u in tune["us"].values())
+    assert tune["best"] == min(tune["us"], key=tune["us"].get)
+    assert (s.get_option("conv_pairs"), s.get_option("face_threads")) == tune["best"]
+    assert s.t == t_before and np.array_equal(s.grid(0), g_before)
+    s.step(acc[100:])
+    got = s.listeners()[:, 0]
+    s.close()
+    o = Oracle(res, h, dt, mn)
+    o.set_mesh(v, f)
+    s2 = Solver(res, h, dt, mn)
+    s2.set_mesh(v, f)
+    o.import_grid_cache(s2.dump("grid_cache"))
+    o.import_face_cache(s2.dump("face_pairs").reshape(-1, 2), s2.dump("face_cache"))
+    s2.close()
+    ref = o.step(acc, listeners=[(20, 20, 20)])[:, 0]
+    o.close()
+    assert rel_l2(got[:50], ref[:50]) < 1e-5
+    assert rel_l2(got, ref) < 1e-3
+
+
+def test_bad_options_rejected(gpu):
+    v, f, h, mn, dt = sphere_small()
+    s = Solver(24, h, dt, mn)
+    from pppm_b200 import PPPMError
+
+    with pytest.raises(PPPMError):
+        s.set_option("face_threads", 96)
+    with pytest.raises(PPPMError):
+        s.set_option("conv_pairs", 2)
+    with pytest.raises(PPPMError):
+        s.autotune()  # no mesh yet
+    s.close()
