@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint", "large"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fp64-check", action="store_true")
     p.add_argument("--summarize-launches", metavar="CSV",
                    help="print per-kernel launches / total time / share from an ncu "
                         "gpu__time_duration.sum CSV log of this benchmark, and exit")
@@ -320,6 +321,7 @@ def run_ours(args, ws, rank, local):
         s2 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
         s2.set_option("conv_pairs", pairs)
         s2.set_option("face_threads", threads)
+        s2.set_option("terms_pairs", tune["terms_pairs"])
         s2.set_mesh(wl.verts[0], wl.tris)
         s2.add_listener(*wl.listener)
         acc_pin = torch.from_numpy(wl.acc).pin_memory()
@@ -351,6 +353,26 @@ def run_ours(args, ws, rank, local):
         s2.close()
         del out_pin
 
+    # error of the timed FP32 run against the FP64 scheme of the same library on the GPU, over the
+    # same frames (set-up and warm-up frames included; outside the timed region)
+    fp64_err = None
+    if not args.no_fp64_check:
+        n = wl.ranges[W + K][1]
+        got = s.listeners(0, n)[:, 0].astype(np.float64)
+        s64 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream, precision="fp64")
+        s64.set_mesh(wl.verts[0], wl.tris)
+        s64.add_listener(*wl.listener)
+        for f in range(0, W + K + 1):
+            a, b = wl.ranges[f]
+            if f > 0 and wl.moving:
+                s64.update_mesh(verts_dev[f])
+            s64.step(acc_dev[a:b])
+        ref = s64.listeners(0, n)[:, 0].astype(np.float64)
+        s64.close()
+        den = float(np.linalg.norm(ref))
+        fp64_err = {"rel_l2": float(np.linalg.norm(got - ref) / den) if den > 0 else None, "time_steps": int(n),
+                    "reference": "the same frames in the FP64 scheme (PPPM_PRECISION_FP64) on the GPU"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl)
@@ -370,8 +392,14 @@ def run_ours(args, ws, rank, local):
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes": int(top_bytes), "kernel_launch_us": round(top_us, 3),
-                     "autotune": {"best": {"two_steps_per_pass": bool(pairs), "threads": threads},
-                                  "us_per_two_steps": {"%s/%d" % ("pairs" if p else "single", t): round(u, 2)
+                     "autotune": {"best": {"two_steps_per_pass": bool(pairs), "threads": threads,
+                                           "terms_two_steps_per_pass": bool(tune["terms_pairs"])},
+                                  "decided_by": "16 recorded steps per option set (phase 2)",
+                                  "finish_us_per_two_steps": {k: round(v, 2) for k, v in tune["finish_us"].items()},
+                                  "step_us_by_config": {"%s/%d/%s" % (("single", "pairs")[p], t,
+                                                                      "terms2" if m else "terms1"): round(u, 2)
+                                                        for (p, t, m), u in (tune["step_us"] or {}).items()},
+                                  "us_per_two_steps": {"%s/%d" % (("single", "pairs")[p], t): round(u, 2)
                                                        for (p, t), u in tune["us"].items()}},
                      "fix_us": round(tune["launch_us"][tune["best"]][1], 3) if pairs else None,
                      "fix_bytes": int(fix_bytes(counts, nt)) if pairs else None,
@@ -379,6 +407,7 @@ def run_ours(args, ws, rank, local):
                      "update_mesh_us": round(us_update, 1), "time_step_us": round(us_per_step, 2),
                      "gb_per_s_all_kernels": round(sum(alg.values()) / (sum(times.values()) * 1e-6) / 1e9, 1)},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+        "error_vs_fp64": fp64_err,
     }
     return line
 

@@ -240,17 +240,26 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
 #define PPPM_OPT_CONV_PAIRS 0   /* 1 (default): the face-pair convolution streams the pairs' weights
                                    once for two consecutive steps; 0: once per step             */
 #define PPPM_OPT_FACE_THREADS 1 /* threads per block of the face-stage kernels: 64, 128, 256    */
+#define PPPM_OPT_TERMS_PAIRS 2  /* 1 (default): the triangles' grid-cache near-field terms are
+                                   evaluated two steps per pass over their records; 0: per step */
 int pppm_set_option(pppm_handle *h, int option, int value);
 int pppm_get_option(pppm_handle *h, int option, int *value);
-/* No counterpart in the reference.  Autotuner of the face stage: on the current mesh and state,
- * times the face-pair convolution of two steps in each of PPPM_TUNE_CANDIDATES configurations
- * (candidate i: pairs = i / 3, threads = {64, 128, 256}[i % 3]), reps launches of each of its two
- * kernels, and sets the options to the fastest.  us_out (may be NULL; 2 * PPPM_TUNE_CANDIDATES
- * floats): microseconds per launch of candidate i's first kernel (us_out[2 i]: the convolution,
- * or the two-step convolution) and second kernel (us_out[2 i + 1]: the next step's convolution,
- * or the two-step pass's completion); *best (may be NULL): the index chosen.  Changes no field
- * or history.  Needs a mesh and the PPPM method. */
-#define PPPM_TUNE_CANDIDATES 6
+/* No counterpart in the reference.  Autotuner of the face stage, on the current mesh and state.
+ * Phase 1 times kernels alone: two steps of the face-pair convolution in 6 configurations
+ * (candidate i < 6: PPPM_OPT_CONV_PAIRS = i / 3, threads = {64, 128, 256}[i % 3]), then two steps
+ * of the rest of the face stage with the near-field terms one pass per step (candidate 6) or two
+ * steps per pass (candidate 7), reps launches of each kernel.  Phase 2 (absorbing boundary) times
+ * 64 recorded steps (zero accelerations) of each of PPPM_TUNE_CONFIGS option sets (config j: conv_pairs = j / 6,
+ * threads = {64, 128, 256}[(j / 2) % 3], terms_pairs = j % 2) from a device snapshot of the
+ * fields and histories (a warm-up replay, then a timed one; best of reps) and sets the options to
+ * the fastest (with a PML, phase 1 decides).  us_out (may be NULL; 2 * PPPM_TUNE_CANDIDATES +
+ * PPPM_TUNE_CONFIGS floats): microseconds per launch of candidate i's first kernel (us_out[2 i])
+ * and second kernel (us_out[2 i + 1]), then microseconds per step of each config; *best (may be
+ * NULL): the config chosen (or, with a PML, the convolution candidate).  The fields, histories,
+ * time and recorded listener samples are as before the call; it allocates a snapshot of the
+ * fields and histories for its duration.  Needs a mesh and the PPPM method. */
+#define PPPM_TUNE_CANDIDATES 8
+#define PPPM_TUNE_CONFIGS 12
 int pppm_autotune(pppm_handle *h, int reps, float *us_out, int *best);
 
 /* ------------------------------------------------------------ diagnostics ------------ */

@@ -651,19 +651,28 @@ __global__ void fc_finish_kernel_d(DevConsts dc, const float *verts, const int *
     pack_double(ws, wd, pool_w + (size_t)face_pool[p] * kTaps);
 }
 
+// dense face weights in hot-path order from the pool: one thread per 16-byte chunk of a record
+// (4 chunks per fp16 record, 16 per FP64 record)
 template <typename Rec>
 __global__ void gather_face_kernel(const int *face_pool, long long pf, const Rec *pool_w, const float2 *pool_scale,
                                    Rec *face_w, float2 *face_scale)
 {
+    constexpr int kChunks = (int)(kTaps * sizeof(Rec) / sizeof(uint4));
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= pf * kTaps)
+    if (g >= pf * kChunks)
         return;
-    long long p = g / kTaps;
-    int k = (int)(g % kTaps);
+    long long p = g / kChunks;
+    int k = (int)(g % kChunks);
     int slot = face_pool[p];
-    face_w[p * kTaps + k] = pool_w[(size_t)slot * kTaps + k];
+    ((uint4 *)face_w)[p * kChunks + k] = ((const uint4 *)pool_w)[(size_t)slot * kChunks + k];
     if (k == 0 && pool_scale)
         face_scale[p] = pool_scale[slot];
+}
+
+template <typename Rec>
+inline long long gather_face_threads(long long pf)
+{
+    return pf * (long long)(kTaps * sizeof(Rec) / sizeof(uint4));
 }
 
 // 0.5 * area - sum_j factor_j with factor_j = double-layer weight 0 of pair j, summed in
@@ -738,7 +747,37 @@ DevConsts make_consts(const Handle &h)
     return dc;
 }
 
+// Per grid-cache record, the factor of the triangle's NEW Dirichlet value in the record's term
+// one step later (the step's two-step near-field terms, step.cu: near_terms2): double-layer tap 1
+// of the FDTD-near records (r < 27; they pair record tap j + 1 with history tap j) and tap 0 of the
+// BEM-near records, with the record's scale applied as the step applies it.
+__global__ void gc_factor_kernel(const __half2 *w, const float2 *scale, const double2 *wd, long long n, float *f,
+                                 double *fd)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int tap = (i % 54) < 27 ? 1 : 0;
+    if (wd)
+        fd[i] = wd[i * kTaps + tap].y;
+    else
+        f[i] = __high2float(w[i * kTaps + tap]) * scale[i].y;
+}
+
 }  // namespace
+
+int gc_factors(Handle &h)
+{
+    const long long n = (long long)h.nt * 54;
+    if (!h.d_gc_f || n == 0)
+        return PPPM_OK;
+    gc_factor_kernel<<<div_up(n, 256), 256, 0, h.stream>>>(
+        h.fp64 ? nullptr : (const __half2 *)h.d_gc_w, h.d_gc_scale, h.fp64 ? (const double2 *)h.d_gc_w : nullptr, n,
+        h.fp64 ? nullptr : (float *)h.d_gc_f, h.fp64 ? (double *)h.d_gc_f : nullptr);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
+}
 
 int cache_refresh(Handle &h)
 {
@@ -751,6 +790,7 @@ int cache_refresh(Handle &h)
     if (!h.d_gc_w)
     {
         PB_TRY(dev_alloc(&h.d_gc_w, (size_t)nt * 54 * rec_bytes));
+        PB_TRY(dev_alloc(&h.d_gc_f, (size_t)nt * 54 * h.real_size));
         if (!h.fp64)
             PB_TRY(dalloc(&h.d_gc_scale, (size_t)nt * 54));
         PB_TRY(dalloc(&h.d_gc_snap, (size_t)nt * 7));
@@ -789,6 +829,7 @@ int cache_refresh(Handle &h)
     h.launches++;
     PB_CHECK_LAUNCH();
     h.gc_empty = false;
+    PB_TRY(gc_factors(h));
 
     // ---- face cache
     const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
@@ -883,10 +924,10 @@ int cache_refresh(Handle &h)
             PB_CHECK_LAUNCH();
         }
         if (h.fp64)
-            gather_face_kernel<double2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+            gather_face_kernel<double2><<<div_up(gather_face_threads<double2>(h.pf), T), T, 0, s>>>(
                 h.d_face_pool, h.pf, (const double2 *)h.d_pool_w, nullptr, (double2 *)h.d_face_w, nullptr);
         else
-            gather_face_kernel<__half2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+            gather_face_kernel<__half2><<<div_up(gather_face_threads<__half2>(h.pf), T), T, 0, s>>>(
                 h.d_face_pool, h.pf, (const __half2 *)h.d_pool_w, h.d_pool_scale, (__half2 *)h.d_face_w,
                 h.d_face_scale);
         h.launches++;
@@ -903,6 +944,8 @@ int cache_refresh(Handle &h)
 
 int cache_free(Handle &h)
 {
+    dev_free(h.d_gc_f);
+    h.d_gc_f = nullptr;
     void *ptrs[] = {h.d_gc_w,      h.d_gc_scale,  h.d_gc_snap,   h.d_gc_flag,    h.d_fc_keys,
                     h.d_fc_slot,   h.d_pool_w,    h.d_pool_scale, h.d_pool_meta, h.d_pool_count,
                     h.d_face_interp, h.d_face_interp_d, h.d_face_denom, h.d_spec, h.d_tw};
@@ -978,10 +1021,10 @@ int cache_regather(Handle &h)
     if (h.pf > 0)
     {
         if (h.fp64)
-            gather_face_kernel<double2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+            gather_face_kernel<double2><<<div_up(gather_face_threads<double2>(h.pf), T), T, 0, s>>>(
                 h.d_face_pool, h.pf, (const double2 *)h.d_pool_w, nullptr, (double2 *)h.d_face_w, nullptr);
         else
-            gather_face_kernel<__half2><<<div_up(h.pf * kTaps, T), T, 0, s>>>(
+            gather_face_kernel<__half2><<<div_up(gather_face_threads<__half2>(h.pf), T), T, 0, s>>>(
                 h.d_face_pool, h.pf, (const __half2 *)h.d_pool_w, h.d_pool_scale, (__half2 *)h.d_face_w,
                 h.d_face_scale);
         h.launches++;
@@ -1012,6 +1055,7 @@ int cache_import_grid(Handle &h, const void *records)
     PB_CUDA(cudaStreamSynchronize(s));
     dev_free(tmp);
     h.gc_empty = false;
+    PB_TRY(gc_factors(h));
     return cache_regather(h);
 }
 

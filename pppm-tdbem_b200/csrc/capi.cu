@@ -143,7 +143,7 @@ void free_mesh(Handle &h)
                      (void **)&h.d_status,     (void **)&h.d_neumann,     (void **)&h.d_dirichlet,
                      (void **)&h.d_hist,       (void **)&h.d_terms,       (void **)&h.d_conv,
                      (void **)&h.d_gneu,       (void **)&h.d_gneu_old,    (void **)&h.d_face_d1,
-                     (void **)&h.d_conv1,      (void **)&h.d_dlast};
+                     (void **)&h.d_conv1,      (void **)&h.d_dlast,       (void **)&h.d_terms1};
     for (void **q : ptrs)
     {
         dev_free(*q);
@@ -411,6 +411,7 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_TRY(dev_alloc(&h.d_conv, (size_t)nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_conv1, (size_t)nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_dlast, (size_t)nt * h.real_size));
+    PB_TRY(dev_alloc(&h.d_terms1, (size_t)54 * nt * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_dlast, 0, (size_t)nt * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
@@ -1215,12 +1216,17 @@ int pppm_set_option(pppm_handle *ph, int option, int value)
     case PPPM_OPT_CONV_PAIRS:
         if (value != 0 && value != 1)
             break;
-        h.conv_pairs = value != 0;
+        h.conv_pairs = value;
         return PPPM_OK;
     case PPPM_OPT_FACE_THREADS:
         if (value != 64 && value != 128 && value != 256)
             break;
         h.face_threads = value;
+        return PPPM_OK;
+    case PPPM_OPT_TERMS_PAIRS:
+        if (value != 0 && value != 1)
+            break;
+        h.terms_pairs = value != 0;
         return PPPM_OK;
     default:
         set_error("unknown option %d", option);
@@ -1237,9 +1243,11 @@ int pppm_get_option(pppm_handle *ph, int option, int *value)
         return PPPM_ERR_ARG;
     Handle &h = ph->h;
     if (option == PPPM_OPT_CONV_PAIRS)
-        *value = h.conv_pairs ? 1 : 0;
+        *value = h.conv_pairs;
     else if (option == PPPM_OPT_FACE_THREADS)
         *value = h.face_threads;
+    else if (option == PPPM_OPT_TERMS_PAIRS)
+        *value = h.terms_pairs ? 1 : 0;
     else
     {
         set_error("unknown option %d", option);
@@ -1258,8 +1266,9 @@ int pppm_autotune(pppm_handle *ph, int reps, float *us_out, int *best)
     }
     Handle &h = ph->h;
     cudaSetDevice(h.prm.device);
-    float us[2 * PPPM_TUNE_CANDIDATES] = {0};
+    float us[2 * PPPM_TUNE_CANDIDATES + PPPM_TUNE_CONFIGS] = {0};
     int b = 0;
+    PB_TRY(ensure_series(h, 64));  // the timed step graphs write listener rows past the recorded ones
     PB_TRY(step_autotune(h, reps, us, &b));
     if (us_out)
         memcpy(us_out, us, sizeof(us));

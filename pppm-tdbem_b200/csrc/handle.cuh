@@ -43,6 +43,7 @@ struct StepState
     // batched runs: steps of time pair0, pair0 + 2, ... start a two-step pass over the face pairs
     // when their partner (the next time) is at most pair_end; pair_end < pair0: one pass per step
     int pair0 = 0, pair_end = -1;
+    int conv_pairs = 0, terms_pairs = 0;  // which stages use the pairing (the handle's options)
 };
 
 // what step k of a call produces: its time index, listener-series row and acceleration row
@@ -137,6 +138,7 @@ struct Handle
     bool gc_empty = true;
     void *d_gc_w = nullptr;        // FP32: __half2[nt][54][16]; FP64: double[nt][54][32]
     float2 *d_gc_scale = nullptr;  // FP32: [nt][54]
+    void *d_gc_f = nullptr;        // [nt][54] factor of the new Dirichlet value per record (gc_factors)
     float *d_gc_snap = nullptr;    // nt x 7 centre, normal, area at last refresh
     int *d_gc_flag = nullptr;      // nt recompute flags
     int *d_fc_keys = nullptr;      // nt x kFaceCacheSlots neighbour ids, -1 = empty
@@ -160,8 +162,10 @@ struct Handle
     void *d_conv = nullptr;   // nt face-pair convolution sums of the pipelined step (step.cu)
     void *d_conv1 = nullptr;  // nt partial sums of the following step (step.cu: conv2_kernel)
     void *d_dlast = nullptr;  // nt Dirichlet values of the last finished step (step.cu: fix_kernel)
-    bool conv_pairs = true;   // recorded step graphs convolve the face pairs two steps per pass
+    void *d_terms1 = nullptr; // nt x 54 partial near-field terms of the following step (near_terms2)
+    int conv_pairs = 1;       // recorded step graphs convolve the face pairs two steps per pass
     int face_threads = 256;   // threads per block of their face-stage kernels (step_autotune)
+    bool terms_pairs = true;  // ... and the grid-cache near-field terms two steps per pass
 
     // ---- listeners
     std::vector<int> listen_xyz;
@@ -263,6 +267,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 // step.cu
 int step_prime(Handle &h);
 int step_autotune(Handle &h, int reps, float *us, int *best);
+int gc_factors(Handle &h);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state
 // batched scenes (step.cu): one set of stage launches advances every scene

@@ -140,25 +140,22 @@ __device__ inline R abc_cell(R *cur, const R *prev, int res, int x, int y, int z
 }
 
 // interior leapfrog (fdtd.cu:7-33): float storage, double arithmetic, "6 * p" in the
-// storage precision
+// storage precision; the neighbours summed in the reference's order (x-1, x+1, y-1, y+1, z-1, z+1)
 template <typename R>
-__device__ inline R interior_cell(const R *cur, const R *prev, int res, int x, int y, int z, double coefd, double hd)
+__device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, double coefd, double hd)
 {
-    long long i = ((long long)x * res + y) * res + z;
-    long long sx = (long long)res * res;
-    R pc = cur[i];
     double sum = 0;
-    sum += cur[i - sx];
-    sum += cur[i + sx];
-    sum += cur[i - res];
-    sum += cur[i + res];
-    sum += cur[i - 1];
-    sum += cur[i + 1];
+    sum += xm;
+    sum += xp;
+    sum += ym;
+    sum += yp;
+    sum += zm;
+    sum += zp;
     sum -= 6 * pc;
     double lap = sum / (hd * hd);
     double p = 2 * pc;
     p += coefd * lap;
-    p += -prev[i];
+    p += -pprev;
     return (R)p;
 }
 
@@ -228,8 +225,10 @@ __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, cons
             return;
         int x = 2 + i / (mi * mi), r = i % (mi * mi);
         int y = 2 + r / mi, z = 2 + r % mi;
-        R v = interior_cell<R>(cur, prev, res, x, y, z, a.lap_coef, a.hd);
-        finish_cell<R>(a, dy.row, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        const long long c = ((long long)x * res + y) * res + z, sx = (long long)res * res;
+        R v = leapfrog<R>(cur[c], cur[c - sx], cur[c + sx], cur[c - res], cur[c + res], cur[c - 1], cur[c + 1], prev[c],
+                          a.lap_coef, a.hd);
+        finish_cell<R>(a, dy.row, c, v, next, corr_mask, series);
         return;
     }
     b -= sp.nb_in;
@@ -388,6 +387,8 @@ struct FaceArgs
     const typename WRec<R>::T *gc_w;
     const float2 *gc_scale;
     R *terms;  // [nt][54]
+    R *terms1;        // [nt][54] partial terms of the next step (near_terms2)
+    const R *gc_f;    // [nt][54] factor of the next step's Dirichlet value per record (near_terms2)
 };
 
 constexpr int kGcRecords = 54;  // per triangle: 27 FDTD-near then 27 BEM-near records (offsets in 3^3)
@@ -448,6 +449,99 @@ __device__ inline void near_terms(const Ring<R> &ring, int t, const FaceArgs<R> 
         if (q == 0)
             out[r] = v;
     }
+}
+
+// The near-field terms of time t (as near_terms with d0 set) and, from the same pass over the
+// 54 records, the terms of time t+1 without the one product that needs D[t+1], which this step
+// cannot know yet: BEM-near records pair record tap m with history tap m of time t+1 (tap 0 holds
+// D[t+1]); FDTD-near records pair record tap m with history tap m-1 (record tap 1 meets D[t+1]).
+// History tap j of time t+1 is tap j-1 of time t, so the time-(t+1) windows are the time-t window
+// shifted by one and two taps (quad shuffles); tap -1 is N[t+1] = nnext (known: the acceleration
+// row of the next step) and D[t+1] (left out).  face_finish of the next step adds
+// gc_f[r] * D[t+1] to terms1[r] (gc_factors holds those factors).
+template <typename R>
+__device__ inline void near_terms2(const Ring<R> &ring, int t, const FaceArgs<R> &f, int tri, int lane, R dnew,
+                                   R nnext)
+{
+    using W4 = typename WRec<R>::W4;
+    using H4 = typename WRec<R>::H4;
+    const int g = lane >> 2, q = lane & 3;
+    const int copy = t & 3, off = (hist_index(copy, t) + 4 * q) & (kRing - 1);
+    const H4 hn = *(const H4 *)(ring.hrow(0, copy, tri) + off);
+    H4 hd = *(const H4 *)(ring.hrow(1, copy, tri) + off);
+    if (q == 0)
+        hd.v[0] = dnew;
+    // time-t taps shifted by one (4q+i-1) and by two (4q+i-2)
+    const R pn3 = __shfl_up_sync(kFull, hn.v[3], 1), pd3 = __shfl_up_sync(kFull, hd.v[3], 1);
+    const R pn2 = __shfl_up_sync(kFull, hn.v[2], 1), pd2 = __shfl_up_sync(kFull, hd.v[2], 1);
+    H4 sn, sd, bn, tn, td;
+    sn.v[0] = q ? pn3 : (R)0;   // FDTD-near, time t: tap -1 does not exist
+    bn.v[0] = q ? pn3 : nnext;  // BEM-near, time t+1: tap 0 of t+1 is N[t+1]
+    sd.v[0] = q ? pd3 : (R)0;   // D: tap -1 is D[t+1], left out in both
+#pragma unroll
+    for (int i = 1; i < 4; i++)
+    {
+        sn.v[i] = hn.v[i - 1];
+        bn.v[i] = hn.v[i - 1];
+        sd.v[i] = hd.v[i - 1];
+    }
+    // FDTD-near, time t+1: record tap m pairs with time-t tap m-2; m = 0 has no term, m = 1 meets
+    // time t+1 (N[t+1] included, D[t+1] left out)
+    tn.v[0] = q ? pn2 : (R)0;
+    td.v[0] = q ? pd2 : (R)0;
+    tn.v[1] = q ? pn3 : nnext;
+    td.v[1] = q ? pd3 : (R)0;
+    tn.v[2] = hn.v[0];
+    td.v[2] = hd.v[0];
+    tn.v[3] = hn.v[1];
+    td.v[3] = hd.v[1];
+    const unsigned quad = 0xfu << (lane & ~3);
+    const typename WRec<R>::T *rec = f.gc_w + (long long)tri * kGcRecords * kTaps;
+    R *out = f.terms + (long long)tri * kGcRecords;
+    R *out1 = f.terms1 + (long long)tri * kGcRecords;
+    for (int r = g; r < kGcRecords; r += 8)
+    {
+        const W4 w = *(const W4 *)(rec + (long long)r * kTaps + 4 * q);
+        const float2 s = f.gc_scale ? f.gc_scale[(long long)tri * kGcRecords + r] : make_float2(1, 1);
+        R v = 0, v1 = 0;
+        if (r < kGcRecords / 2)
+        {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+            {
+                v += conv_tap(w.v[i], s, sn.v[i], sd.v[i]);
+                v1 += conv_tap(w.v[i], s, tn.v[i], td.v[i]);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+            {
+                v += conv_tap(w.v[i], s, hn.v[i], hd.v[i]);
+                v1 += conv_tap(w.v[i], s, bn.v[i], sd.v[i]);
+            }
+        }
+        v += __shfl_xor_sync(quad, v, 1);
+        v += __shfl_xor_sync(quad, v, 2);
+        v1 += __shfl_xor_sync(quad, v1, 1);
+        v1 += __shfl_xor_sync(quad, v1, 2);
+        if (q == 0)
+        {
+            out[r] = v;
+            out1[r] = v1;
+        }
+    }
+}
+
+// the second step of a two-step pass: its near-field terms from the partial terms and the new
+// Dirichlet value
+template <typename R>
+__device__ inline void near_terms_complete(const FaceArgs<R> &f, int tri, int lane, R dnew)
+{
+    const long long o = (long long)tri * kGcRecords;
+    for (int r = lane; r < kGcRecords; r += 32)
+        f.terms[o + r] = f.terms1[o + r] + f.gc_f[o + r] * dnew;
 }
 
 // The face stage of centre triangle tri (whole warp) in two parts.  face_conv: the face-pair
@@ -554,9 +648,11 @@ __device__ inline void face_corners(const Ring<R> &ring, int tnew, const FaceArg
     }
 }
 
+// mode 0: one step; 1: first step of a two-step pass (nnext = N[t+1] of this triangle);
+// 2: second step of a two-step pass.  commit = false: no history / Dirichlet writes (timing)
 template <typename R>
 __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane, R iw, R pv,
-                                   R conv)
+                                   R conv, int mode = 0, R nnext = 0, bool commit = true)
 {
     R far_sum = 0;  // corners in order 0..7
 #pragma unroll
@@ -564,11 +660,24 @@ __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs
         far_sum += __shfl_sync(kFull, iw, wi) * __shfl_sync(kFull, pv, wi);
     R num = far_sum * (R)f.reflect + conv;
     const R dnew = (R)(num / f.denom[tri]);
-    if (lane < 4)
+    if (commit && lane < 4)
         ring.hrow(1, lane, tri)[hist_index(lane, tnew)] = dnew;  // lane c: copy c
-    else if (lane == 4 && f.dlast)
+    else if (commit && lane == 4 && f.dlast)
         f.dlast[tri] = dnew;
-    near_terms<R>(ring, tnew, f, tri, lane, true, dnew);
+    if (mode == 1)
+        near_terms2<R>(ring, tnew, f, tri, lane, dnew, nnext);
+    else if (mode == 2)
+        near_terms_complete<R>(f, tri, lane, dnew);
+    else
+        near_terms<R>(ring, tnew, f, tri, lane, true, dnew);
+}
+
+// N[t+1] of triangle tri for a two-step pass: the next step's acceleration row, or, without one,
+// the ring slot the step would read
+template <typename R>
+__device__ inline R next_neumann(const Ring<R> &ring, const StepDyn &dn, int tri)
+{
+    return dn.acc ? (R)dn.acc[tri] : ring.hrow(0, 0, tri)[hist_index(0, dn.tnew)];
 }
 
 // the fused face stage (corner loads issued first so their latency overlaps the convolution)
@@ -653,7 +762,9 @@ __global__ void __launch_bounds__(256) fix_kernel(int nt, const __grid_constant_
 // pipelined step: the rest of the face stage of step kstep; next != 0: also the Neumann value of
 // step kstep + 1 into the history (its slot is outside every window of this step), so the next
 // step's convolution can start before that step's stencil
-template <typename R>
+// (one instantiation per mode: the two-step variants need more registers, which the one-step
+// path should not carry)
+template <typename R, int mode>
 __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
                                                       int kstep, int nt, const __grid_constant__ FaceArgs<R> f,
                                                       const R *conv, int next)
@@ -663,15 +774,33 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Rin
         return;
     const int lane = threadIdx.x & 31;
     const StepDyn dy = bind_step(st, kstep, nt);
+    const StepDyn dn = bind_step(st, kstep + 1, nt);
     R iw, pv;
     face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
-    face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri]);
-    if (next && lane == 0)
-    {
-        const StepDyn dn = bind_step(st, kstep + 1, nt);
-        if (dn.acc)
-            ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
-    }
+    face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri], mode,
+                   mode == 1 ? next_neumann<R>(ring, dn, tri) : (R)0);
+    if (next && lane == 0 && dn.acc)
+        ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
+}
+
+// the autotuner's finish: the same work without the history and Dirichlet writes, so that timing
+// it changes no state (the near-field terms it writes are rebuilt by every step before they are
+// read)
+template <typename R, int mode>
+__global__ void __launch_bounds__(256) finish_dry_kernel(const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                          int kstep, int nt, const __grid_constant__ FaceArgs<R> f,
+                                                          const R *conv)
+{
+    const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (tri >= nt)
+        return;
+    const int lane = threadIdx.x & 31;
+    const StepDyn dy = bind_step(st, kstep, nt);
+    const StepDyn dn = bind_step(st, kstep + 1, nt);
+    R iw, pv;
+    face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
+    face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri], mode,
+                   mode == 1 ? next_neumann<R>(ring, dn, tri) : (R)0, false);
 }
 
 // the Neumann value of step kstep into the history (first step of a pipelined call)
@@ -814,6 +943,7 @@ struct StepLaunch
     R *conv1;  // partial sums of the second step of a pipelined pair
     int pairs;         // pipelined graphs convolve the face pairs for two steps per pass (conv2 + fix)
     int face_threads;  // threads per block of the pipelined face-stage kernels
+    int tpairs;        // the near-field terms two steps per pass (near_terms2)
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
     int ghost;     // ghost-cell method: the ghost kernel after the stencil instead of face / near
     GhostStep gs;  // its arguments
@@ -870,11 +1000,14 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.fa.terms = (R *)h.d_terms;
         L.conv = (R *)h.d_conv;
         L.conv1 = (R *)h.d_conv1;
-        L.pairs = h.conv_pairs ? 1 : 0;
+        L.pairs = h.conv_pairs;
         L.face_threads = h.face_threads;
+        L.tpairs = h.terms_pairs ? 1 : 0;
         L.fa.face_d1 = (const R *)h.d_face_d1;
         L.fa.order = h.d_base_tris;
         L.fa.dlast = (R *)h.d_dlast;
+        L.fa.terms1 = (R *)h.d_terms1;
+        L.fa.gc_f = (const R *)h.d_gc_f;
         L.na.n3_cell = h.d_n3_cell;
         L.na.n3_start = h.d_n3_start;
         L.na.p3_tri = h.d_p3_tri;
@@ -955,80 +1088,22 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
         // the stencil without its Neumann block range (finish / nwrite wrote N[t])
         stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
         cudaStreamWaitEvent(s, h.ev_conv, 0);
-        finish_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, k + 1 < nsteps ? 1 : 0);
+        // the call's last step computes its terms in one pass (mode 0): the FDTD-near sums it
+        // leaves for the next call are then exactly those that prime() rebuilds after a state
+        // restore or a mesh update
+        const int mode = L.tpairs && k + 1 < nsteps ? ((k & 1) ? 2 : 1) : 0;
+        const int nx = k + 1 < nsteps ? 1 : 0;
+        if (mode == 1)
+            finish_kernel<R, 1><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+        else if (mode == 2)
+            finish_kernel<R, 2><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+        else
+            finish_kernel<R, 0><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
         cudaEventRecord(h.ev_fin, s);
         near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
     }
 }
 
-// Autotuner of the face stage: on the handle's current mesh and state, time the face-pair
-// convolution of two consecutive steps in every candidate configuration - one pass per step
-// (conv, conv) or one pass for both (conv2, fix) - at 64, 128 and 256 threads per block, each of
-// the two launches reps times back to back on the handle's stream between CUDA events, and keep
-// the fastest for the recorded step graphs.  The kernels write only the convolution scratch
-// sums, so no state of the scene changes.  us[2 i], us[2 i + 1]: microseconds per launch of the
-// first and second kernel of candidate i, in the order (pairs 0, 64), (pairs 0, 128),
-// (pairs 0, 256), (pairs 1, 64), ...
-constexpr int kTuneThreads[3] = {64, 128, 256};
-
-template <typename R>
-int autotune(Handle &h, int reps, float *us, int *best)
-{
-    if (!h.mesh_set || h.prm.method != PPPM_METHOD_PPPM || h.nt == 0)
-    {
-        set_error("autotune needs a mesh (PPPM method)");
-        return PPPM_ERR_STATE;
-    }
-    if (!h.d_state)
-        PB_TRY(dalloc(&h.d_state, 1));
-    cudaStream_t s = h.stream;
-    StepState stt{h.t + 1, h.n3, 0, nullptr};
-    set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
-    StepLaunch<R> L;
-    PB_TRY(make_launch<R>(h, L));
-    const int nt = h.nt;
-    auto run = [&](int c, int which) {
-        const int FT = kTuneThreads[c % 3], nb = div_up((long long)nt * 32, FT);
-        if (c < 3)
-            conv_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, which, nt, L.fa, L.conv);
-        else if (which == 0)
-            conv2_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, L.conv1);
-        else
-            fix_kernel<R><<<nb, FT, 0, s>>>(nt, L.fa, L.conv1, L.conv);
-    };
-    for (int c = 0; c < 6; c++)
-    {
-        run(c, 0);
-        run(c, 1);
-    }
-    PB_CHECK_LAUNCH();
-    int bi = 0;
-    float tot[6];
-    for (int c = 0; c < 6; c++)
-    {
-        PB_CUDA(cudaEventRecord(h.ev[0], s));
-        for (int r = 0; r < reps; r++)
-            run(c, 0);
-        PB_CUDA(cudaEventRecord(h.ev[1], s));
-        for (int r = 0; r < reps; r++)
-            run(c, 1);
-        PB_CUDA(cudaEventRecord(h.ev[2], s));
-        PB_CUDA(cudaEventSynchronize(h.ev[2]));
-        float ma = 0, mb = 0;
-        PB_CUDA(cudaEventElapsedTime(&ma, h.ev[0], h.ev[1]));
-        PB_CUDA(cudaEventElapsedTime(&mb, h.ev[1], h.ev[2]));
-        us[2 * c] = 1000.0f * ma / reps;
-        us[2 * c + 1] = 1000.0f * mb / reps;
-        tot[c] = us[2 * c] + us[2 * c + 1];
-        if (tot[c] < tot[bi])
-            bi = c;
-    }
-    h.launches += 2LL * reps * 6 + 13;
-    h.conv_pairs = bi >= 3;
-    h.face_threads = kTuneThreads[bi % 3];
-    *best = bi;
-    return PPPM_OK;
-}
 
 // Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
 // first call with that step count and launch set (the graph removes the host launch cost and
@@ -1160,6 +1235,210 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     return PPPM_OK;
 }
 
+// Autotuner of the face stage: on the handle's current mesh and state, time the face-pair
+// convolution of two consecutive steps in every candidate configuration - one pass per step
+// (conv, conv) or one pass for both (conv2, fix) - at 64, 128 and 256 threads per block, each of
+// the two launches reps times back to back on the handle's stream between CUDA events; then the
+// rest of the face stage with the near-field terms one or two steps per pass.  The kernels write
+// only scratch sums and derived terms, so no state of the scene changes.  us[2 i], us[2 i + 1]:
+// microseconds per launch of the first and second kernel of candidate i, in the order
+// (pairs 0, 64), (pairs 0, 128), (pairs 0, 256), (pairs 1, 64), ..., finish single, finish pairs.
+constexpr int kTuneThreads[3] = {64, 128, 256};
+constexpr int kTuneConfigs = 12;     // conv_pairs x face threads x terms_pairs (phase 2)
+constexpr int kTuneGraphSteps = 64;  // recorded steps timed per configuration
+
+template <typename R>
+int autotune(Handle &h, int reps, float *us, int *best)
+{
+    if (!h.mesh_set || h.prm.method != PPPM_METHOD_PPPM || h.nt == 0)
+    {
+        set_error("autotune needs a mesh (PPPM method)");
+        return PPPM_ERR_STATE;
+    }
+    if (!h.d_state)
+        PB_TRY(dalloc(&h.d_state, 1));
+    cudaStream_t s = h.stream;
+    StepState stt{h.t + 1, h.n3, 0, nullptr};
+    set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
+    StepLaunch<R> L;
+    PB_TRY(make_launch<R>(h, L));
+    const int nt = h.nt;
+    auto run = [&](int c, int which) {
+        const int FT = kTuneThreads[c % 3], nb = div_up((long long)nt * 32, FT);
+        if (c < 3)
+            conv_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, which, nt, L.fa, L.conv);
+        else if (which == 1)
+            fix_kernel<R><<<nb, FT, 0, s>>>(nt, L.fa, L.conv1, L.conv);
+        else
+            conv2_kernel<R><<<nb, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, L.conv1);
+    };
+    constexpr int kConv = 6;
+    for (int c = 0; c < kConv; c++)
+    {
+        run(c, 0);
+        run(c, 1);
+    }
+    PB_CHECK_LAUNCH();
+    int bi = 0;
+    float tot[kConv];
+    for (int c = 0; c < kConv; c++)
+    {
+        PB_CUDA(cudaEventRecord(h.ev[0], s));
+        for (int r = 0; r < reps; r++)
+            run(c, 0);
+        PB_CUDA(cudaEventRecord(h.ev[1], s));
+        for (int r = 0; r < reps; r++)
+            run(c, 1);
+        PB_CUDA(cudaEventRecord(h.ev[2], s));
+        PB_CUDA(cudaEventSynchronize(h.ev[2]));
+        float ma = 0, mb = 0;
+        PB_CUDA(cudaEventElapsedTime(&ma, h.ev[0], h.ev[1]));
+        PB_CUDA(cudaEventElapsedTime(&mb, h.ev[1], h.ev[2]));
+        us[2 * c] = 1000.0f * ma / reps;
+        us[2 * c + 1] = 1000.0f * mb / reps;
+        tot[c] = us[2 * c] + us[2 * c + 1];
+        if (tot[c] < tot[bi])
+            bi = c;
+    }
+    // the rest of the face stage (finish, the near-field terms): one pass per step, or two steps
+    // per pass (candidates 9 and 10), at the chosen block size
+    {
+        const int FT = kTuneThreads[bi % 3], nb = div_up((long long)nt * 32, FT);
+        for (int c = kConv; c < kConv + 2; c++)
+        {
+            const bool two = c != kConv;
+            auto first = [&]() {
+                if (two)
+                    finish_dry_kernel<R, 1><<<nb, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv);
+                else
+                    finish_dry_kernel<R, 0><<<nb, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv);
+            };
+            auto second = [&]() {
+                if (two)
+                    finish_dry_kernel<R, 2><<<nb, FT, 0, s>>>(L.ring, L.st, 1, nt, L.fa, L.conv);
+                else
+                    finish_dry_kernel<R, 0><<<nb, FT, 0, s>>>(L.ring, L.st, 1, nt, L.fa, L.conv);
+            };
+            first();
+            second();
+            PB_CUDA(cudaEventRecord(h.ev[0], s));
+            for (int r = 0; r < reps; r++)
+                first();
+            PB_CUDA(cudaEventRecord(h.ev[1], s));
+            for (int r = 0; r < reps; r++)
+                second();
+            PB_CUDA(cudaEventRecord(h.ev[2], s));
+            PB_CUDA(cudaEventSynchronize(h.ev[2]));
+            PB_CHECK_LAUNCH();
+            float ma = 0, mb = 0;
+            PB_CUDA(cudaEventElapsedTime(&ma, h.ev[0], h.ev[1]));
+            PB_CUDA(cudaEventElapsedTime(&mb, h.ev[1], h.ev[2]));
+            us[2 * c] = 1000.0f * ma / reps;
+            us[2 * c + 1] = 1000.0f * mb / reps;
+        }
+        h.launches += 4LL * reps + 4;
+    }
+    h.launches += 2LL * reps * kConv + 2 * kConv + 1;
+    h.conv_pairs = bi / 3;
+    h.face_threads = kTuneThreads[bi % 3];
+    h.terms_pairs = us[2 * kConv + 2] + us[2 * kConv + 3] < us[2 * kConv] + us[2 * kConv + 1];
+    *best = bi;
+    if (!h.side || h.prm.pml_width > 0)
+        return PPPM_OK;  // no two-branch step graphs: the kernel timings decide
+
+    // Phase 2: the kernels compete inside the two-branch step graph (the convolution beside the
+    // stencil and the near stage, the finish on the critical path), which isolated launches do not
+    // show.  Time kTuneGraphSteps recorded steps (zero accelerations) of every configuration from
+    // one device snapshot of the fields and histories: per candidate and rep, restore the snapshot,
+    // replay the graph once (warm-up, weights into L2 as in a long run), replay it again timed; keep
+    // the fastest.  us[2 * PPPM_TUNE_CANDIDATES + i]: microseconds per step of configuration i
+    // (conv_pairs = i / 6, threads = {64, 128, 256}[(i / 2) % 3], terms_pairs = i % 2).  The steps
+    // write listener rows past the recorded ones, which the next call overwrites; the fields and
+    // histories are restored from the snapshot at the end; h.t and the series count do not move.
+    const size_t gbytes = (size_t)h.n_cells * h.real_size, hbytes = (size_t)8 * nt * kRing * h.real_size;
+    const size_t abytes = (size_t)kTuneGraphSteps * nt * sizeof(float);
+    void *snap = nullptr;
+    PB_TRY(dev_alloc(&snap, 3 * gbytes + hbytes + abytes));
+    // zero accelerations for the timed steps (the code paths of a call with accelerations)
+    const float *zacc = (const float *)((char *)snap + 3 * gbytes + hbytes);
+    PB_CUDA(cudaMemsetAsync((void *)zacc, 0, abytes, s));
+    auto copy_state = [&](bool save) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < 3 && e == cudaSuccess; i++)
+            e = save ? cudaMemcpyAsync((char *)snap + i * gbytes, h.grid[i], gbytes, cudaMemcpyDeviceToDevice, s)
+                     : cudaMemcpyAsync(h.grid[i], (char *)snap + i * gbytes, gbytes, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess)
+            e = save ? cudaMemcpyAsync((char *)snap + 3 * gbytes, h.d_hist, hbytes, cudaMemcpyDeviceToDevice, s)
+                     : cudaMemcpyAsync(h.d_hist, (char *)snap + 3 * gbytes, hbytes, cudaMemcpyDeviceToDevice, s);
+        return e;
+    };
+    const int keep_pairs = h.conv_pairs, keep_threads = h.face_threads;
+    const bool keep_terms = h.terms_pairs;
+    int rc = PPPM_OK, gbest = -1;
+    float *gus = us + 2 * PPPM_TUNE_CANDIDATES;
+    cudaError_t e = copy_state(true);
+    StepState sg{h.t + 1, h.n3, h.series_count, zacc};
+    for (int c = 0; c < kTuneConfigs && e == cudaSuccess && rc == PPPM_OK; c++)
+    {
+        h.conv_pairs = c / 6;
+        h.face_threads = kTuneThreads[(c / 2) % 3];
+        h.terms_pairs = (c & 1) != 0;
+        StepLaunch<R> G;
+        rc = make_launch<R>(h, G);
+        cudaGraphExec_t exec = nullptr;
+        if (rc == PPPM_OK)
+            rc = graph_for<R>(h, G, kTuneGraphSteps, &exec);
+        if (rc != PPPM_OK)
+            break;
+        float best_ms = 1e30f;
+        for (int r = 0; r <= reps && e == cudaSuccess; r++)  // r = 0: warm-up
+        {
+            e = copy_state(false);
+            set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sg);
+            if (e == cudaSuccess)
+                e = cudaGraphLaunch(exec, s);
+            set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sg);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(h.ev[0], s);
+            if (e == cudaSuccess)
+                e = cudaGraphLaunch(exec, s);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(h.ev[1], s);
+            if (e == cudaSuccess)
+                e = cudaEventSynchronize(h.ev[1]);
+            float ms = 0;
+            if (e == cudaSuccess && r > 0 && cudaEventElapsedTime(&ms, h.ev[0], h.ev[1]) == cudaSuccess)
+                best_ms = std::min(best_ms, ms);
+        }
+        h.launches += (long long)(reps + 1) * 2 * (kTuneGraphSteps * 4 + 1);
+        gus[c] = 1000.0f * best_ms / kTuneGraphSteps;
+        if (gbest < 0 || gus[c] < gus[gbest])
+            gbest = c;
+    }
+    if (e == cudaSuccess)
+        e = copy_state(false);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    dev_free(snap);
+    if (rc == PPPM_OK && e != cudaSuccess)
+    {
+        set_error("autotune: %s", cudaGetErrorString(e));
+        rc = PPPM_ERR_CUDA;
+    }
+    if (rc != PPPM_OK || gbest < 0)
+    {
+        h.conv_pairs = keep_pairs;
+        h.face_threads = keep_threads;
+        h.terms_pairs = keep_terms;
+        return rc;
+    }
+    h.conv_pairs = gbest / 6;
+    h.face_threads = kTuneThreads[(gbest / 2) % 3];
+    h.terms_pairs = (gbest & 1) != 0;
+    *best = gbest;
+    return PPPM_OK;
+}
+
 template <typename R>
 int prime(Handle &h)
 {
@@ -1170,6 +1449,7 @@ int prime(Handle &h)
     // taps t-k of the current time: the FDTD-near sum of step t + 1 into its slot
     StepState stt{h.t, h.n3, 0, nullptr};
     set_state_kernel<<<1, 1, 0, h.stream>>>(h.d_state, stt);
+
     StepLaunch<R> L;
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
@@ -1321,7 +1601,7 @@ __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc
         return;
     const int tri = centre_of(S.fa, w);
     const int tnew = S.st->tnew0 + k, p0 = S.st->pair0, pe = S.st->pair_end;
-    const bool paired = pe >= p0;
+    const bool paired = pe >= p0 && S.st->conv_pairs;
     if (paired && ((tnew - p0) & 1))
         face_fix<R>(S.fa, S.conv1, S.conv, tri, lane);  // second step of a pair
     else if (paired && tnew + 1 <= pe)
@@ -1352,15 +1632,16 @@ __global__ void __launch_bounds__(256) batch_finish_kernel(const BatchScene<R> *
     if (tri >= S.a.nt)
         return;
     const StepDyn dy = bind_step(S.st, k, S.a.nt);
+    const StepDyn dn = bind_step(S.st, k + 1, S.a.nt);
+    // the scene's pairing of steps (batch_conv_kernel)
+    const int p0 = S.st->pair0, pe = S.st->pair_end;
+    const int mode = pe >= p0 && S.st->terms_pairs && dy.tnew < pe ? (((dy.tnew - p0) & 1) ? 2 : 1) : 0;
     R iw, pv;
     face_corners<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv);
-    face_finish<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv, S.conv[tri]);
-    if (next && lane == 0)
-    {
-        const StepDyn dn = bind_step(S.st, k + 1, S.a.nt);
-        if (dn.acc)
-            S.ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
-    }
+    face_finish<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv, S.conv[tri], mode,
+                   mode == 1 ? next_neumann<R>(S.ring, dn, tri) : (R)0);
+    if (next && lane == 0 && dn.acc)
+        S.ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
 }
 
 template <typename R>
@@ -1598,7 +1879,9 @@ int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
         // the scene's steps pair up as in one pppm_step call of nsteps[i] steps (recorded graphs:
         // at least kGraphSteps steps)
         stt.pair0 = h.t + 1;
-        stt.pair_end = h.conv_pairs && nsteps[i] >= kGraphSteps ? h.t + nsteps[i] : h.t;
+        stt.pair_end = nsteps[i] >= kGraphSteps ? h.t + nsteps[i] : h.t;
+        stt.conv_pairs = h.conv_pairs ? 1 : 0;
+        stt.terms_pairs = h.terms_pairs ? 1 : 0;
         set_state_kernel<<<1, 1, 0, b.stream>>>(h.d_state, stt);
         b.launches++;
     }

@@ -425,12 +425,13 @@ class Solver:
         check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
         return v.value
 
-    OPTIONS = {"conv_pairs": 0, "face_threads": 1}
+    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2}
     TUNE_CANDIDATES = [(pairs, threads) for pairs in (0, 1) for threads in (64, 128, 256)]
+    TUNE_CONFIGS = [(pairs, threads, terms) for pairs in (0, 1) for threads in (64, 128, 256) for terms in (0, 1)]
 
     def set_option(self, name, value):
-        """Launch option of the recorded step graphs (pppm_set_option): conv_pairs (0/1),
-        face_threads (64/128/256)."""
+        """Launch option of the recorded step graphs (pppm_set_option): conv_pairs (0: one pass
+        per step, 1: two steps per pass), face_threads (64/128/256), terms_pairs (0/1)."""
         check(lib.pppm_set_option(self.h, self.OPTIONS[name], int(value)), "set_option")
 
     def get_option(self, name):
@@ -443,12 +444,18 @@ class Solver:
         fastest.  Returns {"us": {(pairs, threads): us per two steps}, "launch_us":
         {(pairs, threads): (first kernel, second kernel) us per launch}, "best": (pairs, threads)}."""
         n = len(self.TUNE_CANDIDATES)
-        us = (ctypes.c_float * (2 * n))()
+        us = (ctypes.c_float * (2 * (n + 2) + len(self.TUNE_CONFIGS)))()
         best = ctypes.c_int()
         check(lib.pppm_autotune(self.h, int(reps), us, ctypes.byref(best)), "autotune")
-        per = [(float(us[2 * i]), float(us[2 * i + 1])) for i in range(n)]
+        per = [(float(us[2 * i]), float(us[2 * i + 1])) for i in range(n + 2)]
+        step_us = [float(us[2 * (n + 2) + j]) for j in range(len(self.TUNE_CONFIGS))]
+        chosen = (self.get_option("conv_pairs"), self.get_option("face_threads"))
         return {"us": {c: a + b for c, (a, b) in zip(self.TUNE_CANDIDATES, per)},
-                "launch_us": dict(zip(self.TUNE_CANDIDATES, per)), "best": self.TUNE_CANDIDATES[best.value]}
+                "launch_us": dict(zip(self.TUNE_CANDIDATES, per)), "best": chosen,
+                "finish_us": {"single": sum(per[n]), "pairs": sum(per[n + 1])},
+                "finish_launch_us": {"single": per[n], "pairs": per[n + 1]},
+                "step_us": dict(zip(self.TUNE_CONFIGS, step_us)) if any(step_us) else None,
+                "terms_pairs": self.get_option("terms_pairs")}
 
     def enable_timing(self, on=True):
         check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")

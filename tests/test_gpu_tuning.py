@@ -17,11 +17,12 @@ from pppm_b200 import Solver
 pytestmark = pytest.mark.gpu
 
 
-def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False):
+def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None):
     v0, f, h, mn, dt = sphere_small()
     res = 24
     s = Solver(res, h, dt, mn, precision=precision)
     s.set_option("conv_pairs", pairs)
+    s.set_option("terms_pairs", (1 if pairs else 0) if terms is None else terms)
     s.set_option("face_threads", threads)
     s.set_mesh(moving_small_verts(v0, 0, dt) if moving else v0, f)
     s.add_listener(20, 20, 20)
@@ -43,6 +44,14 @@ def test_pairs_match_single_pass_fp64(gpu):
     assert rel_l2(b, a) < 1e-12
 
 
+@pytest.mark.parametrize("conv,terms", [(1, 0), (0, 1)])
+def test_pairing_each_stage_fp64(gpu, conv, terms):
+    # the convolution and the near-field terms pair their steps independently
+    a = _series("fp64", 0, terms=0)
+    b = _series("fp64", conv, terms=terms)
+    assert rel_l2(b, a) < 1e-12
+
+
 def test_pairs_match_single_pass_fp32(gpu):
     a = _series("fp32", 0)
     b = _series("fp32", 1)
@@ -60,10 +69,10 @@ def test_pairs_odd_calls_and_motion(gpu, chunk):
     assert rel_l2(b, a) < 1e-12
 
 
-@pytest.mark.parametrize("threads", [64, 128])
-def test_face_threads(gpu, threads):
-    a = _series("fp32", 1)
-    b = _series("fp32", 1, threads=threads)
+@pytest.mark.parametrize("pairs,threads", [(1, 64), (1, 128), (0, 64)])
+def test_face_threads(gpu, pairs, threads):
+    a = _series("fp32", pairs)
+    b = _series("fp32", pairs, threads=threads)
     assert np.array_equal(a, b)  # same arithmetic, other block shape
 
 
@@ -76,12 +85,19 @@ def test_autotune_keeps_results(gpu):
     acc = sine_acc(200, len(f), 1500.0, dt)
     s.step(acc[:100])
     t_before = s.t
-    g_before = s.grid(0).copy()
-    tune = s.autotune(reps=5)
+    before = [s.grid(r).copy() for r in (0, -1, -2)] + [s.dump("neumann"), s.dump("dirichlet"), s.listeners()]
+    tune = s.autotune(reps=3)
     assert len(tune["us"]) == 6 and all(u > 0 for u in tune["us"].values())
-    assert tune["best"] == min(tune["us"], key=tune["us"].get)
-    assert (s.get_option("conv_pairs"), s.get_option("face_threads")) == tune["best"]
-    assert s.t == t_before and np.array_equal(s.grid(0), g_before)
+    # phase 2 (whole recorded steps of every option set) decides
+    assert tune["step_us"] is not None and len(tune["step_us"]) == 12
+    assert all(u > 0 for u in tune["step_us"].values())
+    chosen = (s.get_option("conv_pairs"), s.get_option("face_threads"), s.get_option("terms_pairs"))
+    assert chosen == min(tune["step_us"], key=tune["step_us"].get)
+    # fields, histories, time and recorded samples are as before
+    after = [s.grid(r) for r in (0, -1, -2)] + [s.dump("neumann"), s.dump("dirichlet"), s.listeners()]
+    assert s.t == t_before
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
     s.step(acc[100:])
     got = s.listeners()[:, 0]
     s.close()
@@ -107,6 +123,8 @@ def test_bad_options_rejected(gpu):
         s.set_option("face_threads", 96)
     with pytest.raises(PPPMError):
         s.set_option("conv_pairs", 2)
+    with pytest.raises(PPPMError):
+        s.set_option("terms_pairs", -1)
     with pytest.raises(PPPMError):
         s.autotune()  # no mesh yet
     s.close()
