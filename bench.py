@@ -394,7 +394,7 @@ def run_ours(args, ws, rank, local):
                      "traffic": traffic, "algorithmic_bytes": int(top_bytes), "kernel_launch_us": round(top_us, 3),
                      "autotune": {"best": {"two_steps_per_pass": bool(pairs), "threads": threads,
                                            "terms_two_steps_per_pass": bool(tune["terms_pairs"])},
-                                  "decided_by": "16 recorded steps per option set (phase 2)",
+                                  "decided_by": "64 recorded steps per option set (phase 2)",
                                   "finish_us_per_two_steps": {k: round(v, 2) for k, v in tune["finish_us"].items()},
                                   "step_us_by_config": {"%s/%d/%s" % (("single", "pairs")[p], t,
                                                                       "terms2" if m else "terms1"): round(u, 2)

@@ -251,7 +251,7 @@ int pppm_get_option(pppm_handle *h, int option, int *value);
  * steps per pass (candidate 7), reps launches of each kernel.  Phase 2 (absorbing boundary) times
  * 64 recorded steps (zero accelerations) of each of PPPM_TUNE_CONFIGS option sets (config j: conv_pairs = j / 6,
  * threads = {64, 128, 256}[(j / 2) % 3], terms_pairs = j % 2) from a device snapshot of the
- * fields and histories (a warm-up replay, then a timed one; best of reps) and sets the options to
+ * fields and histories (a warm-up replay, then a timed one; best of min(reps, 3)) and sets the options to
  * the fastest (with a PML, phase 1 decides).  us_out (may be NULL; 2 * PPPM_TUNE_CANDIDATES +
  * PPPM_TUNE_CONFIGS floats): microseconds per launch of candidate i's first kernel (us_out[2 i])
  * and second kernel (us_out[2 i + 1]), then microseconds per step of each config; *best (may be

@@ -1351,7 +1351,7 @@ int autotune(Handle &h, int reps, float *us, int *best)
     // show.  Time kTuneGraphSteps recorded steps (zero accelerations) of every configuration from
     // one device snapshot of the fields and histories: per candidate and rep, restore the snapshot,
     // replay the graph once (warm-up, weights into L2 as in a long run), replay it again timed; keep
-    // the fastest.  us[2 * PPPM_TUNE_CANDIDATES + i]: microseconds per step of configuration i
+    // the fastest of up to 3 reps.  us[2 * PPPM_TUNE_CANDIDATES + i]: microseconds per step of configuration i
     // (conv_pairs = i / 6, threads = {64, 128, 256}[(i / 2) % 3], terms_pairs = i % 2).  The steps
     // write listener rows past the recorded ones, which the next call overwrites; the fields and
     // histories are restored from the snapshot at the end; h.t and the series count do not move.
@@ -1391,7 +1391,7 @@ int autotune(Handle &h, int reps, float *us, int *best)
         if (rc != PPPM_OK)
             break;
         float best_ms = 1e30f;
-        for (int r = 0; r <= reps && e == cudaSuccess; r++)  // r = 0: warm-up
+        for (int r = 0; r <= std::min(reps, 3) && e == cudaSuccess; r++)  // r = 0: warm-up
         {
             e = copy_state(false);
             set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sg);
@@ -1410,7 +1410,7 @@ int autotune(Handle &h, int reps, float *us, int *best)
             if (e == cudaSuccess && r > 0 && cudaEventElapsedTime(&ms, h.ev[0], h.ev[1]) == cudaSuccess)
                 best_ms = std::min(best_ms, ms);
         }
-        h.launches += (long long)(reps + 1) * 2 * (kTuneGraphSteps * 4 + 1);
+        h.launches += (long long)(std::min(reps, 3) + 1) * 2 * (kTuneGraphSteps * 4 + 1);
         gus[c] = 1000.0f * best_ms / kTuneGraphSteps;
         if (gbest < 0 || gus[c] < gus[gbest])
             gbest = c;
