@@ -257,7 +257,8 @@ int pppm_get_option(pppm_handle *h, int option, int *value);
  * and second kernel (us_out[2 i + 1]), then microseconds per step of each config; *best (may be
  * NULL): the config chosen (or, with a PML, the convolution candidate).  The fields, histories,
  * time and recorded listener samples are as before the call; it allocates a snapshot of the
- * fields and histories for its duration.  Needs a mesh and the PPPM method. */
+ * fields and histories for its duration and records CUDA graphs, so it must not be called while
+ * the handle's stream is being captured.  Needs a mesh and the PPPM method. */
 #define PPPM_TUNE_CANDIDATES 8
 #define PPPM_TUNE_CONFIGS 12
 int pppm_autotune(pppm_handle *h, int reps, float *us_out, int *best);
