@@ -734,37 +734,46 @@ def run_reference(args, ws, rank, local):
     sc = wl.scene
     from oracle import oracle as O
 
+    ndebug = None
     if O.reference_available():
         import torch
 
-        r = O.Reference(wl.res, sc.h, sc.dt, sc.min_pos)
-        r.set_mesh(wl.verts[0], wl.tris)
-        if wl.moving:
-            for v in wl.verts[1:]:
-                r.check_mesh(v)  # validate the whole trajectory against the reference capacities
-            r.set_checks(False)
         acc_dev = torch.from_numpy(wl.acc).cuda()
         nt = len(wl.tris)
         ptr0 = acc_dev.data_ptr()
 
-        def frame(f):
-            a, b = wl.ranges[f]
-            if f > 0 and wl.moving:
-                r.update_mesh(wl.verts[f])
-            r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
+        def timed_run(nd):
+            """W warm-up and K timed frames of the reference build (nd: the -DNDEBUG build)."""
+            r = O.Reference(wl.res, sc.h, sc.dt, sc.min_pos, ndebug=nd)
+            r.set_mesh(wl.verts[0], wl.tris)
+            if wl.moving:
+                for v in wl.verts[1:]:
+                    r.check_mesh(v)  # validate the whole trajectory against the reference capacities
+                r.set_checks(False)
 
-        for f in range(0, W + 1):
-            frame(f)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        steps = 0
-        for f in range(W + 1, W + K + 1):
-            frame(f)
-            steps += wl.ranges[f][1] - wl.ranges[f][0]
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        r.close()
-        value = float(wl.res) ** 3 * steps / dt / 1e9
+            def frame(f):
+                a, b = wl.ranges[f]
+                if f > 0 and wl.moving:
+                    r.update_mesh(wl.verts[f])
+                r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
+
+            for f in range(0, W + 1):
+                frame(f)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            steps = 0
+            for f in range(W + 1, W + K + 1):
+                frame(f)
+                steps += wl.ranges[f][1] - wl.ranges[f][0]
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            r.close()
+            return float(wl.res) ** 3 * steps / dt / 1e9
+
+        value = timed_run(False)
+        if O.reference_available(ndebug=True):
+            ndebug = {"value": round(timed_run(True), 5), "unit": "Gcell-steps/s",
+                      "build": "the same reference sources built with -DNDEBUG (no device sync after every launch)"}
         kind, cores, sample = "reference", 0, ("reference CUDA solver built from source (oracle/_ref, upstream flags: "
                                                 "device sync after every launch), %d frames" % K)
     else:
@@ -791,7 +800,8 @@ def run_reference(args, ws, rank, local):
             "cpu_baseline": {"value": round(value, 5), "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(value, 5), "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_ndebug": ndebug}
 
 
 def run_reference_batch(args):
