@@ -11,12 +11,17 @@
 // the cross-fade restart of main.cu:212-263.  Output: outputDir/result.txt, line 0 the frame
 // rate, then one "%e" sample per step.
 //
+// Modal objects (RigidBody): their IIR runs at the step rate; the run starts at the latest first
+// contact, whose leading samples stay silent (zero) at the front of result.txt (main.cu:104-125,153).
+//
 // Differences, all where the reference is undefined or unavailable: no FixMesh (the reference
 // shells out to a pymesh docker image); chunkSize <= 0 disables the cross-fade (the reference
 // evaluates i % 0); a non-finite sample stops the run (the reference tests an index one past
 // the sample it just wrote).  Steps between mesh updates are submitted to the device in one
 // call and the listener samples read back once per batch instead of once per step.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <filesystem>
@@ -86,11 +91,56 @@ int fail(const char *what, int rc)
 
 }  // namespace
 
+// pppm_demo --modal-accs DIR RATE NSAMPLES OUT: the surface accelerations of one Modal object
+// (material "plastic") sampled at RATE from its first contact on, without the solver (the
+// reference's RigidBody::export_surface_accs).  OUT: "faces modes time" on line 1, the faces'
+// vertex triples, then one line of face accelerations per sample.
+int export_modal(char **argv)
+{
+    ModalObject m;
+    std::string err;
+    if (!m.load(argv[2], "plastic", err))
+    {
+        fprintf(stderr, "pppm_demo: %s\n", err.c_str());
+        return 1;
+    }
+    const float rate = (float)atof(argv[3]);
+    const int n = atoi(argv[4]);
+    if (!(rate > 0) || n < 0)
+    {
+        fprintf(stderr, "pppm_demo: bad RATE or NSAMPLES\n");
+        return 2;
+    }
+    m.set_sample_rate(rate);
+    m.move_to_first_impulse();
+    FILE *f = fopen(argv[5], "w");
+    if (!f)
+    {
+        fprintf(stderr, "pppm_demo: cannot write %s\n", argv[5]);
+        return 1;
+    }
+    fprintf(f, "%zu %d %.9e\n", m.tris.size(), m.n_modes(), m.current_time);
+    for (auto &t : m.tris)
+        fprintf(f, "%d %d %d\n", t[0], t[1], t[2]);
+    const float half = 0.5f / rate;
+    for (int s = 0; s < n; s++)
+    {
+        m.update_until(m.current_time + half);  // one audio sample
+        const auto &a = m.surface_acc();
+        for (size_t k = 0; k < a.size(); k++)
+            fprintf(f, k + 1 < a.size() ? "%.9e " : "%.9e\n", a[k]);
+    }
+    fclose(f);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 6 && std::strcmp(argv[1], "--modal-accs") == 0)
+        return export_modal(argv);
     if (argc < 2)
     {
-        fprintf(stderr, "usage: %s CONFIG\n", argv[0]);
+        fprintf(stderr, "usage: %s CONFIG\n       %s --modal-accs DIR RATE NSAMPLES OUT\n", argv[0], argv[0]);
         return 2;
     }
     SceneConfig cfg;
@@ -122,6 +172,16 @@ int main(int argc, char **argv)
     int frame_rate = (int)(1.01f / (grid_size / std::sqrt(3) / 340.3f));
     float dt = 1.0f / frame_rate;
     float curr_time = 0;
+    // Modal objects: their IIR runs at the step rate, and the run starts at the latest first
+    // contact, with that many leading samples left silent in the output (main.cu:104-125)
+    for (ModalObject *m : col.modal)
+        m->set_sample_rate((float)frame_rate);
+    for (ModalObject *m : col.modal)
+    {
+        m->move_to_first_impulse();
+        curr_time = std::max(curr_time, m->current_time);
+    }
+    const int mute_frames = (int)(curr_time * frame_rate);
     curr_time += cfg.num("startTime");
     float max_time = cfg.num("maxTime") + curr_time;
     int frame_num = (int)((max_time - curr_time) / dt);
@@ -147,7 +207,7 @@ int main(int argc, char **argv)
     if (rc)
         return fail("pppm_add_listener (checkCoord outside the grid?)", rc);
 
-    std::vector<float> result(frame_num + 2, 0.0f);
+    std::vector<float> result(mute_frames + frame_num + 2, 0.0f);
     result[0] = (float)frame_rate;
     Runner run;
     run.h = h;
@@ -199,7 +259,7 @@ int main(int argc, char **argv)
             for (auto &o : col.objects)
                 o->save_state();
             for (int j = i; j < end; j++)
-                if ((rc = update_sound(true, j + 1, 0, 1.0f - (float)(j - i) / (float)(end - i))))
+                if ((rc = update_sound(true, mute_frames + j + 1, 0, 1.0f - (float)(j - i) / (float)(end - i))))
                     return fail("step", rc);
             if ((rc = run.flush()))
                 return fail("step", rc);
@@ -211,14 +271,14 @@ int main(int argc, char **argv)
             for (auto &o : col.objects)
                 o->load_state();
             for (int j = i; j < end; j++)
-                if ((rc = update_sound(false, j + 1, 1, 1.0f)))
+                if ((rc = update_sound(false, mute_frames + j + 1, 1, 1.0f)))
                     return fail("step", rc);
             if ((rc = run.flush()))
                 return fail("step", rc);
             progress += end - i;
             continue;
         }
-        if ((rc = update_sound(false, i + 1, 0, 1.0f)))
+        if ((rc = update_sound(false, mute_frames + i + 1, 0, 1.0f)))
             return fail("step", rc);
         progress++;
     }

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <fstream>
 #include <sstream>
+#include <unordered_map>
 
 namespace pppm_host
 {
@@ -230,6 +231,30 @@ Vec3 rotate(const std::array<float, 4> &q, const Vec3 &v)
 }
 }  // namespace
 
+namespace
+{
+// motion.txt: "time tx ty tz qx qy qz qw" per frame (Object.cu: LoadMotion_)
+void load_motion(const std::string &path, std::vector<float> &frame_time, std::vector<Vec3> &translations,
+                 std::vector<std::array<float, 4>> &rotations)
+{
+    std::ifstream in(path);
+    std::string line;
+    while (in.good() && std::getline(in, line))
+    {
+        if (line.empty())
+            continue;
+        std::istringstream ss(line);
+        float t;
+        Vec3 tr;
+        std::array<float, 4> q;
+        ss >> t >> tr[0] >> tr[1] >> tr[2] >> q[0] >> q[1] >> q[2] >> q[3];
+        frame_time.push_back(t);
+        translations.push_back(tr);
+        rotations.push_back(q);
+    }
+}
+}  // namespace
+
 bool AudioObject::load(const std::string &dir, std::string &err)
 {
     Mesh m;
@@ -237,23 +262,7 @@ bool AudioObject::load(const std::string &dir, std::string &err)
         return false;
     verts = standard = m.verts;
     tris = m.tris;
-    {
-        std::ifstream in(dir + "/motion.txt");
-        std::string line;
-        while (in.good() && std::getline(in, line))
-        {
-            if (line.empty())
-                continue;
-            std::istringstream ss(line);
-            float t;
-            Vec3 tr;
-            std::array<float, 4> q;
-            ss >> t >> tr[0] >> tr[1] >> tr[2] >> q[0] >> q[1] >> q[2] >> q[3];
-            frame_time.push_back(t);
-            translations.push_back(tr);
-            rotations.push_back(q);
-        }
-    }
+    load_motion(dir + "/motion.txt", frame_time, translations, rotations);
     {
         std::ifstream in(dir + "/accs.txt");
         float a;
@@ -364,6 +373,380 @@ void AudioObject::load_state()
     acc_step = saved.acc_step;
 }
 
+
+// ------------------------------------------------------------------ modal objects --------
+// Rayleigh damping per material (src/utils/material.h); unknown names give no damping
+bool Material::set(const std::string &name)
+{
+    static const struct
+    {
+        const char *name;
+        float alpha, beta;
+    } table[] = {{"ceramic", 40.0f, 1e-7f}, {"plastic", 30.0f, 1e-6f}, {"steel", 5.0f, 3e-8f},
+                 {"mdf", 35.0f, 5e-6f},     {"wood", 60.0f, 2e-6f}};
+    for (auto &m : table)
+        if (name == m.name)
+        {
+            alpha = m.alpha;
+            beta = m.beta;
+            return true;
+        }
+    alpha = beta = 0.0f;
+    return false;
+}
+
+namespace
+{
+// Boundary faces of a tet mesh: faces that belong to one tet only, wound so that the normal points
+// away from that tet's fourth vertex (Object.cu: FindAllSurfaces).  The faces are visited in the
+// iteration order of a hash map keyed by the sorted vertex triple with the reference's hash, so
+// the face order (and with it the triangle numbering of the scene) is the reference's.
+struct TriKeyHash
+{
+    size_t operator()(const std::array<int, 3> &k) const
+    {
+        unsigned u = ((unsigned)k[0] << 20) + ((unsigned)k[1] << 10) + (unsigned)k[2];
+        return (size_t)(long long)(int)u;  // an int hash widened as the reference's is
+    }
+};
+
+void boundary_faces(const std::vector<std::array<int, 4>> &tets, const std::vector<Vec3> &v,
+                    std::vector<std::array<int, 3>> &faces, std::vector<Vec3> &normals)
+{
+    struct Info
+    {
+        int cnt = 0, tet = 0, except = 0;
+    };
+    std::unordered_map<std::array<int, 3>, Info, TriKeyHash> cand;
+    for (int i = 0; i < (int)tets.size(); i++)
+        for (int i0 = 0; i0 < 4; i0++)
+        {
+            std::array<int, 3> tri;
+            for (int j = 0, k = 0; j < 4; j++)
+                if (j != i0)
+                    tri[k++] = tets[i][j];
+            Info &in = cand[tri];
+            in.cnt++;
+            in.tet = i;
+            in.except = i0;
+        }
+    for (auto &kv : cand)
+    {
+        if (kv.second.cnt != 1)
+            continue;
+        std::array<int, 3> t = kv.first;
+        const Vec3 &a = v[t[0]], &b = v[t[1]], &c = v[t[2]];
+        Vec3 centre, ex, e1, e2, n;
+        for (int k = 0; k < 3; k++)
+        {
+            centre[k] = (a[k] + b[k] + c[k]) / 3;
+            e1[k] = b[k] - a[k];
+            e2[k] = c[k] - a[k];
+        }
+        const Vec3 &far = v[tets[kv.second.tet][kv.second.except]];
+        for (int k = 0; k < 3; k++)
+            ex[k] = far[k] - centre[k];
+        n = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        float inv = 1.0f / std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        for (int k = 0; k < 3; k++)
+            n[k] *= inv;
+        if (n[0] * ex[0] + n[1] * ex[1] + n[2] * ex[2] > 0)
+        {
+            std::swap(t[1], t[2]);
+            for (int k = 0; k < 3; k++)
+                n[k] = -n[k];
+        }
+        faces.push_back(t);
+        normals.push_back(n);
+    }
+}
+}  // namespace
+
+bool ModalObject::load(const std::string &dir, const std::string &material_name, std::string &err,
+                       float max_frequency)
+{
+    material.set(material_name);
+    load_motion(dir + "/motion.txt", frame_time, translations, rotations);
+    {
+        std::ifstream in(dir + "/contact.txt");
+        if (!in.good())
+        {
+            err = "cannot read " + dir + "/contact.txt";
+            return false;
+        }
+        std::string line;
+        while (std::getline(in, line))
+        {
+            if (line.empty())
+                continue;
+            std::istringstream ss(line);
+            float t, vid, nx, ny, nz, mag;
+            ss >> t >> vid >> nx >> ny >> nz >> mag;
+            impulses.push_back({t, (int)(vid + 0.5f), Vec3{nx * mag, ny * mag, nz * mag}});
+        }
+    }
+    {
+        std::ifstream in(dir + "/vertices.txt");
+        if (!in.good())
+        {
+            err = "cannot read " + dir + "/vertices.txt";
+            return false;
+        }
+        std::string line;
+        while (std::getline(in, line))
+        {
+            if (line.empty())
+                continue;
+            std::istringstream ss(line);
+            Vec3 p;
+            ss >> p[0] >> p[1] >> p[2];
+            standard.push_back(p);
+        }
+    }
+    std::vector<std::array<int, 4>> tets;
+    {
+        std::ifstream in(dir + "/tets.txt");
+        if (!in.good())
+        {
+            err = "cannot read " + dir + "/tets.txt";
+            return false;
+        }
+        std::string line;
+        while (std::getline(in, line))
+        {
+            if (line.empty())
+                continue;
+            std::istringstream ss(line);
+            float f[4];
+            ss >> f[0] >> f[1] >> f[2] >> f[3];
+            std::array<int, 4> t;
+            for (int k = 0; k < 4; k++)
+                t[k] = (int)(f[k] + 0.5f);
+            std::sort(t.begin(), t.end());
+            for (int k = 0; k < 4; k++)
+                if (t[k] < 0 || t[k] >= (int)standard.size())
+                {
+                    err = "tet vertex index out of range in " + dir + "/tets.txt";
+                    return false;
+                }
+            tets.push_back(t);
+        }
+    }
+    boundary_faces(tets, standard, tris, normals);
+    verts = standard;
+    // eigenvalues ascending; modes below max_frequency kept (RigidBody.cu: LoadEigen_)
+    std::vector<float> all;
+    {
+        std::ifstream in(dir + "/eigenvalues.txt");
+        if (!in.good())
+        {
+            err = "cannot read " + dir + "/eigenvalues.txt";
+            return false;
+        }
+        std::string line;
+        int keep = 0;
+        while (std::getline(in, line))
+        {
+            if (line.empty())
+                continue;
+            std::istringstream ss(line);
+            float val;
+            ss >> val;
+            all.push_back(val);
+            if (std::sqrt(val) / (2 * M_PI) < max_frequency)
+                keep = (int)all.size();
+        }
+        eigen.assign(all.begin(), all.begin() + keep);
+    }
+    const int dim = 3 * (int)standard.size(), nm = (int)eigen.size();
+    vecs.assign((size_t)dim * nm, 0.0f);
+    {
+        std::ifstream in(dir + "/eigenvectors.txt");
+        if (!in.good())
+        {
+            err = "cannot read " + dir + "/eigenvectors.txt";
+            return false;
+        }
+        for (int i = 0; i < dim; i++)
+            for (int j = 0; j < (int)all.size(); j++)
+            {
+                float val = 0;
+                in >> val;
+                if (j < nm)
+                    vecs[(size_t)i * nm + j] = val;
+            }
+        if (in.fail())
+        {
+            err = "eigenvectors.txt holds fewer than 3 x vertices x eigenvalues values";
+            return false;
+        }
+    }
+    // per face: normal . mean of its vertices' mode shapes (RigidBody.cu: MatrixVertToTri)
+    surf.assign(tris.size() * (size_t)nm, 0.0f);
+    for (size_t f = 0; f < tris.size(); f++)
+        for (int i = 0; i < nm; i++)
+        {
+            float m[3];
+            for (int k = 0; k < 3; k++)
+                m[k] = (vecs[(size_t)(3 * tris[f][0] + k) * nm + i] + vecs[(size_t)(3 * tris[f][1] + k) * nm + i] +
+                        vecs[(size_t)(3 * tris[f][2] + k) * nm + i]) /
+                       3;
+            surf[f * nm + i] = m[0] * normals[f][0] + m[1] * normals[f][1] + m[2] * normals[f][2];
+        }
+    accs.assign(tris.size(), 0.0f);
+    return true;
+}
+
+// IIR coefficients of one damped mode (RigidBody.cu: ModalInfo::SetCoeffs), in float
+void ModalObject::set_sample_rate(float rate)
+{
+    timestep = 1.0f / rate;
+    modes.assign(eigen.size(), Mode{});
+    for (size_t i = 0; i < eigen.size(); i++)
+    {
+        float lambda = eigen[i];
+        float omega = std::sqrt(lambda);
+        float ksi = (material.alpha + material.beta * lambda) / (2 * omega);
+        float omega_d = omega * std::sqrt(1 - ksi * ksi);
+        float eps = std::exp(-ksi * omega * timestep);
+        float eps2 = eps * eps;
+        float theta = omega_d * timestep;
+        float gamma = std::asin(ksi);
+        Mode &m = modes[i];
+        m.c1 = 2 * eps * std::cos(theta);
+        m.c2 = -eps2;
+        float a = eps * std::cos(theta + gamma);
+        float b = eps2 * std::cos(2 * theta + gamma);
+        m.c3 = 2 * (a - b) / (3 * omega * omega_d);
+    }
+    active.clear();
+    current_time = 0;
+    anim_step = 0;
+}
+
+void ModalObject::transform(int frame)
+{
+    for (size_t i = 0; i < verts.size(); i++)
+    {
+        Vec3 r = rotate(rotations[frame], standard[i]);
+        for (int k = 0; k < 3; k++)
+            verts[i][k] = r[k] + translations[frame][k];
+    }
+}
+
+// one audio sample (RigidBody.cu: audio_step, CalculateIIR_): the motion frame due, then the
+// contact forces of the impulses active at the new time (half sines of 0.5 ms), the modal IIR
+// step and the faces' accelerations
+void ModalObject::audio_step()
+{
+    moved_ = false;
+    if (anim_step < (int)frame_time.size() && frame_time[anim_step] <= current_time)
+    {
+        transform(anim_step);
+        anim_step++;
+        moved_ = true;
+    }
+    current_time += timestep;
+    const float now = current_time, tau = 0.0005f;
+    while (impulse_step < (int)impulses.size() && now >= impulses[impulse_step].time)
+        active.push_back(impulses[impulse_step++]);
+    while (!active.empty() && now - active.front().time > tau)
+        active.erase(active.begin());
+    const int nm = (int)modes.size();
+    std::vector<float> qdd(nm);
+    for (int i = 0; i < nm; i++)
+    {
+        Mode &m = modes[i];
+        m.f = 0;
+        for (auto &imp : active)
+        {
+            const float amp = (float)std::sin(M_PI * (now - imp.time) / tau);
+            const float jx = imp.vec[0] * amp, jy = imp.vec[1] * amp, jz = imp.vec[2] * amp;
+            const size_t r = (size_t)imp.vertex * 3;
+            m.f += vecs[r * nm + i] * jx + vecs[(r + 1) * nm + i] * jy + vecs[(r + 2) * nm + i] * jz;
+        }
+        const float q0 = m.c1 * m.q1 + m.c2 * m.q2 + m.c3 * m.f;
+        m.q3 = m.q2;
+        m.q2 = m.q1;
+        m.q1 = q0;
+        qdd[i] = (m.q1 + m.q3 - 2 * m.q2) / (timestep * timestep);
+    }
+    for (size_t f = 0; f < tris.size(); f++)
+    {
+        float a = 0;
+        for (int i = 0; i < nm; i++)
+            a += surf[f * nm + i] * qdd[i];
+        accs[f] = a;
+    }
+}
+
+bool ModalObject::update_until(float time)
+{
+    bool moved = false;
+    while (current_time < time)
+    {
+        audio_step();
+        moved = moved_;
+    }
+    return moved;
+}
+
+void ModalObject::move_to_first_impulse()
+{
+    if (impulses.empty() || timestep <= 0)
+        return;
+    while (current_time + timestep < impulses[0].time)
+        audio_step();
+}
+
+void ModalObject::submit_acc(float *dst) const { std::copy(accs.begin(), accs.end(), dst); }
+
+BBox ModalObject::bbox() const
+{
+    BBox b;
+    if (translations.empty())
+    {
+        for (auto &p : verts)
+            b.add(p);
+        return b;
+    }
+    // motion frames from the one in force at the first contact on (RigidBody.cu: get_bbox)
+    size_t t = 1;
+    if (!impulses.empty())
+        while (t < frame_time.size() && frame_time[t] < impulses[0].time)
+            t++;
+    t = t > 0 ? t - 1 : 0;
+    for (; t < translations.size(); t++)
+        for (auto &p : standard)
+        {
+            Vec3 r = rotate(rotations[t], p);
+            b.add(Vec3{r[0] + translations[t][0], r[1] + translations[t][1], r[2] + translations[t][2]});
+        }
+    return b;
+}
+
+// the reference's saved state: vertices, modal IIR state, face accelerations, time stamps and time
+// (the list of active impulses is not part of it)
+void ModalObject::save_state()
+{
+    saved.verts = verts;
+    saved.modes = modes;
+    saved.accs = accs;
+    saved.anim_step = anim_step;
+    saved.impulse_step = impulse_step;
+    saved.current_time = current_time;
+}
+
+void ModalObject::load_state()
+{
+    verts = saved.verts;
+    modes = saved.modes;
+    accs = saved.accs;
+    anim_step = saved.anim_step;
+    impulse_step = saved.impulse_step;
+    current_time = saved.current_time;
+}
+
 // ------------------------------------------------------------------ collection -----------
 bool Collection::load(const std::string &root, const SceneConfig &cfg, std::string &err)
 {
@@ -393,9 +776,20 @@ bool Collection::load(const std::string &root, const SceneConfig &cfg, std::stri
             o->name = nit->second;
             objects.push_back(std::move(o));
         }
+        else if (tit->second == "Modal")
+        {
+            // the demo driver builds every Modal object with the "plastic" material
+            // (experiments/demo/main.cu:62-66)
+            auto o = std::make_unique<ModalObject>();
+            if (!o->load(dir, "plastic", err))
+                return false;
+            o->name = nit->second;
+            modal.push_back(o.get());
+            objects.push_back(std::move(o));
+        }
         else
         {
-            err = "unsupported object type: " + tit->second + " (Audio and Manual are supported)";
+            err = "unsupported object type: " + tit->second + " (Audio, Manual and Modal are supported)";
             return false;
         }
     }

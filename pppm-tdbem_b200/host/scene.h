@@ -12,6 +12,17 @@
 //                  motion frames applied when frame time <= t with the unnormalised quaternion
 //                  rotation of Object.cu:6-11, accelerations held per sample, filled into the
 //                  selected triangles.
+//   ModalObject    the reference's RigidBody ("Modal" type, src/utils/RigidBody.h/.cu): a tet mesh
+//                  (vertices.txt, tets.txt) whose boundary faces are the sound surface, rigid
+//                  motion (motion.txt), contact impulses (contact.txt: time vertex nx ny nz |J|)
+//                  and its eigenmodes (eigenvalues.txt, eigenvectors.txt: 3 nv rows, one column
+//                  per mode, modes up to 15 kHz kept).  Each audio sample advances one
+//                  Rayleigh-damped modal IIR per mode (material "plastic", as the demo driver
+//                  uses) driven by the impulses' half-sine contact forces; the surface
+//                  acceleration of a face is its normal . (mean of its vertices' mode shapes)
+//                  times the modal accelerations.  FixMesh (pymesh) is not done.  Boundary faces
+//                  come in the reference's order (the iteration order of its hash map of face
+//                  keys), so the scene's triangle numbering matches.
 //   Collection     objects concatenated into one triangle soup in config order
 //                  (src/utils/ObjectCollection.cu:21-207).
 #pragma once
@@ -105,6 +116,67 @@ class AudioObject : public Object
     } saved;
 };
 
+// material damping of the modal IIR (src/utils/material.h: Rayleigh alpha, beta per material)
+struct Material
+{
+    float alpha = 0, beta = 0;
+    bool set(const std::string &name);
+};
+
+class ModalObject : public Object
+{
+  public:
+    bool load(const std::string &dir, const std::string &material, std::string &err, float max_frequency = 15000.0f);
+    void set_sample_rate(float rate);  // the modal IIR runs at the solver's step rate
+    void move_to_first_impulse();      // audio samples up to the first contact
+    bool update_until(float time) override;
+    void submit_acc(float *dst) const override;
+    BBox bbox() const override;        // over the motion frames from the first contact on
+    void save_state() override;
+    void load_state() override;
+    float current_time = 0;
+    int n_modes() const { return (int)eigen.size(); }
+    const std::vector<float> &surface_acc() const { return accs; }
+
+  private:
+    struct Impulse
+    {
+        float time;
+        int vertex;
+        Vec3 vec;  // normal * magnitude
+    };
+    struct Mode
+    {
+        float c1 = 0, c2 = 0, c3 = 0, f = 0, q1 = 0, q2 = 0, q3 = 0;
+    };
+    void audio_step();
+    void transform(int frame);
+    std::vector<Vec3> standard;
+    std::vector<Vec3> normals;  // per surface face, of the rest shape
+    std::vector<Vec3> translations;
+    std::vector<std::array<float, 4>> rotations;
+    std::vector<float> frame_time;
+    std::vector<Impulse> impulses;
+    std::vector<float> eigen;  // kept eigenvalues
+    std::vector<float> vecs;   // (3 nv) x modes, row-major
+    std::vector<float> surf;   // faces x modes
+    std::vector<Mode> modes;
+    std::vector<float> accs;   // per face
+    std::vector<Impulse> active;
+    Material material;
+    float timestep = 0;
+    int anim_step = 0, impulse_step = 0;
+    bool moved_ = false;  // the last audio sample applied a motion frame
+    struct
+    {
+        std::vector<Vec3> verts;
+        std::vector<Mode> modes;
+        std::vector<float> accs;
+        int anim_step, impulse_step;
+        float current_time;
+    } saved;
+};
+
 class Collection
 {
   public:
@@ -116,6 +188,7 @@ class Collection
     int n_verts() const;
     int n_tris() const;
     std::vector<std::unique_ptr<Object>> objects;
+    std::vector<ModalObject *> modal;  // the Modal objects among them
 };
 
 }  // namespace pppm_host
