@@ -3,22 +3,24 @@
 
 Workload (default, --workload moving): a moving perturbed icosphere (5120 triangles, radius
 0.08 m, translating 0.05 sin(2 pi 3 t) m and rotating 2 rad/s) beside a static 1280-triangle
-plate at res 64, band-limited noise accelerations, motion frames at 1 kHz (69 PPPM steps per
-frame).  One benchmark step = one motion frame: update_mesh (lists + cache refresh) plus the
-69 time steps of that frame.  `value` is device-resident (inputs uploaded before timing);
-`e2e` drives the same frames through the public API from pinned host buffers and reads the
-listener samples back every frame.  --workload static runs the 1280-triangle sphere at
-res 32 without motion (benchmark step = 100 time steps).  --workload large runs two moving
-20480-triangle icospheres at res 128 (2.1 M cells, ~6.2 M face pairs; one benchmark step = one
-1 kHz motion frame of 82 time steps).  --workload batch: 64 independent scenes in one batched
-run (scenes/s); --workload adjoint: the transposed step against the forward step.
+plate at res 64, band-limited noise accelerations, motion frames at 1 kHz: 8820 time steps in
+128 frames.  One benchmark step = that whole run on a fresh handle (set_mesh of frame 0 is the
+untimed set-up; then frame 0's steps and 127 x (update_mesh + the frame's steps)).  `value` is
+device-resident (inputs uploaded before timing); `e2e` drives the same runs through the public
+API from pinned host buffers and reads the listener samples back every frame.  --workload static
+runs the 1280-triangle sphere at res 32 without motion (benchmark step = its whole 2000-step
+run).  --workload large runs two moving 20480-triangle icospheres at res 128 (2.1 M cells, ~6.2 M
+face pairs; one benchmark step = one 1 kHz motion frame of 82 time steps).  --workload batch: 64
+independent scenes in one batched run (scenes/s); --workload adjoint: the transposed step
+against the forward step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU (torchrun): every rank advances its own copy of the scene (replicas, weak
-scaling); value = cells x steps over all ranks / max rank time.  The reference arm runs the
-reference CUDA solver compiled from source (oracle/_ref) on rank 0, or the CPU oracle when
-that build is absent.
+Multi-GPU: with --gpus N > 1 and no torchrun environment the script starts N ranks itself
+(torch.distributed.run on 127.0.0.1).  Every rank advances its own copy of the scene (replicas,
+weak scaling); value = cells x steps over all ranks / max rank time; the batch workload shards
+its scenes over the ranks.  The reference arm runs the reference CUDA solver compiled from
+source (oracle/_ref) on rank 0, or the CPU oracle when that build is absent.
 """
 import argparse
 import json
@@ -45,13 +47,16 @@ CPU_SAMPLE_STEPS = 10
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=60, help="timed benchmark steps (motion frames)")
+    p.add_argument("--steps", type=int, default=10, help="timed benchmark steps (whole runs; frames for large)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint", "large"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64-check", action="store_true")
+    p.add_argument("--profile-frame", type=int, metavar="F",
+                   help="profiling driver: run the workload's frames 0..F-1, then frame F (update_mesh + its "
+                        "steps) inside the NVTX range 'profile_frame', and exit (for ncu --nvtx-include)")
     p.add_argument("--summarize-launches", metavar="CSV",
                    help="print per-kernel launches / total time / share from an ncu "
                         "gpu__time_duration.sum CSV log of this benchmark, and exit")
@@ -115,7 +120,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -146,26 +151,40 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workloads -----------
 class Workload:
-    """Frames of the benchmark: per frame the vertex positions and the step range."""
+    """The scene of a single-scene benchmark and its motion frames.
 
-    def __init__(self, kind, nframes):
+    moving  the whole 8820-step run of the moving sphere + plate (128 motion frames at 1 kHz);
+            one benchmark step = that whole run on a fresh handle: frame 0 after set_mesh, then
+            127 x (update_mesh + the frame's steps)
+    static  the whole 2000-step run of the pulsating sphere; one benchmark step = that run
+    large   two moving 20480-triangle spheres at res 128; one benchmark step = one motion frame
+            (update_mesh + its ~82 steps) of a continuing run (the whole 20000-step run takes
+            seconds per repetition)
+    """
+
+    def __init__(self, kind, nframes=None):
         self.kind = kind
         self.moving = kind in ("moving", "large")
-        if self.moving:
-            sc = scenes.MovingScene() if kind == "moving" else scenes.LargeScene()
-            self.scene = sc
-            self.ranges = scenes.frame_ranges(sc, nframes)
-            self.verts = [sc.frame_verts(f) for f in range(nframes + 1)]
-            self.name = ("moving icosphere (5120 tris) + static plate (1280 tris), res 64, 1 kHz motion frames"
-                         if kind == "moving" else
-                         "two moving icospheres (2 x 20480 tris), res 128, 1 kHz motion frames")
+        self.whole_run = kind in ("moving", "static")
+        if kind == "moving":
+            sc = scenes.MovingScene()
+            self.name = "moving icosphere (5120 tris) + static plate (1280 tris), res 64, 1 kHz motion frames"
+        elif kind == "large":
+            sc = scenes.LargeScene()
+            self.name = "two moving icospheres (2 x 20480 tris), res 128, 1 kHz motion frames"
         else:
             sc = scenes.StaticSphere()
-            self.scene = sc
-            per = 100
-            self.ranges = [(f * per, (f + 1) * per) for f in range(nframes + 1)]
-            self.verts = [sc.verts for _ in range(nframes + 1)]
             self.name = "static icosphere (1280 tris), res 32"
+        self.scene = sc
+        if kind == "moving":
+            n = sc.frame_of_step(sc.steps - 1) + 1
+            self.ranges = scenes.frame_ranges(sc, n - 1)
+            self.ranges[-1] = (self.ranges[-1][0], sc.steps)
+        elif kind == "large":
+            self.ranges = scenes.frame_ranges(sc, nframes)
+        else:
+            self.ranges = [(0, sc.steps)]
+        self.verts = [sc.frame_verts(f) for f in range(len(self.ranges))] if self.moving else [sc.verts]
         self.total_steps = self.ranges[-1][1]
         self.res = sc.res
         self.tris = sc.tris
@@ -174,33 +193,30 @@ class Workload:
 
 
 def algorithmic_bytes(counts, res, nt):
-    """Compulsory bytes per launch of each per-step kernel (FP32 scheme)."""
+    """Compulsory bytes per launch of each step kernel kind (FP32 scheme), by the arrays each
+    reads and writes once: counts = pppm_dump(COUNTS) of the current mesh."""
     m = res - 2
     n3, p3, pf = counts[0], counts[1], counts[4]
-    abc = 6 * m * m
-    stencil = 12 * m ** 3 + 16 * abc + 4 * n3 + 16 * nt  # p^t, p^{t-1}, p^{t+1}; ghosts; corrections; acc -> 4 ring copies
-    # face pairs (weights 64, scale 8, neighbour index 4); per triangle: corners, interpolation
-    # weights, far-field values, start, denominator, 4 Dirichlet copies, its own history windows;
-    # the near-field terms: 54 grid-cache records (64 + scale 8) read, 54 terms written
-    face = pf * (64 + 8 + 4) + nt * (8 * 4 + 8 * 4 + 8 * 4 + 8 + 8 + 16 + 2 * 64) + nt * 54 * (64 + 8 + 4)
-    # per pair: triangle index 4, record offset 1, two terms 8; per cell: index, start, p read/write, next
-    near = p3 * (4 + 1 + 8) + n3 * (4 + 8 + 4 + 4 + 4)
-    return {"stencil": stencil, "face": face, "near": near}
-
-
-def conv_bytes(counts, nt, pairs):
-    """Compulsory bytes of one launch of the face-pair convolution: per pair its weights (64),
-    scale (8) and neighbour index (4); per triangle its list start, its own two history windows
-    (2 x 64) and its output sum(s); the two-step pass also reads the next acceleration row."""
-    pf = counts[4]
-    return pf * (64 + 8 + 4) + nt * (4 + 2 * 64 + (8 + 4 if pairs else 4))
-
-
-def fix_bytes(counts, nt):
-    """Compulsory bytes of the completion of a two-step pass: per pair its tap-1 factor and
-    neighbour index; per triangle its list start, the neighbour value it gathers, the partial sum
-    read and the sum written."""
-    return counts[4] * (4 + 4) + nt * (4 + 4 + 4 + 4)
+    # p^t and p^{t-1} read, p^{t+1} written per cell; the ghost layer of p^t written; the
+    # correction read at corrected cells; the corrected-cell bit mask
+    stencil = 12 * m ** 3 + 4 * 6 * m * m + 4 * n3 + m ** 3 // 8
+    # per pair: weights 64 (16 taps x half2), scale 8, neighbour 4; per triangle: list start 8,
+    # its two history windows 2 x 64 (read once whatever the number of pairs naming it), sum out
+    conv = pf * 76 + nt * (8 + 128 + 4 + 4)
+    conv2 = pf * 76 + nt * (8 + 128 + 4 + 4 + 8)  # + next acceleration row, second sum
+    fix = pf * 8 + nt * 20  # per pair tap-1 factor and neighbour; per triangle start, D, sums
+    # per triangle: 8 corners (interp weight, cell index, far value), conv sum, denominator,
+    # 4 Dirichlet copies + last D, own N and D windows, 54 grid-cache records (64 + 8), 54 terms
+    # written, next Neumann value (4 copies) from the acceleration row
+    corners = 8 * (4 + 4 + 4)
+    finish = nt * (corners + 4 + 8 + 20 + 128 + 54 * 72 + 54 * 4 + 20)
+    finish1 = finish + nt * (54 * 4 + 4)  # + partial terms of the next step
+    finish2 = nt * (corners + 4 + 8 + 20 + 3 * 54 * 4 + 20)  # terms from partials and factors
+    near = p3 * (4 + 1 + 8) + n3 * (4 + 4 + 4 + 4 + 4 + 4)
+    nwrite = nt * 20
+    face = pf * 76 + nt * (8 + 4) + finish
+    return {"stencil": stencil, "conv": conv, "conv2": conv2, "fix": fix, "finish": finish, "finish1": finish1,
+            "finish2": finish2, "near": near, "nwrite": nwrite, "face": face}
 
 
 def load_traffic(workload):
@@ -229,6 +245,21 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def config_of(wl):
+    """The workload's config dict, printed alike by both arms."""
+    sc = wl.scene
+    return {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris)),
+            "time_steps_per_bench_step": wl.total_steps if wl.whole_run else "one motion frame (~%d)" %
+            round(wl.total_steps / len(wl.ranges)),
+            "motion_frames_per_bench_step": len(wl.ranges) if wl.whole_run else 1,
+            "bench_step": ("the whole %d-step run on a fresh handle (set_mesh untimed, then every frame's "
+                           "update_mesh and steps)" % sc.steps) if wl.whole_run and wl.moving else
+                          ("the whole %d-step run on a fresh handle (set_mesh untimed)" % sc.steps)
+                          if wl.whole_run else "one motion frame of a continuing run: update_mesh + its steps",
+            "l2": "flushed (256 MiB write) before each timed benchmark step",
+            "precision": "fp32 grids, fp16+scale weights (the reference's scheme)"}
+
+
 # ---------------------------------------------------------------- our arm -------------
 def run_ours(args, ws, rank, local):
     import torch
@@ -236,7 +267,7 @@ def run_ours(args, ws, rank, local):
     from pppm_b200 import Solver
 
     W, K = args.warmup, args.steps
-    wl = Workload(args.workload, W + K)
+    wl = Workload(args.workload, None if args.workload != "large" else W + K + 1)
     sc = wl.scene
     dev = torch.device("cuda", local)
     # one non-default stream for the solver, the L2 flush and every timing event (with the
@@ -246,166 +277,257 @@ def run_ours(args, ws, rank, local):
     acc_dev = torch.from_numpy(wl.acc).to(dev)
     verts_dev = [torch.from_numpy(v).to(dev) for v in wl.verts]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    nt = len(wl.tris)
+    cells = float(wl.res) ** 3
 
-    s = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
-    s.set_mesh(wl.verts[0], wl.tris)
-    s.add_listener(*wl.listener)
-    # face-stage autotuner on the first frame's mesh (setup, untimed): picks one or two steps per
-    # pass over the face pairs and the block size of the face kernels
-    tune = s.autotune(reps=20)
+    def new_solver(opts=None, precision="fp32", on_stream=True):
+        s = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream if on_stream else None,
+                   precision=precision)
+        for k, v in (opts or {}).items():
+            s.set_option(k, v)
+        s.set_mesh(wl.verts[0], wl.tris)
+        s.add_listener(*wl.listener)
+        return s
 
-    def frame(f, timed_events=None):
+    # face-stage autotuner on the first frame's mesh (set-up, untimed): one or two steps per pass
+    # over the face pairs and over the grid-cache records, block size of the face kernels
+    s0 = new_solver()
+    tune = s0.autotune(reps=20)
+    opts = {"conv_pairs": tune["best"][0], "face_threads": tune["best"][1], "terms_pairs": tune["terms_pairs"]}
+
+    if args.profile_frame is not None:
+        # the frames before the profiled one run as usual; the profiled frame is bracketed by an
+        # NVTX range so that a profiler can take exactly its launches
+        s = new_solver(opts)
+        f_prof = min(args.profile_frame, len(wl.ranges) - 1)
+        for f in range(f_prof):
+            a, b = wl.ranges[f]
+            if f > 0 and wl.moving:
+                s.update_mesh(verts_dev[f])
+            s.step(acc_dev[a:b])
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profile_frame")
+        a, b = wl.ranges[f_prof]
+        if f_prof > 0 and wl.moving:
+            s.update_mesh(verts_dev[f_prof])
+        s.step(acc_dev[a:b])
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        s.close()
+        s0.close()
+        return None
+
+    def frames(s, fr, events=None):
+        for f in fr:
+            a, b = wl.ranges[f]
+            if f > 0 and wl.moving:
+                if events is not None:
+                    events[f][0].record(stream)
+                s.update_mesh(verts_dev[f])
+                if events is not None:
+                    events[f][1].record(stream)
+            s.step(acc_dev[a:b])
+
+    clocks = ClockSampler(local)
+    total_ms = upd_ms = 0.0
+    steps = 0
+    launches = 0
+    series_last = None
+    if wl.whole_run:
+        all_frames = range(len(wl.ranges))
+        for _ in range(W):
+            s = new_solver(opts)
+            frames(s, all_frames)
+            s.close()
+        torch.cuda.synchronize()
+        clocks.start()
+        barrier(ws)
+        for r in range(K):
+            s = new_solver(opts)  # set_mesh of frame 0: the one-off set-up, untimed
+            launches0 = s.launch_count()
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in wl.ranges]
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            frames(s, all_frames, ev)
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            upd_ms += sum(ev[f][0].elapsed_time(ev[f][1]) for f in range(1, len(wl.ranges))) if wl.moving else 0.0
+            steps += wl.total_steps
+            launches += s.launch_count() - launches0
+            if r == K - 1:
+                series_last = s.listeners()[:, 0]
+            s.close()
+        barrier(ws)
+    else:
+        s = s0
+        frames(s, range(0, W + 1))  # frame 0 = the set_mesh frame, then W warm-up frames
+        torch.cuda.synchronize()
+        launches0 = s.launch_count()
+        clocks.start()
+        barrier(ws)
+        for f in range(W + 1, W + K + 1):
+            flush.zero_()
+            e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a, b = wl.ranges[f]
+            e0.record(stream)
+            s.update_mesh(verts_dev[f])
+            em.record(stream)
+            s.step(acc_dev[a:b])
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            upd_ms += e0.elapsed_time(em)
+            steps += b - a
+        barrier(ws)
+        launches = s.launch_count() - launches0
+    clk = clocks.stop()
+    t_max = max_over_ranks(ws, total_ms)
+    value = cells * steps * ws / (t_max * 1e-3) / 1e9
+    n_upd = K * (len(wl.ranges) - 1) if wl.whole_run else K
+    us_update = upd_ms * 1e3 / max(n_upd, 1)
+    us_per_step = (total_ms - upd_ms) * 1e3 / steps
+
+    # per-kernel durations (measurement mode: the recorded graphs' kernels serialised with an event
+    # between consecutive kernels) over the same frames as one timed benchmark step, with the
+    # algorithmic bytes of each launch from the mesh counts of its frame
+    sp = new_solver(opts) if wl.whole_run else s0
+    sp.enable_timing(True)
+    kind_bytes = {}
+    prof_frames = range(len(wl.ranges)) if wl.whole_run else range(W + K + 1, W + K + 2)
+    prev = {}
+    for f in prof_frames:
         a, b = wl.ranges[f]
         if f > 0 and wl.moving:
-            s.update_mesh(verts_dev[f])
-        s.step(acc_dev[a:b])
-
-    for f in range(0, W + 1):  # frame 0 = the set_mesh frame, then W warm-up frames
-        frame(f)
-    torch.cuda.synchronize()
-    launches0 = s.launch_count()
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier(ws)
-    total_ms = 0.0
-    step_ms = 0.0
-    steps = 0
-    for f in range(W + 1, W + K + 1):
-        flush.zero_()
-        e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        a, b = wl.ranges[f]
-        e0.record(stream)
-        if wl.moving:
-            s.update_mesh(verts_dev[f])
-        em.record(stream)
-        s.step(acc_dev[a:b])
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        step_ms += em.elapsed_time(e1)
-        steps += b - a
-    barrier(ws)
-    clk = clocks.stop()
-    launches = s.launch_count() - launches0
-    t_max = max_over_ranks(ws, total_ms)
-    cells = float(wl.res) ** 3
-    value = cells * steps * ws / (t_max * 1e-3) / 1e9
-
-    # per-kernel durations (measurement mode: events around each kernel, synchronised)
-    s.enable_timing(True)
-    a, b = wl.ranges[W + K]
-    s.step(acc_dev[a:b])
-    us_st, us_face, us_near, nt_timed = s.kernel_times()
-    s.enable_timing(False)
-    counts = [int(x) for x in s.dump("counts")]
-    alg = {k: int(v) for k, v in algorithmic_bytes(counts, wl.res, len(wl.tris)).items()}
-    times = {"stencil": us_st, "face": us_face, "near": us_near}
-    # the dominant kernel of the recorded steps: the tuned face-pair convolution (its launch time
-    # from the autotuner's events on the solver's stream, last frame's mesh: re-tuned here)
-    tune = s.autotune(reps=20)
-    pairs, threads = tune["best"]
-    nt = len(wl.tris)
-    top = "conv2" if pairs else "conv"
-    top_us = tune["launch_us"][tune["best"]][0]
-    top_bytes = conv_bytes(counts, nt, pairs)
+            sp.update_mesh(verts_dev[f])
+        counts = [int(x) for x in sp.dump("counts")]
+        sp.step(acc_dev[a:b])
+        prof = sp.kernel_profile()
+        alg = algorithmic_bytes(counts, wl.res, nt)
+        for k, (us, n) in prof.items():
+            dn = n - prev.get(k, 0)
+            kind_bytes[k] = kind_bytes.get(k, 0.0) + dn * alg[k]
+            prev[k] = n
+    prof = sp.kernel_profile()
+    sp.enable_timing(False)
+    counts_last = [int(x) for x in sp.dump("counts")]
+    if wl.whole_run:
+        sp.close()
     peak, peak_kind = measured_peak()
-    achieved = float(top_bytes / (top_us * 1e-6) / 1e9)
+    # event-to-event times inside a graph carry the event nodes' own cost: the empty kernel of the
+    # profile graph measures that floor, which is taken off every kind's mean
+    floor = prof.pop("empty", (0.0, 0))[0]
+    corr = {k: (max(us - floor, 0.05), n) for k, (us, n) in prof.items()}
+    total_us = sum(us * n for us, n in corr.values())
+    kernels = {}
+    for k, (us, n) in sorted(corr.items(), key=lambda kv: -kv[1][0] * kv[1][1]):
+        b = kind_bytes.get(k, 0.0) / n
+        kernels[k] = {"launches": n, "us_per_launch": round(us, 3), "us_event_to_event": round(prof[k][0], 3),
+                      "share": round(us * n / total_us, 4),
+                      "algorithmic_bytes_per_launch": int(b), "gb_per_s": round(b / (us * 1e-6) / 1e9, 1),
+                      "frac": round(b / (us * 1e-6) / 1e9 / peak, 4)}
+    top = next(iter(kernels))
+    prof = corr
     traffic = load_traffic(args.workload).get(top)
-    # split of a timed frame: update_mesh, then the frame's time steps (one recorded graph)
-    us_update = (total_ms - step_ms) * 1e3 / K
-    us_per_step = step_ms * 1e3 / steps
+    main_path = [k for k in ("stencil", "finish", "finish1", "finish2", "near") if k in kernels]
+    path_bytes = sum(kind_bytes.get(k, 0.0) for k in main_path)
+    path_us = sum(prof[k][0] * prof[k][1] for k in main_path)
 
-    # end-to-end through the public API from pinned host buffers
+    # end-to-end through the public API from pinned host buffers: vertices and accelerations
+    # copied in and the listener samples read back every frame
     e2e = None
     if not args.no_e2e:
-        s2 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
-        s2.set_option("conv_pairs", pairs)
-        s2.set_option("face_threads", threads)
-        s2.set_option("terms_pairs", tune["terms_pairs"])
-        s2.set_mesh(wl.verts[0], wl.tris)
-        s2.add_listener(*wl.listener)
         acc_pin = torch.from_numpy(wl.acc).pin_memory()
         verts_pin = [torch.from_numpy(v).pin_memory() for v in wl.verts]
-        out_pin = torch.empty((200,), dtype=torch.float32).pin_memory()
-        h2d = d2h = 0
-        for f in range(0, W + 1):
-            a, b = wl.ranges[f]
-            if f > 0 and wl.moving:
-                s2.update_mesh(verts_pin[f])
-            s2.step(acc_pin[a:b])
-        barrier(ws)
-        t0 = time.perf_counter()
-        steps2 = 0
-        for f in range(W + 1, W + K + 1):
-            a, b = wl.ranges[f]
-            if wl.moving:
-                s2.update_mesh(verts_pin[f])
-                h2d += verts_pin[f].numel() * 4
-            s2.step(acc_pin[a:b])
-            h2d += (b - a) * len(wl.tris) * 4
-            done = s2.listeners(first=a, count=b - a)
-            d2h += done.nbytes
-            steps2 += b - a
-        torch.cuda.synchronize()
-        te = max_over_ranks(ws, time.perf_counter() - t0)
-        e2e = {"value": cells * steps2 * ws / te / 1e9, "unit": "Gcell-steps/s",
+
+        def run_e2e(s, fr):
+            h2d = d2h = n = 0
+            for f in fr:
+                a, b = wl.ranges[f]
+                if f > 0 and wl.moving:
+                    s.update_mesh(verts_pin[f])
+                    h2d += verts_pin[f].numel() * 4
+                s.step(acc_pin[a:b])
+                h2d += (b - a) * nt * 4
+                d2h += s.listeners(first=a, count=b - a).nbytes
+                n += b - a
+            return h2d, d2h, n
+
+        te, h2d, d2h, steps2 = 0.0, 0, 0, 0
+        if wl.whole_run:
+            for r in range(W + K):
+                s2 = new_solver(opts)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                x = run_e2e(s2, range(len(wl.ranges)))
+                torch.cuda.synchronize()
+                if r >= W:
+                    te += time.perf_counter() - t0
+                    h2d, d2h, steps2 = h2d + x[0], d2h + x[1], steps2 + x[2]
+                s2.close()
+        else:
+            s2 = new_solver(opts)
+            run_e2e(s2, range(0, W + 1))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h2d, d2h, steps2 = run_e2e(s2, range(W + 1, W + K + 1))
+            torch.cuda.synchronize()
+            te = time.perf_counter() - t0
+            s2.close()
+        te = max_over_ranks(ws, te)
+        e2e = {"value": round(cells * steps2 * ws / te / 1e9, 4), "unit": "Gcell-steps/s",
                "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K}
-        s2.close()
-        del out_pin
 
     # error of the timed FP32 run against the FP64 scheme of the same library on the GPU, over the
-    # same frames (set-up and warm-up frames included; outside the timed region)
+    # same steps (outside the timed region)
     fp64_err = None
     if not args.no_fp64_check:
-        n = wl.ranges[W + K][1]
-        got = s.listeners(0, n)[:, 0].astype(np.float64)
-        s64 = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream, precision="fp64")
-        s64.set_mesh(wl.verts[0], wl.tris)
-        s64.add_listener(*wl.listener)
-        for f in range(0, W + K + 1):
-            a, b = wl.ranges[f]
-            if f > 0 and wl.moving:
-                s64.update_mesh(verts_dev[f])
-            s64.step(acc_dev[a:b])
-        ref = s64.listeners(0, n)[:, 0].astype(np.float64)
+        if wl.whole_run:
+            got = series_last.astype(np.float64)
+            fr = range(len(wl.ranges))
+        else:
+            got = s0.listeners(0, wl.ranges[W + K + 1][1])[:, 0].astype(np.float64)
+            fr = range(0, W + K + 2)
+        s64 = new_solver(precision="fp64")
+        frames(s64, fr)
+        ref = s64.listeners(0, len(got))[:, 0].astype(np.float64)
         s64.close()
         den = float(np.linalg.norm(ref))
-        fp64_err = {"rel_l2": float(np.linalg.norm(got - ref) / den) if den > 0 else None, "time_steps": int(n),
-                    "reference": "the same frames in the FP64 scheme (PPPM_PRECISION_FP64) on the GPU"}
+        fp64_err = {"rel_l2": float(np.linalg.norm(got - ref) / den) if den > 0 else None, "time_steps": int(len(got)),
+                    "reference": "the same steps in the FP64 scheme (PPPM_PRECISION_FP64) on the GPU"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl)
 
-    s.close()
+    s0.close()
+    cfg = config_of(wl)
+    cfg.update({"parallelism": "replicas x%d" % ws, "n3_cells": int(counts_last[0]),
+                "pairs_3x3x3": int(counts_last[1]), "face_pairs": int(counts_last[4])})
     line = {
         "metric": "Gcell-steps/s, %s (time step + motion-frame refresh)" % wl.name,
         "value": round(value, 4), "unit": "Gcell-steps/s", "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": round(t_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded meshes, trajectories and accelerations)",
-        "config": {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris)),
-                   "time_steps_per_bench_step": round(steps / K, 2), "time_steps_timed": steps,
-                   "bench_step": "one motion frame: update_mesh + its time steps" if wl.moving
-                   else "100 time steps", "l2": "flushed (256 MiB write) between timed iterations",
-                   "parallelism": "replicas x%d" % ws, "precision": "fp32 grids, fp16+scale weights",
-                   "n3_cells": int(counts[0]), "pairs_3x3x3": int(counts[1]), "face_pairs": int(counts[4])},
-        "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes": int(top_bytes), "kernel_launch_us": round(top_us, 3),
-                     "autotune": {"best": {"two_steps_per_pass": bool(pairs), "threads": threads,
-                                           "terms_two_steps_per_pass": bool(tune["terms_pairs"])},
-                                  "decided_by": "64 recorded steps per option set (phase 2)",
-                                  "finish_us_per_two_steps": {k: round(v, 2) for k, v in tune["finish_us"].items()},
+        "dtype": "f32", "data": "synthetic (seeded meshes, trajectories and accelerations)", "config": cfg,
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": kernels[top]["gb_per_s"], "peak": peak,
+                     "unit": "GB/s", "frac": kernels[top]["frac"], "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes": kernels[top]["algorithmic_bytes_per_launch"],
+                     "kernel_launch_us": kernels[top]["us_per_launch"],
+                     "how": "kernel with the largest share of measurement-mode time over one benchmark step's "
+                            "frames (the recorded graphs' kernels serialised, events between them); achieved = "
+                            "its algorithmic bytes per launch / its mean event-to-event time less that of an "
+                            "empty kernel in the same graph (%.2f us)" % floor,
+                     "kernels": kernels,
+                     "main_path": {"kernels": main_path, "achieved": round(path_bytes / (path_us * 1e-6) / 1e9, 1),
+                                   "frac": round(path_bytes / (path_us * 1e-6) / 1e9 / peak, 4)},
+                     "autotune": {"best": {"two_steps_per_pass": bool(opts["conv_pairs"]),
+                                           "threads": opts["face_threads"],
+                                           "terms_two_steps_per_pass": bool(opts["terms_pairs"])},
                                   "step_us_by_config": {"%s/%d/%s" % (("single", "pairs")[p], t,
                                                                       "terms2" if m else "terms1"): round(u, 2)
-                                                        for (p, t, m), u in (tune["step_us"] or {}).items()},
-                                  "us_per_two_steps": {"%s/%d" % (("single", "pairs")[p], t): round(u, 2)
-                                                       for (p, t), u in tune["us"].items()}},
-                     "fix_us": round(tune["launch_us"][tune["best"]][1], 3) if pairs else None,
-                     "fix_bytes": int(fix_bytes(counts, nt)) if pairs else None,
-                     "kernel_us_measurement_mode": {k: round(v, 3) for k, v in times.items()},
-                     "update_mesh_us": round(us_update, 1), "time_step_us": round(us_per_step, 2),
-                     "gb_per_s_all_kernels": round(sum(alg.values()) / (sum(times.values()) * 1e-6) / 1e9, 1)},
+                                                        for (p, t, m), u in (tune["step_us"] or {}).items()}},
+                     "update_mesh_us": round(us_update, 1), "time_step_us": round(us_per_step, 2)},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
         "error_vs_fp64": fp64_err,
     }
@@ -512,7 +634,8 @@ def run_batch(args, ws, rank, local):
     job_bytes = 0.0
     for sp, s in zip(specs, solvers):
         counts = [int(x) for x in s.dump("counts")]
-        job_bytes += sum(algorithmic_bytes(counts, sp["res"], len(sp["tris"])).values()) * sp["steps"]
+        alg = algorithmic_bytes(counts, sp["res"], len(sp["tris"]))
+        job_bytes += (alg["stencil"] + alg["face"] + alg["near"]) * sp["steps"]
     gather_ms, gathered = 0.0, len(specs)
     if ws > 1:
         import torch.distributed as dist
@@ -691,36 +814,64 @@ def cpu_batch_baseline(specs, sample=4, steps=20):
                       "with OpenMP)" % (sample, steps)}
 
 
-def cpu_baseline(wl):
-    """The CPU restatement (oracle/) on the host cores: one benchmark step of the same
-    workload (set_mesh untimed)."""
+def cpu_baseline(wl, budget_s=10.0):
+    """The CPU restatement (oracle/) on the host cores over a bounded sample of the same workload
+    (set_mesh untimed): motion frames from frame 1 on (update_mesh + the frame's steps) until about
+    budget_s seconds have passed; the static run in chunks of 100 steps likewise; the large scene's
+    first frame with its steps sampled (a whole frame takes about a minute on the host)."""
     from oracle.oracle import Oracle, oracle_threads
 
     sc = wl.scene
     o = Oracle(wl.res, sc.h, sc.dt, sc.min_pos)
     o.set_mesh(wl.verts[0], wl.tris)
-    f = 1
-    a, b = wl.ranges[f]
-    # the large scene's frame takes about a minute on the host: time update_mesh and the first
-    # CPU_SAMPLE_STEPS of its steps, and extrapolate the steps to the whole frame
-    n = b - a if wl.kind != "large" else min(b - a, CPU_SAMPLE_STEPS)
-    t0 = time.perf_counter()
-    if wl.moving:
-        o.update_mesh(wl.verts[f])
-    t1 = time.perf_counter()
-    o.step(wl.acc[a:a + n], listeners=[wl.listener])
-    t2 = time.perf_counter()
+    elapsed, steps, nframes = 0.0, 0, 0
+    if wl.kind == "large":
+        a, b = wl.ranges[1]
+        n = min(b - a, CPU_SAMPLE_STEPS)
+        t0 = time.perf_counter()
+        o.update_mesh(wl.verts[1])
+        t1 = time.perf_counter()
+        o.step(wl.acc[a:a + n], listeners=[wl.listener])
+        t2 = time.perf_counter()
+        elapsed, steps = (t1 - t0) + (t2 - t1) * (b - a) / n, b - a
+        sample = ("frame 1 of the same workload: update_mesh and the first %d of its %d time steps timed, the "
+                  "steps extrapolated to the frame; C restatement with OpenMP" % (n, b - a))
+    elif wl.moving:
+        for f in range(1, len(wl.ranges)):
+            a, b = wl.ranges[f]
+            t0 = time.perf_counter()
+            o.update_mesh(wl.verts[f])
+            o.step(wl.acc[a:b], listeners=[wl.listener])
+            elapsed += time.perf_counter() - t0
+            steps += b - a
+            nframes += 1
+            if elapsed >= budget_s:
+                break
+        sample = ("motion frames 1-%d of the same run (update_mesh + %d time steps), C restatement with "
+                  "OpenMP" % (nframes, steps))
+    else:
+        while steps < wl.total_steps and elapsed < budget_s:
+            n = min(100, wl.total_steps - steps)
+            t0 = time.perf_counter()
+            o.step(wl.acc[steps:steps + n], listeners=[wl.listener])
+            elapsed += time.perf_counter() - t0
+            steps += n
+        sample = "the first %d time steps of the same run, C restatement with OpenMP" % steps
     o.close()
-    dt = (t1 - t0) + (t2 - t1) * (b - a) / n
-    sample = "one benchmark step (%d time steps%s) of the same workload, C restatement with OpenMP" % (
-        b - a, " + update_mesh" if wl.moving else "")
-    if n < b - a:
-        sample += "; update_mesh and the first %d time steps timed, the steps extrapolated to %d" % (n, b - a)
-    return {"value": round(float(wl.res) ** 3 * (b - a) / dt / 1e9, 5), "unit": "Gcell-steps/s",
+    return {"value": round(float(wl.res) ** 3 * steps / elapsed / 1e9, 5), "unit": "Gcell-steps/s",
             "cores": oracle_threads(), "kind": "port", "sample": sample}
 
 
 # ---------------------------------------------------------------- reference arm -------
+def own_library_mapped():
+    """Paths of this repository's native library mapped into this process (must be none in the
+    reference arm)."""
+    try:
+        return sorted({line.split()[-1] for line in open("/proc/self/maps") if "libpppm_b200" in line})
+    except OSError:
+        return []
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
@@ -730,7 +881,7 @@ def run_reference(args, ws, rank, local):
     if args.workload == "adjoint":
         return {"impl": "reference", "metric": "adjoint / forward cost, %s" % ADJ_NAME,
                 "unavailable": "the reference has no adjoint"}
-    wl = Workload(args.workload, W + K)
+    wl = Workload(args.workload, None if args.workload != "large" else W + K + 1)
     sc = wl.scene
     from oracle import oracle as O
 
@@ -742,40 +893,60 @@ def run_reference(args, ws, rank, local):
         nt = len(wl.tris)
         ptr0 = acc_dev.data_ptr()
 
-        def timed_run(nd):
-            """W warm-up and K timed frames of the reference build (nd: the -DNDEBUG build)."""
+        def new_ref(nd):
             r = O.Reference(wl.res, sc.h, sc.dt, sc.min_pos, ndebug=nd)
             r.set_mesh(wl.verts[0], wl.tris)
+            return r
+
+        def frame(r, f):
+            a, b = wl.ranges[f]
+            if f > 0 and wl.moving:
+                r.update_mesh(wl.verts[f])
+            r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
+            return b - a
+
+        def timed_run(nd, W=W, K=K):
+            """W warm-up and K timed benchmark steps of the reference build (nd: the -DNDEBUG
+            build); whole-run workloads on a fresh solver per benchmark step (set_mesh untimed)."""
             if wl.moving:
+                r = new_ref(nd)
                 for v in wl.verts[1:]:
                     r.check_mesh(v)  # validate the whole trajectory against the reference capacities
+                r.close()
+            dt, steps = 0.0, 0
+            if wl.whole_run:
+                for i in range(W + K):
+                    r = new_ref(nd)
+                    r.set_checks(False)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    n = sum(frame(r, f) for f in range(len(wl.ranges)))
+                    torch.cuda.synchronize()
+                    if i >= W:
+                        dt += time.perf_counter() - t0
+                        steps += n
+                    r.close()
+            else:
+                r = new_ref(nd)
                 r.set_checks(False)
-
-            def frame(f):
-                a, b = wl.ranges[f]
-                if f > 0 and wl.moving:
-                    r.update_mesh(wl.verts[f])
-                r.run_device(ptr0 + a * nt * 4, b - a, wl.listener)
-
-            for f in range(0, W + 1):
-                frame(f)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            steps = 0
-            for f in range(W + 1, W + K + 1):
-                frame(f)
-                steps += wl.ranges[f][1] - wl.ranges[f][0]
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            r.close()
+                for f in range(0, W + 1):
+                    frame(r, f)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                steps = sum(frame(r, f) for f in range(W + 1, W + K + 1))
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                r.close()
             return float(wl.res) ** 3 * steps / dt / 1e9
 
         value = timed_run(False)
         if O.reference_available(ndebug=True):
-            ndebug = {"value": round(timed_run(True), 5), "unit": "Gcell-steps/s",
+            nd_k = min(K, 5)
+            ndebug = {"value": round(timed_run(True, 1, nd_k), 5), "unit": "Gcell-steps/s", "steps": nd_k,
                       "build": "the same reference sources built with -DNDEBUG (no device sync after every launch)"}
-        kind, cores, sample = "reference", 0, ("reference CUDA solver built from source (oracle/_ref, upstream flags: "
-                                                "device sync after every launch), %d frames" % K)
+        kind, cores, sample = "reference", 1, ("reference CUDA solver built from source (oracle/_ref, upstream "
+                                               "flags: device sync after every launch) driven by one host thread, "
+                                               "%d benchmark steps" % K)
     else:
         from oracle.oracle import Oracle, oracle_threads
 
@@ -783,7 +954,7 @@ def run_reference(args, ws, rank, local):
         o.set_mesh(wl.verts[0], wl.tris)
         t0 = time.perf_counter()
         steps = 0
-        for f in range(1, min(W + K, 3) + 1):
+        for f in range(1, min(len(wl.ranges) - 1, 3) + 1):
             a, b = wl.ranges[f]
             if wl.moving:
                 o.update_mesh(wl.verts[f])
@@ -791,17 +962,21 @@ def run_reference(args, ws, rank, local):
             steps += b - a
         dt = time.perf_counter() - t0
         value = float(wl.res) ** 3 * steps / dt / 1e9
-        kind, cores, sample = "port", oracle_threads(), "CPU restatement, %d frames" % min(W + K, 3)
+        kind, cores, sample = "port", oracle_threads(), "CPU restatement, motion frames 1-3"
+    mapped = own_library_mapped()
+    if mapped:
+        raise RuntimeError("reference arm has this repository's library mapped: %s" % mapped)
+    cfg = config_of(wl)
+    cfg["parallelism"] = "one GPU (rank 0)"
     return {"impl": "reference", "metric": "Gcell-steps/s, %s (time step + motion-frame refresh)" % wl.name,
-            "value": round(value, 5), "unit": "Gcell-steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "value": round(value, 5), "unit": "Gcell-steps/s", "n_gpus": ws, "steps": K, "warmup": W,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded meshes, trajectories and accelerations)",
-            "config": {"workload": wl.name, "res": wl.res, "triangles": int(len(wl.tris))},
+            "data": "synthetic (seeded meshes, trajectories and accelerations)", "config": cfg,
             "cpu_baseline": {"value": round(value, 5), "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(value, 5), "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "reference_ndebug": ndebug}
+            "reference_ndebug": ndebug, "native_libraries_of_this_repo_mapped": mapped}
 
 
 def run_reference_batch(args):
@@ -837,6 +1012,9 @@ def run_reference_batch(args):
         line["unavailable"] = "reference solver rejected a batch scene: %s" % e
         return line
     value = BATCH_SCENES / total
+    mapped = own_library_mapped()
+    if mapped:
+        raise RuntimeError("reference arm has this repository's library mapped: %s" % mapped)
     line.update({"value": round(value, 4), "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True,
                  "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                  "data": "synthetic (seeded meshes and accelerations)",
@@ -871,12 +1049,29 @@ def summarize_launches(path):
         print("| %s | %d | %.1f | %.2f | %.1f%% |" % (name, n, t, t / n, 100 * t / total))
 
 
+def relaunch_under_torchrun(n):
+    """bench.py --gpus N outside torchrun: start N ranks of this same command on this node and
+    return their exit status (rank 0 prints the line)."""
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
     if args.summarize_launches:
         summarize_launches(args.summarize_launches)
         return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_under_torchrun(args.gpus))
     ws, rank, local = dist_setup()
+    if ws != args.gpus and rank == 0:
+        print("warning: --gpus %d but %d ranks" % (args.gpus, ws), file=sys.stderr)
     if args.impl == "reference":
         line = run_reference(args, ws, rank, local)
     elif args.workload == "batch":
@@ -887,6 +1082,8 @@ def main():
         line = run_ours(args, ws, rank, local)
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
+    elif args.profile_frame is not None and rank == 0:
+        print("profiled frame %d" % args.profile_frame, flush=True)
     if ws > 1:
         import torch.distributed as dist
 

@@ -92,8 +92,17 @@ int pppm_update_mesh(pppm_handle *h, const float *verts, int verts_on_device);
 /* Replaces nsteps calls of PPPMSolver::update_grid_and_face(acc) (pppm.h:138-145).
  * acc holds nsteps rows of nt per-triangle normal accelerations (row s drives step s);
  * acc_on_device != 0: acc is a device pointer.  Listener values are recorded on the device
- * after every step (the demo's per-step read, experiments/demo/main.cu:266). */
+ * after every step (the demo's per-step read, experiments/demo/main.cu:266).  The call returns
+ * once the steps are queued.  The step kernels raise a device status bit when a Dirichlet value
+ * or a listener sample is not finite (the reference aborts on a NaN listener sample,
+ * experiments/demo/main.cu:161-168); a copy of that word is queued behind the steps, and a later
+ * pppm_step whose predecessors' copy has arrived returns PPPM_ERR_NAN without queuing anything,
+ * until pppm_reset_fields or pppm_restore_state clears it. */
 int pppm_step(pppm_handle *h, const float *acc, int acc_on_device, int nsteps);
+
+/* No counterpart in the reference.  Waits for the handle's queued work and returns its step
+ * status: PPPM_ERR_NAN once a non-finite Dirichlet value or listener sample appeared. */
+int pppm_sync(pppm_handle *h);
 
 /* Listener cells (experiments/demo/main.cu:148: int3(checkCoord * res)). */
 int pppm_add_listener(pppm_handle *h, int x, int y, int z);
@@ -214,15 +223,20 @@ int pppm_adjoint(pppm_handle *h, const void *dL_dsignal, int nsteps, int on_devi
 int pppm_tdbem_constants(float dt, float dl, float c, float *lambda, float *wave32);
 /* TDBEM::laplace_weight (bem.h:306-330) of one pair evaluated on device `device` with the
  * FP32 weight arithmetic of the caches: src triangle (indices into verts) onto a point
- * (to_point != 0) or onto dst_face.  out32: 16 single-layer then 16 double-layer taps. */
+ * (to_point != 0) or onto dst_face.  out32: 16 single-layer then 16 double-layer taps.  The
+ * calling thread's current device is restored before the call returns. */
 int pppm_pair_weights(int device, float dt, float dl, float c, const float *verts, int nv, const int *src,
                       int to_point, const int *dst_face, const float *dst_point, float *out32);
 /* No counterpart in the reference.  pppm_pair_weights without any device allocation, for
  * callers that cannot allocate: a thread working beside a handle that is stepping on the same
  * device (cudaMalloc / cudaFree may synchronise the whole device and stall that handle's stream)
  * or a process whose device memory is already held by another allocator.  Same arguments and
- * result as pppm_pair_weights, plus the stream the copies and the kernel run on (NULL: the
- * default stream); returns after out32 is written.  The vertex rows are staged in a static
+ * result as pppm_pair_weights, plus the stream the copies and the kernel run on; returns after
+ * out32 is written.  NULL means the legacy default stream, which waits for every blocking stream
+ * on the device (a handle's stepping stream included, unless it was created non-blocking): pass a
+ * stream created with cudaStreamNonBlocking to work beside queued steps.  A stream that is being
+ * captured returns PPPM_ERR_STATE (the call synchronises its stream).  The calling thread's
+ * current device is restored before the call returns.  The vertex rows are staged in a static
  * device array of PPPM_STATIC_MAX_VERTS rows (768 KiB) inside the library; nv above that limit
  * returns PPPM_ERR_CAPACITY.  Nothing in that array has to start at zero: each call copies its
  * rows in and the kernel writes all 32 taps.  The first call on a device does one-time setup
@@ -273,6 +287,27 @@ int pppm_launch_count(pppm_handle *h, long long *count);
  * microseconds over the steps timed since pppm_enable_timing, and their number. */
 int pppm_enable_timing(pppm_handle *h, int enable);
 int pppm_kernel_times(pppm_handle *h, float *us_stencil, float *us_face, float *us_near, int *timed_steps);
+/* No counterpart in the reference.  Measurement mode per kernel: where the recorded step graphs
+ * run the split face stage (absorbing boundary, PPPM method, mesh set), steps in measurement mode
+ * go in groups of four through a recorded graph of exactly those kernels (Neumann write, then per
+ * step the face-pair convolution, the stencil, finish, near), serialised on the handle's stream
+ * with an event between consecutive kernels; remaining steps and other handles time the fused
+ * kernels.  Per kind: us_per_launch[k] = mean event-to-event time of its launches, launches[k]
+ * their number (both arrays of nkinds entries, nkinds <= PPPM_KERNEL_KINDS). */
+#define PPPM_KERNEL_STENCIL 0 /* FDTD / absorbing-boundary stencil (or the PML stencil)       */
+#define PPPM_KERNEL_CONV 1    /* face-pair convolution, one step per pass                    */
+#define PPPM_KERNEL_CONV2 2   /* face-pair convolution, two steps per pass                   */
+#define PPPM_KERNEL_FIX 3     /* completion of the second step of a two-step pass            */
+#define PPPM_KERNEL_FINISH 4  /* far field, Dirichlet update, near-field terms in one pass    */
+#define PPPM_KERNEL_FINISH1 5 /* ... first step of a two-step pass over the grid-cache records */
+#define PPPM_KERNEL_FINISH2 6 /* ... second step (completion of its terms)                    */
+#define PPPM_KERNEL_NEAR 7    /* corrected cells: sums of the near-field terms                */
+#define PPPM_KERNEL_NWRITE 8  /* Neumann history write of a call's first step                 */
+#define PPPM_KERNEL_FACE 9    /* the fused face stage of direct launches                      */
+#define PPPM_KERNEL_EMPTY 10  /* an empty one-block kernel between the Neumann write and the first
+                                 convolution: the event-to-event floor of this measurement      */
+#define PPPM_KERNEL_KINDS 11
+int pppm_kernel_profile(pppm_handle *h, int nkinds, float *us_per_launch, long long *launches);
 
 #ifdef __cplusplus
 }

@@ -216,6 +216,57 @@ int d2h(Handle &h, std::vector<T> &v, const void *src, size_t n)
 
 extern "C" {
 
+// The step status of the calls whose copy has arrived: PPPM_ERR_NAN once a step kernel saw a
+// non-finite Dirichlet value or listener sample.  wait: block until the last copy has arrived.
+static int poll_step_status(Handle &h, bool wait)
+{
+    if (h.status_pending)
+    {
+        cudaError_t e = wait ? cudaEventSynchronize(h.ev_status) : cudaEventQuery(h.ev_status);
+        if (e == cudaSuccess)
+        {
+            h.status_pending = false;
+            if (*h.h_step_status & 1)
+                h.nonfinite = true;
+        }
+        else if (e != cudaErrorNotReady)
+            PB_CUDA(e);
+    }
+    if (h.nonfinite)
+    {
+        set_error("a non-finite Dirichlet value or listener sample appeared in an earlier step (reset the fields or "
+                  "restore a saved state to go on)");
+        return PPPM_ERR_NAN;
+    }
+    return PPPM_OK;
+}
+
+// queue a copy of the step status word behind the work on the handle's stream (not while the
+// caller captures the stream: the copy would become part of the graph)
+static int queue_step_status(Handle &h)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PB_CUDA(cudaStreamIsCapturing(h.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        return PPPM_OK;
+    PB_CUDA(cudaMemcpyAsync(h.h_step_status, h.d_step_status, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    PB_CUDA(cudaEventRecord(h.ev_status, h.stream));
+    h.status_pending = true;
+    return PPPM_OK;
+}
+
+// forget a non-finite flag: the fields it concerned are being replaced
+static int clear_step_status(Handle &h)
+{
+    if (h.status_pending)
+        PB_CUDA(cudaEventSynchronize(h.ev_status));
+    h.status_pending = false;
+    h.nonfinite = false;
+    *h.h_step_status = 0;
+    PB_CUDA(cudaMemsetAsync(h.d_step_status, 0, sizeof(int), h.stream));
+    return PPPM_OK;
+}
+
 int pppm_params_default(pppm_params *p)
 {
     if (!p)
@@ -309,6 +360,22 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
     }
     for (int i = 0; i < 4; i++)
         cudaEventCreate(&h.ev[i]);
+    for (auto &e : h.evk)
+        cudaEventCreate(&e);
+    {
+        int rc = dalloc(&h.d_step_status, 1);
+        if (rc)
+            return fail(rc);
+        cudaMemsetAsync(h.d_step_status, 0, sizeof(int), h.stream);
+        if (cudaMallocHost((void **)&h.h_step_status, sizeof(int)) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h.ev_status, cudaEventDisableTiming) != cudaSuccess)
+        {
+            h.h_step_status = nullptr;
+            set_error("cudaMallocHost / cudaEventCreate failed");
+            return fail(PPPM_ERR_NOMEM);
+        }
+        *h.h_step_status = 0;
+    }
     if (cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h.ev_fin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h.ev_conv, cudaEventDisableTiming) != cudaSuccess)
@@ -357,6 +424,14 @@ int pppm_destroy(pppm_handle *ph)
     for (int i = 0; i < 4; i++)
         if (h.ev[i])
             cudaEventDestroy(h.ev[i]);
+    for (auto &e : h.evk)
+        if (e)
+            cudaEventDestroy(e);
+    dev_free(h.d_step_status);
+    if (h.h_step_status)
+        cudaFreeHost(h.h_step_status);
+    if (h.ev_status)
+        cudaEventDestroy(h.ev_status);
     if (h.h_pin)
         cudaFreeHost(h.h_pin);
     if (h.ev_fin)
@@ -495,6 +570,7 @@ int pppm_step(pppm_handle *ph, const float *acc, int acc_on_device, int nsteps)
         return PPPM_ERR_ARG;
     }
     cudaSetDevice(h.prm.device);
+    PB_TRY(poll_step_status(h, false));
     const float *dacc = nullptr;
     if (h.mesh_set)
     {
@@ -515,7 +591,20 @@ int pppm_step(pppm_handle *ph, const float *acc, int acc_on_device, int nsteps)
         }
     }
     PB_TRY(ensure_series(h, nsteps));
-    return step_run(h, dacc, nsteps);
+    PB_TRY(step_run(h, dacc, nsteps));
+    return queue_step_status(h);
+}
+
+int pppm_sync(pppm_handle *ph)
+{
+    PB_TRY(check_handle(ph));
+    Handle &h = ph->h;
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    PB_CUDA(cudaMemcpy(h.h_step_status, h.d_step_status, sizeof(int), cudaMemcpyDeviceToHost));
+    h.status_pending = false;
+    if (*h.h_step_status & 1)
+        h.nonfinite = true;
+    return poll_step_status(h, false);
 }
 
 struct pppm_batch
@@ -782,6 +871,7 @@ int pppm_reset_fields(pppm_handle *ph)
         PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * h.nt * kRing * h.real_size, h.stream));
     }
     PB_TRY(step_prime(h));
+    PB_TRY(clear_step_status(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
     return PPPM_OK;
 }
@@ -866,6 +956,7 @@ int pppm_restore_state(pppm_handle *ph, const void *src, size_t bytes)
         PB_TRY(hist_import(h));
     }
     PB_TRY(step_prime(h));
+    PB_TRY(clear_step_status(h));
     PB_CUDA(cudaStreamSynchronize(h.stream));
     return PPPM_OK;
 }
@@ -1283,6 +1374,25 @@ int pppm_enable_timing(pppm_handle *ph, int enable)
     ph->h.timing = enable != 0;
     ph->h.us_stencil = ph->h.us_face = ph->h.us_near = 0;
     ph->h.timed_steps = 0;
+    for (int k = 0; k < PPPM_KERNEL_KINDS; k++)
+    {
+        ph->h.kind_us[k] = 0;
+        ph->h.kind_n[k] = 0;
+    }
+    return PPPM_OK;
+}
+
+int pppm_kernel_profile(pppm_handle *ph, int nkinds, float *us_per_launch, long long *launches)
+{
+    PB_TRY(check_handle(ph));
+    if (nkinds < 0 || nkinds > PPPM_KERNEL_KINDS || (nkinds > 0 && (!us_per_launch || !launches)))
+        return PPPM_ERR_ARG;
+    const Handle &h = ph->h;
+    for (int k = 0; k < nkinds; k++)
+    {
+        launches[k] = h.kind_n[k];
+        us_per_launch[k] = h.kind_n[k] ? (float)(h.kind_us[k] / (double)h.kind_n[k]) : 0.0f;
+    }
     return PPPM_OK;
 }
 

@@ -17,9 +17,6 @@ constexpr int kRing = 32;
 // Reference capacities that define parity-mode limits (particle_grid.h:9-11,
 // pppm_cache.h:79); the B200 lists are CSR and only the face cache keeps a per-face bound.
 constexpr int kFaceCacheSlots = 1024;
-// Bound for every device-side wait (iterations of a spin loop) before it reports
-// PPPM_ERR_TIMEOUT instead of waiting further.
-constexpr long long kSpinLimit = 1ll << 26;
 
 void set_error(const char *fmt, ...);
 const char *last_error();

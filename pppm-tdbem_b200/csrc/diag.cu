@@ -38,6 +38,28 @@ __global__ void pair_weight_kernel(TdbemConsts tc, const float *verts, int3 src,
     ref32::scaled_fft(s, tc.lambda, out);
     ref32::scaled_fft(d, tc.lambda, out + kTaps);
 }
+
+// Makes `device` current for the scope of an entry point and gives the calling thread its
+// previous current device back on every return path: these entry points may run on threads that
+// drive other devices.
+struct DeviceScope
+{
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int device)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        err = cudaSetDevice(device);
+        if (err != cudaSuccess)
+            cudaGetLastError();  // not left for the caller's next error check to find
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
 }  // namespace
 
 extern "C" {
@@ -65,21 +87,28 @@ int pppm_pair_weights(int device, float dt, float dl, float c, const float *vert
     for (int k = 0; k < 3; k++)
         if (src[k] < 0 || src[k] >= nv || (!to_point && (dst_face[k] < 0 || dst_face[k] >= nv)))
             return PPPM_ERR_ARG;
-    PB_CUDA(cudaSetDevice(device));
+    DeviceScope scope(device);
+    PB_CUDA(scope.err);
     TdbemConsts tc;
     tdbem_init(tc, dt, dl, c);
-    float *dv = nullptr, *dout = nullptr;
-    PB_TRY(dalloc(&dv, 3 * (size_t)nv));
-    PB_TRY(dalloc(&dout, 2 * kTaps));
-    PB_CUDA(cudaMemcpy(dv, verts, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice));
+    struct Buffers
+    {
+        float *dv = nullptr, *dout = nullptr;
+        ~Buffers()
+        {
+            dev_free(dv);
+            dev_free(dout);
+        }
+    } b;
+    PB_TRY(dalloc(&b.dv, 3 * (size_t)nv));
+    PB_TRY(dalloc(&b.dout, 2 * kTaps));
+    PB_CUDA(cudaMemcpy(b.dv, verts, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice));
     int3 s = make_int3(src[0], src[1], src[2]);
     int3 d = to_point ? make_int3(0, 0, 0) : make_int3(dst_face[0], dst_face[1], dst_face[2]);
     f3 p = to_point ? f3{dst_point[0], dst_point[1], dst_point[2]} : f3{0, 0, 0};
-    pair_weight_kernel<<<1, 1>>>(tc, dv, s, to_point, d, p, dout);
+    pair_weight_kernel<<<1, 1>>>(tc, b.dv, s, to_point, d, p, b.dout);
     PB_CHECK_LAUNCH();
-    PB_CUDA(cudaMemcpy(out32, dout, sizeof(float) * 2 * kTaps, cudaMemcpyDeviceToHost));
-    dev_free(dv);
-    dev_free(dout);
+    PB_CUDA(cudaMemcpy(out32, b.dout, sizeof(float) * 2 * kTaps, cudaMemcpyDeviceToHost));
     return PPPM_OK;
 }
 }
@@ -91,7 +120,10 @@ int pppm_pair_weights(int device, float dt, float dl, float c, const float *vert
 // device and stall that handle's stream for the length of its queued steps), and processes whose
 // device memory is fully held by another allocator (a framework's caching pool), where a fresh
 // cudaMalloc fails.  One scratch array per device and per process; calls that overlapped would
-// race on it, so they are serialised by a process-wide lock.
+// race on it, so they are serialised by a process-wide lock.  The call leaves the calling
+// thread's current device as it found it, refuses a stream that is being captured, and has
+// finished with the scratch (its stream synchronised) on every return after the first copy was
+// queued, so the next caller may overwrite it.
 
 namespace
 {
@@ -125,7 +157,16 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
     if (device < 0 || device >= kMaxDevices)
         return PPPM_ERR_ARG;
     std::lock_guard<std::mutex> lock(g_static_lock);
-    PB_CUDA(cudaSetDevice(device));
+    DeviceScope scope(device);
+    PB_CUDA(scope.err);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PB_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+    {
+        pb::set_error("pppm_pair_weights_static: the stream is being captured; this call synchronises it");
+        return PPPM_ERR_STATE;
+    }
     if (!g_scratch_ptr[device])
     {
         // first call on this device: resolves the symbol (may load the module)
@@ -135,9 +176,15 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
     }
     float *dv = g_scratch_ptr[device];
     float *dout = dv + 3 * kStaticMaxVerts;
-    cudaStream_t s = (cudaStream_t)stream;
     TdbemConsts tc;
     tdbem_init(tc, dt, dl, c);
+    // from the first queued copy on, every return waits for the stream: the lock is released only
+    // once this call's copies and kernel no longer touch the shared scratch
+    struct Drain
+    {
+        cudaStream_t s;
+        ~Drain() { cudaStreamSynchronize(s); }
+    } drain{s};
     // nothing has to start at zero: the rows are copied in and the kernel writes all 32 taps
     PB_CUDA(cudaMemcpyAsync(dv, verts, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice, s));
     int3 si = make_int3(src[0], src[1], src[2]);

@@ -151,6 +151,11 @@ struct Handle
     long long pool_used = 0;
     int *d_pair_flag = nullptr;  // pf scratch: 1 = recompute
     int *d_status = nullptr;     // device-side status word (capacity / timeout)
+    int *d_step_status = nullptr;  // step status word: non-finite values seen by the step kernels
+    int *h_step_status = nullptr;  // pinned copy, written behind each pppm_step call
+    cudaEvent_t ev_status = nullptr;  // recorded after that copy
+    bool status_pending = false;   // a copy is queued and not yet looked at
+    bool nonfinite = false;        // a non-finite value was seen (until the fields are reset)
     void *d_spec = nullptr;      // recompute scratch spectra
     size_t spec_bytes = 0;
     double *d_tw = nullptr;      // 8 radix-2 FFT twiddles (cos, sin)
@@ -185,6 +190,14 @@ struct Handle
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float us_stencil = 0, us_face = 0, us_near = 0;  // summed over timed_steps
     long long timed_steps = 0;
+    // per kernel kind (PPPM_KERNEL_*): event time and launches summed in measurement mode
+    double kind_us[PPPM_KERNEL_KINDS] = {};
+    long long kind_n[PPPM_KERNEL_KINDS] = {};
+    static constexpr int kProfileSteps = 4;
+    static constexpr int kProfileEvents = 3 + 4 * kProfileSteps;  // Neumann write, empty, 4 kernels per step, end
+    cudaEvent_t evk[kProfileEvents] = {};
+    int evk_kind[kProfileEvents] = {};
+    StepGraph profile_graph;  // kProfileSteps split-stage steps with events between the kernels
 
     // ---- step launches
     StepState *d_state = nullptr;  // per-call values the step kernels read

@@ -43,7 +43,18 @@ struct StepArgs
     int nt;
     int n_listen;
     int listen_cell[8];
+    int *status;  // the handle's step status word: kStepNonFinite once a listener sample is not finite
 };
+
+// bit of the step status word: a non-finite Dirichlet value or listener sample appeared
+constexpr int kStepNonFinite = 1;
+
+template <typename R>
+__device__ inline void flag_nonfinite(int *status, R v)
+{
+    if (status && !isfinite(v))
+        atomicOr(status, kStepNonFinite);
+}
 
 
 // History rings in the step.  The reference keeps per triangle a ring of 32 values indexed by
@@ -193,7 +204,10 @@ __device__ inline void finish_cell(const StepArgs &a, long long row, long long c
     if (!corrected)
         for (int l = 0; l < a.n_listen; l++)
             if (a.listen_cell[l] == (int)c)
+            {
                 series[row * a.n_listen + l] = v;
+                flag_nonfinite(a.status, v);
+            }
 }
 
 // the stencil work of block b of one scene's stencil grid (256 threads)
@@ -319,7 +333,10 @@ __global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepAr
     if (!corrected)
         for (int l = 0; l < a.n_listen; l++)
             if (a.listen_cell[l] == (int)ci)
+            {
                 series[dy.row * a.n_listen + l] = v;
+                flag_nonfinite(a.status, v);
+            }
 }
 
 // ---- convolution helpers
@@ -389,6 +406,7 @@ struct FaceArgs
     R *terms;  // [nt][54]
     R *terms1;        // [nt][54] partial terms of the next step (near_terms2)
     const R *gc_f;    // [nt][54] factor of the next step's Dirichlet value per record (near_terms2)
+    int *status;      // step status word (kStepNonFinite)
 };
 
 constexpr int kGcRecords = 54;  // per triangle: 27 FDTD-near then 27 BEM-near records (offsets in 3^3)
@@ -664,6 +682,8 @@ __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs
         ring.hrow(1, lane, tri)[hist_index(lane, tnew)] = dnew;  // lane c: copy c
     else if (commit && lane == 4 && f.dlast)
         f.dlast[tri] = dnew;
+    else if (commit && lane == 5)
+        flag_nonfinite(f.status, dnew);  // a NaN acceleration or field reaches D within a step or two
     if (mode == 1)
         near_terms2<R>(ring, tnew, f, tri, lane, dnew, nnext);
     else if (mode == 2)
@@ -876,7 +896,10 @@ __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const S
                 cur[c] = v;
                 for (int l = 0; l < a.n_listen; l++)
                     if (a.listen_cell[l] == c)
+                    {
                         na.series[dy.row * a.n_listen + l] = v;
+                        flag_nonfinite(a.status, v);
+                    }
             }
         }
     }
@@ -907,6 +930,7 @@ StepArgs make_args(Handle &h)
     a.damp = 2.0f / h.prm.dl;
     a.nt = h.mesh_set ? h.nt : 0;
     a.n_listen = (int)h.listen_xyz.size() / 3;
+    a.status = h.d_step_status;
     return a;
 }
 
@@ -1008,6 +1032,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.fa.dlast = (R *)h.d_dlast;
         L.fa.terms1 = (R *)h.d_terms1;
         L.fa.gc_f = (const R *)h.d_gc_f;
+        L.fa.status = h.d_step_status;
         L.na.n3_cell = h.d_n3_cell;
         L.na.n3_start = h.d_n3_start;
         L.na.p3_tri = h.d_p3_tri;
@@ -1105,6 +1130,97 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
 }
 
 
+__global__ void empty_kernel() {}
+
+// Measurement mode per kernel: the kernels of Handle::kProfileSteps steps exactly as
+// capture_pipelined issues them for a call of that many steps, but serialised on the handle's
+// stream with an event record between consecutive kernels; evk_kind[i] names the kind of the
+// kernel between events i and i + 1.
+template <typename R>
+int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
+{
+    const unsigned char *sig = (const unsigned char *)&L;
+    StepGraph &g = h.profile_graph;
+    if (g.exec && g.sig.size() == sizeof(L) && memcmp(g.sig.data(), sig, sizeof(L)) == 0)
+    {
+        *out = g.exec;
+        return PPPM_OK;
+    }
+    if (g.exec)
+        cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    const int T = 256, FT = L.face_threads, nt = L.a.nt, n = Handle::kProfileSteps;
+    const int wblocks = div_up((long long)nt * 32, FT);
+    const bool pair = L.pairs != 0;
+    cudaStream_t s = h.stream;
+    int e = 0;
+    auto mark = [&](int kind) {
+        h.evk_kind[e] = kind;
+        cudaEventRecordWithFlags(h.evk[e++], s, cudaEventRecordExternal);
+    };
+    cudaGraph_t graph = nullptr;
+    PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    mark(PPPM_KERNEL_NWRITE);
+    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
+    mark(PPPM_KERNEL_EMPTY);
+    empty_kernel<<<1, 32, 0, s>>>();
+    for (int k = 0; k < n; k++)
+    {
+        if (pair && (k & 1))
+        {
+            mark(PPPM_KERNEL_FIX);
+            fix_kernel<R><<<wblocks, FT, 0, s>>>(nt, L.fa, L.conv1, L.conv);
+        }
+        else if (pair && k + 1 < n)
+        {
+            mark(PPPM_KERNEL_CONV2);
+            conv2_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, L.conv1);
+        }
+        else
+        {
+            mark(PPPM_KERNEL_CONV);
+            conv_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv);
+        }
+        mark(PPPM_KERNEL_STENCIL);
+        stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
+        const int mode = L.tpairs && k + 1 < n ? ((k & 1) ? 2 : 1) : 0;
+        const int nx = k + 1 < n ? 1 : 0;
+        if (mode == 1)
+        {
+            mark(PPPM_KERNEL_FINISH1);
+            finish_kernel<R, 1><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+        }
+        else if (mode == 2)
+        {
+            mark(PPPM_KERNEL_FINISH2);
+            finish_kernel<R, 2><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+        }
+        else
+        {
+            mark(PPPM_KERNEL_FINISH);
+            finish_kernel<R, 0><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+        }
+        mark(PPPM_KERNEL_NEAR);
+        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
+    }
+    mark(-1);
+    cudaError_t err = cudaStreamEndCapture(s, &graph);
+    if (err == cudaSuccess)
+        err = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (err != cudaSuccess)
+    {
+        g.exec = nullptr;
+        set_error("recording the profile graph failed: %s", cudaGetErrorString(err));
+        return PPPM_ERR_CUDA;
+    }
+    g.nsteps = n;
+    g.sig.assign(sig, sig + sizeof(L));
+    *out = g.exec;
+    return PPPM_OK;
+}
+
 // Calls of at least kGraphSteps steps replay a CUDA graph of their kernels, recorded on the
 // first call with that step count and launch set (the graph removes the host launch cost and
 // most of the gap between dependent kernels); shorter calls, measurement mode and calls on a
@@ -1175,12 +1291,49 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     PB_CUDA(cudaStreamIsCapturing(s, &cs));
     if (h.timing && cs == cudaStreamCaptureStatusNone)
     {
-        // Measurement mode: every step replays a one-step graph whose event-record nodes sit
-        // between its kernels, so each kernel's duration is measured the way it runs inside the
-        // recorded step graphs (no host launch gaps); the step state is rewritten per step.
+        // Measurement mode.  Where the recorded graphs run the split face stage, groups of
+        // kProfileSteps steps replay the profile graph (those kernels serialised, events between
+        // them); the other steps replay a one-step graph of the fused kernels with event records
+        // between them.  Either way each kernel's duration is measured the way it runs inside a
+        // recorded graph (no host launch gaps); the step state is rewritten per replay.
+        int done = 0;
+        if (L.mesh && !L.pml && h.side && nsteps >= Handle::kProfileSteps)
+        {
+            cudaGraphExec_t pexec = nullptr;
+            PB_TRY(profile_graph<R>(h, L, &pexec));
+            const int n = Handle::kProfileSteps;
+            for (; done + n <= nsteps; done += n)
+            {
+                StepState sk{stt.tnew0 + done, stt.n3, stt.row0 + done,
+                             acc_dev ? acc_dev + (long long)done * h.nt : nullptr};
+                set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sk);
+                PB_CHECK_LAUNCH();
+                PB_CUDA(cudaGraphLaunch(pexec, s));
+                PB_CUDA(cudaEventSynchronize(h.evk[Handle::kProfileEvents - 1]));
+                for (int i = 0; i + 1 < Handle::kProfileEvents; i++)
+                {
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, h.evk[i], h.evk[i + 1]);
+                    const int kind = h.evk_kind[i];
+                    h.kind_us[kind] += 1000.0 * ms;
+                    h.kind_n[kind]++;
+                    if (kind == PPPM_KERNEL_EMPTY)
+                        continue;
+                    if (kind == PPPM_KERNEL_STENCIL)
+                        h.us_stencil += 1000 * ms;
+                    else if (kind == PPPM_KERNEL_NEAR)
+                        h.us_near += 1000 * ms;
+                    else
+                        h.us_face += 1000 * ms;
+                }
+                h.timed_steps += n;
+                h.launches += 2 + 4 * n - per_step * n;  // per_step * nsteps is added below
+            }
+        }
         cudaGraphExec_t exec = nullptr;
-        PB_TRY(graph_for<R>(h, L, 1, &exec, true));
-        for (int k = 0; k < nsteps; k++)
+        if (done < nsteps)
+            PB_TRY(graph_for<R>(h, L, 1, &exec, true));
+        for (int k = done; k < nsteps; k++)
         {
             StepState sk{stt.tnew0 + k, stt.n3, stt.row0 + k,
                          acc_dev ? acc_dev + (long long)k * (h.mesh_set ? h.nt : 0) : nullptr};
@@ -1199,6 +1352,15 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
             h.us_face += 1000 * tb;
             h.us_near += 1000 * tc;
             h.timed_steps++;
+            h.kind_us[PPPM_KERNEL_STENCIL] += 1000.0 * ta;
+            h.kind_n[PPPM_KERNEL_STENCIL]++;
+            if (h.mesh_set)
+            {
+                h.kind_us[PPPM_KERNEL_FACE] += 1000.0 * tb;
+                h.kind_us[PPPM_KERNEL_NEAR] += 1000.0 * tc;
+                h.kind_n[PPPM_KERNEL_FACE]++;
+                h.kind_n[PPPM_KERNEL_NEAR]++;
+            }
         }
     }
     else if (cs == cudaStreamCaptureStatusNone && nsteps >= kGraphSteps)
@@ -1515,7 +1677,7 @@ int step_run(Handle &h, const float *acc_dev, int nsteps)
 
 int step_free(Handle &h)
 {
-    for (auto *g : {&h.graphs[0], &h.graphs[1], &h.graphs[2], &h.graphs[3], &h.timing_graph})
+    for (auto *g : {&h.graphs[0], &h.graphs[1], &h.graphs[2], &h.graphs[3], &h.timing_graph, &h.profile_graph})
     {
         if (g->exec)
             cudaGraphExecDestroy(g->exec);

@@ -4,7 +4,7 @@
 grid, `set_mesh`, `update_mesh` on motion frames, `update_grid_and_face(acc)` per step
 (`step(acc_rows)` for many), listener cells read per step like the demo driver
 (experiments/demo/main.cu:266).  Errors raise PPPMError; the CUDA library is required - a
-missing library raises at import, there is no CPU fallback.
+missing library raises at its first use (ImportError), there is no CPU fallback.
 """
 import ctypes
 import os
@@ -96,6 +96,8 @@ def _load():
         "pppm_get_option": [vp, i, ip],
         "pppm_autotune": [vp, i, fp, ip],
         "pppm_kernel_times": [vp, fp, fp, fp, ip],
+        "pppm_kernel_profile": [vp, i, fp, ctypes.POINTER(ctypes.c_longlong)],
+        "pppm_sync": [vp],
     }
     fl = ctypes.c_float
     sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
@@ -112,7 +114,30 @@ def _load():
     return lib
 
 
-lib = _load()
+class _Lib:
+    """libpppm_b200.so, mapped into the process at the first call through it.  Importing the
+    package (for `scenes`, say) maps no native code; the first Solver, Batch or entry-point call
+    loads the library and raises ImportError when it is not built."""
+
+    _cdll = None
+
+    def __getattr__(self, name):
+        return getattr(load(), name)
+
+
+def load():
+    """Map libpppm_b200.so now (idempotent) and return the ctypes handle."""
+    if _Lib._cdll is None:
+        _Lib._cdll = _load()
+    return _Lib._cdll
+
+
+def loaded():
+    """True once the native library is mapped into this process."""
+    return _Lib._cdll is not None
+
+
+lib = _Lib()
 
 
 def check(status, where):
@@ -261,6 +286,11 @@ class Solver:
         if a.ndim == 1:
             a = a.reshape(1, -1)
         check(lib.pppm_step(self.h, a.ctypes.data_as(ctypes.c_void_p), 0, a.shape[0]), "step")
+
+    def sync(self):
+        """Wait for the queued work (pppm_sync); raises PPPMError(ERR_NAN) once a non-finite
+        Dirichlet value or listener sample has appeared."""
+        check(lib.pppm_sync(self.h), "sync")
 
     def update_grid_and_face(self, acc):
         self.step(np.asarray(acc, dtype=np.float32).reshape(1, -1))
@@ -459,6 +489,18 @@ class Solver:
 
     def enable_timing(self, on=True):
         check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")
+
+    KERNEL_KINDS = ("stencil", "conv", "conv2", "fix", "finish", "finish1", "finish2", "near", "nwrite", "face",
+                    "empty")
+
+    def kernel_profile(self):
+        """{kind: (mean us per launch, launches)} of the kernels timed in measurement mode
+        (pppm_kernel_profile), kinds with no launch left out."""
+        n = len(self.KERNEL_KINDS)
+        us = (ctypes.c_float * n)()
+        cnt = (ctypes.c_longlong * n)()
+        check(lib.pppm_kernel_profile(self.h, n, us, cnt), "kernel_profile")
+        return {k: (float(us[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_KINDS) if cnt[i]}
 
     def kernel_times(self):
         a, b, c, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_int()

@@ -19,7 +19,8 @@ compressed .npz fixtures:
                      and the fresh-cell fill of grid slots t and t-1
 
 Usage (on a machine with a GPU and oracle/_ref built):
-    python tests/golden/make_golden.py OUTDIR
+    python tests/golden/make_golden.py OUTDIR            # every fixture but noise.npz
+    python tests/golden/make_golden.py OUTDIR --noise    # noise.npz: repeats of three scenes
 """
 import os
 import sys
@@ -199,7 +200,8 @@ def main(out):
 def noise_floor(out, repeats=3):
     """The reference's own run-to-run spread: the same inputs run several times (its float
     atomics sum in a different order each run).  noise.npz: series of each repeat for the
-    static sphere (2000 steps) and the small sphere (300 steps)."""
+    static sphere (2000 steps), the small sphere (300 steps) and the benchmarked moving scene
+    (res 64, 8820 steps in 128 motion frames)."""
     os.makedirs(out, exist_ok=True)
     sc = scenes.StaticSphere()
     big = []
@@ -216,13 +218,33 @@ def noise_floor(out, repeats=3):
         r.set_mesh(v, fc)
         small.append(r.run(acc, [(20, 20, 20)])[:, 0])
         r.close()
-    np.savez_compressed(os.path.join(out, "noise.npz"), static_sphere=np.array(big), sphere_small=np.array(small))
+    # the benchmarked moving scene (res 64, 5120 + 1280 triangles), its whole 8820-step run
+    ms = scenes.MovingScene()
+    nframes = ms.frame_of_step(ms.steps - 1) + 1
+    ranges = scenes.frame_ranges(ms, nframes - 1)
+    ranges[-1] = (ranges[-1][0], ms.steps)
+    acc = ms.acc(0, ms.steps)
+    moving = []
+    for _ in range(repeats):
+        r = O.Reference(ms.res, ms.h, ms.dt, ms.min_pos)
+        r.set_mesh(ms.frame_verts(0), ms.tris)
+        run = []
+        for f, (a, b) in enumerate(ranges):
+            if f:
+                r.update_mesh(ms.frame_verts(f))
+            run.append(r.run(acc[a:b], [ms.listener])[:, 0])
+        moving.append(np.concatenate(run))
+        r.close()
+    np.savez_compressed(os.path.join(out, "noise.npz"), static_sphere=np.array(big), sphere_small=np.array(small),
+                        moving64=np.array(moving))
     print("noise floor written to", out)
 
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    out = args[0] if args else os.path.join(ROOT, "gpurun_out", "golden")
+    if not args:
+        sys.exit("usage: make_golden.py OUTDIR [--noise]  (then copy the .npz files into tests/golden/)")
+    out = args[0]
     if "--noise" in sys.argv:
         noise_floor(out)
     else:

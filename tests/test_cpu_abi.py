@@ -54,3 +54,18 @@ def test_oracle_library_loads():
 
     assert oracle_lib() is not None
     assert oracle_threads() >= 1
+
+
+def test_package_import_maps_no_native_code():
+    """Importing the package (for its scene generators, as the benchmark's reference arm does)
+    loads no native library; the first call through the library maps it."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r); import pppm_b200; from pppm_b200 import scenes; "
+            "maps = open('/proc/self/maps').read(); assert 'libpppm_b200' not in maps, 'mapped at import'; "
+            "assert not pppm_b200.loaded(); pppm_b200.lib.pppm_status_string(0); "
+            "assert 'libpppm_b200' in open('/proc/self/maps').read(); print('ok')"
+            % os.path.join(ROOT, "pppm-tdbem_b200", "python"))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr

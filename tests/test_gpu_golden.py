@@ -143,10 +143,13 @@ def test_series_with_reference_tables(gpu):
     got = _series(s, g)
     e50 = max(rel_l2(got[:50, l], g["series"][:50, l]) for l in range(got.shape[1]))
     eall = max(rel_l2(got[:, l], g["series"][:, l]) for l in range(got.shape[1]))
+    floor = reference_noise_floor("sphere_small")
     METRICS["series_reference_tables"] = {"rel_l2_first50": e50, "rel_l2_300": eall,
-                                          "final_grid_rel_l2": rel_l2(s.grid(0), g["final_grid"])}
+                                          "final_grid_rel_l2": rel_l2(s.grid(0), g["final_grid"]),
+                                          "reference_noise_floor": floor}
     assert e50 < 1e-5
-    assert eall < 1e-3
+    # over the 300 steps: within twice the spread of the reference's own repeats
+    assert eall < 2 * max(floor or 0.0, 1e-5)
     s.close()
 
 
@@ -157,10 +160,8 @@ def test_series_with_own_tables(gpu):
     eall = max(rel_l2(got[:, l], g["series"][:, l]) for l in range(got.shape[1]))
     floor = reference_noise_floor("sphere_small")
     METRICS["series_own_tables"] = {"rel_l2_first50": e50, "rel_l2_300": eall, "reference_noise_floor": floor}
-    assert eall < 1e-2
-    if floor:
-        # within a few times the spread of the reference's own repeats
-        assert rel_l2(got[:, 0], g["series"][:, 0]) < 5 * floor
+    assert e50 < 1e-5
+    assert eall < 2 * max(floor or 0.0, 1e-5)
     s.close()
 
 
@@ -180,9 +181,8 @@ def test_static_sphere_2000_steps(gpu):
     floor = reference_noise_floor("static_sphere")
     METRICS["static_sphere"] = {"rel_l2_2000": rel_l2(got, ref), "rel_l2_first200": rel_l2(got[:200], ref[:200]),
                                 "reference_noise_floor": floor}
-    assert rel_l2(got, ref) < 1e-2
-    if floor:
-        assert rel_l2(got, ref) < 5 * floor
+    assert rel_l2(got[:200], ref[:200]) < 1e-5
+    assert rel_l2(got, ref) < 2 * max(floor or 0.0, 1e-5)
     s.close()
 
 
@@ -203,7 +203,8 @@ def test_moving_small_vs_reference(gpu):
     n3 = s.dump("n3_cells").reshape(-1, 4)
     assert per_cell_sets(n3, s.dump("n3_tris")) == per_cell_sets(g["n3_cells"], g["n3_tris"])
     METRICS["moving_small"] = {"rel_l2_200": rel_l2(got, ref), "rel_l2_first50": rel_l2(got[:50], ref[:50])}
-    assert rel_l2(got, ref) < 1e-2
+    assert rel_l2(got[:50], ref[:50]) < 1e-5
+    assert rel_l2(got, ref) < 5e-5  # measured 9.6e-6 over the 200 steps and 10 mesh updates
     s.close()
 
 
@@ -221,11 +222,76 @@ def test_cell_labels_and_fresh_cells_vs_reference(gpu):
     n = s.fill_fresh_cells(g["acc1"], g["acc0"])
     assert np.array_equal(s.dump("cell_type"), g["type1"])
     assert np.array_equal(s.dump("cell_ghost"), g["ghost1"])
-    near_same = float(np.mean(s.dump("cell_nearest") == g["nearest1"]))
+    ours_near = s.dump("cell_nearest")
+    near_same = float(np.mean(ours_near == g["nearest1"]))
+    ties = _nearest_ties(s, g, ours_near)
     d_t = float(np.abs(s.grid(0) - g["out_t"]).max())
     d_tm1 = float(np.abs(s.grid(-1) - g["out_tm1"]).max())
     METRICS["cells"] = {"fresh_cells": n, "nearest_equal_fraction": near_same, "fresh_max_abs_diff_t": d_t,
-                        "fresh_max_abs_diff_tm1": d_tm1}
+                        "fresh_max_abs_diff_tm1": d_tm1, **ties}
     assert n > 0
     assert d_t < 1e-5 and d_tm1 < 1e-5
+    # the nearest triangle: same cells have one; where the minimum over the search window is
+    # unique the index is the reference's; everywhere the distance and the closest point are
+    assert ties["found_differs"] == 0
+    assert ties["unique_index_differs"] == 0
+    assert ties["max_distance_diff_over_h"] < 1e-4
+    assert ties["max_point_diff_over_h"] < 1e-3
     s.close()
+
+
+def _nearest_ties(s, g, ours):
+    """Nearest-triangle agreement modulo ties.  The reference takes the first strict minimum of
+    the point-triangle distance in the order of its per-cell lists (ghost_cell_util.cu:40-48),
+    which its atomic list fill leaves unspecified, so between triangles at the same distance
+    (a closest point on a shared vertex or edge) either index is right; a cell without any
+    candidate (no triangle centre within +-3 cells, the reference's search window) keeps an
+    uninitialised index there (ghost_cell_util.cu:18-52) and -1 here.  In float64, for every
+    cell with candidates: the distance to each side's triangle, the closest points, and whether
+    the minimum over the candidates is unique by more than 1e-4 h."""
+    from helpers import closest_point_on_triangle
+
+    res, h = int(g["res"]), float(g["h"])
+    mn = np.asarray(g["min_pos"], np.float64)
+    v = np.asarray(g["v1"], np.float64)
+    f = np.asarray(g["tris"], np.int64)
+    nt = len(f)
+    ref = np.asarray(g["nearest1"], np.int64)
+    tcell = s.dump("tri_cells").reshape(-1, 6)[:, :3].astype(np.int64)
+    a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    allc = np.arange(res ** 3)
+    xyz_all = np.stack([allc // (res * res), (allc // res) % res, allc % res], 1)
+    has = np.zeros(res ** 3, bool)
+    best2 = np.full((res ** 3, 2), np.inf)
+    for lo in range(0, res ** 3, 512):
+        sl = slice(lo, lo + 512)
+        near = np.all(np.abs(tcell[None, :, :] - xyz_all[sl, None, :]) <= 3, axis=2)  # (k, nt)
+        has[sl] = near.any(1)
+        k = near.shape[0]
+        rows = np.nonzero(near.any(1))[0]
+        if len(rows) == 0:
+            continue
+        pp = np.repeat((xyz_all[sl][rows] + 0.5) * h + mn, nt, 0)
+        tt = np.tile(np.arange(nt), len(rows))
+        d = np.linalg.norm(pp - closest_point_on_triangle(pp, a[tt], b[tt], c[tt]), axis=1).reshape(len(rows), nt)
+        d[~near[rows]] = np.inf
+        best2[lo + rows] = np.sort(d, 1)[:, :2]
+    found_differs = int(np.sum(has & ((ours < 0) | (ref < 0) | (ref >= nt))) + np.sum(~has & (ours >= 0)))
+    cells = np.nonzero(has & (ours >= 0) & (ref >= 0) & (ref < nt))[0]
+    p = (xyz_all[cells] + 0.5) * h + mn
+
+    def dist_to(idx):
+        q = closest_point_on_triangle(p, a[idx], b[idx], c[idx])
+        return np.linalg.norm(p - q, axis=1), q
+
+    d_ref, q_ref = dist_to(ref[cells])
+    d_our, q_our = dist_to(ours[cells])
+    unique = best2[cells, 1] - best2[cells, 0] > 1e-4 * h
+    differs = ours[cells] != ref[cells]
+    return {"cells_with_candidates": int(has.sum()), "found_differs": found_differs,
+            "index_differs": int(differs.sum()), "unique_minimum": int(unique.sum()),
+            "unique_index_differs": int((differs & unique).sum()),
+            "max_distance_diff_over_h": float(np.abs(d_ref - d_our).max() / h) if len(cells) else 0.0,
+            "max_point_diff_over_h": float(np.linalg.norm(q_ref - q_our, axis=1).max() / h) if len(cells) else 0.0,
+            "max_distance_vs_float64_min_over_h": float(np.abs(d_our - best2[cells, 0]).max() / h)
+            if len(cells) else 0.0}
