@@ -50,13 +50,17 @@ def parse():
     p.add_argument("--steps", type=int, default=10, help="timed benchmark steps (whole runs; frames for large)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="moving", choices=["moving", "static", "batch", "adjoint", "large"])
+    p.add_argument("--workload", default="moving",
+                   choices=["moving", "static", "batch", "adjoint", "large", "large-batch"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64-check", action="store_true")
     p.add_argument("--profile-frame", type=int, metavar="F",
                    help="profiling driver: run the workload's frames 0..F-1, then frame F (update_mesh + its "
-                        "steps) inside the NVTX range 'profile_frame', and exit (for ncu --nvtx-include)")
+                        "steps) inside the NVTX range 'profile_frame', and exit (for ncu --nvtx-include); the "
+                        "launch options are --options, not the autotuner's (a profiler distorts its timings)")
+    p.add_argument("--options", default="1,128,0", metavar="PAIRS,THREADS,TERMS",
+                   help="launch options of --profile-frame: conv_pairs, face_threads, terms_pairs")
     p.add_argument("--summarize-launches", metavar="CSV",
                    help="print per-kernel launches / total time / share from an ncu "
                         "gpu__time_duration.sum CSV log of this benchmark, and exit")
@@ -215,8 +219,13 @@ def algorithmic_bytes(counts, res, nt):
     near = p3 * (4 + 1 + 8) + n3 * (4 + 4 + 4 + 4 + 4 + 4)
     nwrite = nt * 20
     face = pf * 76 + nt * (8 + 4) + finish
+    # the split stencil: the corrected cells (list index, p^t, p^{t-1}, the correction, p^{t+1}) and
+    # the rest of the grid (as the whole stencil without the corrected cells)
+    stencil_corr = n3 * (4 + 12 + 4)
+    stencil_bulk = 12 * (m ** 3 - n3) + 4 * 6 * m * m + m ** 3 // 8
     return {"stencil": stencil, "conv": conv, "conv2": conv2, "fix": fix, "finish": finish, "finish1": finish1,
-            "finish2": finish2, "near": near, "nwrite": nwrite, "face": face}
+            "finish2": finish2, "near": near, "nwrite": nwrite, "face": face, "stencil_corr": stencil_corr,
+            "stencil_bulk": stencil_bulk}
 
 
 def load_traffic(workload):
@@ -292,8 +301,12 @@ def run_ours(args, ws, rank, local):
     # face-stage autotuner on the first frame's mesh (set-up, untimed): one or two steps per pass
     # over the face pairs and over the grid-cache records, block size of the face kernels
     s0 = new_solver()
-    tune = s0.autotune(reps=20)
-    opts = {"conv_pairs": tune["best"][0], "face_threads": tune["best"][1], "terms_pairs": tune["terms_pairs"]}
+    if args.profile_frame is not None:
+        p_, t_, m_ = (int(x) for x in args.options.split(","))
+        tune, opts = None, {"conv_pairs": p_, "face_threads": t_, "terms_pairs": m_}
+    else:
+        tune = s0.autotune(reps=20)
+        opts = {"conv_pairs": tune["best"][0], "face_threads": tune["best"][1], "terms_pairs": tune["terms_pairs"]}
 
     if args.profile_frame is not None:
         # the frames before the profiled one run as usual; the profiled frame is bracketed by an
@@ -389,25 +402,31 @@ def run_ours(args, ws, rank, local):
     us_update = upd_ms * 1e3 / max(n_upd, 1)
     us_per_step = (total_ms - upd_ms) * 1e3 / steps
 
-    # per-kernel durations (measurement mode: the recorded graphs' kernels serialised with an event
-    # between consecutive kernels) over the same frames as one timed benchmark step, with the
-    # algorithmic bytes of each launch from the mesh counts of its frame
+    # per-kernel table over the frames of one benchmark step: launches of each kind and their
+    # algorithmic bytes from a measurement-mode run (its per-kind launch counts, each frame's mesh
+    # counts), durations from pppm_time_kernels (each kind's launches back to back in one recorded
+    # graph, no event between them) at eight frames spread over the run
     sp = new_solver(opts) if wl.whole_run else s0
     sp.enable_timing(True)
     kind_bytes = {}
-    prof_frames = range(len(wl.ranges)) if wl.whole_run else range(W + K + 1, W + K + 2)
+    prof_frames = list(range(len(wl.ranges))) if wl.whole_run else [W + K + 1]
+    sampled = set(prof_frames[:: max(1, len(prof_frames) // 8)])
+    dur = {}
     prev = {}
     for f in prof_frames:
         a, b = wl.ranges[f]
         if f > 0 and wl.moving:
             sp.update_mesh(verts_dev[f])
         counts = [int(x) for x in sp.dump("counts")]
+        if f in sampled:
+            for k, us in sp.time_kernels(20).items():
+                dur.setdefault(k, []).append(us)
         sp.step(acc_dev[a:b])
         prof = sp.kernel_profile()
         alg = algorithmic_bytes(counts, wl.res, nt)
         for k, (us, n) in prof.items():
             dn = n - prev.get(k, 0)
-            kind_bytes[k] = kind_bytes.get(k, 0.0) + dn * alg[k]
+            kind_bytes[k] = kind_bytes.get(k, 0.0) + dn * alg.get(k, 0)
             prev[k] = n
     prof = sp.kernel_profile()
     sp.enable_timing(False)
@@ -415,22 +434,21 @@ def run_ours(args, ws, rank, local):
     if wl.whole_run:
         sp.close()
     peak, peak_kind = measured_peak()
-    # event-to-event times inside a graph carry the event nodes' own cost: the empty kernel of the
-    # profile graph measures that floor, which is taken off every kind's mean
-    floor = prof.pop("empty", (0.0, 0))[0]
-    corr = {k: (max(us - floor, 0.05), n) for k, (us, n) in prof.items()}
-    total_us = sum(us * n for us, n in corr.values())
+    prof.pop("empty", None)
+    prof.pop("nwrite", None)  # a 20-byte-per-triangle copy at the start of each call
+    per = {k: statistics.mean(dur[k]) for k in prof if k in dur}
+    total_us = sum(per[k] * prof[k][1] for k in per)
     kernels = {}
-    for k, (us, n) in sorted(corr.items(), key=lambda kv: -kv[1][0] * kv[1][1]):
+    for k in sorted(per, key=lambda k: -per[k] * prof[k][1]):
+        n = prof[k][1]
         b = kind_bytes.get(k, 0.0) / n
-        kernels[k] = {"launches": n, "us_per_launch": round(us, 3), "us_event_to_event": round(prof[k][0], 3),
-                      "share": round(us * n / total_us, 4),
-                      "algorithmic_bytes_per_launch": int(b), "gb_per_s": round(b / (us * 1e-6) / 1e9, 1),
-                      "frac": round(b / (us * 1e-6) / 1e9 / peak, 4)}
+        kernels[k] = {"launches": n, "us_per_launch": round(per[k], 3), "share": round(per[k] * n / total_us, 4),
+                      "algorithmic_bytes_per_launch": int(b), "gb_per_s": round(b / (per[k] * 1e-6) / 1e9, 1),
+                      "frac": round(b / (per[k] * 1e-6) / 1e9 / peak, 4)}
     top = next(iter(kernels))
-    prof = corr
     traffic = load_traffic(args.workload).get(top)
-    main_path = [k for k in ("stencil", "finish", "finish1", "finish2", "near") if k in kernels]
+    prof = {k: (per[k], prof[k][1]) for k in per}
+    main_path = [k for k in ("stencil", "stencil_corr", "finish", "finish1", "finish2", "near") if k in kernels]
     path_bytes = sum(kind_bytes.get(k, 0.0) for k in main_path)
     path_us = sum(prof[k][0] * prof[k][1] for k in main_path)
 
@@ -514,10 +532,10 @@ def run_ours(args, ws, rank, local):
                      "unit": "GB/s", "frac": kernels[top]["frac"], "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": kernels[top]["algorithmic_bytes_per_launch"],
                      "kernel_launch_us": kernels[top]["us_per_launch"],
-                     "how": "kernel with the largest share of measurement-mode time over one benchmark step's "
-                            "frames (the recorded graphs' kernels serialised, events between them); achieved = "
-                            "its algorithmic bytes per launch / its mean event-to-event time less that of an "
-                            "empty kernel in the same graph (%.2f us)" % floor,
+                     "how": "kernel with the largest share of time (launches x duration) over one benchmark "
+                            "step's frames; achieved = its algorithmic bytes per launch / its duration per launch "
+                            "(pppm_time_kernels: 20 back-to-back launches in one recorded graph, events around "
+                            "the graph, at %d frames spread over the run)" % len(sampled),
                      "kernels": kernels,
                      "main_path": {"kernels": main_path, "achieved": round(path_bytes / (path_us * 1e-6) / 1e9, 1),
                                    "frac": round(path_bytes / (path_us * 1e-6) / 1e9 / peak, 4)},
@@ -707,6 +725,110 @@ def run_batch(args, ws, rank, local):
     }
 
 
+# ---------------------------------------------------------------- large scene batched --
+LARGE_BATCH = 4
+LARGE_BATCH_NAME = ("4 large moving scenes (res 128, two 20480-tri perturbed icospheres each, seeds 23, 123, 223, "
+                    "323), 1 kHz motion frames, batched")
+
+
+def run_large_batch(args, ws, rank, local):
+    """The large moving scene batched x4 with different seeds: one benchmark step = one motion
+    frame of all four scenes (each scene's update_mesh, then one pppm_batch_run over the frame's
+    steps), against the same frames stepped scene by scene (update_mesh + pppm_step per scene)."""
+    import torch
+
+    from pppm_b200 import Batch, Solver
+
+    W, K = args.warmup, args.steps
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    nfr = 2 * (W + K) + 2
+    scs = [scenes.LargeScene(seed=23 + 100 * i) for i in range(LARGE_BATCH)]
+    ranges = [scenes.frame_ranges(sc, nfr) for sc in scs]
+    accs = [torch.from_numpy(sc.acc(0, r[-1][1])).to(dev) for sc, r in zip(scs, ranges)]
+    verts = [[torch.from_numpy(sc.frame_verts(f)).to(dev) for f in range(nfr + 1)] for sc in scs]
+
+    def make():
+        out = []
+        for sc in scs:
+            s = Solver(sc.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+            s.set_mesh(sc.frame_verts(0), sc.tris)
+            s.add_listener(*sc.listener)
+            out.append(s)
+        return out
+
+    def frame_batched(ss, b, f):
+        rows = []
+        for i, s in enumerate(ss):
+            if f:
+                s.update_mesh(verts[i][f])
+            a, e = ranges[i][f]
+            rows.append(accs[i][a:e])
+        b.run(rows)
+
+    def frame_sequential(ss, f):
+        for i, s in enumerate(ss):
+            if f:
+                s.update_mesh(verts[i][f])
+            a, e = ranges[i][f]
+            s.step(accs[i][a:e])
+
+    def timed(run, frames_timed, clocks=None):
+        ms, steps = 0.0, 0
+        if clocks:
+            clocks.start()
+        barrier(ws)
+        for f in frames_timed:
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(f)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            steps += sum(r[f][1] - r[f][0] for r in ranges)
+        barrier(ws)
+        return max_over_ranks(ws, ms), steps, (clocks.stop() if clocks else None)
+
+    bat = make()
+    b = Batch(bat)
+    for f in range(0, W + 1):
+        frame_batched(bat, b, f)
+    launches0 = sum(s.launch_count() for s in bat)
+    ms_b, steps_b, clk = timed(lambda f: frame_batched(bat, b, f), range(W + 1, W + K + 1), ClockSampler(local))
+    launches = sum(s.launch_count() for s in bat) - launches0
+    series_b = [s.listeners() for s in bat]
+    b.close()
+    for s in bat:
+        s.close()
+    seq = make()
+    for f in range(0, W + 1):
+        frame_sequential(seq, f)
+    ms_s, steps_s, _ = timed(lambda f: frame_sequential(seq, f), range(W + 1, W + K + 1))
+    same = all(np.array_equal(a, s.listeners()) for a, s in zip(series_b, seq))
+    for s in seq:
+        s.close()
+    cells = float(scs[0].res) ** 3
+    value = cells * steps_b * ws / (ms_b * 1e-3) / 1e9
+    seq_value = cells * steps_s * ws / (ms_s * 1e-3) / 1e9
+    return {
+        "metric": "Gcell-steps/s, %s" % LARGE_BATCH_NAME, "value": round(value, 4), "unit": "Gcell-steps/s",
+        "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": round(ms_b / K, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes, trajectories "
+        "and accelerations)",
+        "config": {"workload": LARGE_BATCH_NAME, "scenes": LARGE_BATCH, "res": scs[0].res,
+                   "triangles_per_scene": int(len(scs[0].tris)),
+                   "bench_step": "one motion frame of all scenes: update_mesh per scene + one pppm_batch_run",
+                   "l2": "flushed (256 MiB write) before each timed frame", "parallelism": "replicas x%d" % ws},
+        "sequential": {"value": round(seq_value, 4), "unit": "Gcell-steps/s",
+                       "how": "the same frames, update_mesh + pppm_step scene by scene"},
+        "batched_over_sequential": round(value / seq_value, 3), "listeners_bit_identical": bool(same),
+        "cpu_baseline": None, "e2e": None, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
 # ---------------------------------------------------------------- adjoint -------------
 ADJ_NAME = ("moving-scene geometry held static at res 48 (5120-tri perturbed sphere + 1280-tri plate), "
             "4000 steps, loss ||s - s_target||^2, gradient w.r.t. every acceleration (FP32)")
@@ -881,6 +1003,8 @@ def run_reference(args, ws, rank, local):
     if args.workload == "adjoint":
         return {"impl": "reference", "metric": "adjoint / forward cost, %s" % ADJ_NAME,
                 "unavailable": "the reference has no adjoint"}
+    if args.workload == "large-batch":
+        return run_reference_large_batch(args)
     wl = Workload(args.workload, None if args.workload != "large" else W + K + 1)
     sc = wl.scene
     from oracle import oracle as O
@@ -977,6 +1101,64 @@ def run_reference(args, ws, rank, local):
             "e2e": {"value": round(value, 5), "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "reference_ndebug": ndebug, "native_libraries_of_this_repo_mapped": mapped}
+
+
+def run_reference_large_batch(args):
+    """The reference solver on the four large scenes, scene by scene within each motion frame
+    (update_mesh + the frame's steps), over the same timed frames as the batched arm."""
+    from oracle import oracle as O
+
+    line = {"impl": "reference", "metric": "Gcell-steps/s, %s" % LARGE_BATCH_NAME, "unit": "Gcell-steps/s"}
+    if not O.reference_available():
+        line["unavailable"] = "reference solver not built (oracle/_ref)"
+        return line
+    import torch
+
+    W, K = args.warmup, args.steps
+    nfr = W + K + 1
+    scs = [scenes.LargeScene(seed=23 + 100 * i) for i in range(LARGE_BATCH)]
+    ranges = [scenes.frame_ranges(sc, nfr) for sc in scs]
+    accs = [torch.from_numpy(sc.acc(0, r[-1][1])).cuda() for sc, r in zip(scs, ranges)]
+    refs = []
+    for sc in scs:
+        r = O.Reference(sc.res, sc.h, sc.dt, sc.min_pos)
+        r.set_mesh(sc.frame_verts(0), sc.tris)
+        refs.append(r)
+    try:
+        dt, steps = 0.0, 0
+        for f in range(0, W + K + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n = 0
+            for i, (sc, r) in enumerate(zip(scs, refs)):
+                if f:
+                    r.update_mesh(sc.frame_verts(f))
+                a, e = ranges[i][f]
+                r.run_device(accs[i].data_ptr() + a * len(sc.tris) * 4, e - a, sc.listener)
+                n += e - a
+            torch.cuda.synchronize()
+            if f > W:
+                dt += time.perf_counter() - t0
+                steps += n
+    finally:
+        for r in refs:
+            r.close()
+    value = float(scs[0].res) ** 3 * steps / dt / 1e9
+    mapped = own_library_mapped()
+    if mapped:
+        raise RuntimeError("reference arm has this repository's library mapped: %s" % mapped)
+    line.update({"value": round(value, 5), "n_gpus": 1, "steps": K, "warmup": W, "higher_is_better": True,
+                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                 "data": "synthetic (seeded meshes, trajectories and accelerations)",
+                 "config": {"workload": LARGE_BATCH_NAME, "scenes": LARGE_BATCH, "res": scs[0].res,
+                            "triangles_per_scene": int(len(scs[0].tris)),
+                            "bench_step": "one motion frame of all scenes, scene by scene"},
+                 "cpu_baseline": {"value": round(value, 5), "unit": "Gcell-steps/s", "cores": 1, "kind": "reference",
+                                  "sample": "reference CUDA solver built from source, the four scenes one after "
+                                            "another within each frame, %d frames" % K},
+                 "e2e": {"value": round(value, 5), "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    return line
 
 
 def run_reference_batch(args):
@@ -1078,6 +1260,8 @@ def main():
         line = run_batch(args, ws, rank, local)
     elif args.workload == "adjoint":
         line = run_adjoint(args, ws, rank, local)
+    elif args.workload == "large-batch":
+        line = run_large_batch(args, ws, rank, local)
     else:
         line = run_ours(args, ws, rank, local)
     if rank == 0 and line is not None:

@@ -256,6 +256,10 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
 #define PPPM_OPT_FACE_THREADS 1 /* threads per block of the face-stage kernels: 64, 128, 256    */
 #define PPPM_OPT_TERMS_PAIRS 2  /* 1 (default): the triangles' grid-cache near-field terms are
                                    evaluated two steps per pass over their records; 0: per step */
+#define PPPM_OPT_SPLIT_STENCIL 3 /* 1 (default): the stencil of the corrected cells stays on the
+                                    graph's critical branch (the face and near stages read no other
+                                    cell) and the rest of the grid runs on a branch beside them;
+                                    0: one stencil launch before the face stage.  Same results.  */
 int pppm_set_option(pppm_handle *h, int option, int value);
 int pppm_get_option(pppm_handle *h, int option, int *value);
 /* No counterpart in the reference.  Autotuner of the face stage, on the current mesh and state.
@@ -306,8 +310,18 @@ int pppm_kernel_times(pppm_handle *h, float *us_stencil, float *us_face, float *
 #define PPPM_KERNEL_FACE 9    /* the fused face stage of direct launches                      */
 #define PPPM_KERNEL_EMPTY 10  /* an empty one-block kernel between the Neumann write and the first
                                  convolution: the event-to-event floor of this measurement      */
-#define PPPM_KERNEL_KINDS 11
+#define PPPM_KERNEL_STENCIL_BULK 11 /* the split stencil: every cell but the corrected ones     */
+#define PPPM_KERNEL_STENCIL_CORR 12 /* the split stencil: the corrected cells                   */
+#define PPPM_KERNEL_KINDS 13
 int pppm_kernel_profile(pppm_handle *h, int nkinds, float *us_per_launch, long long *launches);
+/* No counterpart in the reference.  Duration of each step kernel kind on the current mesh and
+ * state: reps back-to-back launches of the kind (those of the next step) recorded as one CUDA
+ * graph, replayed once to warm up and once between two events; us_per_launch[k] = that time / reps
+ * (the kernel plus the gap between dependent graph nodes; 0 for kinds not timed: NWRITE, EMPTY).
+ * The launches write only the next step's grid slot, history slots and scratch, and the handle
+ * rebuilds the state the next step reads afterwards, so stepping continues unchanged.  Absorbing
+ * boundary, PPPM method, mesh set; not while the handle's stream is being captured. */
+int pppm_time_kernels(pppm_handle *h, int reps, int nkinds, float *us_per_launch);
 
 #ifdef __cplusplus
 }

@@ -377,8 +377,11 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
         *h.h_step_status = 0;
     }
     if (cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h.side2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h.ev_fin, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h.ev_conv, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&h.ev_conv, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_near, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_bulk, cudaEventDisableTiming) != cudaSuccess)
     {
         set_error("cudaStreamCreate / cudaEventCreate failed");
         return fail(PPPM_ERR_CUDA);
@@ -438,8 +441,14 @@ int pppm_destroy(pppm_handle *ph)
         cudaEventDestroy(h.ev_fin);
     if (h.ev_conv)
         cudaEventDestroy(h.ev_conv);
+    if (h.ev_near)
+        cudaEventDestroy(h.ev_near);
+    if (h.ev_bulk)
+        cudaEventDestroy(h.ev_bulk);
     if (h.side)
         cudaStreamDestroy(h.side);
+    if (h.side2)
+        cudaStreamDestroy(h.side2);
     if (h.own_stream && h.stream)
         cudaStreamDestroy(h.stream);
     delete ph;
@@ -1319,6 +1328,11 @@ int pppm_set_option(pppm_handle *ph, int option, int value)
             break;
         h.terms_pairs = value != 0;
         return PPPM_OK;
+    case PPPM_OPT_SPLIT_STENCIL:
+        if (value != 0 && value != 1)
+            break;
+        h.split_stencil = value != 0;
+        return PPPM_OK;
     default:
         set_error("unknown option %d", option);
         return PPPM_ERR_ARG;
@@ -1339,6 +1353,8 @@ int pppm_get_option(pppm_handle *ph, int option, int *value)
         *value = h.face_threads;
     else if (option == PPPM_OPT_TERMS_PAIRS)
         *value = h.terms_pairs ? 1 : 0;
+    else if (option == PPPM_OPT_SPLIT_STENCIL)
+        *value = h.split_stencil ? 1 : 0;
     else
     {
         set_error("unknown option %d", option);
@@ -1379,6 +1395,24 @@ int pppm_enable_timing(pppm_handle *ph, int enable)
         ph->h.kind_us[k] = 0;
         ph->h.kind_n[k] = 0;
     }
+    return PPPM_OK;
+}
+
+int pppm_time_kernels(pppm_handle *ph, int reps, int nkinds, float *us_per_launch)
+{
+    PB_TRY(check_handle(ph));
+    if (nkinds < 0 || nkinds > PPPM_KERNEL_KINDS || (nkinds > 0 && !us_per_launch))
+        return PPPM_ERR_ARG;
+    Handle &h = ph->h;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PB_CUDA(cudaStreamIsCapturing(h.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        return PPPM_ERR_STATE;
+    float us[PPPM_KERNEL_KINDS];
+    PB_TRY(step_time_kernels(h, reps, us));
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    for (int k = 0; k < nkinds; k++)
+        us_per_launch[k] = us[k];
     return PPPM_OK;
 }
 

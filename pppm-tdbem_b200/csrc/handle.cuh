@@ -80,7 +80,9 @@ struct Handle
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t side = nullptr;                         // second branch of the recorded step graphs
+    cudaStream_t side2 = nullptr;                        // third branch: the bulk of the split stencil
     cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;     // fork / join points while recording
+    cudaEvent_t ev_near = nullptr, ev_bulk = nullptr;
     int res = 0;
     long long n_cells = 0;
     int t = -1;
@@ -171,6 +173,7 @@ struct Handle
     int conv_pairs = 1;       // recorded step graphs convolve the face pairs two steps per pass
     int face_threads = 256;   // threads per block of their face-stage kernels (step_autotune)
     bool terms_pairs = true;  // ... and the grid-cache near-field terms two steps per pass
+    bool split_stencil = true;  // ... and the stencil split into corrected cells and the bulk
 
     // ---- listeners
     std::vector<int> listen_xyz;
@@ -194,9 +197,12 @@ struct Handle
     double kind_us[PPPM_KERNEL_KINDS] = {};
     long long kind_n[PPPM_KERNEL_KINDS] = {};
     static constexpr int kProfileSteps = 4;
-    static constexpr int kProfileEvents = 3 + 4 * kProfileSteps;  // Neumann write, empty, 4 kernels per step, end
+    // Neumann write, empty kernel, up to 5 kernels per step (convolution, bulk and corrected-cell
+    // stencil, finish, near), end
+    static constexpr int kProfileEvents = 3 + 5 * kProfileSteps;
     cudaEvent_t evk[kProfileEvents] = {};
     int evk_kind[kProfileEvents] = {};
+    int evk_used = 0;  // event marks of the recorded profile graph
     StepGraph profile_graph;  // kProfileSteps split-stage steps with events between the kernels
 
     // ---- step launches
@@ -205,6 +211,7 @@ struct Handle
     StepGraph timing_graph;  // one step with event records between its kernels (measurement mode)
     int graph_next = 0;
     int near_blocks = 0;  // resident grid of the near kernel
+    int batch_near_cells = 0;  // corrected cells the batch block map covers (grow-only, step.cu)
 
     // ---- ghost-cell method (ghost.cu)
     struct Ghost *ghost = nullptr;
@@ -280,6 +287,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 // step.cu
 int step_prime(Handle &h);
 int step_autotune(Handle &h, int reps, float *us, int *best);
+int step_time_kernels(Handle &h, int reps, float *us);  // us: PPPM_KERNEL_KINDS entries
 int gc_factors(Handle &h);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state

@@ -37,6 +37,7 @@ struct StepArgs
     int res;
     double lap_coef;     // (c dt)^2 in double, reference arithmetic
     double hd;           // h in double
+    double h2, rh2;      // h^2 in double and its correctly rounded reciprocal (leapfrog)
     float c, dt, h;
     int pml_width;
     float damp;
@@ -151,9 +152,13 @@ __device__ inline R abc_cell(R *cur, const R *prev, int res, int x, int y, int z
 }
 
 // interior leapfrog (fdtd.cu:7-33): float storage, double arithmetic, "6 * p" in the
-// storage precision; the neighbours summed in the reference's order (x-1, x+1, y-1, y+1, z-1, z+1)
+// storage precision; the neighbours summed in the reference's order (x-1, x+1, y-1, y+1, z-1, z+1).
+// The division by h^2 is Markstein's correction of a product with the correctly rounded
+// reciprocal (P. Markstein, IBM J. Res. Dev. 34(1), 1990: with r = RN(1/d), q = RN(a r) and the
+// exact remainder a - d q from an FMA, RN(q + (a - d q) r) = RN(a / d)), so the quotient is the
+// one the reference's division rounds to, without a division per cell.
 template <typename R>
-__device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, double coefd, double hd)
+__device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, double coefd, double h2, double rh2)
 {
     double sum = 0;
     sum += xm;
@@ -163,7 +168,8 @@ __device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, 
     sum += zm;
     sum += zp;
     sum -= 6 * pc;
-    double lap = sum / (hd * hd);
+    const double q = sum * rh2;
+    const double lap = fma(fma(-q, h2, sum), rh2, q);
     double p = 2 * pc;
     p += coefd * lap;
     p += -pprev;
@@ -173,27 +179,54 @@ __device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, 
 // Work split of the stencil launch into three block ranges so no warp mixes the short
 // interior update with the long boundary solve; the boundary blocks come first, so they are
 // scheduled first and their long solves overlap the interior blocks instead of trailing them:
-//   [0, nb_bd)              boundary-layer cells (a coordinate equal to 1 or res-2)
-//   [nb_bd, nb_bd + nb_in)  interior cells [2, res-3]^3, consecutive threads along z
+//   [0, nb_bd)              boundary-layer cells (a coordinate equal to 1 or res-2), 256 per block
+//   [nb_bd, nb_bd + nb_in)  interior cells [2, res-3]^3 by x plane: a block covers zlen (a power of
+//                           two, at most 256) consecutive z of 256 / zlen consecutive y rows, so
+//                           threads find their cell without a division
 //   the rest                Neumann ring write, one thread per triangle
+// skip_corrected: the bulk of a split step (corrected cells are left to stencil_corr_kernel).
+// The tiles of a plane are counted in powers of two (blocks past the last tile exit at once), so a
+// block finds its plane and tile by shifts.
 struct StencilSplit
 {
     int nb_in, nb_bd, nb_nt;
+    int zlog;              // log2 of the threads along z of an interior block
+    int ytlog, ztlog;      // log2 of the interior blocks per x plane along y and along z
+    int skip_corrected;
 };
+
+inline int ceil_log2(long long v)
+{
+    int l = 0;
+    while ((1ll << l) < v)
+        l++;
+    return l;
+}
 
 inline StencilSplit stencil_split(int res, int nt)
 {
     long long mi = res - 4, m = res - 2;
-    long long n_in = mi * mi * mi;
     long long n_bd = 2 * m * m + 2 * (m - 2) * m + 2 * (m - 2) * (m - 2);
-    return StencilSplit{div_up(n_in, 256), div_up(n_bd, 256), div_up(nt, 256)};
+    StencilSplit sp{};
+    sp.zlog = std::min(std::max(ceil_log2(mi), 5), 8);
+    sp.ztlog = ceil_log2(div_up(mi, 1 << sp.zlog));
+    sp.ytlog = ceil_log2(div_up(mi, 256 >> sp.zlog));
+    sp.nb_in = (int)(mi << (sp.ytlog + sp.ztlog));
+    sp.nb_bd = div_up(n_bd, 256);
+    sp.nb_nt = div_up(nt, 256);
+    sp.skip_corrected = 0;
+    return sp;
+}
+
+__device__ inline bool is_corrected(const unsigned *corr_mask, long long c)
+{
+    return (corr_mask[c >> 5] >> (c & 31)) & 1u;
 }
 
 template <typename R>
-__device__ inline void finish_cell(const StepArgs &a, long long row, long long c, R v, R *next,
-                                   const unsigned *corr_mask, R *series)
+__device__ inline void finish_cell(const StepArgs &a, long long row, long long c, R v, R *next, bool corrected,
+                                   R *series)
 {
-    const bool corrected = (corr_mask[c >> 5] >> (c & 31)) & 1u;
     if (corrected)
     {
         R corr = next[c];
@@ -208,6 +241,17 @@ __device__ inline void finish_cell(const StepArgs &a, long long row, long long c
                 series[row * a.n_listen + l] = v;
                 flag_nonfinite(a.status, v);
             }
+}
+
+// the stencil at interior cell (x, y, z)
+template <typename R>
+__device__ inline R interior_cell(const StepArgs &a, const R *__restrict__ cur, const R *__restrict__ prev,
+                                  long long c)
+{
+    const int res = a.res;
+    const long long sx = (long long)res * res;
+    return leapfrog<R>(cur[c], cur[c - sx], cur[c + sx], cur[c - res], cur[c + res], cur[c - 1], cur[c + 1], prev[c],
+                       a.lap_coef, a.h2, a.rh2);
 }
 
 // the stencil work of block b of one scene's stencil grid (256 threads)
@@ -226,23 +270,29 @@ __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, cons
             return;
         int x, y, z;
         boundary_cell(i, res, x, y, z);
+        const long long c = ((long long)x * res + y) * res + z;
+        const bool corrected = is_corrected(corr_mask, c);
+        if (sp.skip_corrected && corrected)
+            return;
         R v = abc_cell<R>(cur, prev, res, x, y, z, (R)a.c, (R)a.dt, (R)a.h);
-        finish_cell<R>(a, dy.row, ((long long)x * res + y) * res + z, v, next, corr_mask, series);
+        finish_cell<R>(a, dy.row, c, v, next, corrected, series);
         return;
     }
     b -= sp.nb_bd;
     if (b < sp.nb_in)
     {
         const int mi = res - 4;
-        int i = b * 256 + threadIdx.x;
-        if (i >= mi * mi * mi)
+        const int plane = b >> (sp.ytlog + sp.ztlog), r = b & ((1 << (sp.ytlog + sp.ztlog)) - 1);
+        const int yt = r >> sp.ztlog, zt = r & ((1 << sp.ztlog) - 1);
+        const int z = 2 + (zt << sp.zlog) + (threadIdx.x & ((1 << sp.zlog) - 1));
+        const int y = 2 + (yt << (8 - sp.zlog)) + (threadIdx.x >> sp.zlog);
+        if (z >= 2 + mi || y >= 2 + mi)
             return;
-        int x = 2 + i / (mi * mi), r = i % (mi * mi);
-        int y = 2 + r / mi, z = 2 + r % mi;
-        const long long c = ((long long)x * res + y) * res + z, sx = (long long)res * res;
-        R v = leapfrog<R>(cur[c], cur[c - sx], cur[c + sx], cur[c - res], cur[c + res], cur[c - 1], cur[c + 1], prev[c],
-                          a.lap_coef, a.hd);
-        finish_cell<R>(a, dy.row, c, v, next, corr_mask, series);
+        const long long c = ((long long)(2 + plane) * res + y) * res + z;
+        const bool corrected = is_corrected(corr_mask, c);
+        if (sp.skip_corrected && corrected)
+            return;
+        finish_cell<R>(a, dy.row, c, interior_cell<R>(a, cur, prev, c), next, corrected, series);
         return;
     }
     b -= sp.nb_in;
@@ -257,6 +307,34 @@ __global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ St
                                                        StencilSplit sp, const unsigned *corr_mask, R *series)
 {
     stencil_body<R>(a0, ring, bind_step(st, k, a0.nt), blockIdx.x, sp, corr_mask, series);
+}
+
+// The stencil at the corrected cells only (the split step's critical branch: the face stage reads
+// the far field at the triangles' trilinear corners, which all lie in the 3^3 blocks of the
+// triangles' cells, i.e. at corrected cells).  Threads stride over the corrected-cell list (its
+// length is read from the step state); the arithmetic per cell is that of stencil_body.
+template <typename R>
+__global__ void __launch_bounds__(256) stencil_corr_kernel(const __grid_constant__ StepArgs a0,
+                                                            const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                            int k, const int *n3_cell)
+{
+    const StepDyn dy = bind_step(st, k, a0.nt);
+    R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
+    const R *prev = ring.slot(dy.tnew - 2);
+    const int res = a0.res, n3 = st->n3;
+    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < n3; ci += gridDim.x * blockDim.x)
+    {
+        const int c = n3_cell[ci];
+        const int x = c / (res * res), y = (c / res) % res, z = c % res;
+        R v;
+        if (x == 1 || x == res - 2 || y == 1 || y == res - 2 || z == 1 || z == res - 2)
+            v = abc_cell<R>(cur, prev, res, x, y, z, (R)a0.c, (R)a0.dt, (R)a0.h);
+        else if (x >= 2 && x < res - 2 && y >= 2 && y < res - 2 && z >= 2 && z < res - 2)
+            v = interior_cell<R>(a0, cur, prev, c);
+        else
+            continue;  // the ghost layer holds no unknown of the stencil
+        next[c] = v - next[c];  // the FDTD-near correction the near stage left in this slot
+    }
 }
 
 // split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
@@ -926,6 +1004,8 @@ StepArgs make_args(Handle &h)
     double cd = h.prm.c, dtd = h.prm.dt;
     a.lap_coef = cd * cd * dtd * dtd;
     a.hd = h.prm.dl;
+    a.h2 = a.hd * a.hd;
+    a.rh2 = 1.0 / a.h2;
     a.pml_width = h.prm.pml_width;
     a.damp = 2.0f / h.prm.dl;
     a.nt = h.mesh_set ? h.nt : 0;
@@ -968,6 +1048,8 @@ struct StepLaunch
     int pairs;         // pipelined graphs convolve the face pairs for two steps per pass (conv2 + fix)
     int face_threads;  // threads per block of the pipelined face-stage kernels
     int tpairs;        // the near-field terms two steps per pass (near_terms2)
+    int split;         // recorded graphs: corrected-cell stencil on the main branch, the bulk beside it
+    int corr_blocks;   // grid of stencil_corr_kernel (threads stride over the corrected cells)
     int mesh, pml, pml_blocks, stencil_blocks, face_blocks, near_blocks;
     int ghost;     // ghost-cell method: the ghost kernel after the stencil instead of face / near
     GhostStep gs;  // its arguments
@@ -1027,6 +1109,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.pairs = h.conv_pairs;
         L.face_threads = h.face_threads;
         L.tpairs = h.terms_pairs ? 1 : 0;
+        L.split = h.split_stencil ? 1 : 0;
         L.fa.face_d1 = (const R *)h.d_face_d1;
         L.fa.order = h.d_base_tris;
         L.fa.dlast = (R *)h.d_dlast;
@@ -1048,6 +1131,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
             h.near_blocks = std::max(per_sm, 1) * std::max(sms, 1);
         }
         L.near_blocks = h.near_blocks;
+        L.corr_blocks = std::max(1, h.near_blocks / 4);
     }
     return PPPM_OK;
 }
@@ -1083,23 +1167,36 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
     mark(3);
 }
 
-// The kernels of nsteps steps as a two-branch graph (absorbing boundary with a mesh).  Per step:
+// The kernels of nsteps steps as a multi-branch graph (absorbing boundary with a mesh).  Per step:
 //   side   conv(k)                       after finish(k-1): needs D[t-1] and N[t]
 //   main   stencil(k) -> finish(k) -> near(k)   finish waits for conv(k) too
 // so each step's face-pair convolution (the heavy part of the face stage) runs beside the
 // previous step's near stage and this step's stencil; finish(k) also writes N[t+1] for conv(k+1).
 // With pair set, steps go in pairs (k, k+1): conv2(k) streams the face pairs once for both steps
 // and fix(k+1), after finish(k), adds the one term of step k+1 that needs D of step k.
-// Only used under stream capture: main = h.stream, side = h.side, joined back before the end.
+// With the split stencil (L.split), the main branch computes only the corrected cells
+// (stencil_corr_kernel: the face stage and the near stage read and write nothing else) and a
+// third branch the rest of the grid:
+//   bulk   stencil(k) without corrected cells   after near(k-1): p^t complete at corrected cells
+//   main   corr(k) -> finish(k) -> near(k)       corr(k) after bulk(k-1): p^t complete elsewhere
+// The bulk writes p^{t+1} at other cells than the main branch reads or writes in the meantime (the
+// near stage's next-step sums go to corrected cells of slot t+2 = t-1, which the bulk reads only
+// elsewhere), so it leaves the step's critical path.  Only used under stream capture: main =
+// h.stream, side = h.side, bulk = h.side2, joined back before the end.
 template <typename R>
 void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
 {
     const int T = 256, FT = L.face_threads;
     const int nt = L.a.nt;
     const int wblocks = div_up((long long)nt * 32, FT);
-    cudaStream_t s = h.stream, side = h.side;
+    cudaStream_t s = h.stream, side = h.side, bulk = h.side2;
+    const bool split = L.split && bulk;
+    StencilSplit bsp = L.sp;
+    bsp.skip_corrected = 1;
     nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
     cudaEventRecord(h.ev_fin, s);
+    if (split)
+        cudaEventRecord(h.ev_near, s);
     for (int k = 0; k < nsteps; k++)
     {
         cudaStreamWaitEvent(side, h.ev_fin, 0);
@@ -1110,8 +1207,20 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
         else
             conv_kernel<R><<<wblocks, FT, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv);
         cudaEventRecord(h.ev_conv, side);
-        // the stencil without its Neumann block range (finish / nwrite wrote N[t])
-        stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
+        if (split)
+        {
+            if (k > 0)
+                cudaStreamWaitEvent(s, h.ev_bulk, 0);  // bulk(k-1)
+            cudaStreamWaitEvent(bulk, h.ev_near, 0);   // near(k-1), or the call's start
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, bulk>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask,
+                                                                     L.series);
+            cudaEventRecord(h.ev_bulk, bulk);
+            stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na.n3_cell);
+        }
+        else
+            // the stencil without its Neumann block range (finish / nwrite wrote N[t])
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask,
+                                                                  L.series);
         cudaStreamWaitEvent(s, h.ev_conv, 0);
         // the call's last step computes its terms in one pass (mode 0): the FDTD-near sums it
         // leaves for the next call are then exactly those that prime() rebuilds after a state
@@ -1126,7 +1235,11 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
             finish_kernel<R, 0><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
         cudaEventRecord(h.ev_fin, s);
         near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
+        if (split)
+            cudaEventRecord(h.ev_near, s);
     }
+    if (split)
+        cudaStreamWaitEvent(s, h.ev_bulk, 0);
 }
 
 
@@ -1154,7 +1267,13 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
     const bool pair = L.pairs != 0;
     cudaStream_t s = h.stream;
     int e = 0;
+    bool overflow = false;
     auto mark = [&](int kind) {
+        if (e >= Handle::kProfileEvents)
+        {
+            overflow = true;
+            return;
+        }
         h.evk_kind[e] = kind;
         cudaEventRecordWithFlags(h.evk[e++], s, cudaEventRecordExternal);
     };
@@ -1181,8 +1300,21 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
             mark(PPPM_KERNEL_CONV);
             conv_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv);
         }
-        mark(PPPM_KERNEL_STENCIL);
-        stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
+        if (L.split)
+        {
+            StencilSplit bsp = L.sp;
+            bsp.skip_corrected = 1;
+            mark(PPPM_KERNEL_STENCIL_BULK);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask, L.series);
+            mark(PPPM_KERNEL_STENCIL_CORR);
+            stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na.n3_cell);
+        }
+        else
+        {
+            mark(PPPM_KERNEL_STENCIL);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask,
+                                                                  L.series);
+        }
         const int mode = L.tpairs && k + 1 < n ? ((k & 1) ? 2 : 1) : 0;
         const int nx = k + 1 < n ? 1 : 0;
         if (mode == 1)
@@ -1205,10 +1337,17 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
     }
     mark(-1);
     cudaError_t err = cudaStreamEndCapture(s, &graph);
-    if (err == cudaSuccess)
+    if (err == cudaSuccess && !overflow)
         err = cudaGraphInstantiate(&g.exec, graph, 0);
     if (graph)
         cudaGraphDestroy(graph);
+    h.evk_used = overflow ? 0 : e;
+    if (overflow)
+    {
+        g.exec = nullptr;
+        set_error("profile graph: more event marks than its %d slots", Handle::kProfileEvents);
+        return PPPM_ERR_STATE;
+    }
     if (err != cudaSuccess)
     {
         g.exec = nullptr;
@@ -1309,8 +1448,8 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
                 set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sk);
                 PB_CHECK_LAUNCH();
                 PB_CUDA(cudaGraphLaunch(pexec, s));
-                PB_CUDA(cudaEventSynchronize(h.evk[Handle::kProfileEvents - 1]));
-                for (int i = 0; i + 1 < Handle::kProfileEvents; i++)
+                PB_CUDA(cudaEventSynchronize(h.evk[h.evk_used - 1]));
+                for (int i = 0; i + 1 < h.evk_used; i++)
                 {
                     float ms = 0;
                     cudaEventElapsedTime(&ms, h.evk[i], h.evk[i + 1]);
@@ -1327,7 +1466,7 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
                         h.us_face += 1000 * ms;
                 }
                 h.timed_steps += n;
-                h.launches += 2 + 4 * n - per_step * n;  // per_step * nsteps is added below
+                h.launches += 2 + (4 + L.split - per_step) * n;  // per_step * nsteps is added below
             }
         }
         cudaGraphExec_t exec = nullptr;
@@ -1368,6 +1507,10 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
         cudaGraphExec_t exec = nullptr;
         PB_TRY(graph_for<R>(h, L, nsteps, &exec));
         PB_CUDA(cudaGraphLaunch(exec, s));
+        // the pipelined graph launches the Neumann write, then per step the convolution, the
+        // stencil (and its bulk), finish and near: counted here in place of per_step below
+        if (L.mesh && !L.pml && h.side)
+            h.launches += 1 + (4 + L.split - per_step) * (long long)nsteps;
     }
     else
         for (int k = 0; k < nsteps; k++)
@@ -1658,7 +1801,135 @@ int hist_copy(Handle &h, int to_copies)
     return PPPM_OK;
 }
 
+// Per-kernel timing on the current mesh and state: for each step kernel kind, reps back-to-back
+// launches recorded as one CUDA graph, replayed once to warm up and once between two events, so a
+// launch is timed the way it runs inside the recorded step graphs (its duration plus the gap
+// between dependent graph nodes) without event nodes between the kernels.  The launches are those
+// of the step after the current time and write only that step's grid slot, history slots and
+// scratch sums (listener recording off); prime() then rebuilds the correction that slot must hold,
+// so stepping continues as if nothing had run.
+template <typename R>
+int time_kernels(Handle &h, int reps, float *us)
+{
+    if (!h.mesh_set || h.prm.method != PPPM_METHOD_PPPM || h.nt == 0 || h.prm.pml_width > 0)
+    {
+        set_error("kernel timing needs a mesh (PPPM method, absorbing boundary)");
+        return PPPM_ERR_STATE;
+    }
+    if (reps < 1)
+        return PPPM_ERR_ARG;
+    if (!h.d_state)
+        PB_TRY(dalloc(&h.d_state, 1));
+    cudaStream_t s = h.stream;
+    StepState stt{h.t + 1, h.n3, 0, nullptr};
+    set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
+    h.launches++;
+    StepLaunch<R> L;
+    PB_TRY(make_launch<R>(h, L));
+    L.a.n_listen = 0;
+    L.na.series = nullptr;
+    L.series = nullptr;
+    const int T = 256, FT = L.face_threads, nt = L.a.nt;
+    const int wblocks = div_up((long long)nt * 32, FT);
+    for (int k = 0; k < PPPM_KERNEL_KINDS; k++)
+        us[k] = 0;
+    auto launch = [&](int kind) {
+        switch (kind)
+        {
+        case PPPM_KERNEL_STENCIL:
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, L.sp, L.corr_mask, L.series);
+            break;
+        case PPPM_KERNEL_CONV: conv_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv); break;
+        case PPPM_KERNEL_CONV2:
+            conv2_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, L.conv1);
+            break;
+        case PPPM_KERNEL_FIX: fix_kernel<R><<<wblocks, FT, 0, s>>>(nt, L.fa, L.conv1, L.conv); break;
+        case PPPM_KERNEL_FINISH:
+            finish_kernel<R, 0><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, 0);
+            break;
+        case PPPM_KERNEL_FINISH1:
+            finish_kernel<R, 1><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, 0);
+            break;
+        case PPPM_KERNEL_FINISH2:
+            finish_kernel<R, 2><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv, 0);
+            break;
+        case PPPM_KERNEL_NEAR: near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, 0, L.na, 0); break;
+        case PPPM_KERNEL_FACE: face_kernel<R><<<L.face_blocks, T, 0, s>>>(L.a, L.ring, L.st, 0, L.fa); break;
+        case PPPM_KERNEL_STENCIL_BULK:
+        {
+            StencilSplit bsp = L.sp;
+            bsp.skip_corrected = 1;
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, bsp, L.corr_mask, L.series);
+            break;
+        }
+        case PPPM_KERNEL_STENCIL_CORR:
+            stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, 0, L.na.n3_cell);
+            break;
+        default: break;
+        }
+    };
+    const int kinds[] = {PPPM_KERNEL_STENCIL,      PPPM_KERNEL_CONV,         PPPM_KERNEL_CONV2,
+                         PPPM_KERNEL_FIX,          PPPM_KERNEL_FINISH,       PPPM_KERNEL_FINISH1,
+                         PPPM_KERNEL_FINISH2,      PPPM_KERNEL_NEAR,         PPPM_KERNEL_FACE,
+                         PPPM_KERNEL_STENCIL_BULK, PPPM_KERNEL_STENCIL_CORR};
+    // the near kernel also writes the FDTD-near sums of the step after next into the slot two
+    // ahead, which is time t-1, a level the next step still reads: kept aside and put back
+    const size_t slot_bytes = (size_t)h.n_cells * sizeof(R);
+    void *keep = nullptr;
+    PB_TRY(dev_alloc(&keep, slot_bytes));
+    struct Free
+    {
+        void *p;
+        ~Free() { dev_free(p); }
+    } free_keep{keep};
+    PB_CUDA(cudaMemcpyAsync(keep, h.slot(h.t - 1), slot_bytes, cudaMemcpyDeviceToDevice, s));
+    for (int kind : kinds)
+    {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < reps; r++)
+            launch(kind);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph)
+            cudaGraphDestroy(graph);
+        if (e == cudaSuccess)
+            e = cudaGraphLaunch(exec, s);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(h.ev[0], s);
+        if (e == cudaSuccess)
+            e = cudaGraphLaunch(exec, s);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(h.ev[1], s);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(h.ev[1]);
+        float ms = 0;
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, h.ev[0], h.ev[1]);
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (e != cudaSuccess)
+        {
+            set_error("kernel timing failed: %s", cudaGetErrorString(e));
+            return PPPM_ERR_CUDA;
+        }
+        us[kind] = 1000.0f * ms / reps;
+        h.launches += 2ll * reps;
+    }
+    PB_CUDA(cudaMemcpyAsync(h.slot(h.t - 1), keep, slot_bytes, cudaMemcpyDeviceToDevice, s));
+    PB_TRY(prime<R>(h));
+    PB_CUDA(cudaStreamSynchronize(s));  // the kept slot is freed on return
+    return PPPM_OK;
+}
+
 }  // namespace
+
+int step_time_kernels(Handle &h, int reps, float *us)
+{
+    return h.fp64 ? time_kernels<double>(h, reps, us) : time_kernels<float>(h, reps, us);
+}
 
 int hist_import(Handle &h) { return h.fp64 ? hist_copy<double>(h, 1) : hist_copy<float>(h, 1); }
 int hist_export(Handle &h) { return h.fp64 ? hist_copy<double>(h, 0) : hist_copy<float>(h, 0); }
@@ -1915,7 +2186,12 @@ int batch_tables(Batch &b, const std::vector<int> &active)
         S.st = h.d_state;
         S.conv = L.conv;
         S.conv1 = L.conv1;
-        const int near_blocks = std::max(1, div_up((long long)h.n3 * 32, T));
+        // near-stage warps stride over the scene's corrected cells (their count is read on the
+        // device), so the block map may exceed it: it grows with headroom and never shrinks, so a
+        // moving scene, whose count changes at every update_mesh, keeps its recorded batch graphs
+        if (h.n3 > h.batch_near_cells)
+            h.batch_near_cells = h.n3 + h.n3 / 8 + 256;
+        const int near_blocks = std::max(1, div_up((long long)h.batch_near_cells * 32, T));
         S.near_warps = near_blocks * (T / 32);
         memcpy(b.host_scenes.data() + ai * sizeof(S), &S, sizeof(S));
         for (int k = 0; k < L.stencil_blocks; k++)

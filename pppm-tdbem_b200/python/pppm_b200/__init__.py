@@ -98,6 +98,7 @@ def _load():
         "pppm_kernel_times": [vp, fp, fp, fp, ip],
         "pppm_kernel_profile": [vp, i, fp, ctypes.POINTER(ctypes.c_longlong)],
         "pppm_sync": [vp],
+        "pppm_time_kernels": [vp, i, i, fp],
     }
     fl = ctypes.c_float
     sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
@@ -455,7 +456,7 @@ class Solver:
         check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
         return v.value
 
-    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2}
+    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2, "split_stencil": 3}
     TUNE_CANDIDATES = [(pairs, threads) for pairs in (0, 1) for threads in (64, 128, 256)]
     TUNE_CONFIGS = [(pairs, threads, terms) for pairs in (0, 1) for threads in (64, 128, 256) for terms in (0, 1)]
 
@@ -491,7 +492,7 @@ class Solver:
         check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")
 
     KERNEL_KINDS = ("stencil", "conv", "conv2", "fix", "finish", "finish1", "finish2", "near", "nwrite", "face",
-                    "empty")
+                    "empty", "stencil_bulk", "stencil_corr")
 
     def kernel_profile(self):
         """{kind: (mean us per launch, launches)} of the kernels timed in measurement mode
@@ -501,6 +502,15 @@ class Solver:
         cnt = (ctypes.c_longlong * n)()
         check(lib.pppm_kernel_profile(self.h, n, us, cnt), "kernel_profile")
         return {k: (float(us[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_KINDS) if cnt[i]}
+
+    def time_kernels(self, reps=20):
+        """{kind: us per launch} of every step kernel kind on the current mesh and state
+        (pppm_time_kernels: reps back-to-back launches in one recorded graph); stepping continues
+        unchanged afterwards."""
+        n = len(self.KERNEL_KINDS)
+        us = (ctypes.c_float * n)()
+        check(lib.pppm_time_kernels(self.h, int(reps), n, us), "time_kernels")
+        return {k: float(us[i]) for i, k in enumerate(self.KERNEL_KINDS) if us[i] > 0}
 
     def kernel_times(self):
         a, b, c, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_int()

@@ -17,10 +17,11 @@ from pppm_b200 import Solver
 pytestmark = pytest.mark.gpu
 
 
-def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None):
+def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None, split=1):
     v0, f, h, mn, dt = sphere_small()
     res = 24
     s = Solver(res, h, dt, mn, precision=precision)
+    s.set_option("split_stencil", split)
     s.set_option("conv_pairs", pairs)
     s.set_option("terms_pairs", (1 if pairs else 0) if terms is None else terms)
     s.set_option("face_threads", threads)
@@ -128,3 +129,67 @@ def test_bad_options_rejected(gpu):
     with pytest.raises(PPPMError):
         s.autotune()  # no mesh yet
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_kernel_timing_leaves_the_run_unchanged(gpu, precision):
+    """pppm_time_kernels between two step calls (each kernel kind of the next step launched back
+    to back, then the state the next step reads rebuilt): the series and fields are bit-identical
+    to the same run without it, and every kind gets a positive duration."""
+    v0, f, h, mn, dt = sphere_small()
+    acc = sine_acc(120, len(f), 1500.0, dt)
+    out = []
+    for timed in (False, True):
+        s = Solver(24, h, dt, mn, precision=precision)
+        s.set_mesh(v0, f)
+        s.add_listener(20, 20, 20)
+        s.step(acc[:60])
+        if timed:
+            t = s.time_kernels(5)
+            for k in ("stencil", "conv", "conv2", "fix", "finish", "finish1", "finish2", "near", "face"):
+                assert t.get(k, 0) > 0, (k, t)
+        s.step(acc[60:])
+        out.append((s.listeners(), s.grid(0), s.grid(-1), s.dump("dirichlet")))
+        s.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_split_stencil_is_bit_identical(gpu, precision):
+    """The corrected-cell stencil on the critical branch plus the bulk beside it computes every cell
+    with the same arithmetic as one stencil launch: series bit-identical, across motion frames and
+    call lengths that leave single steps."""
+    for moving in (False, True):
+        a = _series(precision, 1, steps=150, chunk=23, moving=moving, split=0)
+        b = _series(precision, 1, steps=150, chunk=23, moving=moving, split=1)
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_measurement_mode_profiles_every_kernel(gpu, split):
+    """Measurement mode (pppm_enable_timing) with the split face stage: groups of four steps replay
+    the recorded graph's kernels serialised with events between them; every kind is counted once
+    per launch and timed, and the run stays finite."""
+    v0, f, h, mn, dt = sphere_small()
+    s = Solver(24, h, dt, mn)
+    s.set_option("split_stencil", split)
+    s.set_option("conv_pairs", 1)
+    s.set_option("terms_pairs", 1)
+    s.set_mesh(v0, f)
+    s.add_listener(20, 20, 20)
+    s.enable_timing(True)
+    s.step(sine_acc(42, len(f), 1500.0, dt))  # 10 groups of 4 steps, then 2 steps of the fused kernels
+    prof = s.kernel_profile()
+    s.enable_timing(False)
+    assert np.all(np.isfinite(s.listeners()))
+    s.close()
+    n = {k: c for k, (us, c) in prof.items()}
+    assert all(us > 0 for us, c in prof.values()), prof
+    if split:
+        assert n["stencil_bulk"] == 40 and n["stencil_corr"] == 40 and n["stencil"] == 2
+    else:
+        assert n["stencil"] == 42 and "stencil_bulk" not in n
+    assert n["conv2"] == 20 and n["fix"] == 20 and n["near"] == 42 and n["face"] == 2
+    assert n["finish1"] == 20 and n["finish2"] == 10 and n["finish"] == 10
+    assert n["nwrite"] == 10 and n["empty"] == 10
