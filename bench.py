@@ -289,9 +289,9 @@ def run_ours(args, ws, rank, local):
     nt = len(wl.tris)
     cells = float(wl.res) ** 3
 
-    def new_solver(opts=None, precision="fp32", on_stream=True):
+    def new_solver(opts=None, precision="fp32", on_stream=True, weights="ref32"):
         s = Solver(wl.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream if on_stream else None,
-                   precision=precision)
+                   precision=precision, weights=weights)
         for k, v in (opts or {}).items():
             s.set_option(k, v)
         s.set_mesh(wl.verts[0], wl.tris)
@@ -514,6 +514,33 @@ def run_ours(args, ws, rank, local):
         den = float(np.linalg.norm(ref))
         fp64_err = {"rel_l2": float(np.linalg.norm(got - ref) / den) if den > 0 else None, "time_steps": int(len(got)),
                     "reference": "the same steps in the FP64 scheme (PPPM_PRECISION_FP64) on the GPU"}
+        if wl.moving and wl.whole_run:
+            # PPPM_WEIGHTS_FP64 (singular face integrals in FP64): its refresh cost beside the default
+            # weights over the first 17 frames, and its listener error against the FP64 scheme
+            nfr = min(17, len(wl.ranges))
+            cost = {}
+            for wname in ("ref32", "fp64"):
+                sw = new_solver(opts, weights=wname)
+                upd = []
+                for f in range(nfr):
+                    a, b = wl.ranges[f]
+                    if f:
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        sw.update_mesh(verts_dev[f])
+                        e1.record(stream)
+                        e1.synchronize()
+                        upd.append(e0.elapsed_time(e1) * 1e3)
+                    sw.step(acc_dev[a:b])
+                n = wl.ranges[nfr - 1][1]
+                sv = sw.listeners(0, n)[:, 0].astype(np.float64)
+                sw.close()
+                d0 = float(np.linalg.norm(ref[:n]))
+                cost[wname] = {"update_mesh_us": round(statistics.median(upd), 1),
+                               "rel_l2_vs_fp64": float(np.linalg.norm(sv - ref[:n]) / d0) if d0 > 0 else None}
+            fp64_err["weights_fp64"] = {"frames": nfr, "time_steps": int(wl.ranges[nfr - 1][1]), **{
+                "update_mesh_us_" + k: v["update_mesh_us"] for k, v in cost.items()}, **{
+                "rel_l2_vs_fp64_" + k: v["rel_l2_vs_fp64"] for k, v in cost.items()}}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
