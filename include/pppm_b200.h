@@ -203,19 +203,35 @@ int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, in
 /* ------------------------------------------------------------ adjoint ---------------- */
 /* No counterpart in the reference.  Gradient of L = sum_s sum_l dL_dsignal[s][l] * p_l(s)
  * over nsteps consecutive forward steps with respect to those steps' accelerations,
- * dL_dacc[s][tri], with the geometry, the labels and so every weight table held as they are
- * now (the absorbing boundary; PML handles return PPPM_ERR_ARG).  The listener samples are
- * linear in the accelerations, so the gradient does not depend on the forward state and no
- * forward state is stored: the transposed step runs backwards in time on adjoint state of the
- * forward state's size.  fresh != 0 starts a new reverse sweep (the nsteps steps are the last
- * ones of the differentiated run); fresh == 0 continues the sweep the previous call left,
- * for the nsteps steps just before the ones that call covered (a long run differentiated in
- * chunks, latest chunk first).  Element type: float for FP32 handles, double for FP64
- * handles.  dL_dsignal: nsteps x nlisteners; dL_dacc: nsteps x nt; both device pointers on
- * the handle's stream when on_device != 0 (the call returns once the work is queued), else
- * host buffers (the call returns with dL_dacc written).  Listeners must lie in
- * [1, res-2]^3.  Changing the geometry between chunks of one sweep returns PPPM_ERR_STATE. */
+ * dL_dacc[s][tri], with the weight tables, lists and corrected cells the handle holds now
+ * (the absorbing boundary; PML handles return PPPM_ERR_ARG).  The listener samples are linear
+ * in the accelerations, so the gradient does not depend on the forward state and no forward
+ * state is stored: the transposed step runs backwards in time on adjoint state of the forward
+ * state's size.  fresh != 0 starts a new reverse sweep (the nsteps steps are the last ones of
+ * the differentiated run); fresh == 0 continues the sweep the previous call left, for the
+ * nsteps steps just before the ones that call covered (a long run differentiated in chunks,
+ * latest chunk first).  The adjoint state carries over a change of geometry between chunks:
+ * a moving run is differentiated motion frame by motion frame, latest first, each call with
+ * that frame's tables in the handle (pppm_save_cache_state / pppm_restore_cache_state and
+ * pppm_update_mesh rebuild them exactly).  Element type: float for FP32 handles, double for
+ * FP64 handles.  dL_dsignal: nsteps x nlisteners; dL_dacc: nsteps x nt; both device pointers
+ * on the handle's stream when on_device != 0 (the call returns once the work is queued), else
+ * host buffers (the call returns with dL_dacc written).  Listeners must lie in [1, res-2]^3. */
 int pppm_adjoint(pppm_handle *h, const void *dL_dsignal, int nsteps, int on_device, int fresh, void *dL_dacc);
+
+/* No counterpart in the reference.  The motion-frame state of the weight caches: the
+ * grid-cache records with the triangle geometry they were computed for, the face-cache table
+ * with its record pool, and the vertex positions.  A moving run's tables depend on its whole
+ * motion so far: records are recomputed only when their geometry moved past the reference's
+ * criteria (pppm_cache.h:65-70, 123-128).  Saving the state after a frame's pppm_set_mesh /
+ * pppm_update_mesh and restoring it later, followed by pppm_update_mesh with that frame's
+ * vertices (which then recomputes nothing) and with each later frame's vertices in turn,
+ * rebuilds exactly the tables those frames had: the checkpoints of a frame-by-frame adjoint
+ * (pppm_b200.autograd.moving_listener_signal).  Host buffers; a restore leaves the handle's
+ * lists stale, and pppm_step / pppm_adjoint return PPPM_ERR_STATE until pppm_update_mesh. */
+int pppm_cache_state_size(pppm_handle *h, size_t *bytes);
+int pppm_save_cache_state(pppm_handle *h, void *dst, size_t bytes);
+int pppm_restore_cache_state(pppm_handle *h, const void *src, size_t bytes);
 
 /* ------------------------------------------------------------ weight diagnostics ----- */
 /* TDBEM::init (bem.h:264-277) as this library evaluates it on the host: lambda and the 16

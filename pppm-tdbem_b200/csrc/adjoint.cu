@@ -20,27 +20,32 @@
 //                p^t[c] += 0.98 sum_{pairs (c, tr)} sum_k ab_k N[tr][t-k] + bb_k D[tr][t-k]
 //   listeners read p^t after M.
 //
-// Adjoint variables: Lambda(tau) per grid slot (tau mod 3, ghosts included), and rings over
-// time (4 shifted copies each, so a 16-tap window is 4 aligned 16-byte loads): lamF[j] (adjoint
-// of the face numerator), lamP[c] (0.98 x adjoint of the near correction), lamC[c] (adjoint of
-// the stored FDTD-near sum).  The reverse step at sigma runs five kernels:
-//   A1 cells     add dL/dseries[sigma] at the listener cells; lamP[c][sigma] = 0.98
-//                Lambda(sigma)[c]; lamC[c][sigma] = -Lambda(sigma + 1)[c]
-//   A2 faces     per triangle j, gathers over the transposed pair lists:
-//                lamF[j][sigma] = (sum_{face pairs (i, j)} sum_{k=1..15} b_k lamF[i][sigma+k]
-//                  + sum_{near pairs (c, j)} sum_{k=0..15} bb_k lamP[c][sigma+k]
-//                  + bf_k lamC[c][sigma+k]) / denom_j
-//                dL/dacc[sigma+1][j] = sum_{face pairs} sum_{k=0..15} a_k lamF[i][sigma+1+k]
-//                  + the near part of sigma + 1 (kept from the previous reverse step)
-//   A3 corners   Lambda(sigma)[cell] += reflect iw lamF[j][sigma] over the cells that are
-//                trilinear corners of some face
-//   A4 boundary  per boundary-layer cell: lam_b = A^-T (adjoints of its ghost outputs, of
-//                its own output); the ghost adjoints of Lambda(sigma - 1) are consumed
-//   A5 cells     transposed stencil as a gather over the 7 cells that read a cell:
-//                Lambda(sigma - 1) += S_cur^T; Lambda(sigma - 2) = S_prev^T (the first
-//                contribution to that slot's new time, so it overwrites the stale one)
-// After the last reverse step of a call, A2 in flush mode emits dL/dacc of the call's first
-// step.  The gathers (A2, A3, A5) need no atomics: every sum belongs to one thread or warp.
+// Adjoint variables: Lambda(tau) per grid slot (tau mod 3, ghosts included) and, per triangle,
+// two accumulation rings over time (32 slots): accN[j][tau] and accD[j][tau] collect the adjoints
+// of N[j][tau] and D[j][tau] from every later operation that read them.  Each reverse step pushes
+// its operations' adjoints into those rings with the tables of its own step only, and nothing is
+// kept per corrected cell from one step to the next, so the tables (lists, weights, corrected
+// cells, corners) may change between steps: a moving run is differentiated frame by frame with
+// each frame's tables loaded.  The reverse step at sigma runs seven kernels:
+//   P1 listeners  Lambda(sigma)[listener cell] += dL/dseries[sigma]
+//   P2 near BEM   per triangle j, over its near pairs (c, j): the BEM-near record (taps k) times
+//                 0.98 Lambda(sigma)[c] into accN/accD[j][sigma - k]; then D[j][sigma] has all its
+//                 readers: lamF[j] = accD[j][sigma] / denom_j (the adjoint of the face numerator)
+//   P3 faces      per triangle j, over the centres i whose face list holds j: the face record
+//                 (a_m, b_{m+1}) times lamF[i] into accN[j][sigma - m], accD[j][sigma - 1 - m];
+//                 then N[j][sigma] has all its readers: dL/dacc[sigma][j] = accN[j][sigma]
+//   P4 corners    Lambda(sigma)[cell] += reflect iw lamF[j] over the cells that are trilinear
+//                 corners of some face
+//   P5 near C     per triangle j, over its near pairs: the stored FDTD-near sum C^sigma (subtracted
+//                 by the stencil at step sigma, computed from the histories of sigma - 1 with the
+//                 tables of step sigma) gets -Lambda(sigma)[c]; its record (taps shifted by one)
+//                 times that into accN/accD[j][sigma - 1 - k]
+//   P6 boundary   per boundary-layer cell: lam_b = A^-T (adjoints of its ghost outputs, of
+//                 its own output); the ghost adjoints of Lambda(sigma - 1) are consumed
+//   P7 cells      transposed stencil as a gather over the 7 cells that read a cell:
+//                 Lambda(sigma - 1) += S_cur^T; Lambda(sigma - 2) = S_prev^T (the first
+//                 contribution to that slot's new time, so it overwrites the stale one)
+// The gathers (P2, P3, P4, P5, P7) need no atomics: every sum belongs to one thread or warp.
 #include <algorithm>
 #include <vector>
 #include "fdtd.cuh"
@@ -65,8 +70,8 @@ struct Adjoint
     // adjoint state
     void *lam[3] = {nullptr, nullptr, nullptr};
     void *lam_b = nullptr;  // 4 x res^3 (boundary layer only)
-    void *ring_f = nullptr, *ring_p = nullptr, *ring_c = nullptr;
-    void *nearpart = nullptr;  // nt: near part of dL/dacc of the last reverse step's time
+    void *acc_n = nullptr, *acc_d = nullptr;  // [nt][kRing] accumulation rings (slot = tau mod 32)
+    void *lam_f = nullptr;                    // [nt] adjoint of the face numerator at the current step
     int pos = 0;               // one past the next time the reverse sweep processes
     bool started = false;
     // host-call staging
@@ -130,55 +135,20 @@ struct AdjArgs
     float reflect;
     R *lam[3];
     R *lam_b;
-    R *ring_f, *ring_p, *ring_c;
-    R *nearpart;
+    R *acc_n, *acc_d, *lam_f;
     double kappa;                 // (c dt / h)^2: interior leapfrog coefficient
     R coef, coef1, coef2, coef3;  // boundary solve coefficients (fdtd.cu:88-137)
     __device__ R *slot(int tau) const { return lam[((tau % 3) + 3) % 3]; }
 };
 
-// ring copy c holds time tau at index (tau + c) mod 32: a window starting at tau0 read from copy
-// (-tau0) mod 4 starts on a multiple of 4
+// P1: the listener samples' adjoints
 template <typename R>
-__device__ inline void ring_put(R *ring, int rows, int row, int tau, R v)
+__global__ void adj_listen_kernel(const __grid_constant__ AdjArgs<R> a, int sigma, const R *g)
 {
-#pragma unroll
-    for (int c = 0; c < 4; c++)
-        ring[((long long)c * rows + row) * kRing + ((tau + c) & (kRing - 1))] = v;
-}
-
-template <typename R>
-__device__ inline const R *ring_window(const R *ring, int rows, int tau0, int q)
-{
-    const int c = (-tau0) & 3;
-    return ring + (long long)c * rows * kRing + ((tau0 + c + 4 * q) & (kRing - 1));
-}
-
-// A1: corrected cells and listener injection
-template <typename R>
-__global__ void __launch_bounds__(256) adj_cells_kernel(const __grid_constant__ AdjArgs<R> a, int sigma,
-                                                        const R *g)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    R *cur = a.slot(sigma);
-    if (i < a.n3)
-    {
-        const int c = a.n3_cell[i];
-        R v = cur[c];
-        for (int l = 0; l < a.nl; l++)
-            if (a.listen_cell[l] == c)
-                v += g[l];
-        cur[c] = v;
-        ring_put<R>(a.ring_p, a.n3, i, sigma, (R)0.98 * v);
-        ring_put<R>(a.ring_c, a.n3, i, sigma, -a.slot(sigma + 1)[c]);
-    }
-    else if (i == a.n3)
-        for (int l = 0; l < a.nl; l++)
-        {
-            const int c = a.listen_cell[l];
-            if (!((a.corr_mask[c >> 5] >> (c & 31)) & 1u))  // corrected cells: done above
-                cur[c] += g[l];
-        }
+    if (threadIdx.x != 0)
+        return;
+    for (int l = 0; l < a.nl; l++)  // one thread: listeners may share a cell
+        a.slot(sigma)[a.listen_cell[l]] += g[l];
 }
 
 template <typename R>
@@ -190,77 +160,139 @@ __device__ inline R warp_sum_adj(R v)
     return v;
 }
 
-// A2: one warp per triangle j; quad q of lane group g takes window positions 4q..4q+3 of pairs
-// g, g + 8, ...  flush != 0: only dL/dacc of time sigma + 1 (the face part) plus the kept near part
+// sums of the eight quads of a warp per lane position (lanes l, l ^ 4, ..., l ^ 28): lane q < 4 of
+// quad 0 ends with the totals of taps 4q .. 4q + 3
 template <typename R>
-__global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ AdjArgs<R> a, int sigma, R *out_row,
-                                                       int flush)
+__device__ inline void quad_totals(R (&v)[4])
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int off = 4; off < 32; off <<= 1)
+            v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
+}
+
+// the 16 taps of a near record (half = 0: FDTD-near, shifted by one tap; 1: BEM-near) of near pair p
+// times v[pair], accumulated per lane over the pairs of triangle j (quad g takes pairs g, g + 8, ...;
+// lane q taps 4q .. 4q + 3); cell_value(c) gives the factor of corrected cell c
+template <typename R, typename F>
+__device__ inline void near_push_sums(const AdjArgs<R> &a, int j, int half, int g, int q, F cell_value, R (&an)[4],
+                                      R (&ad)[4])
 {
     using W4 = typename AdjWRec<R>::W4;
-    using H4 = typename AdjWRec<R>::H4;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        an[i] = ad[i] = 0;
+    for (int p = a.nT_start[j] + g; p < a.nT_start[j + 1]; p += 8)
+    {
+        const R v = cell_value(a.n3_cell[a.nT_cell[p]]);
+        const W4 w = *(const W4 *)(a.nT_w + ((long long)p * 2 + half) * kTaps + 4 * q);
+        const float2 sc = a.nT_scale ? a.nT_scale[2 * p + half] : make_float2(1, 1);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+        {
+            an[i] += (R)wa(w.v[i], sc) * v;
+            ad[i] += (R)wb(w.v[i], sc) * v;
+        }
+    }
+    quad_totals<R>(an);
+    quad_totals<R>(ad);
+}
+
+// add tap k of lane q's totals into ring slot (tau0 - k) of triangle j (lanes 0-3)
+template <typename R>
+__device__ inline void ring_add(R *ring, int j, int tau0, int q, const R (&v)[4])
+{
+    R *row = ring + (long long)j * kRing;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        row[(tau0 - 4 * q - i) & (kRing - 1)] += v[i];
+}
+
+// P2: near BEM push, then lamF of triangle j (one warp per triangle)
+template <typename R>
+__global__ void __launch_bounds__(256) adj_bem_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+{
     const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (j >= a.nt)
         return;
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    // face pairs: lamF window sigma + 1 .. sigma + 16, shifted records (a_m, b_{m+1})
-    const R *wf = ring_window<R>(a.ring_f, a.nt, sigma + 1, q);
-    R acc_n = 0, acc_d = 0;
-    for (int p = a.fT_start[j] + g; p < a.fT_start[j + 1]; p += 8)
+    const R *lam = a.slot(sigma);
+    R an[4], ad[4];
+    near_push_sums<R>(a, j, 1, g, q, [&](int c) { return (R)0.98 * lam[c]; }, an, ad);
+    if (lane < 4)
     {
-        const W4 w = *(const W4 *)(a.fT_w + (long long)p * kTaps + 4 * q);
-        const float2 s = a.fT_scale ? a.fT_scale[p] : make_float2(1, 1);
-        const H4 h = *(const H4 *)(wf + (long long)a.fT_src[p] * kRing);
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-        {
-            acc_n += (R)wa(w.v[i], s) * h.v[i];
-            acc_d += (R)wb(w.v[i], s) * h.v[i];
-        }
+        ring_add<R>(a.acc_n, j, sigma, q, an);
+        ring_add<R>(a.acc_d, j, sigma, q, ad);
     }
-    R near_n = 0, near_d = 0;
-    if (!flush)
-    {
-        // near pairs: lamP / lamC windows sigma .. sigma + 15
-        const R *wp = ring_window<R>(a.ring_p, a.n3, sigma, q), *wc = ring_window<R>(a.ring_c, a.n3, sigma, q);
-        for (int p = a.nT_start[j] + g; p < a.nT_start[j + 1]; p += 8)
-        {
-            const int ci = a.nT_cell[p];
-            const W4 rf = *(const W4 *)(a.nT_w + (long long)p * 2 * kTaps + 4 * q);
-            const W4 rb = *(const W4 *)(a.nT_w + (long long)p * 2 * kTaps + kTaps + 4 * q);
-            const float2 sf = a.nT_scale ? a.nT_scale[2 * p] : make_float2(1, 1);
-            const float2 sb = a.nT_scale ? a.nT_scale[2 * p + 1] : make_float2(1, 1);
-            const H4 hp = *(const H4 *)(wp + (long long)ci * kRing);
-            const H4 hc = *(const H4 *)(wc + (long long)ci * kRing);
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-            {
-                near_n += (R)wa(rb.v[i], sb) * hp.v[i] + (R)wa(rf.v[i], sf) * hc.v[i];
-                near_d += (R)wb(rb.v[i], sb) * hp.v[i] + (R)wb(rf.v[i], sf) * hc.v[i];
-            }
-        }
-    }
-    acc_n = warp_sum_adj(acc_n);
-    if (!flush)
-    {
-        acc_d = warp_sum_adj(acc_d);
-        near_n = warp_sum_adj(near_n);
-        near_d = warp_sum_adj(near_d);
-        if (lane < 4)
-        {
-            const R lf = (R)((acc_d + near_d) / a.denom[j]);
-            a.ring_f[((long long)lane * a.nt + j) * kRing + ((sigma + lane) & (kRing - 1))] = lf;
-        }
-    }
+    __syncwarp();
     if (lane == 0)
     {
-        if (out_row)
-            out_row[j] = acc_n + a.nearpart[j];
-        if (!flush)
-            a.nearpart[j] = near_n;
+        R *slot = a.acc_d + (long long)j * kRing + (sigma & (kRing - 1));
+        a.lam_f[j] = (R)(*slot / a.denom[j]);
+        *slot = 0;  // the slot is reused for time sigma - 32
     }
 }
 
-// A3: corner cells of the face interpolation
+// P3: face push (one warp per triangle j over the centres i whose face list holds j), then
+// dL/dacc[sigma][j]
+template <typename R>
+__global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ AdjArgs<R> a, int sigma, R *out_row)
+{
+    using W4 = typename AdjWRec<R>::W4;
+    const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (j >= a.nt)
+        return;
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    R an[4] = {0, 0, 0, 0}, ad[4] = {0, 0, 0, 0};
+    for (int p = a.fT_start[j] + g; p < a.fT_start[j + 1]; p += 8)
+    {
+        const R lf = a.lam_f[a.fT_src[p]];
+        const W4 w = *(const W4 *)(a.fT_w + (long long)p * kTaps + 4 * q);  // (a_m, b_{m+1})
+        const float2 sc = a.fT_scale ? a.fT_scale[p] : make_float2(1, 1);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+        {
+            an[i] += (R)wa(w.v[i], sc) * lf;
+            ad[i] += (R)wb(w.v[i], sc) * lf;
+        }
+    }
+    quad_totals<R>(an);
+    quad_totals<R>(ad);
+    if (lane < 4)
+    {
+        ring_add<R>(a.acc_n, j, sigma, q, an);
+        ring_add<R>(a.acc_d, j, sigma - 1, q, ad);
+    }
+    __syncwarp();
+    if (lane == 0)
+    {
+        R *slot = a.acc_n + (long long)j * kRing + (sigma & (kRing - 1));
+        if (out_row)
+            out_row[j] = *slot;
+        *slot = 0;
+    }
+}
+
+// P5: the stored FDTD-near sums of step sigma (one warp per triangle)
+template <typename R>
+__global__ void __launch_bounds__(256) adj_fdtd_near_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+{
+    const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (j >= a.nt)
+        return;
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const R *lam = a.slot(sigma);
+    R an[4], ad[4];
+    near_push_sums<R>(a, j, 0, g, q, [&](int c) { return -lam[c]; }, an, ad);
+    if (lane < 4)
+    {
+        ring_add<R>(a.acc_n, j, sigma - 1, q, an);
+        ring_add<R>(a.acc_d, j, sigma - 1, q, ad);
+    }
+}
+
+// P4: corner cells of the face interpolation
 template <typename R>
 __global__ void __launch_bounds__(256) adj_corner_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
 {
@@ -268,19 +300,18 @@ __global__ void __launch_bounds__(256) adj_corner_kernel(const __grid_constant__
     if (i >= a.ncorner)
         return;
     R v = 0;
-    const int slot = sigma & (kRing - 1);  // copy 0 holds time sigma at index sigma mod 32
     for (int r = a.cT_start[i]; r < a.cT_start[i + 1]; r++)
     {
         const int ref = a.cT_ref[r];
         const R iw = a.interp_d ? (R)a.interp_d[ref] : (R)a.interp[ref];
-        v += iw * a.ring_f[(long long)(ref >> 3) * kRing + slot];
+        v += iw * a.lam_f[ref >> 3];
     }
     a.slot(sigma)[a.cT_cell[i]] += (R)a.reflect * v;
 }
 
 __device__ inline int judge_of(int v, int res) { return -((int)(v == 1)) + ((int)(v == res - 2)); }
 
-// A4: the boundary-layer solve transposed
+// P6: the boundary-layer solve transposed
 template <typename R>
 __global__ void __launch_bounds__(256) adj_boundary_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
 {
@@ -344,7 +375,7 @@ __global__ void __launch_bounds__(256) adj_boundary_kernel(const __grid_constant
             ghosts[gi[d]] = 0;
 }
 
-// A5: the transposed stencil, one thread per cell of the whole grid (ghost layer included)
+// P7: the transposed stencil, one thread per cell of the whole grid (ghost layer included)
 template <typename R>
 __global__ void __launch_bounds__(256) adj_stencil_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
 {
@@ -512,8 +543,7 @@ void adj_free_tables(Adjoint &A)
 
 void adj_free_state(Adjoint &A)
 {
-    void **ptrs[] = {&A.lam[0], &A.lam[1], &A.lam[2], &A.lam_b, &A.ring_f, &A.ring_p, &A.ring_c, &A.nearpart,
-                     &A.d_g,    &A.d_out};
+    void **ptrs[] = {&A.lam[0], &A.lam[1], &A.lam[2], &A.lam_b, &A.acc_n, &A.acc_d, &A.lam_f, &A.d_g, &A.d_out};
     for (void **p : ptrs)
     {
         dev_free(*p);
@@ -622,15 +652,14 @@ int alloc_state(Handle &h, Adjoint &A)
             PB_TRY(dev_alloc(&A.lam[i], (size_t)h.n_cells * rs));
     if (!A.lam_b)
         PB_TRY(dev_alloc(&A.lam_b, (size_t)4 * h.n_cells * rs));
-    dev_free(A.ring_f);
-    dev_free(A.ring_p);
-    dev_free(A.ring_c);
-    dev_free(A.nearpart);
-    A.ring_f = A.ring_p = A.ring_c = A.nearpart = nullptr;
-    PB_TRY(dev_alloc(&A.ring_f, (size_t)4 * std::max(A.nt, 1) * kRing * rs));
-    PB_TRY(dev_alloc(&A.ring_p, (size_t)4 * std::max(A.n3, 1) * kRing * rs));
-    PB_TRY(dev_alloc(&A.ring_c, (size_t)4 * std::max(A.n3, 1) * kRing * rs));
-    PB_TRY(dev_alloc(&A.nearpart, (size_t)std::max(A.nt, 1) * rs));
+    // per triangle: the triangle count is fixed by the topology, so a sweep keeps these across
+    // geometry changes
+    if (!A.acc_n)
+        PB_TRY(dev_alloc(&A.acc_n, (size_t)std::max(h.nt, 1) * kRing * rs));
+    if (!A.acc_d)
+        PB_TRY(dev_alloc(&A.acc_d, (size_t)std::max(h.nt, 1) * kRing * rs));
+    if (!A.lam_f)
+        PB_TRY(dev_alloc(&A.lam_f, (size_t)std::max(h.nt, 1) * rs));
     return PPPM_OK;
 }
 
@@ -640,10 +669,9 @@ int zero_state(Handle &h, Adjoint &A)
     const size_t rs = sizeof(R);
     for (int i = 0; i < 3; i++)
         PB_CUDA(cudaMemsetAsync(A.lam[i], 0, (size_t)h.n_cells * rs, h.stream));
-    PB_CUDA(cudaMemsetAsync(A.ring_f, 0, (size_t)4 * std::max(A.nt, 1) * kRing * rs, h.stream));
-    PB_CUDA(cudaMemsetAsync(A.ring_p, 0, (size_t)4 * std::max(A.n3, 1) * kRing * rs, h.stream));
-    PB_CUDA(cudaMemsetAsync(A.ring_c, 0, (size_t)4 * std::max(A.n3, 1) * kRing * rs, h.stream));
-    PB_CUDA(cudaMemsetAsync(A.nearpart, 0, (size_t)std::max(A.nt, 1) * rs, h.stream));
+    PB_CUDA(cudaMemsetAsync(A.acc_n, 0, (size_t)std::max(h.nt, 1) * kRing * rs, h.stream));
+    PB_CUDA(cudaMemsetAsync(A.acc_d, 0, (size_t)std::max(h.nt, 1) * kRing * rs, h.stream));
+    PB_CUDA(cudaMemsetAsync(A.lam_f, 0, (size_t)std::max(h.nt, 1) * rs, h.stream));
     return PPPM_OK;
 }
 
@@ -684,10 +712,9 @@ AdjArgs<R> make_adj_args(Handle &h, Adjoint &A)
     for (int i = 0; i < 3; i++)
         a.lam[i] = (R *)A.lam[i];
     a.lam_b = (R *)A.lam_b;
-    a.ring_f = (R *)A.ring_f;
-    a.ring_p = (R *)A.ring_p;
-    a.ring_c = (R *)A.ring_c;
-    a.nearpart = (R *)A.nearpart;
+    a.acc_n = (R *)A.acc_n;
+    a.acc_d = (R *)A.acc_d;
+    a.lam_f = (R *)A.lam_f;
     const double cd = h.prm.c, dtd = h.prm.dt, hd = h.prm.dl;
     a.kappa = cd * cd * dtd * dtd / (hd * hd);
     const R c = (R)h.prm.c, dt = (R)h.prm.dt, hh = (R)h.prm.dl;
@@ -710,14 +737,10 @@ int run_adjoint(Handle &h, const R *g, int nsteps, R *out, int fresh)
     Adjoint &A = *h.adj;
     if (A.version != h.mesh_version)
     {
-        if (A.started && !fresh)
-        {
-            set_error("the geometry changed since the adjoint sweep started: start a fresh sweep");
-            return PPPM_ERR_STATE;
-        }
+        // the tables of the steps this call covers; the adjoint state (grid slots and per-triangle
+        // rings) carries over, so a sweep may continue across a motion frame
         PB_TRY(build_tables<R>(h, A));
         PB_TRY(alloc_state<R>(h, A));
-        A.started = false;
     }
     if (fresh || !A.started)
     {
@@ -729,21 +752,21 @@ int run_adjoint(Handle &h, const R *g, int nsteps, R *out, int fresh)
     const int T = 256, top = A.pos, bottom = A.pos - nsteps;
     const long long nbd = boundary_cells(h.res);
     cudaStream_t s = h.stream;
+    const int tw = div_up((long long)a.nt * 32, T);
     for (int sigma = top - 1; sigma >= bottom; sigma--)
     {
-        adj_cells_kernel<R><<<div_up(a.n3 + 1, T), T, 0, s>>>(a, sigma, g + (long long)(sigma - bottom) * a.nl);
-        R *row = sigma + 1 < top ? out + (long long)(sigma + 1 - bottom) * a.nt : nullptr;
-        adj_face_kernel<R><<<div_up((long long)a.nt * 32, T), T, 0, s>>>(a, sigma, row, 0);
+        if (a.nl > 0)
+            adj_listen_kernel<R><<<1, 32, 0, s>>>(a, sigma, g + (long long)(sigma - bottom) * a.nl);
+        adj_bem_kernel<R><<<tw, T, 0, s>>>(a, sigma);
+        adj_face_kernel<R><<<tw, T, 0, s>>>(a, sigma, out + (long long)(sigma - bottom) * a.nt);
         if (a.ncorner > 0)
             adj_corner_kernel<R><<<div_up(a.ncorner, T), T, 0, s>>>(a, sigma);
+        adj_fdtd_near_kernel<R><<<tw, T, 0, s>>>(a, sigma);
         adj_boundary_kernel<R><<<div_up(nbd, T), T, 0, s>>>(a, sigma);
         adj_stencil_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
         PB_CHECK_LAUNCH();
-        h.launches += 4 + (a.ncorner > 0);
+        h.launches += 5 + (a.nl > 0) + (a.ncorner > 0);
     }
-    adj_face_kernel<R><<<div_up((long long)a.nt * 32, T), T, 0, s>>>(a, bottom - 1, out, 1);
-    h.launches++;
-    PB_CHECK_LAUNCH();
     A.pos = bottom;
     return PPPM_OK;
 }

@@ -942,6 +942,127 @@ int cache_refresh(Handle &h)
     return PPPM_OK;
 }
 
+// ---- the motion-frame state of the caches (pppm_save_cache_state / pppm_restore_cache_state)
+// Blob: int64 header[6] = {magic, nt, nv, record bytes, pool_used, gc_empty}, then the vertex
+// positions, the grid-cache records (+ scales), their geometry snapshot, the face-cache key and
+// slot tables, and the pool's first pool_used records (+ scales) with their geometry meta.
+namespace
+{
+constexpr long long kCacheMagic = 0x7070706d63616368ll;
+
+struct CachePart
+{
+    void *dev;
+    size_t bytes;
+};
+
+std::vector<CachePart> cache_parts(Handle &h, long long pool_used)
+{
+    const size_t nt = (size_t)h.nt, rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    std::vector<CachePart> parts = {{h.d_verts, sizeof(float) * 3 * (size_t)h.nv}, {h.d_gc_w, nt * 54 * rec}};
+    if (!h.fp64)
+        parts.push_back({h.d_gc_scale, nt * 54 * sizeof(float2)});
+    parts.push_back({h.d_gc_snap, nt * 7 * sizeof(float)});
+    parts.push_back({h.d_fc_keys, nt * kFaceCacheSlots * sizeof(int)});
+    parts.push_back({h.d_fc_slot, nt * kFaceCacheSlots * sizeof(int)});
+    parts.push_back({h.d_pool_w, (size_t)pool_used * rec});
+    if (!h.fp64)
+        parts.push_back({h.d_pool_scale, (size_t)pool_used * sizeof(float2)});
+    parts.push_back({h.d_pool_meta, (size_t)pool_used * sizeof(float2)});
+    return parts;
+}
+}  // namespace
+
+size_t cache_state_bytes(Handle &h)
+{
+    size_t b = 6 * sizeof(long long);
+    for (const CachePart &p : cache_parts(h, h.pool_used))
+        b += p.bytes;
+    return b;
+}
+
+int cache_state_save(Handle &h, void *dst, size_t bytes)
+{
+    if (!h.mesh_set || !h.d_gc_w || h.prm.method != PPPM_METHOD_PPPM)
+    {
+        set_error("cache state: needs a mesh (PPPM method)");
+        return PPPM_ERR_STATE;
+    }
+    if (bytes < cache_state_bytes(h))
+        return PPPM_ERR_ARG;
+    const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    long long *hdr = (long long *)dst;
+    hdr[0] = kCacheMagic;
+    hdr[1] = h.nt;
+    hdr[2] = h.nv;
+    hdr[3] = (long long)rec;
+    hdr[4] = h.pool_used;
+    hdr[5] = h.gc_empty ? 1 : 0;
+    char *o = (char *)dst + 6 * sizeof(long long);
+    for (const CachePart &p : cache_parts(h, h.pool_used))
+    {
+        if (p.bytes)
+            PB_CUDA(cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDeviceToHost, h.stream));
+        o += p.bytes;
+    }
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    return PPPM_OK;
+}
+
+int cache_state_restore(Handle &h, const void *src, size_t bytes)
+{
+    if (!h.mesh_set || !h.d_gc_w || h.prm.method != PPPM_METHOD_PPPM)
+    {
+        set_error("cache state: needs a mesh (PPPM method)");
+        return PPPM_ERR_STATE;
+    }
+    const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    const long long *hdr = (const long long *)src;
+    if (bytes < 6 * sizeof(long long) || hdr[0] != kCacheMagic || hdr[1] != h.nt || hdr[2] != h.nv ||
+        hdr[3] != (long long)rec || hdr[4] < 0)
+    {
+        set_error("cache state: not a blob of this handle's mesh and precision");
+        return PPPM_ERR_ARG;
+    }
+    const long long used = hdr[4];
+    size_t need = 6 * sizeof(long long);
+    for (const CachePart &p : cache_parts(h, used))
+        need += p.bytes;
+    if (bytes < need)
+        return PPPM_ERR_ARG;
+    if (used > h.pool_cap)
+    {
+        // the blob's pool is larger than this handle's: grow (contents are replaced below)
+        dev_free(h.d_pool_w);
+        dev_free(h.d_pool_scale);
+        dev_free(h.d_pool_meta);
+        h.d_pool_w = nullptr;
+        h.d_pool_scale = nullptr;
+        h.d_pool_meta = nullptr;
+        const long long nc = used + used / 2 + 1024;
+        PB_TRY(dev_alloc(&h.d_pool_w, (size_t)nc * rec));
+        if (!h.fp64)
+            PB_TRY(dalloc(&h.d_pool_scale, (size_t)nc));
+        PB_TRY(dalloc(&h.d_pool_meta, (size_t)nc));
+        h.pool_cap = nc;
+    }
+    const char *o = (const char *)src + 6 * sizeof(long long);
+    for (const CachePart &p : cache_parts(h, used))
+    {
+        if (p.bytes)
+            PB_CUDA(cudaMemcpyAsync(p.dev, o, p.bytes, cudaMemcpyHostToDevice, h.stream));
+        o += p.bytes;
+    }
+    const int u = (int)used;
+    PB_CUDA(cudaMemcpyAsync(h.d_pool_count, &u, sizeof(int), cudaMemcpyHostToDevice, h.stream));
+    PB_CUDA(cudaStreamSynchronize(h.stream));
+    h.pool_used = used;
+    h.gc_empty = hdr[5] != 0;
+    h.tables_stale = true;  // the lists and dense tables still describe the geometry before the restore
+    h.mesh_version++;
+    return PPPM_OK;
+}
+
 int cache_free(Handle &h)
 {
     dev_free(h.d_gc_f);

@@ -550,6 +550,7 @@ int pppm_update_mesh(pppm_handle *ph, const float *verts, int verts_on_device)
     PB_CUDA(cudaMemcpyAsync(h.d_verts, verts, sizeof(float) * 3 * h.nv,
                             verts_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h.stream));
     h.mesh_version++;
+    h.tables_stale = false;
     PB_TRY(mesh_build(h));
     if (h.prm.method == PPPM_METHOD_GHOST)
     {
@@ -579,6 +580,11 @@ int pppm_step(pppm_handle *ph, const float *acc, int acc_on_device, int nsteps)
         return PPPM_ERR_ARG;
     }
     cudaSetDevice(h.prm.device);
+    if (h.tables_stale)
+    {
+        set_error("a cache state was restored: call pppm_update_mesh before stepping");
+        return PPPM_ERR_STATE;
+    }
     PB_TRY(poll_step_status(h, false));
     const float *dacc = nullptr;
     if (h.mesh_set)
@@ -717,6 +723,11 @@ int pppm_adjoint(pppm_handle *ph, const void *dL_dsignal, int nsteps, int on_dev
         return PPPM_ERR_ARG;
     if (nsteps == 0)
         return PPPM_OK;
+    if (h.tables_stale)
+    {
+        set_error("a cache state was restored: call pppm_update_mesh before the adjoint");
+        return PPPM_ERR_STATE;
+    }
     cudaSetDevice(h.prm.device);
     const size_t gb = (size_t)nsteps * nl * h.real_size, ob = (size_t)nsteps * h.nt * h.real_size;
     if (on_device)
@@ -1414,6 +1425,36 @@ int pppm_time_kernels(pppm_handle *ph, int reps, int nkinds, float *us_per_launc
     for (int k = 0; k < nkinds; k++)
         us_per_launch[k] = us[k];
     return PPPM_OK;
+}
+
+int pppm_cache_state_size(pppm_handle *ph, size_t *bytes)
+{
+    PB_TRY(check_handle(ph));
+    if (!bytes)
+        return PPPM_ERR_ARG;
+    Handle &h = ph->h;
+    if (!h.mesh_set || !h.d_gc_w || h.prm.method != PPPM_METHOD_PPPM)
+        return PPPM_ERR_STATE;
+    *bytes = cache_state_bytes(h);
+    return PPPM_OK;
+}
+
+int pppm_save_cache_state(pppm_handle *ph, void *dst, size_t bytes)
+{
+    PB_TRY(check_handle(ph));
+    if (!dst)
+        return PPPM_ERR_ARG;
+    cudaSetDevice(ph->h.prm.device);
+    return cache_state_save(ph->h, dst, bytes);
+}
+
+int pppm_restore_cache_state(pppm_handle *ph, const void *src, size_t bytes)
+{
+    PB_TRY(check_handle(ph));
+    if (!src)
+        return PPPM_ERR_ARG;
+    cudaSetDevice(ph->h.prm.device);
+    return cache_state_restore(ph->h, src, bytes);
 }
 
 int pppm_kernel_profile(pppm_handle *ph, int nkinds, float *us_per_launch, long long *launches)

@@ -219,6 +219,7 @@ struct Handle
 
     // ---- adjoint (adjoint.cu): transposed tables and adjoint state, built on first use
     long long mesh_version = 0;  // bumped whenever the lists or weight tables change
+    bool tables_stale = false;   // a cache state was restored: no step until update_mesh
     struct Adjoint *adj = nullptr;
 
     // ---- pinned host words for batched reads of device counts (read_ints)
@@ -280,6 +281,9 @@ void ghost_free(Handle &h);
 // cache.cu
 int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators
 int cache_free(Handle &h);
+size_t cache_state_bytes(Handle &h);                               // pppm_cache_state_size
+int cache_state_save(Handle &h, void *dst, size_t bytes);          // host buffer
+int cache_state_restore(Handle &h, const void *src, size_t bytes);  // host buffer; tables stale
 int cache_regather(Handle &h);  // dense gathers + denominators from the persistent caches
 int cache_import_grid(Handle &h, const void *records);                         // nt x 54 x 72 B
 int cache_import_face(Handle &h, const int *pairs, const void *records, int n);  // n x 72 B

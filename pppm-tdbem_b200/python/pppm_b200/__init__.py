@@ -99,6 +99,9 @@ def _load():
         "pppm_kernel_profile": [vp, i, fp, ctypes.POINTER(ctypes.c_longlong)],
         "pppm_sync": [vp],
         "pppm_time_kernels": [vp, i, i, fp],
+        "pppm_cache_state_size": [vp, ctypes.POINTER(sz)],
+        "pppm_save_cache_state": [vp, vp, sz],
+        "pppm_restore_cache_state": [vp, vp, sz],
     }
     fl = ctypes.c_float
     sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
@@ -403,6 +406,20 @@ class Solver:
     def restore_state(self, buf):
         buf = np.ascontiguousarray(buf, dtype=np.uint8)
         check(lib.pppm_restore_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.size), "restore_state")
+
+    def save_cache_state(self):
+        """The motion-frame state of the weight caches (pppm_save_cache_state) as a host array."""
+        n = ctypes.c_size_t()
+        check(lib.pppm_cache_state_size(self.h, ctypes.byref(n)), "cache_state_size")
+        buf = np.empty(n.value, np.uint8)
+        check(lib.pppm_save_cache_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), n.value), "save_cache_state")
+        return buf
+
+    def restore_cache_state(self, buf):
+        """Restore a saved cache state (pppm_restore_cache_state); update_mesh must follow."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        check(lib.pppm_restore_cache_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.size),
+              "restore_cache_state")
 
     # -- read-out
     def dump(self, what):

@@ -7,16 +7,27 @@ per-triangle surface accelerations.
 
 Forward runs pppm_step on the accelerations and returns the new listener samples (nsteps,
 nlisteners) in the solver's precision; backward runs pppm_adjoint, the transposed step
-backwards in time.  The samples are linear in the accelerations with the geometry held fixed,
+backwards in time (the gradient comes back in acc's dtype; the step itself reads the
+accelerations as float32).  The samples are linear in the accelerations with the geometry held fixed,
 so backward needs no stored forward state.  Chunks of one run are chained through the token:
 each chunk's backward continues the reverse sweep the later chunk left, so the gradient of an
 early chunk includes its effect on every later chunk.  The geometry must not change between
-the forward calls and the backward pass (update_mesh invalidates the sweep), and no other
-steps may be taken on the solver between chained chunks.
+the forward calls and the backward pass, and no other steps may be taken on the solver between
+chained chunks.
+
+    sig = moving_listener_signal(solver, acc, frames, checkpoint_steps=200)
+
+differentiates a moving run: frames = [(first_step, vertices), ...], motion frame f covering
+steps [first_f, first_{f+1}).  Its tables depend on the whole motion (the caches refresh only
+what moved), so the forward saves the caches' state at the start of every segment of about
+checkpoint_steps steps, and the backward differentiates the frames latest first, each with its
+own tables rebuilt from its segment's checkpoint (restore, then the segment's update_mesh calls
+up to that frame) - the geometry-side form of checkpointing with recomputation.
 """
+import numpy as np
 import torch
 
-__all__ = ["listener_signal"]
+__all__ = ["listener_signal", "moving_listener_signal"]
 
 
 def _solver_stream(solver, device):
@@ -45,7 +56,7 @@ class _ListenerSignal(torch.autograd.Function):
             # later work on the caller's stream (including reuse of a's and out's memory) comes
             # after the solver's; no record_stream: the solver's stream may be destroyed first
             cur.wait_stream(ext)
-        ctx.solver = solver
+        ctx.solver, ctx.acc_dtype = solver, acc.dtype
         ctx.span = (t0 + 1, t0 + 1 + n)  # forward time indices of the chunk's steps
         ctx.set_materialize_grads(False)
         return out, torch.zeros((), device=dev)
@@ -73,7 +84,7 @@ class _ListenerSignal(torch.autograd.Function):
         if ext is not None:
             cur.wait_stream(ext)
         solver._adjoint_pos = a
-        return grad.to(torch.float32), torch.zeros((), device=dev), None
+        return grad.to(ctx.acc_dtype), torch.zeros((), device=dev), None
 
 
 def listener_signal(solver, acc, token=None):
@@ -82,3 +93,87 @@ def listener_signal(solver, acc, token=None):
     if token is None:
         token = torch.zeros((), device=acc.device)
     return _ListenerSignal.apply(acc, token, solver)
+
+
+def _segments(bounds, k):
+    """start frames of the checkpoint segments: a new segment when at least k steps passed"""
+    starts, last = [0], bounds[0]
+    for f in range(1, len(bounds) - 1):
+        if bounds[f] - last >= k:
+            starts.append(f)
+            last = bounds[f]
+    return starts
+
+
+class _MovingSignal(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, acc, solver, frames, k):
+        if not acc.is_cuda or acc.dim() != 2 or acc.shape[1] != solver.nt:
+            raise ValueError("acc must be a (nsteps, %d) CUDA tensor" % solver.nt)
+        if not frames or frames[0][0] != 0 or any(b[0] <= a[0] for a, b in zip(frames, frames[1:])):
+            raise ValueError("frames must start at step 0 with increasing first steps")
+        dev = acc.device
+        a = acc.detach().to(torch.float32).contiguous()
+        n = a.shape[0]
+        bounds = [f[0] for f in frames] + [n]
+        if bounds[-2] >= n:
+            raise ValueError("the last frame starts after the last step")
+        starts = _segments(bounds, k)
+        first = solver.series_count
+        ext = _solver_stream(solver, dev)
+        cur = torch.cuda.current_stream(dev)
+        if ext is not None:
+            ext.wait_stream(cur)
+        checkpoints = {}
+        for f in range(len(frames)):
+            if f:
+                solver.update_mesh(frames[f][1])
+            if f in starts:
+                checkpoints[f] = solver.save_cache_state()
+            solver.step(a[bounds[f]: bounds[f + 1]])
+        dtype = torch.float64 if solver.precision == "fp64" else torch.float32
+        out = torch.empty((n, solver.n_listeners), dtype=dtype, device=dev)
+        solver.series(first, n, out=out)
+        if ext is not None:
+            cur.wait_stream(ext)
+        ctx.solver, ctx.frames, ctx.bounds, ctx.starts, ctx.checkpoints = solver, frames, bounds, starts, checkpoints
+        ctx.acc_dtype = acc.dtype
+        ctx.set_materialize_grads(False)
+        return out
+
+    @staticmethod
+    def backward(ctx, g_sig):
+        solver, frames, bounds, starts = ctx.solver, ctx.frames, ctx.bounds, ctx.starts
+        n = bounds[-1]
+        dtype = torch.float64 if solver.precision == "fp64" else torch.float32
+        if g_sig is None:
+            g_sig = torch.zeros((n, solver.n_listeners), dtype=dtype, device="cuda")
+        dev = g_sig.device
+        g = g_sig.to(dtype).contiguous()
+        grad = torch.empty((n, solver.nt), dtype=dtype, device=dev)
+        ext = _solver_stream(solver, dev)
+        cur = torch.cuda.current_stream(dev)
+        if ext is not None:
+            ext.wait_stream(cur)
+        fresh = True
+        ends = starts[1:] + [len(frames)]
+        for s0, s1 in reversed(list(zip(starts, ends))):
+            for f in range(s1 - 1, s0 - 1, -1):
+                # frame f's tables: the segment's checkpoint, then its meshes up to frame f
+                solver.restore_cache_state(ctx.checkpoints[s0])
+                for ff in range(s0, f + 1):
+                    solver.update_mesh(frames[ff][1])
+                a, b = bounds[f], bounds[f + 1]
+                solver.adjoint(g[a:b], fresh=fresh, out=grad[a:b])
+                fresh = False
+        if ext is not None:
+            cur.wait_stream(ext)
+        return grad.to(ctx.acc_dtype), None, None, None
+
+
+def moving_listener_signal(solver, acc, frames, checkpoint_steps=200):
+    """The listener samples (nsteps, nlisteners) of a moving run of `solver` over the rows of
+    `acc`, differentiable with respect to acc.  frames: [(first_step, vertices), ...] with
+    first_step 0 first (its vertices are those the solver's mesh holds now).  After backward the
+    solver's geometry and fields are those of the replay, not of the run's end."""
+    return _MovingSignal.apply(acc, solver, list(frames), int(checkpoint_steps))

@@ -29,3 +29,16 @@ def test_window_counts_and_face_pairs_match_the_fixture():
     codes = face_pair_codes(g["b4_cells"], g["b4_tris"], g["n4_tris"], n4_len, nt)
     want = np.sort(g["face_pairs"][:, 0].astype(np.int64) * nt + g["face_pairs"][:, 1])
     assert np.array_equal(codes, want)
+
+
+def test_moving_checkpoint_segments():
+    """moving_listener_signal's checkpoint segments: a new one at the first frame at least k steps
+    after the current segment's start; every frame belongs to exactly one segment"""
+    from pppm_b200.autograd import _segments
+
+    bounds = [0, 15, 30, 45, 60, 75]
+    assert _segments(bounds, 30) == [0, 2, 4]
+    assert _segments(bounds, 1) == [0, 1, 2, 3, 4]
+    assert _segments(bounds, 10 ** 9) == [0]
+    assert _segments([0, 7, 9, 40, 41, 100], 20) == [0, 3]
+    assert _segments([0, 5], 1) == [0]
