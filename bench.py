@@ -12,7 +12,9 @@ runs the 1280-triangle sphere at res 32 without motion (benchmark step = its who
 run).  --workload large runs two moving 20480-triangle icospheres at res 128 (2.1 M cells, ~6.2 M
 face pairs; one benchmark step = one 1 kHz motion frame of 82 time steps).  --workload batch: 64
 independent scenes in one batched run (scenes/s); --workload adjoint: the transposed step
-against the forward step.
+against the forward step (static geometry, res 48); --workload adjoint-moving: the gradient of the
+large scene's moving run through motion checkpoints every 200 steps, against the run;
+--workload large-batch: the large scene batched x4 with four seeds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -51,7 +53,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="moving",
-                   choices=["moving", "static", "batch", "adjoint", "large", "large-batch"])
+                   choices=["moving", "static", "batch", "adjoint", "adjoint-moving", "large", "large-batch"])
+    p.add_argument("--adjoint-steps", type=int, default=20000,
+                   help="time steps of the adjoint-moving run (the large scene's 20000 by default)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64-check", action="store_true")
@@ -944,6 +948,111 @@ def run_adjoint(args, ws, rank, local):
     }
 
 
+ADJM_NAME = ("two moving icospheres (2 x 20480 tris), res 128, loss ||s - s_target||^2, gradient w.r.t. "
+             "every acceleration, motion checkpoints every 200 steps (FP32)")
+
+
+def run_adjoint_moving(args, ws, rank, local):
+    """Cost of the gradient of a moving run against the run itself: one benchmark step = the
+    forward run of the large scene (update_mesh per 1 kHz motion frame, a motion checkpoint every
+    200 steps, device-resident accelerations) and the backward (each frame's tables rebuilt from
+    its segment's checkpoint, the adjoint sweep), both through autograd.moving_listener_signal;
+    beside it the same run without checkpoints."""
+    import torch
+
+    from pppm_b200 import Solver
+    from pppm_b200.autograd import moving_listener_signal
+
+    W, K = args.warmup, args.steps
+    sc = scenes.LargeScene()
+    nsteps = min(args.adjoint_steps, sc.steps)
+    nframes = sc.frame_of_step(nsteps - 1) + 1
+    ranges = scenes.frame_ranges(sc, nframes - 1)
+    ranges[-1] = (ranges[-1][0], nsteps)
+    frames = [(a, sc.frame_verts(f)) for f, (a, b) in enumerate(ranges)]
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    s = Solver(sc.res, sc.h, sc.dt, sc.min_pos, device=local, stream=stream.cuda_stream)
+    s.set_mesh(frames[0][1], sc.tris)
+    s.add_listener(*sc.listener)
+    acc = torch.from_numpy(sc.acc(0, nsteps)).to(dev).requires_grad_(True)
+    target = torch.zeros((nsteps, 1), dtype=torch.float32, device=dev)
+    t0 = s.t
+    peak = {"checkpoints": 0, "bytes": 0}
+
+    def restart():
+        s.reset_fields()
+        s.rewind_listeners()
+        s.t = t0
+
+    def plain():
+        restart()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for f, (a, b) in enumerate(ranges):
+            if f:
+                s.update_mesh(frames[f][1])
+            s.step(acc.detach()[a:b])
+        e1.record(stream)
+        s.update_mesh(frames[0][1])
+        return e0, e1
+
+    def forward_backward():
+        restart()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        sig = moving_listener_signal(s, acc, frames, checkpoint_steps=200)
+        e[1].record(stream)
+        n, b = s.checkpoint_info()
+        peak["checkpoints"], peak["bytes"] = max(peak["checkpoints"], n), max(peak["bytes"], b)
+        loss = ((sig - target) ** 2).sum()
+        e[2].record(stream)
+        (grad,) = torch.autograd.grad(loss, acc)
+        e[3].record(stream)
+        return e, grad
+
+    for _ in range(W):
+        plain()
+        forward_backward()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    launches0 = s.launch_count()
+    p_ms = f_ms = b_ms = 0.0
+    for _ in range(K):
+        p0, p1 = plain()
+        e, grad = forward_backward()
+        e[3].synchronize()
+        p_ms += p0.elapsed_time(p1)
+        f_ms += e[0].elapsed_time(e[1])
+        b_ms += e[2].elapsed_time(e[3])
+    barrier(ws)
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    p_ms, f_ms, b_ms = max_over_ranks(ws, p_ms), max_over_ranks(ws, f_ms), max_over_ranks(ws, b_ms)
+    finite = bool(torch.isfinite(grad).all().item())
+    s.close()
+    cells = float(sc.res) ** 3
+    return {
+        "metric": "adjoint / forward cost, %s" % ADJM_NAME, "value": round(b_ms / f_ms, 4), "unit": "x forward",
+        "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": round((p_ms + f_ms + b_ms) / K, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded meshes, trajectories and accelerations)",
+        "config": {"workload": ADJM_NAME, "res": sc.res, "triangles": int(len(sc.tris)), "time_steps": nsteps,
+                   "motion_frames": nframes, "checkpoint_steps": 200,
+                   "bench_step": "plain run + forward run with checkpoints + backward",
+                   "l2": "inputs (a %d MB acceleration history) larger than L2" % (nsteps * len(sc.tris) * 4 >> 20),
+                   "parallelism": "replicas x%d" % ws},
+        "plain_run_ms": round(p_ms / K, 2), "forward_ms": round(f_ms / K, 2), "backward_ms": round(b_ms / K, 2),
+        "checkpoint_overhead": round(f_ms / p_ms - 1, 4), "backward_vs_plain_run": round(b_ms / p_ms, 4),
+        "checkpoints": peak["checkpoints"], "checkpoint_bytes": int(peak["bytes"]),
+        "plain_gcell_steps_per_s": round(cells * nsteps * K * ws / (p_ms * 1e-3) / 1e9, 3),
+        "gradient_finite": finite, "cpu_baseline": None, "e2e": None, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
 def cpu_batch_baseline(specs, sample=4, steps=20):
     """The CPU restatement on the first `sample` batch scenes, `steps` time steps each (set_mesh
     untimed), extrapolated to every step of those scenes: scenes/s on the host cores."""
@@ -1029,6 +1138,9 @@ def run_reference(args, ws, rank, local):
         return run_reference_batch(args)
     if args.workload == "adjoint":
         return {"impl": "reference", "metric": "adjoint / forward cost, %s" % ADJ_NAME,
+                "unavailable": "the reference has no adjoint"}
+    if args.workload == "adjoint-moving":
+        return {"impl": "reference", "metric": "adjoint / forward cost, %s" % ADJM_NAME,
                 "unavailable": "the reference has no adjoint"}
     if args.workload == "large-batch":
         return run_reference_large_batch(args)
@@ -1287,6 +1399,8 @@ def main():
         line = run_batch(args, ws, rank, local)
     elif args.workload == "adjoint":
         line = run_adjoint(args, ws, rank, local)
+    elif args.workload == "adjoint-moving":
+        line = run_adjoint_moving(args, ws, rank, local)
     elif args.workload == "large-batch":
         line = run_large_batch(args, ws, rank, local)
     else:

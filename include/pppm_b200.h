@@ -227,11 +227,29 @@ int pppm_adjoint(pppm_handle *h, const void *dL_dsignal, int nsteps, int on_devi
  * pppm_update_mesh and restoring it later, followed by pppm_update_mesh with that frame's
  * vertices (which then recomputes nothing) and with each later frame's vertices in turn,
  * rebuilds exactly the tables those frames had: the checkpoints of a frame-by-frame adjoint
- * (pppm_b200.autograd.moving_listener_signal).  Host buffers; a restore leaves the handle's
- * lists stale, and pppm_step / pppm_adjoint return PPPM_ERR_STATE until pppm_update_mesh. */
+ * (pppm_b200.autograd.moving_listener_signal).  The blob may sit in host memory or in device
+ * memory (a checkpoint kept in HBM: copies go through unified addressing); both calls return
+ * once the copies are done.  A restore leaves the handle's lists stale, and pppm_step /
+ * pppm_adjoint return PPPM_ERR_STATE until pppm_update_mesh. */
 int pppm_cache_state_size(pppm_handle *h, size_t *bytes);
 int pppm_save_cache_state(pppm_handle *h, void *dst, size_t bytes);
 int pppm_restore_cache_state(pppm_handle *h, const void *src, size_t bytes);
+
+/* No counterpart in the reference.  Motion checkpoints for differentiating long moving runs,
+ * kept by the handle in device memory: a checkpoint holds the vertex positions and the
+ * grid-cache records of the current frame (a res-128 scene of 40960 triangles: about 160 MB)
+ * and the size of the face-cache record pool; the pool itself stays in place, later refreshes
+ * log the old records of the pool entries they rewrite.  pppm_checkpoint_push takes one after
+ * the frame's pppm_set_mesh / pppm_update_mesh (*id: its index, 0 first); pppm_checkpoint_rewind
+ * brings the caches back to checkpoint id and drops the later ones (a pppm_update_mesh with
+ * that frame's vertices must follow before pppm_step / pppm_adjoint, which return
+ * PPPM_ERR_STATE until then; further pppm_update_mesh calls replay the motion with the tables
+ * the run had).  Checkpoints go on pppm_checkpoint_clear, pppm_set_mesh, a cache-state restore
+ * or a weight import.  pppm_checkpoint_info: how many are held and the device bytes they use. */
+int pppm_checkpoint_push(pppm_handle *h, int *id);
+int pppm_checkpoint_rewind(pppm_handle *h, int id);
+int pppm_checkpoint_clear(pppm_handle *h);
+int pppm_checkpoint_info(pppm_handle *h, int *count, size_t *bytes);
 
 /* ------------------------------------------------------------ weight diagnostics ----- */
 /* TDBEM::init (bem.h:264-277) as this library evaluates it on the host: lambda and the 16

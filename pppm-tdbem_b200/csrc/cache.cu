@@ -408,9 +408,12 @@ __device__ inline unsigned hash_slot(int key) { return ((unsigned)key * 26544357
 
 // one warp per centre face: find or insert each (centre, neighbour) pair in the centre's
 // table, decide whether its record must be recomputed.
+// A rewritten slot below log_floor (the newest motion checkpoint's pool size) gets its old meta
+// kept in old_meta[p] and is counted in n_log; fresh slots record their key.
 __global__ void fc_lookup_kernel(const int *face_start, const int *face_nbr, int nt, const float *center,
                                  const float *normal, int *keys, int *slots, int *pool_count, long long pool_cap,
-                                 float2 *pool_meta, int *face_pool, int *pair_flag, int *status)
+                                 float2 *pool_meta, int2 *pool_key, long long log_floor, float2 *old_meta,
+                                 int *n_log, int *face_pool, int *pair_flag, int *status)
 {
     int warp = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     int lane = threadIdx.x & 31;
@@ -465,11 +468,19 @@ __global__ void fc_lookup_kernel(const int *face_start, const int *face_nbr, int
         float dist = len3(nc - cc);
         int recompute = 0;
         if (fresh)
+        {
             recompute = 1;
+            pool_key[slot] = make_int2(ctr, nbr);
+        }
         else
         {
             float2 m = pool_meta[slot];
             recompute = (abs(m.x - angle) > 0.01 || abs(m.y - dist) > 0.01 * dist) ? 1 : 0;
+            if (recompute && slot < log_floor)
+            {
+                old_meta[p] = m;
+                atomicAdd(n_log, 1);
+            }
         }
         if (recompute)
             pool_meta[slot] = make_float2(angle, dist);
@@ -483,6 +494,75 @@ __global__ void compact_pairs_kernel(const int *flag, const int *pos, long long 
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && flag[i])
         out[pos[i]] = (int)i;
+}
+
+// ---- motion checkpoints: undo log of pool rewrites, table rebuild
+
+__device__ inline void copy_record(const int4 *src, int4 *dst, int words)
+{
+    for (int k = 0; k < words; k++)
+        dst[k] = src[k];
+}
+
+// one thread per pair to recompute: a slot below the floor (written before the newest
+// checkpoint) has its record, scale and old meta appended to the log before the refresh
+// overwrites it
+__global__ void log_rewrites_kernel(const int *work, int nwork, const int *face_pool, long long floor,
+                                    const float2 *old_meta, const int4 *pool_w, const float2 *pool_scale,
+                                    int rec_words, int cap, int *cursor, int *out_slot, int4 *out_rec,
+                                    float2 *out_scale, float2 *out_meta)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwork)
+        return;
+    const int p = work[w], slot = face_pool[p];
+    if (slot >= floor)
+        return;
+    const int i = atomicAdd(cursor, 1);
+    if (i >= cap)
+        return;  // cannot happen: cap is the lookup's count of these pairs
+    out_slot[i] = slot;
+    copy_record(pool_w + (size_t)slot * rec_words, out_rec + (size_t)i * rec_words, rec_words);
+    if (out_scale)
+        out_scale[i] = pool_scale[slot];
+    out_meta[i] = old_meta[p];
+}
+
+// a log batch written back (its slots are distinct: a refresh recomputes each pair once)
+__global__ void apply_log_kernel(int n, const int *slot, const int4 *rec, const float2 *scale, const float2 *meta,
+                                 int rec_words, int4 *pool_w, float2 *pool_scale, float2 *pool_meta)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int s = slot[i];
+    copy_record(rec + (size_t)i * rec_words, pool_w + (size_t)s * rec_words, rec_words);
+    if (scale)
+        pool_scale[s] = scale[i];
+    pool_meta[s] = meta[i];
+}
+
+// the per-centre tables from the pool keys of slots [0, used): the same (centre, neighbour) ->
+// slot map as when those slots were inserted (probe positions may differ)
+__global__ void fc_rebuild_kernel(const int2 *pool_key, long long used, int *keys, int *slots, int *status)
+{
+    long long sl = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= used)
+        return;
+    const int2 k = pool_key[sl];
+    int *tk = keys + (size_t)k.x * kFaceCacheSlots;
+    int *ts = slots + (size_t)k.x * kFaceCacheSlots;
+    const unsigned hsh = hash_slot(k.y);
+    for (int probe = 0; probe < kFaceCacheSlots; probe++)
+    {
+        const unsigned pos = (hsh + probe) & (kFaceCacheSlots - 1);
+        if (atomicCAS(&tk[pos], -1, k.y) == -1)
+        {
+            ts[pos] = (int)sl;
+            return;
+        }
+    }
+    atomicCAS(status, 0, PPPM_ERR_CAPACITY);
 }
 
 __device__ inline int centre_of(const int *face_start, int nt, int p)
@@ -766,6 +846,242 @@ __global__ void gc_factor_kernel(const __half2 *w, const float2 *scale, const do
 
 }  // namespace
 
+// ---- motion checkpoints (pppm_checkpoint_*)
+// A checkpoint keeps in device memory what a refresh overwrites wholesale - the vertex
+// positions, the grid-cache records with their geometry snapshot - and the pool size.  The
+// pool itself stays live: later refreshes only append to it, except for the in-place rewrites
+// of pairs whose geometry moved, whose old records the newest checkpoint logs (log_rewrites_
+// kernel).  A rewind writes the logs back, newest first, truncates the pool and rebuilds the
+// per-centre tables from the pool keys.  Checkpoints form a stack: rewinding to one drops the
+// later ones, and its own log restarts empty (the handle is back at its state).
+struct LogBatch
+{
+    void *buf = nullptr;
+    int n = 0;
+};
+
+struct MotionCheckpoint
+{
+    void *buf = nullptr;
+    size_t bytes = 0;
+    long long used = 0;
+    bool gc_empty = false;
+    std::vector<LogBatch> log;
+};
+
+struct Journal
+{
+    std::vector<MotionCheckpoint> stack;
+};
+
+namespace
+{
+struct Span
+{
+    void *dev;
+    size_t bytes;
+};
+
+std::vector<Span> checkpoint_parts(Handle &h)
+{
+    const size_t nt = (size_t)h.nt, rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    std::vector<Span> parts = {{h.d_verts, sizeof(float) * 3 * (size_t)h.nv}, {h.d_gc_w, nt * 54 * rec}};
+    if (!h.fp64)
+        parts.push_back({h.d_gc_scale, nt * 54 * sizeof(float2)});
+    parts.push_back({h.d_gc_snap, nt * 7 * sizeof(float)});
+    return parts;
+}
+
+size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// byte offsets of a log batch of n entries: slots, records, scales (FP32), metas
+void log_layout(const Handle &h, int n, size_t off[4], size_t *total)
+{
+    const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    off[0] = 0;
+    off[1] = align16(sizeof(int) * (size_t)n);
+    off[2] = off[1] + rec * (size_t)n;
+    off[3] = off[2] + (h.fp64 ? 0 : sizeof(float2) * (size_t)n);
+    *total = off[3] + sizeof(float2) * (size_t)n;
+}
+
+void free_checkpoint(MotionCheckpoint &c)
+{
+    for (LogBatch &b : c.log)
+        dev_free(b.buf);
+    c.log.clear();
+    dev_free(c.buf);
+    c.buf = nullptr;
+}
+}  // namespace
+
+int journal_count(const Handle &h) { return h.journal ? (int)h.journal->stack.size() : 0; }
+
+long long journal_floor(const Handle &h) { return journal_count(h) ? h.journal->stack.back().used : 0; }
+
+size_t journal_bytes(const Handle &h)
+{
+    size_t b = 0;
+    if (h.journal)
+        for (const MotionCheckpoint &c : h.journal->stack)
+        {
+            b += c.bytes;
+            for (const LogBatch &l : c.log)
+            {
+                size_t off[4], total;
+                log_layout(h, l.n, off, &total);
+                b += total;
+            }
+        }
+    return b;
+}
+
+void journal_clear(Handle &h)
+{
+    if (!h.journal)
+        return;
+    cudaStreamSynchronize(h.stream);
+    for (MotionCheckpoint &c : h.journal->stack)
+        free_checkpoint(c);
+    delete h.journal;
+    h.journal = nullptr;
+}
+
+// the old records of the n slots below `floor` that this refresh recomputes, appended to the
+// newest checkpoint's log (before the recompute kernels overwrite them)
+int journal_log(Handle &h, const int *work, int nwork, long long floor, int n)
+{
+    const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    size_t off[4], total;
+    log_layout(h, n, off, &total);
+    LogBatch b;
+    PB_TRY(dev_alloc(&b.buf, total));
+    b.n = n;
+    char *base = (char *)b.buf;
+    log_rewrites_kernel<<<div_up(nwork, 256), 256, 0, h.stream>>>(
+        work, nwork, h.d_face_pool, floor, h.d_pair_old_meta, (const int4 *)h.d_pool_w, h.d_pool_scale,
+        (int)(rec / sizeof(int4)), n, h.d_log_count + 1, (int *)(base + off[0]), (int4 *)(base + off[1]),
+        h.fp64 ? nullptr : (float2 *)(base + off[2]), (float2 *)(base + off[3]));
+    h.launches++;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        dev_free(b.buf);
+        set_error("CUDA error %s at %s:%d", cudaGetErrorString(e), __FILE__, __LINE__);
+        return PPPM_ERR_CUDA;
+    }
+    h.journal->stack.back().log.push_back(b);
+    return PPPM_OK;
+}
+
+int journal_push(Handle &h, int *id)
+{
+    if (!h.mesh_set || !h.d_gc_w || h.prm.method != PPPM_METHOD_PPPM)
+    {
+        set_error("checkpoint: needs a mesh (PPPM method)");
+        return PPPM_ERR_STATE;
+    }
+    if (h.tables_stale)
+    {
+        set_error("checkpoint: call pppm_update_mesh after a rewind or restore first");
+        return PPPM_ERR_STATE;
+    }
+    if (!h.journal)
+    {
+        h.journal = new (std::nothrow) Journal();
+        if (!h.journal)
+            return PPPM_ERR_NOMEM;
+    }
+    MotionCheckpoint c;
+    for (const Span &p : checkpoint_parts(h))
+        c.bytes += align16(p.bytes);
+    PB_TRY(dev_alloc(&c.buf, c.bytes));
+    char *o = (char *)c.buf;
+    for (const Span &p : checkpoint_parts(h))
+    {
+        const cudaError_t e = cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDeviceToDevice, h.stream);
+        if (e != cudaSuccess)
+        {
+            dev_free(c.buf);
+            set_error("CUDA error %s at %s:%d", cudaGetErrorString(e), __FILE__, __LINE__);
+            return PPPM_ERR_CUDA;
+        }
+        o += align16(p.bytes);
+    }
+    c.used = h.pool_used;
+    c.gc_empty = h.gc_empty;
+    h.journal->stack.push_back(std::move(c));
+    *id = (int)h.journal->stack.size() - 1;
+    return PPPM_OK;
+}
+
+int journal_rewind(Handle &h, int id)
+{
+    if (id < 0 || id >= journal_count(h))
+    {
+        set_error("checkpoint %d: no such checkpoint (%d held)", id, journal_count(h));
+        return PPPM_ERR_ARG;
+    }
+    cudaStream_t s = h.stream;
+    const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    const int words = (int)(rec / sizeof(int4));
+    std::vector<MotionCheckpoint> &st = h.journal->stack;
+    // undo the logged rewrites, newest first
+    for (int k = (int)st.size() - 1; k >= id; k--)
+        for (int b = (int)st[k].log.size() - 1; b >= 0; b--)
+        {
+            const LogBatch &l = st[k].log[b];
+            size_t off[4], total;
+            log_layout(h, l.n, off, &total);
+            const char *base = (const char *)l.buf;
+            apply_log_kernel<<<div_up(l.n, 256), 256, 0, s>>>(
+                l.n, (const int *)(base + off[0]), (const int4 *)(base + off[1]),
+                h.fp64 ? nullptr : (const float2 *)(base + off[2]), (const float2 *)(base + off[3]), words,
+                (int4 *)h.d_pool_w, h.d_pool_scale, h.d_pool_meta);
+            h.launches++;
+            PB_CHECK_LAUNCH();
+        }
+    // the checkpoint's grid cache and vertices, the pool truncated to its size, the tables
+    const MotionCheckpoint &c = st[id];
+    const char *o = (const char *)c.buf;
+    for (const Span &p : checkpoint_parts(h))
+    {
+        PB_CUDA(cudaMemcpyAsync(p.dev, o, p.bytes, cudaMemcpyDeviceToDevice, s));
+        o += align16(p.bytes);
+    }
+    const int u = (int)c.used;
+    PB_CUDA(cudaMemcpyAsync(h.d_pool_count, &u, sizeof(int), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemsetAsync(h.d_fc_keys, 0xff, sizeof(int) * (size_t)h.nt * kFaceCacheSlots, s));
+    PB_CUDA(cudaMemsetAsync(h.d_status, 0, sizeof(int), s));
+    if (c.used > 0)
+    {
+        fc_rebuild_kernel<<<div_up(c.used, 256), 256, 0, s>>>(h.d_pool_key, c.used, h.d_fc_keys, h.d_fc_slot,
+                                                              h.d_status);
+        h.launches++;
+        PB_CHECK_LAUNCH();
+    }
+    int st_word = 0;
+    PB_TRY(read_int(h, h.d_status, &st_word));  // also orders the frees below after the copies
+    if (st_word)
+    {
+        set_error("checkpoint rewind: face-cache table overflow while rebuilding");
+        return st_word;
+    }
+    for (LogBatch &l : st[id].log)
+        dev_free(l.buf);
+    st[id].log.clear();
+    for (int k = (int)st.size() - 1; k > id; k--)
+    {
+        free_checkpoint(st[k]);
+        st.pop_back();
+    }
+    h.pool_used = c.used;
+    h.gc_empty = c.gc_empty;
+    h.tables_stale = true;  // lists and dense tables still describe the geometry before the rewind
+    h.mesh_version++;
+    return PPPM_OK;
+}
+
 int gc_factors(Handle &h)
 {
     const long long n = (long long)h.nt * 54;
@@ -800,6 +1116,7 @@ int cache_refresh(Handle &h)
         PB_CUDA(cudaMemsetAsync(h.d_fc_keys, 0xff, sizeof(int) * (size_t)nt * kFaceCacheSlots, s));
         PB_TRY(dalloc(&h.d_pool_count, 1));
         PB_CUDA(cudaMemsetAsync(h.d_pool_count, 0, sizeof(int), s));
+        PB_TRY(dalloc(&h.d_log_count, 2));
         PB_TRY(dalloc(&h.d_face_interp, (size_t)nt * 8));
         if (h.fp64)
             PB_TRY(dalloc(&h.d_face_interp_d, (size_t)nt * 8));
@@ -846,12 +1163,16 @@ int cache_refresh(Handle &h)
             long long nc = need + need / 2 + 1024;
             void *nw = nullptr;
             float2 *nsc = nullptr, *nmeta = nullptr;
+            int2 *nkey = nullptr;
             PB_TRY(dev_alloc(&nw, (size_t)nc * rec_bytes));
             if (!h.fp64)
                 PB_TRY(dalloc(&nsc, (size_t)nc));
             PB_TRY(dalloc(&nmeta, (size_t)nc));
+            PB_TRY(dalloc(&nkey, (size_t)nc));
             if (h.pool_used > 0)
             {
+                PB_CUDA(cudaMemcpyAsync(nkey, h.d_pool_key, (size_t)h.pool_used * sizeof(int2),
+                                        cudaMemcpyDeviceToDevice, s));
                 PB_CUDA(cudaMemcpyAsync(nw, h.d_pool_w, (size_t)h.pool_used * rec_bytes, cudaMemcpyDeviceToDevice, s));
                 if (!h.fp64)
                     PB_CUDA(cudaMemcpyAsync(nsc, h.d_pool_scale, (size_t)h.pool_used * sizeof(float2),
@@ -863,26 +1184,34 @@ int cache_refresh(Handle &h)
             dev_free(h.d_pool_w);
             dev_free(h.d_pool_scale);
             dev_free(h.d_pool_meta);
+            dev_free(h.d_pool_key);
             h.d_pool_w = nw;
             h.d_pool_scale = nsc;
             h.d_pool_meta = nmeta;
+            h.d_pool_key = nkey;
             h.pool_cap = nc;
         }
+        // rewrites of slots that the newest motion checkpoint holds are logged (journal_rewind)
+        const long long log_floor = journal_count(h) > 0 ? journal_floor(h) : 0;
+        if (log_floor > 0)
+            PB_TRY(dgrow(&h.d_pair_old_meta, h.pair_old_meta_cap, h.pf, s));
         PB_CUDA(cudaMemsetAsync(h.d_status, 0, sizeof(int), s));
+        PB_CUDA(cudaMemsetAsync(h.d_log_count, 0, 2 * sizeof(int), s));
         fc_lookup_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(
             h.d_face_start, h.d_face_nbr, nt, h.d_center, h.d_normal, h.d_fc_keys, h.d_fc_slot, h.d_pool_count,
-            h.pool_cap, h.d_pool_meta, h.d_face_pool, h.d_pair_flag, h.d_status);
+            h.pool_cap, h.d_pool_meta, h.d_pool_key, log_floor, h.d_pair_old_meta, h.d_log_count, h.d_face_pool,
+            h.d_pair_flag, h.d_status);
         h.launches++;
         PB_CHECK_LAUNCH();
         // compact the recompute list; one synchronisation reads the lookup status, the pool
-        // size and the number of pairs to recompute
+        // size, the number of pairs to recompute and the number of logged rewrites
         PB_TRY(dgrow(&h.d_pair_work, h.pair_work_cap, 2 * (h.pf + 1), s));
         int *pos = h.d_pair_work;
         int *work = h.d_pair_work + (h.pf + 1);
         PB_TRY(exclusive_scan(h, h.d_pair_flag, pos, h.pf));
-        int v[3];
-        const int *src[3] = {h.d_status, h.d_pool_count, pos + h.pf};
-        PB_TRY(read_ints(h, src, 3, v));
+        int v[4];
+        const int *src[4] = {h.d_status, h.d_pool_count, pos + h.pf, h.d_log_count};
+        PB_TRY(read_ints(h, src, 4, v));
         if (v[0])
         {
             set_error("face cache: more than %d distinct neighbours seen by one face", kFaceCacheSlots);
@@ -894,6 +1223,8 @@ int cache_refresh(Handle &h)
         {
             compact_pairs_kernel<<<div_up(h.pf, T), T, 0, s>>>(h.d_pair_flag, pos, h.pf, work);
             h.launches++;
+            if (v[3] > 0)
+                PB_TRY(journal_log(h, work, nwork, log_floor, v[3]));
             size_t need_spec = (size_t)nwork * 18 * (h.fp64 ? sizeof(cd) : sizeof(cf));
             if (need_spec > h.spec_bytes)
             {
@@ -943,7 +1274,7 @@ int cache_refresh(Handle &h)
 }
 
 // ---- the motion-frame state of the caches (pppm_save_cache_state / pppm_restore_cache_state)
-// Blob: int64 header[6] = {magic, nt, nv, record bytes, pool_used, gc_empty}, then the vertex
+// Blob (host or device memory): int64 header[6] = {magic, nt, nv, record bytes, pool_used, gc_empty}, then the vertex
 // positions, the grid-cache records (+ scales), their geometry snapshot, the face-cache key and
 // slot tables, and the pool's first pool_used records (+ scales) with their geometry meta.
 namespace
@@ -969,6 +1300,7 @@ std::vector<CachePart> cache_parts(Handle &h, long long pool_used)
     if (!h.fp64)
         parts.push_back({h.d_pool_scale, (size_t)pool_used * sizeof(float2)});
     parts.push_back({h.d_pool_meta, (size_t)pool_used * sizeof(float2)});
+    parts.push_back({h.d_pool_key, (size_t)pool_used * sizeof(int2)});
     return parts;
 }
 }  // namespace
@@ -991,21 +1323,17 @@ int cache_state_save(Handle &h, void *dst, size_t bytes)
     if (bytes < cache_state_bytes(h))
         return PPPM_ERR_ARG;
     const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
-    long long *hdr = (long long *)dst;
-    hdr[0] = kCacheMagic;
-    hdr[1] = h.nt;
-    hdr[2] = h.nv;
-    hdr[3] = (long long)rec;
-    hdr[4] = h.pool_used;
-    hdr[5] = h.gc_empty ? 1 : 0;
-    char *o = (char *)dst + 6 * sizeof(long long);
+    const long long hdr[6] = {kCacheMagic, h.nt, h.nv, (long long)rec, h.pool_used, h.gc_empty ? 1 : 0};
+    // host or device memory alike (unified addressing): a checkpoint may stay in HBM
+    PB_CUDA(cudaMemcpyAsync(dst, hdr, sizeof(hdr), cudaMemcpyDefault, h.stream));
+    char *o = (char *)dst + sizeof(hdr);
     for (const CachePart &p : cache_parts(h, h.pool_used))
     {
         if (p.bytes)
-            PB_CUDA(cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDeviceToHost, h.stream));
+            PB_CUDA(cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDefault, h.stream));
         o += p.bytes;
     }
-    PB_CUDA(cudaStreamSynchronize(h.stream));
+    PB_CUDA(cudaStreamSynchronize(h.stream));  // hdr is a stack array; the caller owns dst on return
     return PPPM_OK;
 }
 
@@ -1017,14 +1345,20 @@ int cache_state_restore(Handle &h, const void *src, size_t bytes)
         return PPPM_ERR_STATE;
     }
     const size_t rec = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
-    const long long *hdr = (const long long *)src;
-    if (bytes < 6 * sizeof(long long) || hdr[0] != kCacheMagic || hdr[1] != h.nt || hdr[2] != h.nv ||
+    long long hdr[6] = {0, 0, 0, 0, -1, 0};
+    if (bytes >= sizeof(hdr))
+    {
+        PB_CUDA(cudaMemcpyAsync(hdr, src, sizeof(hdr), cudaMemcpyDefault, h.stream));
+        PB_CUDA(cudaStreamSynchronize(h.stream));
+    }
+    if (bytes < sizeof(hdr) || hdr[0] != kCacheMagic || hdr[1] != h.nt || hdr[2] != h.nv ||
         hdr[3] != (long long)rec || hdr[4] < 0)
     {
         set_error("cache state: not a blob of this handle's mesh and precision");
         return PPPM_ERR_ARG;
     }
     const long long used = hdr[4];
+    journal_clear(h);  // the blob replaces the pool the checkpoints' logs refer to
     size_t need = 6 * sizeof(long long);
     for (const CachePart &p : cache_parts(h, used))
         need += p.bytes;
@@ -1036,21 +1370,25 @@ int cache_state_restore(Handle &h, const void *src, size_t bytes)
         dev_free(h.d_pool_w);
         dev_free(h.d_pool_scale);
         dev_free(h.d_pool_meta);
+        dev_free(h.d_pool_key);
         h.d_pool_w = nullptr;
         h.d_pool_scale = nullptr;
         h.d_pool_meta = nullptr;
+        h.d_pool_key = nullptr;
+        h.pool_cap = 0;
         const long long nc = used + used / 2 + 1024;
         PB_TRY(dev_alloc(&h.d_pool_w, (size_t)nc * rec));
         if (!h.fp64)
             PB_TRY(dalloc(&h.d_pool_scale, (size_t)nc));
         PB_TRY(dalloc(&h.d_pool_meta, (size_t)nc));
+        PB_TRY(dalloc(&h.d_pool_key, (size_t)nc));
         h.pool_cap = nc;
     }
-    const char *o = (const char *)src + 6 * sizeof(long long);
+    const char *o = (const char *)src + sizeof(hdr);
     for (const CachePart &p : cache_parts(h, used))
     {
         if (p.bytes)
-            PB_CUDA(cudaMemcpyAsync(p.dev, o, p.bytes, cudaMemcpyHostToDevice, h.stream));
+            PB_CUDA(cudaMemcpyAsync(p.dev, o, p.bytes, cudaMemcpyDefault, h.stream));
         o += p.bytes;
     }
     const int u = (int)used;
@@ -1065,6 +1403,14 @@ int cache_state_restore(Handle &h, const void *src, size_t bytes)
 
 int cache_free(Handle &h)
 {
+    journal_clear(h);
+    dev_free(h.d_pool_key);
+    dev_free(h.d_pair_old_meta);
+    dev_free(h.d_log_count);
+    h.d_pool_key = nullptr;
+    h.d_pair_old_meta = nullptr;
+    h.d_log_count = nullptr;
+    h.pair_old_meta_cap = 0;
     dev_free(h.d_gc_f);
     h.d_gc_f = nullptr;
     void *ptrs[] = {h.d_gc_w,      h.d_gc_scale,  h.d_gc_snap,   h.d_gc_flag,    h.d_fc_keys,
@@ -1163,6 +1509,7 @@ int cache_import_grid(Handle &h, const void *records)
 {
     if (h.fp64)
         return PPPM_ERR_ARG;
+    journal_clear(h);  // imported records are not logged: the checkpoints would not undo them
     cudaStream_t s = h.stream;
     size_t n = (size_t)h.nt * 54;
     void *tmp = nullptr;
@@ -1184,6 +1531,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n)
 {
     if (h.fp64)
         return PPPM_ERR_ARG;
+    journal_clear(h);  // imported records are not logged: the checkpoints would not undo them
     cudaStream_t s = h.stream;
     // (centre, neighbour) -> pool slot of the current face list
     std::vector<int> start(h.nt + 1), nbr(h.pf), pool(h.pf);

@@ -1457,6 +1457,40 @@ int pppm_restore_cache_state(pppm_handle *ph, const void *src, size_t bytes)
     return cache_state_restore(ph->h, src, bytes);
 }
 
+int pppm_checkpoint_push(pppm_handle *ph, int *id)
+{
+    PB_TRY(check_handle(ph));
+    if (!id)
+        return PPPM_ERR_ARG;
+    cudaSetDevice(ph->h.prm.device);
+    return journal_push(ph->h, id);
+}
+
+int pppm_checkpoint_rewind(pppm_handle *ph, int id)
+{
+    PB_TRY(check_handle(ph));
+    cudaSetDevice(ph->h.prm.device);
+    return journal_rewind(ph->h, id);
+}
+
+int pppm_checkpoint_clear(pppm_handle *ph)
+{
+    PB_TRY(check_handle(ph));
+    cudaSetDevice(ph->h.prm.device);
+    journal_clear(ph->h);
+    return PPPM_OK;
+}
+
+int pppm_checkpoint_info(pppm_handle *ph, int *count, size_t *bytes)
+{
+    PB_TRY(check_handle(ph));
+    if (count)
+        *count = journal_count(ph->h);
+    if (bytes)
+        *bytes = journal_bytes(ph->h);
+    return PPPM_OK;
+}
+
 int pppm_kernel_profile(pppm_handle *ph, int nkinds, float *us_per_launch, long long *launches)
 {
     PB_TRY(check_handle(ph));

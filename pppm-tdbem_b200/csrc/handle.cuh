@@ -149,8 +149,15 @@ struct Handle
     float2 *d_pool_scale = nullptr;
     float2 *d_pool_meta = nullptr;  // (normal angle, distance) at last refresh
     int *d_pool_count = nullptr;    // device counter
+    int2 *d_pool_key = nullptr;     // (centre, neighbour) of each pool slot
     long long pool_cap = 0;
     long long pool_used = 0;
+    // motion checkpoints (cache.cu): rewrites of pool slots below the newest checkpoint's pool
+    // size are logged with their old records, so a rewind undoes them
+    float2 *d_pair_old_meta = nullptr;  // pf scratch: a rewritten pair's meta before the refresh
+    long long pair_old_meta_cap = 0;
+    int *d_log_count = nullptr;         // [0] rewrites to log (lookup), [1] log cursor
+    struct Journal *journal = nullptr;
     int *d_pair_flag = nullptr;  // pf scratch: 1 = recompute
     int *d_status = nullptr;     // device-side status word (capacity / timeout)
     int *d_step_status = nullptr;  // step status word: non-finite values seen by the step kernels
@@ -282,8 +289,13 @@ void ghost_free(Handle &h);
 int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators
 int cache_free(Handle &h);
 size_t cache_state_bytes(Handle &h);                               // pppm_cache_state_size
-int cache_state_save(Handle &h, void *dst, size_t bytes);          // host buffer
-int cache_state_restore(Handle &h, const void *src, size_t bytes);  // host buffer; tables stale
+int cache_state_save(Handle &h, void *dst, size_t bytes);          // host or device buffer
+int cache_state_restore(Handle &h, const void *src, size_t bytes);  // host or device buffer; tables stale
+int journal_push(Handle &h, int *id);    // pppm_checkpoint_push
+int journal_rewind(Handle &h, int id);   // pppm_checkpoint_rewind; tables stale
+void journal_clear(Handle &h);           // pppm_checkpoint_clear
+size_t journal_bytes(const Handle &h);   // device bytes the checkpoints hold
+int journal_count(const Handle &h);
 int cache_regather(Handle &h);  // dense gathers + denominators from the persistent caches
 int cache_import_grid(Handle &h, const void *records);                         // nt x 54 x 72 B
 int cache_import_face(Handle &h, const int *pairs, const void *records, int n);  // n x 72 B

@@ -102,6 +102,10 @@ def _load():
         "pppm_cache_state_size": [vp, ctypes.POINTER(sz)],
         "pppm_save_cache_state": [vp, vp, sz],
         "pppm_restore_cache_state": [vp, vp, sz],
+        "pppm_checkpoint_push": [vp, ctypes.POINTER(i)],
+        "pppm_checkpoint_rewind": [vp, i],
+        "pppm_checkpoint_clear": [vp],
+        "pppm_checkpoint_info": [vp, ctypes.POINTER(i), ctypes.POINTER(sz)],
     }
     fl = ctypes.c_float
     sig["pppm_tdbem_constants"] = [fl, fl, fl, fp, fp]
@@ -235,6 +239,7 @@ class Solver:
         check(lib.pppm_create(ctypes.byref(p), ctypes.byref(self.h)), "pppm_create")
         self.res, self.dl, self.dt = int(res), float(dl), float(dt)
         self.precision = precision
+        self.device = int(device)
         self.real = np.float64 if precision == "fp64" else np.float32
         self.nt = 0
         self.nv = 0
@@ -407,19 +412,56 @@ class Solver:
         buf = np.ascontiguousarray(buf, dtype=np.uint8)
         check(lib.pppm_restore_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.size), "restore_state")
 
-    def save_cache_state(self):
-        """The motion-frame state of the weight caches (pppm_save_cache_state) as a host array."""
+    def save_cache_state(self, on_device=False):
+        """The motion-frame state of the weight caches (pppm_save_cache_state): a host uint8
+        array, or with on_device=True a uint8 CUDA tensor on the handle's device (HBM-resident
+        checkpoint)."""
         n = ctypes.c_size_t()
         check(lib.pppm_cache_state_size(self.h, ctypes.byref(n)), "cache_state_size")
-        buf = np.empty(n.value, np.uint8)
-        check(lib.pppm_save_cache_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), n.value), "save_cache_state")
+        if on_device:
+            import torch
+
+            dev = torch.device("cuda", self.device)
+            buf = torch.empty(n.value, dtype=torch.uint8, device=dev)
+            torch.cuda.current_stream(dev).synchronize()  # the block may still be in use there
+            ptr = ctypes.c_void_p(buf.data_ptr())
+        else:
+            buf = np.empty(n.value, np.uint8)
+            ptr = buf.ctypes.data_as(ctypes.c_void_p)
+        check(lib.pppm_save_cache_state(self.h, ptr, n.value), "save_cache_state")
         return buf
 
     def restore_cache_state(self, buf):
-        """Restore a saved cache state (pppm_restore_cache_state); update_mesh must follow."""
-        buf = np.ascontiguousarray(buf, dtype=np.uint8)
-        check(lib.pppm_restore_cache_state(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.size),
-              "restore_cache_state")
+        """Restore a saved cache state (pppm_restore_cache_state), host array or CUDA tensor;
+        update_mesh must follow."""
+        if hasattr(buf, "data_ptr"):
+            b = buf.contiguous()
+            ptr, size = ctypes.c_void_p(b.data_ptr()), b.numel() * b.element_size()
+        else:
+            b = np.ascontiguousarray(buf, dtype=np.uint8)
+            ptr, size = b.ctypes.data_as(ctypes.c_void_p), b.size
+        check(lib.pppm_restore_cache_state(self.h, ptr, size), "restore_cache_state")
+
+    def checkpoint_push(self):
+        """A motion checkpoint of the current frame's caches, kept in device memory by the
+        handle (pppm_checkpoint_push); returns its index."""
+        i = ctypes.c_int()
+        check(lib.pppm_checkpoint_push(self.h, ctypes.byref(i)), "checkpoint_push")
+        return i.value
+
+    def checkpoint_rewind(self, index):
+        """Caches back to checkpoint `index`, later checkpoints dropped (pppm_checkpoint_rewind);
+        update_mesh with that frame's vertices must follow."""
+        check(lib.pppm_checkpoint_rewind(self.h, int(index)), "checkpoint_rewind")
+
+    def checkpoint_clear(self):
+        check(lib.pppm_checkpoint_clear(self.h), "checkpoint_clear")
+
+    def checkpoint_info(self):
+        """(checkpoints held, device bytes they use)"""
+        n, b = ctypes.c_int(), ctypes.c_size_t()
+        check(lib.pppm_checkpoint_info(self.h, ctypes.byref(n), ctypes.byref(b)), "checkpoint_info")
+        return n.value, b.value
 
     # -- read-out
     def dump(self, what):

@@ -19,10 +19,12 @@ chained chunks.
 
 differentiates a moving run: frames = [(first_step, vertices), ...], motion frame f covering
 steps [first_f, first_{f+1}).  Its tables depend on the whole motion (the caches refresh only
-what moved), so the forward saves the caches' state at the start of every segment of about
-checkpoint_steps steps, and the backward differentiates the frames latest first, each with its
-own tables rebuilt from its segment's checkpoint (restore, then the segment's update_mesh calls
-up to that frame) - the geometry-side form of checkpointing with recomputation.
+what moved), so the forward takes a motion checkpoint of the caches at the start of every
+segment of about checkpoint_steps steps, and the backward differentiates the frames latest
+first, each with its own tables rebuilt from its segment's checkpoint (rewind, then the
+segment's update_mesh calls up to that frame) - checkpointing with recomputation on the
+geometry side.  The step is linear in the accelerations, so the reverse sweep itself needs no
+stored field state.
 """
 import numpy as np
 import torch
@@ -124,19 +126,20 @@ class _MovingSignal(torch.autograd.Function):
         cur = torch.cuda.current_stream(dev)
         if ext is not None:
             ext.wait_stream(cur)
-        checkpoints = {}
+        solver.checkpoint_clear()
+        ids = {}
         for f in range(len(frames)):
             if f:
                 solver.update_mesh(frames[f][1])
             if f in starts:
-                checkpoints[f] = solver.save_cache_state()
+                ids[f] = solver.checkpoint_push()
             solver.step(a[bounds[f]: bounds[f + 1]])
         dtype = torch.float64 if solver.precision == "fp64" else torch.float32
         out = torch.empty((n, solver.n_listeners), dtype=dtype, device=dev)
         solver.series(first, n, out=out)
         if ext is not None:
             cur.wait_stream(ext)
-        ctx.solver, ctx.frames, ctx.bounds, ctx.starts, ctx.checkpoints = solver, frames, bounds, starts, checkpoints
+        ctx.solver, ctx.frames, ctx.bounds, ctx.starts, ctx.ids = solver, frames, bounds, starts, ids
         ctx.acc_dtype = acc.dtype
         ctx.set_materialize_grads(False)
         return out
@@ -160,12 +163,13 @@ class _MovingSignal(torch.autograd.Function):
         for s0, s1 in reversed(list(zip(starts, ends))):
             for f in range(s1 - 1, s0 - 1, -1):
                 # frame f's tables: the segment's checkpoint, then its meshes up to frame f
-                solver.restore_cache_state(ctx.checkpoints[s0])
+                solver.checkpoint_rewind(ctx.ids[s0])
                 for ff in range(s0, f + 1):
                     solver.update_mesh(frames[ff][1])
                 a, b = bounds[f], bounds[f + 1]
                 solver.adjoint(g[a:b], fresh=fresh, out=grad[a:b])
                 fresh = False
+        solver.checkpoint_clear()
         if ext is not None:
             cur.wait_stream(ext)
         return grad.to(ctx.acc_dtype), None, None, None
@@ -173,7 +177,9 @@ class _MovingSignal(torch.autograd.Function):
 
 def moving_listener_signal(solver, acc, frames, checkpoint_steps=200):
     """The listener samples (nsteps, nlisteners) of a moving run of `solver` over the rows of
-    `acc`, differentiable with respect to acc.  frames: [(first_step, vertices), ...] with
-    first_step 0 first (its vertices are those the solver's mesh holds now).  After backward the
-    solver's geometry and fields are those of the replay, not of the run's end."""
+    `acc`, differentiable with respect to acc (one backward pass).  frames: [(first_step,
+    vertices), ...] with first_step 0 first (its vertices are those the solver's mesh holds now).
+    The motion checkpoints (pppm_checkpoint_*) stay in device memory until the backward ends;
+    the solver's own checkpoints are replaced.  After backward the solver's caches are those of
+    frame 0 and its fields those of the reverse sweep, not of the run's end."""
     return _MovingSignal.apply(acc, solver, list(frames), int(checkpoint_steps))

@@ -37,6 +37,12 @@ def sine_acc(steps, nt, freq, dt, first=0):
     return np.repeat(a[:, None], nt, 1)
 
 
+def dyadic(rng, shape, bits=10):
+    """standard normal samples rounded to multiples of 2^-bits (float32): x + eps v and x - eps v
+    are then exact in float32 for eps = 2^-3, so a central difference is taken about x itself"""
+    return (np.round(rng.standard_normal(shape) * 2.0 ** bits) / 2.0 ** bits).astype(np.float32)
+
+
 def rel_l2(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()

@@ -4,8 +4,9 @@ The listener samples of a run from the zero state are a linear function of the a
 series = A acc, so the adjoint must satisfy <g, A x> = <A^T g, x> for any x and g, and equal
 the Jacobian built column by column from unit impulses; both are checked in FP64 to ~1e-10.
 The gradient of a least-squares loss is checked against central finite differences of the
-forward along random directions (FP64: 1e-7; FP32: 1e-3) and the FP32 gradient against the FP64
-one.
+forward along random directions (FP64: 1e-9; FP32: 1e-3) and the FP32 gradient against the FP64
+one.  Inputs and directions are dyadic (multiples of 2^-10), so x +- eps v is exact in float32
+and the difference quotient of the quadratic loss is centred on x itself.
 
 When PPPM_METRICS_DIR is set the measured errors go to adjoint_metrics.json there.
 """
@@ -15,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import sphere_small
+from helpers import dyadic, sphere_small
 from pppm_b200 import PPPMError, Solver
 
 pytestmark = pytest.mark.gpu
@@ -122,13 +123,12 @@ def _fd_check(s, acc, target, grad, rng, ndir):
 
     worst = 0.0
     for _ in range(ndir):
-        v = rng.standard_normal(acc.shape).astype(np.float32)
-        eps = 1e-1
-        xp, xm = acc + np.float32(eps) * v, acc - np.float32(eps) * v  # float32 inputs, as the step takes
+        v = dyadic(rng, acc.shape)
+        eps = 0.125
+        xp, xm = acc + np.float32(eps) * v, acc - np.float32(eps) * v  # exact in float32 (dyadic inputs)
+        assert np.array_equal((xp.astype(np.float64) + xm) / 2, acc)
         fd = (loss(xp) - loss(xm)) / (2 * eps)
-        # the direction the float32 inputs actually differ by (their rounding included)
-        v_eff = (xp.astype(np.float64) - xm.astype(np.float64)) / (2 * eps)
-        an = float(np.sum(grad * v_eff))
+        an = float(np.sum(grad * v.astype(np.float64)))
         worst = max(worst, abs(fd - an) / max(abs(fd), 1e-300))
     return worst
 
@@ -140,8 +140,9 @@ def test_gradient_vs_finite_differences(gpu):
     n = 120
     s32, s64 = _solver("fp32", res=24, sub=2), _solver("fp64", res=24, sub=2)
     rng = np.random.default_rng(4)
-    acc = rng.standard_normal((n, s32.nt)).astype(np.float32)
-    target = rng.standard_normal((n, s32.n_listeners)) * 1e-3
+    acc = dyadic(rng, (n, s32.nt))
+    # a target on the signal's scale, so the difference quotient does not cancel
+    target = rng.standard_normal((n, s32.n_listeners)) * _forward(s64, acc).std()
     grad32 = s32.adjoint(2 * (_forward(s32, acc) - target))
     grad64 = s64.adjoint(2 * (_forward(s64, acc) - target))
     fd64 = _fd_check(s64, acc, target, grad64, rng, 16)
@@ -150,7 +151,7 @@ def test_gradient_vs_finite_differences(gpu):
     _record("fp64_vs_fd_max_rel", fd64)
     _record("fp32_vs_fd_max_rel", fd32)
     _record("fp32_vs_fp64_adjoint_rel_l2", rel)
-    assert fd64 <= 1e-7
+    assert fd64 <= 1e-9
     assert fd32 <= 1e-3
     assert rel <= 1e-2
     s32.close()

@@ -1,20 +1,23 @@
-"""Adjoint of a moving run: the cache checkpoints (pppm_save_cache_state / pppm_restore_cache_state)
-and pppm_b200.autograd.moving_listener_signal.
+"""Adjoint of a moving run: the motion checkpoints (pppm_checkpoint_*), the cache-state blobs
+(pppm_save_cache_state / pppm_restore_cache_state) and pppm_b200.autograd.moving_listener_signal.
 
 A moving run is still linear in the accelerations for a prescribed motion, series = A acc, with
 every step using the tables of its motion frame.  Those tables depend on the whole motion (the
 grid cache recomputes only the triangles that moved past its threshold, the face cache keeps the
 records of pairs it has seen), so the backward rebuilds them frame by frame from checkpoints.  Checked:
 
-  * a restore followed by the frame's update_mesh reproduces that frame's tables byte for byte
-    (FP32: fp16 records with their scales; FP64), and a replayed run reproduces the original
-    run's listener series bit for bit;
-  * stepping after a restore without update_mesh is refused; a blob of another mesh is refused;
+  * a rewind to a motion checkpoint (or a blob restore, host or device memory) followed by the
+    frame's update_mesh reproduces that frame's tables byte for byte (FP32: fp16 records with
+    their scales; FP64), on a breathing sphere whose face records are rewritten every frame, and
+    a replayed run reproduces the original run's listener series bit for bit;
+  * stepping or a new checkpoint after a rewind without update_mesh is refused, as is a rewind
+    to a dropped checkpoint or a blob of another mesh;
   * FP64: <g, A x> = <A^T g, x> to 1e-10 and the Jacobian column by column (unit impulses) to 1e-10,
     across motion frames that move triangles into other cells;
   * the gradient does not depend on the checkpoint spacing (bit-identical);
-  * each precision's gradient against central differences of its own forward, the FP32 gradient
-    against the FP64 one.
+  * each precision's gradient against central differences of its own forward (dyadic inputs and
+    directions, so the difference quotient is centred exactly: FP64 1e-9, FP32 1e-3), the FP32
+    gradient against the FP64 one.
 
 When PPPM_METRICS_DIR is set the measured errors go to adjoint_moving_metrics.json there.
 """
@@ -24,7 +27,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import sphere_small
+from helpers import dyadic, sphere_small
 from pppm_b200 import PPPMError, Solver, scenes
 
 pytestmark = pytest.mark.gpu
@@ -50,6 +53,18 @@ def _frames(v0, h, nframes, every):
     for k in range(nframes):
         R = scenes.rotation_matrix([0.3, 0.5, 0.8], 0.15 * k)
         v = v0.astype(np.float64) @ R.T + np.array([0.35, 0.2, -0.1]) * float(h) * k
+        out.append((k * every, v.astype(np.float32)))
+    return out
+
+
+def _breathing_frames(v0, h, nframes, every):
+    """the drift of _frames with the sphere scaled by 1 + 0.03 k about its centre: every face
+    pair's distance changes by more than 1 % per frame, so the face cache rewrites its records
+    in place (the case the motion checkpoints log)"""
+    c = v0.astype(np.float64).mean(0)
+    out = []
+    for k in range(nframes):
+        v = (v0.astype(np.float64) - c) * (1 + 0.03 * k) + c + np.array([0.35, 0.2, -0.1]) * float(h) * k
         out.append((k * every, v.astype(np.float32)))
     return out
 
@@ -93,9 +108,60 @@ def _replay(s, ckpt0, x, frames):
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_cache_state_restores_the_frame_tables(gpu, precision):
+def test_checkpoint_rewind_restores_the_frame_tables(gpu, precision):
+    """motion checkpoints (pppm_checkpoint_*): the pool stays in place and its rewrites are
+    logged; a rewind plus the frame's update_mesh gives the frame's tables byte for byte"""
     s, v0, h = _solver(precision)
-    frames = _frames(v0, h, 6, 10)
+    frames = _breathing_frames(v0, h, 6, 10)
+    x = np.random.default_rng(11).standard_normal((60, s.nt)).astype(np.float32)
+    bounds = [f[0] for f in frames] + [60]
+    want, ids = {}, {}
+    for k, (_, v) in enumerate(frames):
+        if k:
+            s.update_mesh(v)
+        want[k] = _tables(s)
+        if k in (0, 2, 4):
+            ids[k] = s.checkpoint_push()
+        s.step(x[bounds[k]: bounds[k + 1]])
+    series = s.series(0, 60).astype(np.float64)
+    count, held = s.checkpoint_info()
+    assert count == 3 and held > 0
+    assert want[1]["face_cache"] != want[2]["face_cache"]  # records rewritten in place
+    for ck, frames_to_check in ((4, (5, 4)), (2, (3, 2))):
+        for k in frames_to_check:
+            s.checkpoint_rewind(ids[ck])
+            with pytest.raises(PPPMError):
+                s.step(x[:1])  # the lists still describe the geometry before the rewind
+            with pytest.raises(PPPMError):
+                s.checkpoint_push()
+            for j in range(ck, k + 1):
+                s.update_mesh(frames[j][1])
+            got = _tables(s)
+            assert [t for t in TABLES if got[t] != want[k][t]] == [], (ck, k)
+    assert s.checkpoint_info()[0] == 2  # rewinding to checkpoint 2 dropped the one of frame 4
+    # from frame 0 again: every frame's tables and the whole series as in the first run
+    s.checkpoint_rewind(ids[0])
+    s.update_mesh(frames[0][1])
+    s.reset_fields()
+    s.rewind_listeners()
+    for k, (_, v) in enumerate(frames):
+        if k:
+            s.update_mesh(v)
+        got = _tables(s)
+        assert [t for t in TABLES if got[t] != want[k][t]] == [], k
+        s.step(x[bounds[k]: bounds[k + 1]])
+    assert np.array_equal(s.series(0, 60).astype(np.float64), series)
+    with pytest.raises(PPPMError):
+        s.checkpoint_rewind(3)
+    s.checkpoint_clear()
+    assert s.checkpoint_info() == (0, 0)
+    s.close()
+
+
+@pytest.mark.parametrize("precision,on_device", [("fp32", True), ("fp64", False), ("fp32", False)])
+def test_cache_state_restores_the_frame_tables(gpu, precision, on_device):
+    s, v0, h = _solver(precision)
+    frames = _breathing_frames(v0, h, 6, 10)
     x = np.random.default_rng(1).standard_normal((60, s.nt)).astype(np.float32)
     ckpt0 = s.save_cache_state()
     bounds = [f[0] for f in frames] + [60]
@@ -104,7 +170,7 @@ def test_cache_state_restores_the_frame_tables(gpu, precision):
         if k:
             s.update_mesh(v)
         want[k] = _tables(s)
-        ckpt[k] = s.save_cache_state()
+        ckpt[k] = s.save_cache_state(on_device=on_device)
         s.step(x[bounds[k]: bounds[k + 1]])
     series = s.series(0, 60).astype(np.float64)
     # the motion reaches new cells and new face pairs
@@ -124,7 +190,7 @@ def test_cache_state_restores_the_frame_tables(gpu, precision):
     # a blob of another mesh
     o, _, _ = _solver(precision, sub=0)
     with pytest.raises(PPPMError):
-        o.restore_cache_state(ckpt0)
+        o.restore_cache_state(ckpt[2])
     o.close()
     s.close()
 
@@ -205,9 +271,12 @@ def test_moving_gradient_vs_finite_differences(gpu):
         frames = _frames(v0, h, 6, 15)
         ckpt0 = s.save_cache_state()
         if precision == "fp64":
-            acc = rng.standard_normal((n, s.nt)).astype(np.float32)
-            target = rng.standard_normal((n, s.n_listeners)) * 1e-3
-            dirs = [rng.standard_normal(acc.shape).astype(np.float32) for _ in range(8)]
+            acc = dyadic(rng, (n, s.nt))
+            # a target on the signal's scale: the difference quotient then does not cancel
+            base = _replay(s, ckpt0, acc, frames)
+            target = rng.standard_normal((n, s.n_listeners)) * base.std()
+            dirs = [dyadic(rng, acc.shape) for _ in range(8)]
+            _to_start(s, ckpt0, frames)
         # float64 leaves for the FP64 scheme: the gradient comes back in the leaf's dtype
         x = torch.tensor(acc.astype(s.real), device="cuda", requires_grad=True)
         sig = moving_listener_signal(s, x, frames, checkpoint_steps=40)
@@ -220,11 +289,10 @@ def test_moving_gradient_vs_finite_differences(gpu):
 
         worst = 0.0
         for v in dirs:
-            eps = 1e-1
-            xp, xm = acc + np.float32(eps) * v, acc - np.float32(eps) * v
+            eps = 0.125
+            xp, xm = acc + np.float32(eps) * v, acc - np.float32(eps) * v  # exact: dyadic inputs
             fd = (f(xp) - f(xm)) / (2 * eps)
-            v_eff = (xp.astype(np.float64) - xm.astype(np.float64)) / (2 * eps)
-            an = float(np.sum(grad * v_eff))
+            an = float(np.sum(grad * v.astype(np.float64)))
             worst = max(worst, abs(fd - an) / max(abs(fd), 1e-300))
         res[precision] = (grad, worst)
         s.close()
@@ -232,6 +300,6 @@ def test_moving_gradient_vs_finite_differences(gpu):
     _record("moving_fp64_vs_fd_max_rel", res["fp64"][1])
     _record("moving_fp32_vs_fd_max_rel", res["fp32"][1])
     _record("moving_fp32_vs_fp64_rel_l2", rel)
-    assert res["fp64"][1] <= 1e-7
+    assert res["fp64"][1] <= 1e-9
     assert res["fp32"][1] <= 1e-3
     assert rel <= 1e-2
