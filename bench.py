@@ -1033,6 +1033,22 @@ def run_adjoint_moving(args, ws, rank, local):
     launches = s.launch_count() - launches0
     p_ms, f_ms, b_ms = max_over_ranks(ws, p_ms), max_over_ranks(ws, f_ms), max_over_ranks(ws, b_ms)
     finite = bool(torch.isfinite(grad).all().item())
+
+    # where the backward's time goes: the reverse sweep on one frame's tables, one rebuild of
+    # the transposed tables after a mesh update, one update_mesh
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    g1 = torch.ones((200, 1), dtype=torch.float32, device=dev)
+    s.adjoint(g1[:1], fresh=True)  # tables of the current frame
+    sweep_ms = timed(lambda: s.adjoint(g1, fresh=True))
+    upd_ms = timed(lambda: s.update_mesh(frames[1][1]))
+    one_ms = timed(lambda: s.adjoint(g1[:1], fresh=True))  # rebuilds the tables, then one step
     s.close()
     cells = float(sc.res) ** 3
     return {
@@ -1048,6 +1064,9 @@ def run_adjoint_moving(args, ws, rank, local):
         "plain_run_ms": round(p_ms / K, 2), "forward_ms": round(f_ms / K, 2), "backward_ms": round(b_ms / K, 2),
         "checkpoint_overhead": round(f_ms / p_ms - 1, 4), "backward_vs_plain_run": round(b_ms / p_ms, 4),
         "checkpoints": peak["checkpoints"], "checkpoint_bytes": int(peak["bytes"]),
+        "adjoint_us_per_step_fixed_tables": round(sweep_ms * 1e3 / 200, 2),
+        "forward_us_per_step_plain": round(p_ms * 1e3 / (K * nsteps), 2),
+        "table_rebuild_ms": round(one_ms - sweep_ms / 200, 3), "update_mesh_ms": round(upd_ms, 3),
         "plain_gcell_steps_per_s": round(cells * nsteps * K * ws / (p_ms * 1e-3) / 1e9, 3),
         "gradient_finite": finite, "cpu_baseline": None, "e2e": None, "gpu_launches": int(launches), "clocks": clk,
     }

@@ -245,10 +245,12 @@ int pppm_restore_cache_state(pppm_handle *h, const void *src, size_t bytes);
  * that frame's vertices must follow before pppm_step / pppm_adjoint, which return
  * PPPM_ERR_STATE until then; further pppm_update_mesh calls replay the motion with the tables
  * the run had).  Checkpoints go on pppm_checkpoint_clear, pppm_set_mesh, a cache-state restore
- * or a weight import.  pppm_checkpoint_info: how many are held and the device bytes they use. */
+ * or a weight import.  Their device memory is an arena kept for the next run of checkpoints
+ * until pppm_checkpoint_clear with release != 0 (or pppm_set_mesh / pppm_destroy) frees it.
+ * pppm_checkpoint_info: how many are held and the device bytes the arena and logs use. */
 int pppm_checkpoint_push(pppm_handle *h, int *id);
 int pppm_checkpoint_rewind(pppm_handle *h, int id);
-int pppm_checkpoint_clear(pppm_handle *h);
+int pppm_checkpoint_clear(pppm_handle *h, int release);
 int pppm_checkpoint_info(pppm_handle *h, int *count, size_t *bytes);
 
 /* ------------------------------------------------------------ weight diagnostics ----- */

@@ -67,6 +67,12 @@ struct Adjoint
     void *nT_w = nullptr;        // [p3T][2][16]: the pair's FDTD-near (shifted) and BEM-near records
     float2 *nT_scale = nullptr;  // [p3T][2] (FP32 weights)
     int *cT_cell = nullptr, *cT_start = nullptr, *cT_ref = nullptr;    // corner cells: (tri * 8 + k)
+    // the transposes' scratch; every table array grows only (a moving sweep rebuilds the tables
+    // every motion frame), with its capacity in cap[] (elements; bytes for the weights)
+    int *d_count = nullptr, *d_cursor = nullptr;  // per key
+    int *d_order = nullptr, *d_owner = nullptr;   // per value
+    int *d_flag = nullptr;                        // res^3 + 1 corner-cell flags, then their scan
+    long long cap[17] = {};
     // adjoint state
     void *lam[3] = {nullptr, nullptr, nullptr};
     void *lam_b = nullptr;  // 4 x res^3 (boundary layer only)
@@ -495,50 +501,147 @@ __global__ void near_records_kernel(const typename AdjWRec<R>::T *gc_w, const fl
     }
 }
 
-template <typename T>
-int upload(Handle &h, T **d, const std::vector<T> &v)
+// ---- transposed tables, built on the device (counting transposes, values ascending per key)
+
+__global__ void key_count_kernel(const int *key, long long n, int *count)
 {
-    dev_free(*d);
-    *d = nullptr;
-    PB_TRY(dalloc(d, std::max<size_t>(v.size(), 1)));
-    if (!v.empty())
-        PB_CUDA(cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h.stream));
-    return PPPM_OK;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        atomicAdd(&count[key[i]], 1);
+}
+
+__global__ void key_fill_kernel(const int *key, long long n, const int *start, int *cursor, int *order)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        order[start[key[i]] + atomicAdd(&cursor[key[i]], 1)] = (int)i;
+}
+
+// each key's values ascending: the fill's atomic order is arbitrary, the sweep's sums must not be
+__global__ void key_sort_kernel(const int *start, int nkeys, int *order)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nkeys)
+        return;
+    const int b = start[k], e = start[k + 1];
+    for (int i = b + 1; i < e; i++)
+    {
+        const int v = order[i];
+        int j = i - 1;
+        while (j >= b && order[j] > v)
+        {
+            order[j + 1] = order[j];
+            j--;
+        }
+        order[j + 1] = v;
+    }
+}
+
+// owner[p] = the segment of a CSR (start[nseg + 1]) that holds position p; one warp per segment
+__global__ void owner_kernel(const int *start, int nseg, int *owner)
+{
+    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= nseg)
+        return;
+    for (int p = start[w] + lane; p < start[w + 1]; p += 32)
+        owner[p] = w;
+}
+
+__global__ void gather_int_kernel(const int *src, const int *idx, long long n, int *out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = src[idx[i]];
+}
+
+// corner cells lie in the grid whenever the lists could be built (triangles at least two cells
+// inside it); the bound keeps the writes in range regardless
+__global__ void flag_cells_kernel(const int *cell, long long n, long long ncells, int *flag)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && cell[i] >= 0 && cell[i] < ncells)
+        flag[cell[i]] = 1;
+}
+
+// the distinct corner cells in ascending order (pos: exclusive scan of the flags) and each
+// corner's rank among them
+__global__ void corner_rank_kernel(const int *cell, long long n, long long ncells, const int *pos, int *rank)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        rank[i] = cell[i] >= 0 && cell[i] < ncells ? pos[cell[i]] : 0;
+}
+
+__global__ void compact_cells_kernel(const int *flag, const int *pos, long long ncells, int *out)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncells && flag[c])
+        out[pos[c]] = (int)c;
 }
 
 template <typename T>
-int download(Handle &h, std::vector<T> &v, const T *d, size_t n)
+int grow(T **p, long long &cap, long long need)
 {
-    v.resize(n);
-    if (n)
-        PB_CUDA(cudaMemcpyAsync(v.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, h.stream));
+    need = std::max<long long>(need, 1);
+    if (need <= cap)
+        return PPPM_OK;
+    dev_free(*p);
+    *p = nullptr;
+    const long long nc = need + need / 4 + 64;
+    PB_TRY(dalloc(p, (size_t)nc));
+    cap = nc;
     return PPPM_OK;
 }
 
-// CSR of (key -> values) from pairs given in value order, stable within a key
-void transpose_csr(int nkeys, const std::vector<int> &keys, std::vector<int> &start, std::vector<int> &order)
+int grow_bytes(void **p, long long &cap, long long need)
 {
-    start.assign(nkeys + 1, 0);
-    for (int k : keys)
-        start[k + 1]++;
-    for (int k = 0; k < nkeys; k++)
-        start[k + 1] += start[k];
-    std::vector<int> cursor(start.begin(), start.end() - 1);
-    order.resize(keys.size());
-    for (size_t p = 0; p < keys.size(); p++)
-        order[cursor[keys[p]]++] = (int)p;
+    need = std::max<long long>(need, 1);
+    if (need <= cap)
+        return PPPM_OK;
+    dev_free(*p);
+    *p = nullptr;
+    const long long nc = need + need / 4 + 256;
+    PB_TRY(dev_alloc(p, (size_t)nc));
+    cap = nc;
+    return PPPM_OK;
+}
+
+// start[nkeys + 1], order[n]: the positions p of key[p] grouped by key, ascending inside a key
+int transpose_dev(Handle &h, Adjoint &A, const int *key, long long n, int nkeys, int *start, int *order)
+{
+    cudaStream_t s = h.stream;
+    const int T = 256;
+    PB_TRY(grow(&A.d_count, A.cap[15], (long long)nkeys + 1));
+    PB_TRY(grow(&A.d_cursor, A.cap[16], (long long)nkeys + 1));
+    PB_CUDA(cudaMemsetAsync(A.d_count, 0, sizeof(int) * (size_t)(nkeys + 1), s));
+    PB_CUDA(cudaMemsetAsync(A.d_cursor, 0, sizeof(int) * (size_t)(nkeys + 1), s));
+    if (n > 0)
+        key_count_kernel<<<div_up(n, T), T, 0, s>>>(key, n, A.d_count);
+    PB_TRY(exclusive_scan(h, A.d_count, start, nkeys));
+    if (n > 0)
+    {
+        key_fill_kernel<<<div_up(n, T), T, 0, s>>>(key, n, start, A.d_cursor, order);
+        key_sort_kernel<<<div_up(nkeys, T), T, 0, s>>>(start, nkeys, order);
+        h.launches += 3;
+    }
+    PB_CHECK_LAUNCH();
+    return PPPM_OK;
 }
 
 void adj_free_tables(Adjoint &A)
 {
-    void **ptrs[] = {(void **)&A.fT_start, (void **)&A.fT_src,   &A.fT_w,  (void **)&A.fT_scale,
-                     (void **)&A.nT_start, (void **)&A.nT_cell,  (void **)&A.nT_pair, &A.nT_w,
-                     (void **)&A.nT_scale, (void **)&A.cT_cell,  (void **)&A.cT_start, (void **)&A.cT_ref};
+    void **ptrs[] = {(void **)&A.fT_start, (void **)&A.fT_src,   &A.fT_w,   (void **)&A.fT_scale,
+                     (void **)&A.nT_start, (void **)&A.nT_cell,  (void **)&A.nT_pair,  &A.nT_w,
+                     (void **)&A.nT_scale, (void **)&A.cT_cell,  (void **)&A.cT_start, (void **)&A.cT_ref,
+                     (void **)&A.d_count,  (void **)&A.d_cursor, (void **)&A.d_order,  (void **)&A.d_owner,
+                     (void **)&A.d_flag};
     for (void **p : ptrs)
     {
         dev_free(*p);
         *p = nullptr;
     }
+    for (long long &c : A.cap)
+        c = 0;
 }
 
 void adj_free_state(Adjoint &A)
@@ -552,91 +655,79 @@ void adj_free_state(Adjoint &A)
     A.g_cap = A.out_cap = 0;
 }
 
+// The transposed tables of the current geometry: face pairs by neighbour (with the centre and
+// the re-packed weights), 3^3 pairs by triangle (with the corrected cell and the near records),
+// corner references by cell.  All on the device; one synchronisation reads the number of
+// distinct corner cells.  Capacities only grow, so a sweep over many motion frames allocates
+// once.
 template <typename R>
 int build_tables(Handle &h, Adjoint &A)
 {
     using W = typename AdjWRec<R>::T;
-    adj_free_tables(A);
-    const int nt = h.nt, n3 = h.n3;
-    std::vector<int> face_start, face_nbr, n3_start, p3_tri, corner, n3_cell;
-    PB_TRY(download(h, face_start, h.d_face_start, (size_t)nt + 1));
-    PB_CUDA(cudaStreamSynchronize(h.stream));
-    const long long pf = face_start[nt];
-    PB_TRY(download(h, face_nbr, h.d_face_nbr, (size_t)pf));
-    PB_TRY(download(h, n3_start, h.d_n3_start, (size_t)n3 + 1));
-    PB_TRY(download(h, corner, h.d_face_corner, (size_t)nt * 8));
-    PB_CUDA(cudaStreamSynchronize(h.stream));
-    const long long p3 = n3 ? n3_start[n3] : 0;
-    PB_TRY(download(h, p3_tri, h.d_p3_tri, (size_t)p3));
-    PB_CUDA(cudaStreamSynchronize(h.stream));
-
-    // face pairs by neighbour
-    std::vector<int> start, order;
-    transpose_csr(nt, face_nbr, start, order);
-    std::vector<int> src(pf), pair(pf);
-    {
-        std::vector<int> centre(pf);
-        for (int i = 0; i < nt; i++)
-            for (int p = face_start[i]; p < face_start[i + 1]; p++)
-                centre[p] = i;
-        for (long long k = 0; k < pf; k++)
-        {
-            pair[k] = order[k];
-            src[k] = centre[order[k]];
-        }
-    }
-    PB_TRY(upload(h, &A.fT_start, start));
-    PB_TRY(upload(h, &A.fT_src, src));
-    int *d_pair = nullptr;
-    PB_TRY(upload(h, &d_pair, pair));
-    PB_TRY(dev_alloc(&A.fT_w, (size_t)std::max<long long>(pf, 1) * kTaps * sizeof(W)));
+    cudaStream_t s = h.stream;
+    const int nt = h.nt, n3 = h.n3, T = 256;
+    const long long pf = h.pf, p3 = h.p3, nc8 = (long long)nt * 8, ncells = h.n_cells;
+    const long long wsz = (long long)sizeof(W);
+    long long *c = A.cap;
+    PB_TRY(grow(&A.d_order, c[0], std::max(std::max(pf, p3), nc8)));
+    PB_TRY(grow(&A.d_owner, c[1], std::max(pf, p3)));
+    PB_TRY(grow(&A.fT_start, c[2], nt + 1));
+    PB_TRY(grow(&A.fT_src, c[3], pf));
+    PB_TRY(grow_bytes(&A.fT_w, c[4], pf * kTaps * wsz));
     if (!h.fp64)
-        PB_TRY(dalloc(&A.fT_scale, (size_t)std::max<long long>(pf, 1)));
+        PB_TRY(grow(&A.fT_scale, c[5], pf));
+    PB_TRY(grow(&A.nT_start, c[6], nt + 1));
+    PB_TRY(grow(&A.nT_cell, c[7], p3));
+    PB_TRY(grow(&A.nT_pair, c[8], p3));
+    PB_TRY(grow_bytes(&A.nT_w, c[9], p3 * 2 * kTaps * wsz));
+    if (!h.fp64)
+        PB_TRY(grow(&A.nT_scale, c[10], 2 * p3));
+    PB_TRY(grow(&A.d_flag, c[11], 2 * (ncells + 1)));
+    PB_TRY(grow(&A.cT_ref, c[12], nc8));
+    int *order = A.d_order, *owner = A.d_owner;
+
+    // face pairs by neighbour; fT_src = centre of each transposed pair
+    PB_TRY(transpose_dev(h, A, h.d_face_nbr, pf, nt, A.fT_start, order));
     if (pf > 0)
-        shift_face_kernel<R><<<div_up(pf * kTaps, 256), 256, 0, h.stream>>>(
-            (const W *)h.d_face_w, h.fp64 ? nullptr : h.d_face_scale, d_pair, pf, (W *)A.fT_w, A.fT_scale);
-    h.launches++;
-    A.pfT = pf;
-
-    // near pairs by triangle
-    transpose_csr(nt, p3_tri, start, order);
-    std::vector<int> cell(p3);
     {
-        std::vector<int> owner(p3);
-        for (int c = 0; c < n3; c++)
-            for (int p = n3_start[c]; p < n3_start[c + 1]; p++)
-                owner[p] = c;
-        for (long long k = 0; k < p3; k++)
-            cell[k] = owner[order[k]];
+        owner_kernel<<<div_up((long long)nt * 32, T), T, 0, s>>>(h.d_face_start, nt, owner);
+        gather_int_kernel<<<div_up(pf, T), T, 0, s>>>(owner, order, pf, A.fT_src);
+        shift_face_kernel<R><<<div_up(pf * kTaps, T), T, 0, s>>>(
+            (const W *)h.d_face_w, h.fp64 ? nullptr : h.d_face_scale, order, pf, (W *)A.fT_w, A.fT_scale);
+        h.launches += 3;
     }
-    PB_TRY(upload(h, &A.nT_start, start));
-    PB_TRY(upload(h, &A.nT_cell, cell));
-    PB_TRY(upload(h, &A.nT_pair, order));
-    PB_TRY(dev_alloc(&A.nT_w, (size_t)std::max<long long>(p3, 1) * 2 * kTaps * sizeof(W)));
-    if (!h.fp64)
-        PB_TRY(dalloc(&A.nT_scale, (size_t)std::max<long long>(p3, 1) * 2));
+    A.pfT = pf;
+    PB_CHECK_LAUNCH();
+
+    // 3^3 pairs by triangle; nT_cell = corrected-cell index of each transposed pair
+    PB_TRY(transpose_dev(h, A, h.d_p3_tri, p3, nt, A.nT_start, A.nT_pair));
     if (p3 > 0)
-        near_records_kernel<R><<<div_up(p3 * kTaps, 256), 256, 0, h.stream>>>(
+    {
+        owner_kernel<<<div_up((long long)std::max(n3, 1) * 32, T), T, 0, s>>>(h.d_n3_start, n3, owner);
+        gather_int_kernel<<<div_up(p3, T), T, 0, s>>>(owner, A.nT_pair, p3, A.nT_cell);
+        near_records_kernel<R><<<div_up(p3 * kTaps, T), T, 0, s>>>(
             (const W *)h.d_gc_w, h.fp64 ? nullptr : h.d_gc_scale, h.d_p3_tri, h.d_p3_woff, A.nT_pair, p3,
             (W *)A.nT_w, A.nT_scale);
-    h.launches++;
+        h.launches += 3;
+    }
     A.p3T = p3;
-
-    // corner cells
-    std::vector<int> cells(corner.begin(), corner.end());
-    std::sort(cells.begin(), cells.end());
-    cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
-    std::vector<int> key(corner.size());
-    for (size_t r = 0; r < corner.size(); r++)
-        key[r] = (int)(std::lower_bound(cells.begin(), cells.end(), corner[r]) - cells.begin());
-    transpose_csr((int)cells.size(), key, start, order);
-    PB_TRY(upload(h, &A.cT_cell, cells));
-    PB_TRY(upload(h, &A.cT_start, start));
-    PB_TRY(upload(h, &A.cT_ref, order));
-    A.ncorner = (int)cells.size();
-    PB_CUDA(cudaStreamSynchronize(h.stream));
-    dev_free(d_pair);
     PB_CHECK_LAUNCH();
+
+    // corner references by cell: the distinct corner cells ascending, each corner's rank
+    int *flag = A.d_flag, *pos = A.d_flag + (ncells + 1);
+    PB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)(ncells + 1), s));
+    flag_cells_kernel<<<div_up(nc8, T), T, 0, s>>>(h.d_face_corner, nc8, ncells, flag);
+    h.launches++;
+    PB_TRY(exclusive_scan(h, flag, pos, ncells));
+    int ncorner = 0;
+    PB_TRY(read_int(h, pos + ncells, &ncorner));
+    PB_TRY(grow(&A.cT_cell, c[13], ncorner));
+    PB_TRY(grow(&A.cT_start, c[14], (long long)ncorner + 1));
+    compact_cells_kernel<<<div_up(ncells, T), T, 0, s>>>(flag, pos, ncells, A.cT_cell);
+    corner_rank_kernel<<<div_up(nc8, T), T, 0, s>>>(h.d_face_corner, nc8, ncells, pos, order);
+    h.launches += 2;
+    PB_TRY(transpose_dev(h, A, order, nc8, ncorner, A.cT_start, A.cT_ref));
+    A.ncorner = ncorner;
     A.nt = nt;
     A.n3 = n3;
     A.version = h.mesh_version;

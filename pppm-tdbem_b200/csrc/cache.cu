@@ -862,16 +862,21 @@ struct LogBatch
 
 struct MotionCheckpoint
 {
-    void *buf = nullptr;
+    void *buf = nullptr;  // a chunk of the journal's arena
     size_t bytes = 0;
     long long used = 0;
     bool gc_empty = false;
     std::vector<LogBatch> log;
 };
 
+// Checkpoints live in an arena of slabs (slab i holds 8 * 2^i checkpoints of `chunk` bytes), so
+// a run of many checkpoints costs a few allocations, and a cleared journal keeps its slabs for
+// the next run unless released.
 struct Journal
 {
     std::vector<MotionCheckpoint> stack;
+    std::vector<void *> slabs;
+    size_t chunk = 0;
 };
 
 namespace
@@ -910,8 +915,36 @@ void free_checkpoint(MotionCheckpoint &c)
     for (LogBatch &b : c.log)
         dev_free(b.buf);
     c.log.clear();
-    dev_free(c.buf);
-    c.buf = nullptr;
+    c.buf = nullptr;  // its chunk stays in the arena
+}
+
+// the arena chunk of checkpoint k (slabs allocated as needed)
+int arena_chunk(Journal &J, int k, size_t chunk, void **out)
+{
+    if (J.chunk != chunk)
+    {
+        for (void *p : J.slabs)
+            dev_free(p);
+        J.slabs.clear();
+        J.chunk = chunk;
+    }
+    int base = 0;
+    for (size_t i = 0;; i++)
+    {
+        const int n = 8 << i;
+        if (i == J.slabs.size())
+        {
+            void *p = nullptr;
+            PB_TRY(dev_alloc(&p, chunk * (size_t)n));
+            J.slabs.push_back(p);
+        }
+        if (k < base + n)
+        {
+            *out = (char *)J.slabs[i] + chunk * (size_t)(k - base);
+            return PPPM_OK;
+        }
+        base += n;
+    }
 }
 }  // namespace
 
@@ -923,28 +956,35 @@ size_t journal_bytes(const Handle &h)
 {
     size_t b = 0;
     if (h.journal)
+    {
+        for (size_t i = 0; i < h.journal->slabs.size(); i++)
+            b += h.journal->chunk * (size_t)(8 << i);
         for (const MotionCheckpoint &c : h.journal->stack)
-        {
-            b += c.bytes;
             for (const LogBatch &l : c.log)
             {
                 size_t off[4], total;
                 log_layout(h, l.n, off, &total);
                 b += total;
             }
-        }
+    }
     return b;
 }
 
-void journal_clear(Handle &h)
+void journal_clear(Handle &h, bool release)
 {
     if (!h.journal)
         return;
     cudaStreamSynchronize(h.stream);
     for (MotionCheckpoint &c : h.journal->stack)
         free_checkpoint(c);
-    delete h.journal;
-    h.journal = nullptr;
+    h.journal->stack.clear();
+    if (release)
+    {
+        for (void *p : h.journal->slabs)
+            dev_free(p);
+        delete h.journal;
+        h.journal = nullptr;
+    }
 }
 
 // the old records of the n slots below `floor` that this refresh recomputes, appended to the
@@ -995,17 +1035,11 @@ int journal_push(Handle &h, int *id)
     MotionCheckpoint c;
     for (const Span &p : checkpoint_parts(h))
         c.bytes += align16(p.bytes);
-    PB_TRY(dev_alloc(&c.buf, c.bytes));
+    PB_TRY(arena_chunk(*h.journal, (int)h.journal->stack.size(), (c.bytes + 255) & ~(size_t)255, &c.buf));
     char *o = (char *)c.buf;
     for (const Span &p : checkpoint_parts(h))
     {
-        const cudaError_t e = cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDeviceToDevice, h.stream);
-        if (e != cudaSuccess)
-        {
-            dev_free(c.buf);
-            set_error("CUDA error %s at %s:%d", cudaGetErrorString(e), __FILE__, __LINE__);
-            return PPPM_ERR_CUDA;
-        }
+        PB_CUDA(cudaMemcpyAsync(o, p.dev, p.bytes, cudaMemcpyDeviceToDevice, h.stream));
         o += align16(p.bytes);
     }
     c.used = h.pool_used;
@@ -1358,7 +1392,7 @@ int cache_state_restore(Handle &h, const void *src, size_t bytes)
         return PPPM_ERR_ARG;
     }
     const long long used = hdr[4];
-    journal_clear(h);  // the blob replaces the pool the checkpoints' logs refer to
+    journal_clear(h, false);  // the blob replaces the pool the checkpoints' logs refer to
     size_t need = 6 * sizeof(long long);
     for (const CachePart &p : cache_parts(h, used))
         need += p.bytes;
@@ -1403,7 +1437,7 @@ int cache_state_restore(Handle &h, const void *src, size_t bytes)
 
 int cache_free(Handle &h)
 {
-    journal_clear(h);
+    journal_clear(h, true);
     dev_free(h.d_pool_key);
     dev_free(h.d_pair_old_meta);
     dev_free(h.d_log_count);
@@ -1509,7 +1543,7 @@ int cache_import_grid(Handle &h, const void *records)
 {
     if (h.fp64)
         return PPPM_ERR_ARG;
-    journal_clear(h);  // imported records are not logged: the checkpoints would not undo them
+    journal_clear(h, false);  // imported records are not logged: the checkpoints would not undo them
     cudaStream_t s = h.stream;
     size_t n = (size_t)h.nt * 54;
     void *tmp = nullptr;
@@ -1531,7 +1565,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n)
 {
     if (h.fp64)
         return PPPM_ERR_ARG;
-    journal_clear(h);  // imported records are not logged: the checkpoints would not undo them
+    journal_clear(h, false);  // imported records are not logged: the checkpoints would not undo them
     cudaStream_t s = h.stream;
     // (centre, neighbour) -> pool slot of the current face list
     std::vector<int> start(h.nt + 1), nbr(h.pf), pool(h.pf);

@@ -1473,11 +1473,11 @@ int pppm_checkpoint_rewind(pppm_handle *ph, int id)
     return journal_rewind(ph->h, id);
 }
 
-int pppm_checkpoint_clear(pppm_handle *ph)
+int pppm_checkpoint_clear(pppm_handle *ph, int release)
 {
     PB_TRY(check_handle(ph));
     cudaSetDevice(ph->h.prm.device);
-    journal_clear(ph->h);
+    journal_clear(ph->h, release != 0);
     return PPPM_OK;
 }
 

@@ -293,8 +293,8 @@ int cache_state_save(Handle &h, void *dst, size_t bytes);          // host or de
 int cache_state_restore(Handle &h, const void *src, size_t bytes);  // host or device buffer; tables stale
 int journal_push(Handle &h, int *id);    // pppm_checkpoint_push
 int journal_rewind(Handle &h, int id);   // pppm_checkpoint_rewind; tables stale
-void journal_clear(Handle &h);           // pppm_checkpoint_clear
-size_t journal_bytes(const Handle &h);   // device bytes the checkpoints hold
+void journal_clear(Handle &h, bool release);  // pppm_checkpoint_clear (release: free the arena too)
+size_t journal_bytes(const Handle &h);   // device bytes the checkpoints' arena and logs hold
 int journal_count(const Handle &h);
 int cache_regather(Handle &h);  // dense gathers + denominators from the persistent caches
 int cache_import_grid(Handle &h, const void *records);                         // nt x 54 x 72 B

@@ -104,7 +104,7 @@ def _load():
         "pppm_restore_cache_state": [vp, vp, sz],
         "pppm_checkpoint_push": [vp, ctypes.POINTER(i)],
         "pppm_checkpoint_rewind": [vp, i],
-        "pppm_checkpoint_clear": [vp],
+        "pppm_checkpoint_clear": [vp, i],
         "pppm_checkpoint_info": [vp, ctypes.POINTER(i), ctypes.POINTER(sz)],
     }
     fl = ctypes.c_float
@@ -454,11 +454,13 @@ class Solver:
         update_mesh with that frame's vertices must follow."""
         check(lib.pppm_checkpoint_rewind(self.h, int(index)), "checkpoint_rewind")
 
-    def checkpoint_clear(self):
-        check(lib.pppm_checkpoint_clear(self.h), "checkpoint_clear")
+    def checkpoint_clear(self, release=False):
+        """Drop every checkpoint (pppm_checkpoint_clear); release=True frees their device memory
+        too, else it is kept for the next checkpoints."""
+        check(lib.pppm_checkpoint_clear(self.h, 1 if release else 0), "checkpoint_clear")
 
     def checkpoint_info(self):
-        """(checkpoints held, device bytes they use)"""
+        """(checkpoints held, device bytes their arena and logs use)"""
         n, b = ctypes.c_int(), ctypes.c_size_t()
         check(lib.pppm_checkpoint_info(self.h, ctypes.byref(n), ctypes.byref(b)), "checkpoint_info")
         return n.value, b.value

@@ -179,7 +179,8 @@ def moving_listener_signal(solver, acc, frames, checkpoint_steps=200):
     """The listener samples (nsteps, nlisteners) of a moving run of `solver` over the rows of
     `acc`, differentiable with respect to acc (one backward pass).  frames: [(first_step,
     vertices), ...] with first_step 0 first (its vertices are those the solver's mesh holds now).
-    The motion checkpoints (pppm_checkpoint_*) stay in device memory until the backward ends;
-    the solver's own checkpoints are replaced.  After backward the solver's caches are those of
+    The motion checkpoints (pppm_checkpoint_*) stay in device memory until the backward ends,
+    their arena until solver.checkpoint_clear(release=True) (a training loop reuses it); the
+    solver's own checkpoints are replaced.  After backward the solver's caches are those of
     frame 0 and its fields those of the reverse sweep, not of the run's end."""
     return _MovingSignal.apply(acc, solver, list(frames), int(checkpoint_steps))

@@ -154,6 +154,8 @@ def test_checkpoint_rewind_restores_the_frame_tables(gpu, precision):
     with pytest.raises(PPPMError):
         s.checkpoint_rewind(3)
     s.checkpoint_clear()
+    assert s.checkpoint_info()[0] == 0 and s.checkpoint_info()[1] > 0  # the arena is kept
+    s.checkpoint_clear(release=True)
     assert s.checkpoint_info() == (0, 0)
     s.close()
 
