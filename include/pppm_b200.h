@@ -204,7 +204,7 @@ int pppm_batch_run(pppm_batch *b, const float *const *acc, const int *nsteps, in
 /* No counterpart in the reference.  Gradient of L = sum_s sum_l dL_dsignal[s][l] * p_l(s)
  * over nsteps consecutive forward steps with respect to those steps' accelerations,
  * dL_dacc[s][tri], with the weight tables, lists and corrected cells the handle holds now
- * (the absorbing boundary; PML handles return PPPM_ERR_ARG).  The listener samples are linear
+ * (the absorbing boundary or the PML, whichever the handle uses).  The listener samples are linear
  * in the accelerations, so the gradient does not depend on the forward state and no forward
  * state is stored: the transposed step runs backwards in time on adjoint state of the forward
  * state's size.  fresh != 0 starts a new reverse sweep (the nsteps steps are the last ones of

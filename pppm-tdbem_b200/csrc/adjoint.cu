@@ -76,6 +76,7 @@ struct Adjoint
     // adjoint state
     void *lam[3] = {nullptr, nullptr, nullptr};
     void *lam_b = nullptr;  // 4 x res^3 (boundary layer only)
+    void *psi[2] = {nullptr, nullptr};  // PML: 6 x res^3 each, adjoints of the auxiliary fields
     void *acc_n = nullptr, *acc_d = nullptr;  // [nt][kRing] accumulation rings (slot = tau mod 32)
     void *lam_f = nullptr;                    // [nt] adjoint of the face numerator at the current step
     int pos = 0;               // one past the next time the reverse sweep processes
@@ -144,6 +145,13 @@ struct AdjArgs
     R *acc_n, *acc_d, *lam_f;
     double kappa;                 // (c dt / h)^2: interior leapfrog coefficient
     R coef, coef1, coef2, coef3;  // boundary solve coefficients (fdtd.cu:88-137)
+    // the PML (pml_width > 0): adjoints of the six auxiliary fields per cell at two times
+    // (slot = time mod 2) and the update's coefficients (fdtd.cu:179-232)
+    R *psi[2];
+    int pml_w;
+    double pml_damp;                      // 2 / h inside the layer
+    double pml_k, pml_ih2, pml_ih;        // (c dt)^2, 1 / h^2, 1 / h
+    double pml_cdt, pml_i2h;              // c dt, 1 / (2 h)
     __device__ R *slot(int tau) const { return lam[((tau % 3) + 3) % 3]; }
 };
 
@@ -450,6 +458,97 @@ __global__ void __launch_bounds__(256) adj_stencil_kernel(const __grid_constant_
     lp[i] = (R)prev;
 }
 
+
+// P7 with the PML (pml_width > 0; no boundary solve, P6 does not run): the split-field update
+// (fdtd.cu:179-232) transposed, one thread per cell of the whole grid.  Forward at a cell q of
+// [1, res-2]^3, with K = (c dt)^2, sd = +1 above the grid's middle plane along d and -1 below,
+// ps = q + sd e_d, ms = q - sd e_d, w(x) the damping at cell x (2/h inside the layer, else 0):
+//   p^t[q] = 2 p^{t-1}[q] - p^{t-2}[q] + K sum_d [(p^{t-1}[q+e_d] - 2 p^{t-1}[q] + p^{t-1}[q-e_d]) / h^2
+//            + (w(q) psi^{t-1}[ps]_{3+d} - w(ms) psi^{t-1}[ms]_d) / h]
+// and, where w(q) != 0 (elsewhere the fields stay zero),
+//   psi^t[q]_d     = psi^{t-1}[q]_d + c dt (-(w(ms) psi^{t-1}[ms]_d + w(q) psi^{t-1}[q]_d) / 2 - g_d)
+//   psi^t[q]_{3+d} = psi^{t-1}[q]_{3+d} + c dt (-(w(ms) psi^{t-1}[q]_{3+d} + w(q) psi^{t-1}[ps]_{3+d}) / 2 - g_d)
+// with g_d = (p^{t-1}[ps] - p^{t-1}[ms]) / (2 h).  The ghost layer holds zeros that nothing
+// writes, so only cells of [1, res-2]^3 carry adjoints.  A cell j is read by itself and by its six
+// neighbours q = j + s e_d; for such a q, j is ps of q when sd(q) = -s and ms of q when sd(q) = s.
+__device__ inline bool in_pml(int x, int y, int z, int res, int w)
+{
+    return x < w || x >= res - w || y < w || y >= res - w || z < w || z >= res - w;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) adj_pml_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.ncells)
+        return;
+    const int res = a.res, w = a.pml_w;
+    const int y[3] = {(int)(i / ((long long)res * res)), (int)((i / res) % res), (int)(i % res)};
+    const R *ln = a.slot(sigma);             // adjoint of p^sigma (the stencil's output)
+    const R *pn = a.psi[sigma & 1];          // adjoint of psi^sigma
+    R *lc = a.slot(sigma - 1), *lp = a.slot(sigma - 2);
+    R *pc = a.psi[(sigma - 1) & 1];          // adjoint of psi^{sigma-1}, written here
+    auto inside = [&](const int *x) {
+        return x[0] >= 1 && x[0] <= res - 2 && x[1] >= 1 && x[1] <= res - 2 && x[2] >= 1 && x[2] <= res - 2;
+    };
+    auto damp = [&](const int *x) { return in_pml(x[0], x[1], x[2], res, w) ? a.pml_damp : 0.0; };
+    if (!inside(y))
+    {
+        lp[i] = 0;
+#pragma unroll
+        for (int k = 0; k < 6; k++)
+            pc[6 * i + k] = 0;
+        return;
+    }
+    const double K = a.pml_k, ih2 = a.pml_ih2, ih = a.pml_ih, cdt = a.pml_cdt, i2h = a.pml_i2h;
+    const double wj = damp(y);
+    const double lj = ln[i];
+    double cur = (2 - 6 * K * ih2) * lj;
+    double ps[6] = {0, 0, 0, 0, 0, 0};
+    if (wj != 0)
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+        {
+            // psi^sigma[j] from psi^{sigma-1}[j]
+            int m[3] = {y[0], y[1], y[2]};
+            m[d] -= y[d] > res / 2 ? 1 : -1;
+            ps[d] += (1 - cdt * wj / 2) * (double)pn[6 * i + d];
+            ps[3 + d] += (1 - cdt * damp(m) / 2) * (double)pn[6 * i + 3 + d];
+        }
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int s = -1; s <= 1; s += 2)
+        {
+            int x[3] = {y[0], y[1], y[2]};
+            x[d] += s;  // the reading cell q
+            if (!inside(x))
+                continue;
+            const long long xi = ((long long)x[0] * res + x[1]) * res + x[2];
+            const double lq = ln[xi], wq = damp(x);
+            cur += K * ih2 * lq;
+            const int sq = x[d] > res / 2 ? 1 : -1;
+            const double pd = wq != 0 ? (double)pn[6 * xi + d] : 0.0, pd3 = wq != 0 ? (double)pn[6 * xi + 3 + d] : 0.0;
+            if (sq == -s)
+            {
+                // j = ps of q: p^sigma[q] reads psi_{3+d} of j; psi^sigma[q] reads p of j and psi_{3+d} of j
+                ps[3 + d] += K * wq * ih * lq - cdt * wq / 2 * pd3;
+                cur -= cdt * i2h * (pd + pd3);
+            }
+            else
+            {
+                // j = ms of q: p^sigma[q] reads psi_d of j (damped by w(j)); psi^sigma[q] reads p of j and psi_d of j
+                ps[d] += -K * wj * ih * lq - cdt * wj / 2 * pd;
+                cur += cdt * i2h * (pd + pd3);
+            }
+        }
+    lc[i] = (R)((double)lc[i] + cur);
+    lp[i] = (R)(-lj);
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        pc[6 * i + k] = wj != 0 ? (R)ps[k] : (R)0;  // psi^{sigma-1}[j] is zero where j is undamped
+}
+
 // ---- tables
 template <typename R>
 __global__ void shift_face_kernel(const typename AdjWRec<R>::T *w, const float2 *scale, const int *pair, long long n,
@@ -646,7 +745,8 @@ void adj_free_tables(Adjoint &A)
 
 void adj_free_state(Adjoint &A)
 {
-    void **ptrs[] = {&A.lam[0], &A.lam[1], &A.lam[2], &A.lam_b, &A.acc_n, &A.acc_d, &A.lam_f, &A.d_g, &A.d_out};
+    void **ptrs[] = {&A.lam[0], &A.lam[1], &A.lam[2], &A.lam_b, &A.acc_n, &A.acc_d, &A.lam_f, &A.d_g, &A.d_out,
+                     &A.psi[0], &A.psi[1]};
     for (void **p : ptrs)
     {
         dev_free(*p);
@@ -743,6 +843,10 @@ int alloc_state(Handle &h, Adjoint &A)
             PB_TRY(dev_alloc(&A.lam[i], (size_t)h.n_cells * rs));
     if (!A.lam_b)
         PB_TRY(dev_alloc(&A.lam_b, (size_t)4 * h.n_cells * rs));
+    if (h.prm.pml_width > 0)
+        for (int i = 0; i < 2; i++)
+            if (!A.psi[i])
+                PB_TRY(dev_alloc(&A.psi[i], (size_t)6 * h.n_cells * rs));
     // per triangle: the triangle count is fixed by the topology, so a sweep keeps these across
     // geometry changes
     if (!A.acc_n)
@@ -763,6 +867,9 @@ int zero_state(Handle &h, Adjoint &A)
     PB_CUDA(cudaMemsetAsync(A.acc_n, 0, (size_t)std::max(h.nt, 1) * kRing * rs, h.stream));
     PB_CUDA(cudaMemsetAsync(A.acc_d, 0, (size_t)std::max(h.nt, 1) * kRing * rs, h.stream));
     PB_CUDA(cudaMemsetAsync(A.lam_f, 0, (size_t)std::max(h.nt, 1) * rs, h.stream));
+    for (int i = 0; i < 2; i++)
+        if (A.psi[i])
+            PB_CUDA(cudaMemsetAsync(A.psi[i], 0, (size_t)6 * h.n_cells * rs, h.stream));
     return PPPM_OK;
 }
 
@@ -813,6 +920,17 @@ AdjArgs<R> make_adj_args(Handle &h, Adjoint &A)
     a.coef1 = 1 / (dt * dt);
     a.coef2 = c / (2 * hh * dt);
     a.coef3 = -(c * c) / (2 * hh * hh);
+    for (int i = 0; i < 2; i++)
+        a.psi[i] = (R *)A.psi[i];
+    a.pml_w = h.prm.pml_width;
+    // the forward's own coefficients (pml_kernel: c, dt, h as the step's floats)
+    const double pc = (float)h.prm.c, pdt = (float)h.prm.dt, ph = (float)h.prm.dl;
+    a.pml_damp = (double)(2.0f / h.prm.dl);
+    a.pml_k = pc * pc * pdt * pdt;
+    a.pml_ih2 = 1 / (ph * ph);
+    a.pml_ih = 1 / ph;
+    a.pml_cdt = pc * pdt;
+    a.pml_i2h = 1 / (ph * 2);
     return a;
 }
 
@@ -853,8 +971,13 @@ int run_adjoint(Handle &h, const R *g, int nsteps, R *out, int fresh)
         if (a.ncorner > 0)
             adj_corner_kernel<R><<<div_up(a.ncorner, T), T, 0, s>>>(a, sigma);
         adj_fdtd_near_kernel<R><<<tw, T, 0, s>>>(a, sigma);
-        adj_boundary_kernel<R><<<div_up(nbd, T), T, 0, s>>>(a, sigma);
-        adj_stencil_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
+        if (a.pml_w > 0)
+            adj_pml_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
+        else
+        {
+            adj_boundary_kernel<R><<<div_up(nbd, T), T, 0, s>>>(a, sigma);
+            adj_stencil_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
+        }
         PB_CHECK_LAUNCH();
         h.launches += 5 + (a.nl > 0) + (a.ncorner > 0);
     }

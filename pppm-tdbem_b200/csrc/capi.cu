@@ -707,11 +707,6 @@ int pppm_adjoint(pppm_handle *ph, const void *dL_dsignal, int nsteps, int on_dev
         set_error("adjoint needs a mesh");
         return PPPM_ERR_STATE;
     }
-    if (h.prm.pml_width > 0)
-    {
-        set_error("the adjoint covers the absorbing boundary; this handle uses the PML");
-        return PPPM_ERR_ARG;
-    }
     const int nl = (int)h.listen_xyz.size() / 3;
     for (int k = 0; k < 3 * nl; k++)
         if (h.listen_xyz[k] < 1 || h.listen_xyz[k] > h.res - 2)

@@ -32,15 +32,17 @@ def _record(key, value):
             json.dump(METRICS, f, indent=1)
 
 
-def _solver(precision="fp64", res=20, sub=1, shell_listener=True):
+def _solver(precision="fp64", res=20, sub=1, shell_listener=True, pml_width=0):
     v, f, h, mn, dt = sphere_small(res, sub)
-    s = Solver(res, h, dt, mn, precision=precision)
+    s = Solver(res, h, dt, mn, precision=precision, pml_width=pml_width)
     s.set_mesh(v, f)
     s.add_listener(res - 4, res - 4, res - 4)  # far field
     c = s.dump("n3_cells").reshape(-1, 4)[0]
     s.add_listener(int(c[0]), int(c[1]), int(c[2]))  # a corrected cell
     if shell_listener:
-        s.add_listener(1, res // 2, res // 3)  # boundary layer
+        s.add_listener(1, res // 2, res // 3)  # boundary layer (inside the PML when there is one)
+    if pml_width:
+        s.add_listener(res - 2 - pml_width // 2, res // 2 + 1, res // 2)  # inside the PML, upper side
     return s
 
 
@@ -179,14 +181,46 @@ def test_autograd_chunks(gpu):
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_pml_dot_product(gpu, precision):
+    """The split-field PML (fdtd.cu:179-232) transposed: <g, A x> = <A^T g, x> over a run long
+    enough for the waves to enter the layer and for its auxiliary fields to feed back, with
+    listeners in the field, at a corrected cell, on the boundary layer and inside the PML."""
+    s = _solver(precision, res=20, pml_width=4)
+    n = 110
+    rng = np.random.default_rng(6)
+    x = rng.standard_normal((n, s.nt)).astype(np.float32)
+    g = rng.standard_normal((n, s.n_listeners))
+    y = _forward(s, x)
+    gx = s.adjoint(g)
+    lhs, rhs = float(np.sum(g * y)), float(np.sum(gx * x.astype(np.float64)))
+    scale = float(np.sum(np.abs(g * y)))
+    _record("pml_dot_product_%s_rel" % precision, abs(lhs - rhs) / scale)
+    # FP64: the exact transpose; FP32: the forward rounds in float, the adjoint of the exact map
+    assert abs(lhs - rhs) <= (1e-10 if precision == "fp64" else 1e-4) * scale, (lhs, rhs)
+    s.close()
+
+
+def test_pml_gradient_vs_finite_differences(gpu):
+    n = 100
+    s32, s64 = _solver("fp32", res=22, sub=1, pml_width=4), _solver("fp64", res=22, sub=1, pml_width=4)
+    rng = np.random.default_rng(7)
+    acc = dyadic(rng, (n, s32.nt))
+    target = rng.standard_normal((n, s32.n_listeners)) * _forward(s64, acc).std()
+    grad32 = s32.adjoint(2 * (_forward(s32, acc) - target))
+    grad64 = s64.adjoint(2 * (_forward(s64, acc) - target))
+    fd64 = _fd_check(s64, acc, target, grad64, rng, 8)
+    fd32 = _fd_check(s32, acc, target, grad32, rng, 8)
+    _record("pml_fp64_vs_fd_max_rel", fd64)
+    _record("pml_fp32_vs_fd_max_rel", fd32)
+    assert fd64 <= 1e-9
+    assert fd32 <= 1e-3
+    s32.close()
+    s64.close()
+
+
 def test_adjoint_rejects(gpu):
     v, f, h, mn, dt = sphere_small(24, 1)
-    p = Solver(24, h, dt, mn, pml_width=3)
-    p.set_mesh(v, f)
-    p.add_listener(12, 12, 20)
-    with pytest.raises(PPPMError):
-        p.adjoint(np.zeros((4, 1)))
-    p.close()
     s = Solver(24, h, dt, mn)
     s.set_mesh(v, f)
     s.add_listener(0, 12, 12)  # outer ghost layer: no sample is ever recorded there
