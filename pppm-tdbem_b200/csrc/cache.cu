@@ -142,18 +142,28 @@ __device__ inline void gc_point_offset(int p, int &dx, int &dy, int &dz)
     dz = axis == 2 ? far : b;
 }
 
-__global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float *verts, const int *tris,
-                                                       const int *cellc, const float *center, const float *normal,
-                                                       const float *area, const int *flag, __half2 *gc_w,
-                                                       float2 *gc_scale, float *snap)
+__global__ void __launch_bounds__(256, 4) gc_block_kernel(DevConsts dc, const float *verts, const int *tris,
+                                                          const int *cellc, const float *center, const float *normal,
+                                                          const float *area, const int *flag, __half2 *gc_w,
+                                                          float2 *gc_scale, float *snap)
 {
     const int tri = blockIdx.x;
     if (!flag[tri])
         return;
-    __shared__ ref32::PointTerms terms[kGcPoints][kTaps / 2 + 1];
-    __shared__ short point_of[125];                  // 5^3 offset box -> distinct point
-    __shared__ cf spec[27][kTaps / 2 + 1][4];        // ss, sd, qs, qd per record and wave number
-    __shared__ float wts[27][4][kTaps];              // their 16-tap weights
+    // The point terms of steps 1-2 and, once they are consumed, the 16-tap weights, the two
+    // records' rows and their scales of steps 3-4 share one buffer (37 KB per block in all, so
+    // four blocks fit an SM).
+    constexpr int kWave = kTaps / 2 + 1;
+    __shared__ __align__(16) unsigned char pool[kGcPoints * kWave * sizeof(ref32::PointTerms)];
+    static_assert(2 * 27 * 4 * kTaps * sizeof(float) + 54 * 2 * sizeof(float) <=
+                      kGcPoints * kWave * sizeof(ref32::PointTerms),
+                  "weights, rows and scales fit in the point-term buffer");
+    auto terms = reinterpret_cast<ref32::PointTerms(*)[kWave]>(pool);
+    auto wts = reinterpret_cast<float(*)[4][kTaps]>(pool);  // per offset: ss, sd, qs, qd rows
+    auto rows = reinterpret_cast<float(*)[2][kTaps]>(pool + 27 * 4 * kTaps * sizeof(float));  // 54 records
+    auto rmax = reinterpret_cast<float(*)[2]>(pool + 2 * 27 * 4 * kTaps * sizeof(float));    // their scales
+    __shared__ short point_of[125];            // 5^3 offset box -> distinct point
+    __shared__ cf spec[27][kWave][4];          // ss, sd, qs, qd per record and wave number
     const int tid = threadIdx.x;
     f3 v[3];
     int idx[3];
@@ -164,9 +174,9 @@ __global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float
     const float gx = (float)PB_TRI_X;
     const f3 q = ref32::local_to_global(gx, gx, v);
     // 1. the Green's function terms of every distinct cell centre and wave number
-    for (int it = tid; it < kGcPoints * (kTaps / 2 + 1); it += blockDim.x)
+    for (int it = tid; it < kGcPoints * kWave; it += blockDim.x)
     {
-        const int p = it / (kTaps / 2 + 1), k = it % (kTaps / 2 + 1);
+        const int p = it / kWave, k = it % kWave;
         int dx, dy, dz;
         gc_point_offset(p, dx, dy, dz);
         if (k == 0)
@@ -179,9 +189,9 @@ __global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float
     // its centre (BEM-near), accumulated in the reference's order
     const float scale = dc.c * dc.c * dc.dt * dc.dt / (dc.h * dc.h);
     const double c = 0.5 * 1.0f * jac;
-    for (int it = tid; it < 27 * (kTaps / 2 + 1); it += blockDim.x)
+    for (int it = tid; it < 27 * kWave; it += blockDim.x)
     {
-        const int woff = it / (kTaps / 2 + 1), k = it % (kTaps / 2 + 1);
+        const int woff = it / kWave, k = it % kWave;
         const int ox = woff % 3 - 1, oy = woff / 3 % 3 - 1, oz = woff / 9 - 1;
         const int sx[8] = {0, -1, 1, 0, 0, 0, 0, 0}, sy[8] = {0, 0, 0, -1, 1, 0, 0, 0},
                   sz[8] = {0, 0, 0, 0, 0, -1, 1, 0};
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float
         spec[woff][k][3] = cf{(float)(0.0f + c * bd.re), (float)(0.0f + c * bd.im)};
     }
     __syncthreads();
-    // 3. one 16-point transform per (record, layer row)
+    // 3. one 16-point transform per (record, layer row); the point terms are dead from here on
     for (int it = tid; it < 27 * 4; it += blockDim.x)
     {
         const int woff = it / 4, which = it % 4;
@@ -213,39 +223,56 @@ __global__ void __launch_bounds__(256) gc_block_kernel(DevConsts dc, const float
         spectrum_to_weights(sp, dc.lambda, wts[woff][which], dc.tw);
     }
     __syncthreads();
-    // 4. move(-1), subtract the BEM-near weights two steps back, pack both records
-    for (int woff = tid; woff < 27; woff += blockDim.x)
+    // 4. per (offset, tap): the FDTD-near record (moved by one step, minus the BEM-near weights
+    // two steps back) and the BEM-near record; the triangle's own cell has neither.  Records
+    // 0..26 are the FDTD-near ones, 27..53 the BEM-near ones.
+    for (int it = tid; it < 27 * kTaps; it += blockDim.x)
     {
-        const bool inside = woff == 13;  // the triangle's own cell
-        float ws[kTaps], wd[kTaps];
-        ws[0] = 0;
-        wd[0] = 0;
-        for (int i = 1; i < kTaps; i++)
+        const int woff = it / kTaps, i = it % kTaps;
+        const bool inside = woff == 13;
+        float ws = 0, wd = 0;
+        if (i >= 1)
         {
-            ws[i] = wts[woff][0][i - 1];
-            wd[i] = wts[woff][1][i - 1];
+            ws = wts[woff][0][i - 1];
+            wd = wts[woff][1][i - 1];
         }
+        if (!inside && i >= 2)
+        {
+            ws += wts[woff][2][i - 2] * -1.0f;
+            wd += wts[woff][3][i - 2] * -1.0f;
+        }
+        float bs = 0, bd = 0;
         if (!inside)
-            for (int i = 2; i < kTaps; i++)
-            {
-                ws[i] += wts[woff][2][i - 2] * -1.0f;
-                wd[i] += wts[woff][3][i - 2] * -1.0f;
-            }
-        const size_t rec = (size_t)tri * 54 + woff;
-        pack_half(ws, wd, gc_w + rec * kTaps, gc_scale + rec);
-        float bs[kTaps], bd[kTaps];
+        {
+            bs += wts[woff][2][i] * 1.0f;
+            bd += wts[woff][3][i] * 1.0f;
+        }
+        rows[woff][0][i] = ws;
+        rows[woff][1][i] = wd;
+        rows[27 + woff][0][i] = bs;
+        rows[27 + woff][1][i] = bd;
+    }
+    __syncthreads();
+    // 5. fp16 packing (pack_half, bem.h:171-191): each row's max-abs scale, taps in order ...
+    for (int it = tid; it < 54 * 2; it += blockDim.x)
+    {
+        const float *row = rows[it >> 1][it & 1];
+        float m = 0;
         for (int i = 0; i < kTaps; i++)
-        {
-            bs[i] = 0;
-            bd[i] = 0;
-        }
-        if (!inside)
-            for (int i = 0; i < kTaps; i++)
-            {
-                bs[i] += wts[woff][2][i] * 1.0f;
-                bd[i] += wts[woff][3][i] * 1.0f;
-            }
-        pack_half(bs, bd, gc_w + (rec + 27) * kTaps, gc_scale + rec + 27);
+            m = max(m, abs(row[i]));
+        rmax[it >> 1][it & 1] = m == 0 ? 1.0f : m;
+    }
+    __syncthreads();
+    // ... then every (record, tap) rounded to half, single and double layer in one half2
+    for (int it = tid; it < 54 * kTaps; it += blockDim.x)
+    {
+        const int r = it / kTaps, i = it % kTaps;
+        const float ms = rmax[r][0], md = rmax[r][1];
+        const float a = rows[r][0][i] / ms, b = rows[r][1][i] / md;
+        const size_t rec = (size_t)tri * 54 + r;
+        gc_w[rec * kTaps + i] = __halves2half2(__float2half_rn(a), __float2half_rn(b));
+        if (i == 0)
+            gc_scale[rec] = make_float2(ms, md);
     }
     if (tid == 0)
     {
@@ -1175,8 +1202,18 @@ int cache_refresh(Handle &h)
                                                                              h.d_gc_flag, nt, (double2 *)h.d_gc_w,
                                                                              h.d_gc_snap);
     else
+    {
+        // four blocks of 37 KB shared memory per SM: ask for the largest shared-memory carve-out
+        static bool carveout_set = false;
+        if (!carveout_set)
+        {
+            PB_CUDA(cudaFuncSetAttribute(gc_block_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared));
+            carveout_set = true;
+        }
         gc_block_kernel<<<nt, 256, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc, h.d_center, h.d_normal, h.d_area,
                                            h.d_gc_flag, (__half2 *)h.d_gc_w, h.d_gc_scale, h.d_gc_snap);
+    }
     h.launches++;
     PB_CHECK_LAUNCH();
     h.gc_empty = false;
@@ -1190,11 +1227,13 @@ int cache_refresh(Handle &h)
     PB_CHECK_LAUNCH();
     if (h.pf > 0)
     {
-        // every pair may be new: make room for pf more records
+        // every pair may be new: make room for pf more records.  The first pool holds three
+        // times that (the next update asks for pool_used + pf, about twice pf), so a moving scene
+        // does not move its pool in its first frames; later growth is by half.
         long long need = h.pool_used + h.pf;
         if (need > h.pool_cap)
         {
-            long long nc = need + need / 2 + 1024;
+            long long nc = (h.pool_cap == 0 ? 3 * need : need + need / 2) + 1024;
             void *nw = nullptr;
             float2 *nsc = nullptr, *nmeta = nullptr;
             int2 *nkey = nullptr;

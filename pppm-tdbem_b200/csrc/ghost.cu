@@ -277,10 +277,11 @@ __device__ inline void spmv(const GhostStep &a, const float *in, float *out)
 
 // one step of the ghost-cell method after the FDTD update (one block; tnew: the new time level)
 __global__ void __launch_bounds__(1024) ghost_step_kernel(const __grid_constant__ GhostStep a, const StepState *st,
-                                                          int kstep, int nt, float *series)
+                                                          int kstep, int nt)
 {
     __shared__ float red[32];
     const StepDyn dy = bind_step(st, kstep, nt);
+    float *series = (float *)dy.series;
     float *p = a.grid[((dy.tnew % 3) + 3) % 3];
     const float *acc = dy.acc;
     const int G = a.count, res = a.g.res;
@@ -521,9 +522,9 @@ GhostStep ghost_args(Handle &h, int n_listen, const int *listen_cell)
     return a;
 }
 
-void ghost_launch(const GhostStep &a, const StepState *st, int kstep, int nt, float *series, cudaStream_t s)
+void ghost_launch(const GhostStep &a, const StepState *st, int kstep, int nt, cudaStream_t s)
 {
-    ghost_step_kernel<<<1, 1024, 0, s>>>(a, st, kstep, nt, series);
+    ghost_step_kernel<<<1, 1024, 0, s>>>(a, st, kstep, nt);
 }
 
 int ghost_read(Handle &h, int what, void *dst, size_t bytes)

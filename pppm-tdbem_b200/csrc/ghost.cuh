@@ -28,6 +28,6 @@ struct GhostStep
 // the arguments of the per-step ghost kernel for the handle's current ghost system
 GhostStep ghost_args(Handle &h, int n_listen, const int *listen_cell);
 // one step of the ghost-cell method after the FDTD update of step kstep (one block)
-void ghost_launch(const GhostStep &a, const StepState *st, int kstep, int nt, float *series, cudaStream_t s);
+void ghost_launch(const GhostStep &a, const StepState *st, int kstep, int nt, cudaStream_t s);
 
 }  // namespace pb

@@ -44,6 +44,9 @@ struct StepState
     // when their partner (the next time) is at most pair_end; pair_end < pair0: one pass per step
     int pair0 = 0, pair_end = -1;
     int conv_pairs = 0, terms_pairs = 0;  // which stages use the pairing (the handle's options)
+    // listener series (R elements, row0 is its row of the first step), or null: read from here
+    // rather than recorded into the graphs, so a series that grows keeps the recorded graphs valid
+    void *series = nullptr;
 };
 
 // what step k of a call produces: its time index, listener-series row and acceleration row
@@ -52,6 +55,7 @@ struct StepDyn
     int tnew;
     long long row;
     const float *acc;
+    void *series;
 };
 
 __device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
@@ -60,6 +64,7 @@ __device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
     d.tnew = st->tnew0 + k;
     d.row = st->row0 + k;
     d.acc = st->acc ? st->acc + (long long)k * nt : nullptr;
+    d.series = st->series;
     return d;
 }
 

@@ -257,8 +257,9 @@ __device__ inline R interior_cell(const StepArgs &a, const R *__restrict__ cur, 
 // the stencil work of block b of one scene's stencil grid (256 threads)
 template <typename R>
 __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, int b, StencilSplit sp,
-                                    const unsigned *corr_mask, R *series)
+                                    const unsigned *corr_mask)
 {
+    R *series = (R *)dy.series;
     R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
     const R *prev = ring.slot(dy.tnew - 2);
     const int res = a.res;
@@ -304,9 +305,9 @@ __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, cons
 template <typename R>
 __global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ StepArgs a0,
                                                        const __grid_constant__ Ring<R> ring, const StepState *st, int k,
-                                                       StencilSplit sp, const unsigned *corr_mask, R *series)
+                                                       StencilSplit sp, const unsigned *corr_mask)
 {
-    stencil_body<R>(a0, ring, bind_step(st, k, a0.nt), blockIdx.x, sp, corr_mask, series);
+    stencil_body<R>(a0, ring, bind_step(st, k, a0.nt), blockIdx.x, sp, corr_mask);
 }
 
 // The stencil at the corrected cells only (the split step's critical branch: the face stage reads
@@ -346,10 +347,11 @@ __device__ inline R pml_damp(int x, int y, int z, int res, int w, R damp)
 
 template <typename R>
 __global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepArgs a0, const __grid_constant__ Ring<R> ring, const StepState *st, int k,
-                                                   const unsigned *corr_mask, R *series)
+                                                   const unsigned *corr_mask)
 {
     const StepArgs &a = a0;
     const StepDyn dy = bind_step(st, k, a0.nt);
+    R *series = (R *)dy.series;
     const R *cur = ring.slot(dy.tnew - 1), *prev = ring.slot(dy.tnew - 2);
     R *next = ring.slot(dy.tnew);
     const R *pcur = ring.pml(dy.tnew - 1);
@@ -941,7 +943,6 @@ struct NearArgs
     const int *n3_cell, *n3_start, *p3_tri;
     const unsigned char *p3_woff;  // the pair's record offset in 3^3
     const R *terms;
-    R *series;
 };
 
 // the near-stage work of corrected cells warp0, warp0 + nwarps, ... < n3 of one scene
@@ -975,7 +976,7 @@ __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const S
                 for (int l = 0; l < a.n_listen; l++)
                     if (a.listen_cell[l] == c)
                     {
-                        na.series[dy.row * a.n_listen + l] = v;
+                        ((R *)dy.series)[dy.row * a.n_listen + l] = v;
                         flag_nonfinite(a.status, v);
                     }
             }
@@ -1040,7 +1041,6 @@ struct StepLaunch
     StencilSplit sp;
     const StepState *st;
     const unsigned *corr_mask;
-    R *series;
     FaceArgs<R> fa;
     NearArgs<R> na;
     R *conv;   // per-triangle convolution sums of the pipelined step
@@ -1074,8 +1074,6 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.corr_mask = h.d_corr_mask;
     L.ring.hist = (R *)h.d_hist;
     L.ring.nt = h.mesh_set ? h.nt : 0;
-    L.series = (R *)h.d_series;
-    L.na.series = L.series;
     L.mesh = h.mesh_set && h.prm.method == PPPM_METHOD_PPPM ? 1 : 0;
     L.pml = h.prm.pml_width > 0 ? 1 : 0;
     const int m = h.res - 2, T = 256;
@@ -1148,14 +1146,14 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
     };
     mark(0);
     if (L.pml)
-        pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask, L.series);
+        pml_kernel<R><<<L.pml_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.corr_mask);
     else
-        stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask, L.series);
+        stencil_kernel<R><<<L.stencil_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask);
     mark(1);
     if constexpr (sizeof(R) == 4)
         if (L.ghost)
         {
-            ghost_launch(L.gs, L.st, k, L.a.nt, L.series, s);
+            ghost_launch(L.gs, L.st, k, L.a.nt, s);
             mark(2);
         }
     if (L.mesh)
@@ -1212,15 +1210,13 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
             if (k > 0)
                 cudaStreamWaitEvent(s, h.ev_bulk, 0);  // bulk(k-1)
             cudaStreamWaitEvent(bulk, h.ev_near, 0);   // near(k-1), or the call's start
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, bulk>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask,
-                                                                     L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, bulk>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask);
             cudaEventRecord(h.ev_bulk, bulk);
             stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na.n3_cell);
         }
         else
             // the stencil without its Neumann block range (finish / nwrite wrote N[t])
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask,
-                                                                  L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask);
         cudaStreamWaitEvent(s, h.ev_conv, 0);
         // the call's last step computes its terms in one pass (mode 0): the FDTD-near sums it
         // leaves for the next call are then exactly those that prime() rebuilds after a state
@@ -1305,15 +1301,14 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
             StencilSplit bsp = L.sp;
             bsp.skip_corrected = 1;
             mark(PPPM_KERNEL_STENCIL_BULK);
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask, L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask);
             mark(PPPM_KERNEL_STENCIL_CORR);
             stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na.n3_cell);
         }
         else
         {
             mark(PPPM_KERNEL_STENCIL);
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask,
-                                                                  L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask);
         }
         const int mode = L.tpairs && k + 1 < n ? ((k & 1) ? 2 : 1) : 0;
         const int nx = k + 1 < n ? 1 : 0;
@@ -1420,6 +1415,7 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     if (!h.d_state)
         PB_TRY(dalloc(&h.d_state, 1));
     StepState stt{h.t + 1, h.mesh_set ? h.n3 : 0, h.series_count, acc_dev};
+    stt.series = h.d_series;
     set_state_kernel<<<1, 1, 0, s>>>(h.d_state, stt);
     h.launches++;
     PB_CHECK_LAUNCH();
@@ -1445,6 +1441,7 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
             {
                 StepState sk{stt.tnew0 + done, stt.n3, stt.row0 + done,
                              acc_dev ? acc_dev + (long long)done * h.nt : nullptr};
+                sk.series = h.d_series;
                 set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sk);
                 PB_CHECK_LAUNCH();
                 PB_CUDA(cudaGraphLaunch(pexec, s));
@@ -1476,6 +1473,7 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
         {
             StepState sk{stt.tnew0 + k, stt.n3, stt.row0 + k,
                          acc_dev ? acc_dev + (long long)k * (h.mesh_set ? h.nt : 0) : nullptr};
+            sk.series = h.d_series;
             set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sk);
             PB_CHECK_LAUNCH();
             PB_CUDA(cudaGraphLaunch(exec, s));
@@ -1683,6 +1681,7 @@ int autotune(Handle &h, int reps, float *us, int *best)
     float *gus = us + 2 * PPPM_TUNE_CANDIDATES;
     cudaError_t e = copy_state(true);
     StepState sg{h.t + 1, h.n3, h.series_count, zacc};
+    sg.series = h.d_series;  // the timed graphs write listener rows past the recorded ones
     for (int c = 0; c < kTuneConfigs && e == cudaSuccess && rc == PPPM_OK; c++)
     {
         h.conv_pairs = c / 6;
@@ -1758,7 +1757,6 @@ int prime(Handle &h)
     StepLaunch<R> L;
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
-    L.na.series = nullptr;
     terms_kernel<R><<<div_up((long long)h.nt * 32, 256), 256, 0, h.stream>>>(L.ring, h.nt, h.t, L.fa);
     near_kernel<R><<<L.near_blocks, 256, 0, h.stream>>>(L.a, L.ring, L.st, 0, L.na, 1);
     h.launches += 3;
@@ -1827,8 +1825,6 @@ int time_kernels(Handle &h, int reps, float *us)
     StepLaunch<R> L;
     PB_TRY(make_launch<R>(h, L));
     L.a.n_listen = 0;
-    L.na.series = nullptr;
-    L.series = nullptr;
     const int T = 256, FT = L.face_threads, nt = L.a.nt;
     const int wblocks = div_up((long long)nt * 32, FT);
     for (int k = 0; k < PPPM_KERNEL_KINDS; k++)
@@ -1837,7 +1833,7 @@ int time_kernels(Handle &h, int reps, float *us)
         switch (kind)
         {
         case PPPM_KERNEL_STENCIL:
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, L.sp, L.corr_mask, L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, L.sp, L.corr_mask);
             break;
         case PPPM_KERNEL_CONV: conv_kernel<R><<<wblocks, FT, 0, s>>>(L.ring, L.st, 0, nt, L.fa, L.conv); break;
         case PPPM_KERNEL_CONV2:
@@ -1859,7 +1855,7 @@ int time_kernels(Handle &h, int reps, float *us)
         {
             StencilSplit bsp = L.sp;
             bsp.skip_corrected = 1;
-            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, bsp, L.corr_mask, L.series);
+            stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, 0, bsp, L.corr_mask);
             break;
         }
         case PPPM_KERNEL_STENCIL_CORR:
@@ -1982,7 +1978,6 @@ struct BatchScene
     Ring<R> ring;
     StencilSplit sp;
     const unsigned *corr_mask;
-    R *series;
     FaceArgs<R> fa;
     NearArgs<R> na;
     StepState *st;
@@ -1996,7 +1991,7 @@ __global__ void __launch_bounds__(256) batch_stencil_kernel(const BatchScene<R> 
 {
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    stencil_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), m.y, S.sp, S.corr_mask, S.series);
+    stencil_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), m.y, S.sp, S.corr_mask);
 }
 
 template <typename R>
@@ -2180,7 +2175,6 @@ int batch_tables(Batch &b, const std::vector<int> &active)
         S.ring = L.ring;
         S.sp = L.sp;
         S.corr_mask = L.corr_mask;
-        S.series = L.series;
         S.fa = L.fa;
         S.na = L.na;
         S.st = h.d_state;
@@ -2314,6 +2308,7 @@ int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
         if (!h.d_state)
             PB_TRY(dalloc(&h.d_state, 1));
         StepState stt{h.t + 1, h.n3, h.series_count, dacc[i]};
+        stt.series = h.d_series;
         // the scene's steps pair up as in one pppm_step call of nsteps[i] steps (recorded graphs:
         // at least kGraphSteps steps)
         stt.pair0 = h.t + 1;

@@ -124,6 +124,7 @@ def test_cache_tables_vs_reference(gpu):
                          "grid_cache_max_rel_diff": worst, "face_cache_records_bit_exact": rec_exact_fc,
                          "face_cache_max_rel_diff": worst_fc, "interp_max_abs_diff": interp}
     assert worst < 2e-3 and worst_fc < 2e-3
+    assert rec_exact_gc == 1.0  # grid-cache records: the reference's arithmetic, bit for bit
     s.close()
 
 
