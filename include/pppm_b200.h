@@ -296,6 +296,11 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
                                     graph's critical branch (the face and near stages read no other
                                     cell) and the rest of the grid runs on a branch beside them;
                                     0: one stencil launch before the face stage.  Same results.  */
+#define PPPM_OPT_GRAPH_CHUNK 4  /* 32 (default): a call of more steps replays one recorded graph of
+                                   this many steps as often as it fits, then a graph of the 1..32
+                                   steps left, so frames of uneven length record a few short
+                                   graphs instead of one long graph per length; 0: one graph per
+                                   call; otherwise an even number in [2, 4096].  Same results. */
 int pppm_set_option(pppm_handle *h, int option, int value);
 int pppm_get_option(pppm_handle *h, int option, int *value);
 /* No counterpart in the reference.  Autotuner of the face stage, on the current mesh and state.

@@ -1339,6 +1339,11 @@ int pppm_set_option(pppm_handle *ph, int option, int value)
             break;
         h.split_stencil = value != 0;
         return PPPM_OK;
+    case PPPM_OPT_GRAPH_CHUNK:
+        if (value != 0 && (value < 2 || value > 4096 || (value & 1)))
+            break;
+        h.graph_chunk = value;
+        return PPPM_OK;
     default:
         set_error("unknown option %d", option);
         return PPPM_ERR_ARG;
@@ -1361,6 +1366,8 @@ int pppm_get_option(pppm_handle *ph, int option, int *value)
         *value = h.terms_pairs ? 1 : 0;
     else if (option == PPPM_OPT_SPLIT_STENCIL)
         *value = h.split_stencil ? 1 : 0;
+    else if (option == PPPM_OPT_GRAPH_CHUNK)
+        *value = h.graph_chunk;
     else
     {
         set_error("unknown option %d", option);

@@ -72,10 +72,11 @@ __device__ inline StepDyn bind_step(const StepState *st, int k, int nt)
 struct StepGraph
 {
     int nsteps = 0;
+    bool open = false;               // a chunk of a longer call (more steps follow; see run_steps)
     std::vector<unsigned char> sig;  // the launch set it was recorded with
     cudaGraphExec_t exec = nullptr;
 };
-constexpr int kStepGraphs = 4;
+constexpr int kStepGraphs = 8;
 
 struct Handle
 {
@@ -186,6 +187,7 @@ struct Handle
     int face_threads = 256;   // threads per block of their face-stage kernels (step_autotune)
     bool terms_pairs = true;  // ... and the grid-cache near-field terms two steps per pass
     bool split_stencil = true;  // ... and the stencil split into corrected cells and the bulk
+    int graph_chunk = 32;       // steps per chunk graph of a long pppm_step call (0: one graph per call)
 
     // ---- listeners
     std::vector<int> listen_xyz;

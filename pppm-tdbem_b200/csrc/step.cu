@@ -31,6 +31,27 @@ namespace pb
 namespace
 {
 
+// Programmatic dependent launch on the step graph's main branch (corrected-cell stencil ->
+// finish -> near -> next stencil): the dependent grid is scheduled while its predecessor's last
+// blocks drain, and waits here, before its first read, until the predecessor has completed and
+// its writes are visible.  Launched without the attribute, the wait returns at once.
+__device__ inline void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+void launch_dependent(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
+}
+
 // The values of a scene that every step kernel reads (the per-step ones come from StepState)
 struct StepArgs
 {
@@ -319,6 +340,7 @@ __global__ void __launch_bounds__(256) stencil_corr_kernel(const __grid_constant
                                                             const __grid_constant__ Ring<R> ring, const StepState *st,
                                                             int k, const int *n3_cell)
 {
+    grid_dependency_wait();
     const StepDyn dy = bind_step(st, k, a0.nt);
     R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
     const R *prev = ring.slot(dy.tnew - 2);
@@ -869,6 +891,7 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Rin
                                                       int kstep, int nt, const __grid_constant__ FaceArgs<R> f,
                                                       const R *conv, int next)
 {
+    grid_dependency_wait();
     const int tri = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (tri >= nt)
         return;
@@ -989,6 +1012,7 @@ __global__ void __launch_bounds__(256) near_kernel(const __grid_constant__ StepA
                                                     const __grid_constant__ Ring<R> ring, const StepState *st, int kstep,
                                                     const __grid_constant__ NearArgs<R> na, int prime)
 {
+    grid_dependency_wait();
     near_body<R>(a0, ring, bind_step(st, kstep, a0.nt), na, st->n3,
                  (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5),
                  (int)(((long long)gridDim.x * blockDim.x) >> 5), threadIdx.x & 31, prime);
@@ -1181,8 +1205,21 @@ void launch_step(const StepLaunch<R> &L, int k, cudaStream_t s, Handle *timed)
 // near stage's next-step sums go to corrected cells of slot t+2 = t-1, which the bulk reads only
 // elsewhere), so it leaves the step's critical path.  Only used under stream capture: main =
 // h.stream, side = h.side, bulk = h.side2, joined back before the end.
+// after a chunk graph of g steps (run_steps): the call's state moves on by g steps
+__global__ void advance_state_kernel(StepState *st, int g, int nt)
+{
+    st->tnew0 += g;
+    st->row0 += g;
+    if (st->acc)
+        st->acc += (long long)g * nt;
+}
+
+// open: the nsteps steps are a chunk of a longer call (run_steps), so the last of them is no
+// call's last step: it pairs, computes its terms and writes the next Neumann value as any other
+// step does (nsteps is even then, so the pairs are those of the whole call); a kernel after the
+// joins moves the call's state on by nsteps for the next chunk.
 template <typename R>
-void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
+void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair, bool open)
 {
     const int T = 256, FT = L.face_threads;
     const int nt = L.a.nt;
@@ -1197,10 +1234,11 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
         cudaEventRecord(h.ev_near, s);
     for (int k = 0; k < nsteps; k++)
     {
+        const bool more = open || k + 1 < nsteps;  // a later step follows in this call
         cudaStreamWaitEvent(side, h.ev_fin, 0);
         if (pair && (k & 1))
             fix_kernel<R><<<wblocks, FT, 0, side>>>(nt, L.fa, L.conv1, L.conv);
-        else if (pair && k + 1 < nsteps)
+        else if (pair && more)
             conv2_kernel<R><<<wblocks, FT, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv, L.conv1);
         else
             conv_kernel<R><<<wblocks, FT, 0, side>>>(L.ring, L.st, k, nt, L.fa, L.conv);
@@ -1212,7 +1250,7 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
             cudaStreamWaitEvent(bulk, h.ev_near, 0);   // near(k-1), or the call's start
             stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, bulk>>>(L.a, L.ring, L.st, k, bsp, L.corr_mask);
             cudaEventRecord(h.ev_bulk, bulk);
-            stencil_corr_kernel<R><<<L.corr_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na.n3_cell);
+            launch_dependent(stencil_corr_kernel<R>, L.corr_blocks, T, s, L.a, L.ring, L.st, k, L.na.n3_cell);
         }
         else
             // the stencil without its Neumann block range (finish / nwrite wrote N[t])
@@ -1221,21 +1259,24 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair)
         // the call's last step computes its terms in one pass (mode 0): the FDTD-near sums it
         // leaves for the next call are then exactly those that prime() rebuilds after a state
         // restore or a mesh update
-        const int mode = L.tpairs && k + 1 < nsteps ? ((k & 1) ? 2 : 1) : 0;
-        const int nx = k + 1 < nsteps ? 1 : 0;
+        const int mode = L.tpairs && more ? ((k & 1) ? 2 : 1) : 0;
+        const int nx = more ? 1 : 0;
+        const R *conv = L.conv;
         if (mode == 1)
-            finish_kernel<R, 1><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+            launch_dependent(finish_kernel<R, 1>, wblocks, FT, s, L.ring, L.st, k, nt, L.fa, conv, nx);
         else if (mode == 2)
-            finish_kernel<R, 2><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+            launch_dependent(finish_kernel<R, 2>, wblocks, FT, s, L.ring, L.st, k, nt, L.fa, conv, nx);
         else
-            finish_kernel<R, 0><<<wblocks, FT, 0, s>>>(L.ring, L.st, k, nt, L.fa, L.conv, nx);
+            launch_dependent(finish_kernel<R, 0>, wblocks, FT, s, L.ring, L.st, k, nt, L.fa, conv, nx);
         cudaEventRecord(h.ev_fin, s);
-        near_kernel<R><<<L.near_blocks, T, 0, s>>>(L.a, L.ring, L.st, k, L.na, 0);
+        launch_dependent(near_kernel<R>, L.near_blocks, T, s, L.a, L.ring, L.st, k, L.na, 0);
         if (split)
             cudaEventRecord(h.ev_near, s);
     }
     if (split)
         cudaStreamWaitEvent(s, h.ev_bulk, 0);
+    if (open)
+        advance_state_kernel<<<1, 1, 0, s>>>(const_cast<StepState *>(L.st), nsteps, nt);
 }
 
 
@@ -1362,7 +1403,8 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
 constexpr int kGraphSteps = 4;
 
 template <typename R>
-int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *out, bool timed = false)
+int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *out, bool timed = false,
+              bool open = false)
 {
     const unsigned char *sig = (const unsigned char *)&L;
     StepGraph *slots = timed ? &h.timing_graph : h.graphs;
@@ -1370,7 +1412,8 @@ int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *ou
     for (int i = 0; i < nslots; i++)
     {
         StepGraph &g = slots[i];
-        if (g.exec && g.nsteps == nsteps && g.sig.size() == sizeof(L) && memcmp(g.sig.data(), sig, sizeof(L)) == 0)
+        if (g.exec && g.nsteps == nsteps && g.open == open && g.sig.size() == sizeof(L) &&
+            memcmp(g.sig.data(), sig, sizeof(L)) == 0)
         {
             *out = g.exec;
             return PPPM_OK;
@@ -1385,10 +1428,14 @@ int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *ou
     cudaGraph_t graph = nullptr;
     PB_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
     if (!timed && L.mesh && !L.pml && h.side)
-        capture_pipelined<R>(h, L, nsteps, L.pairs != 0);
+        capture_pipelined<R>(h, L, nsteps, L.pairs != 0, open);
     else
+    {
         for (int k = 0; k < nsteps; k++)
             launch_step<R>(L, k, h.stream, timed ? &h : nullptr);
+        if (open)
+            advance_state_kernel<<<1, 1, 0, h.stream>>>(const_cast<StepState *>(L.st), nsteps, L.a.nt);
+    }
     cudaError_t e = cudaStreamEndCapture(h.stream, &graph);
     if (e == cudaSuccess)
         e = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -1401,6 +1448,7 @@ int graph_for(Handle &h, const StepLaunch<R> &L, int nsteps, cudaGraphExec_t *ou
         return PPPM_ERR_CUDA;
     }
     g.nsteps = nsteps;
+    g.open = open;
     g.sig.assign(sig, sig + sizeof(L));
     *out = g.exec;
     return PPPM_OK;
@@ -1502,13 +1550,31 @@ int run_steps(Handle &h, const float *acc_dev, int nsteps)
     }
     else if (cs == cudaStreamCaptureStatusNone && nsteps >= kGraphSteps)
     {
+        // Calls longer than G = h.graph_chunk steps (even) replay one recorded chunk of G steps
+        // as often as it fits and then a graph of the remaining 1..G steps (with the call's
+        // last-step work), so a run of frames of uneven length records a few short graphs
+        // instead of one long graph per length (recording costs about 0.1 ms per step).  The
+        // kernels, their order and their arguments are those of one graph of nsteps steps.
+        const int G = h.graph_chunk;
+        const int chunks = G > 0 && nsteps > G ? (nsteps - 1) / G : 0;
+        const int rest = nsteps - chunks * G;
+        const bool pipelined = L.mesh && !L.pml && h.side;
+        if (chunks > 0)
+        {
+            cudaGraphExec_t cexec = nullptr;
+            PB_TRY(graph_for<R>(h, L, G, &cexec, false, true));
+            for (int c = 0; c < chunks; c++)
+                PB_CUDA(cudaGraphLaunch(cexec, s));
+        }
         cudaGraphExec_t exec = nullptr;
-        PB_TRY(graph_for<R>(h, L, nsteps, &exec));
+        PB_TRY(graph_for<R>(h, L, rest, &exec));
         PB_CUDA(cudaGraphLaunch(exec, s));
-        // the pipelined graph launches the Neumann write, then per step the convolution, the
-        // stencil (and its bulk), finish and near: counted here in place of per_step below
-        if (L.mesh && !L.pml && h.side)
-            h.launches += 1 + (4 + L.split - per_step) * (long long)nsteps;
+        // a pipelined graph launches the Neumann write, then per step the convolution, the
+        // stencil (and its bulk), finish and near: counted here in place of per_step below; a
+        // chunk also advances the state
+        if (pipelined)
+            h.launches += (chunks + 1) + (4 + L.split - per_step) * (long long)nsteps;
+        h.launches += chunks;
     }
     else
         for (int k = 0; k < nsteps; k++)

@@ -517,13 +517,14 @@ class Solver:
         check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
         return v.value
 
-    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2, "split_stencil": 3}
+    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2, "split_stencil": 3, "graph_chunk": 4}
     TUNE_CANDIDATES = [(pairs, threads) for pairs in (0, 1) for threads in (64, 128, 256)]
     TUNE_CONFIGS = [(pairs, threads, terms) for pairs in (0, 1) for threads in (64, 128, 256) for terms in (0, 1)]
 
     def set_option(self, name, value):
         """Launch option of the recorded step graphs (pppm_set_option): conv_pairs (0: one pass
-        per step, 1: two steps per pass), face_threads (64/128/256), terms_pairs (0/1)."""
+        per step, 1: two steps per pass), face_threads (64/128/256), terms_pairs (0/1),
+        split_stencil (0/1), graph_chunk (steps per chunk graph of a long call; 0: one graph)."""
         check(lib.pppm_set_option(self.h, self.OPTIONS[name], int(value)), "set_option")
 
     def get_option(self, name):

@@ -17,11 +17,14 @@ from pppm_b200 import Solver
 pytestmark = pytest.mark.gpu
 
 
-def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None, split=1):
+def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None, split=1,
+            graph_chunk=None):
     v0, f, h, mn, dt = sphere_small()
     res = 24
     s = Solver(res, h, dt, mn, precision=precision)
     s.set_option("split_stencil", split)
+    if graph_chunk is not None:
+        s.set_option("graph_chunk", graph_chunk)
     s.set_option("conv_pairs", pairs)
     s.set_option("terms_pairs", (1 if pairs else 0) if terms is None else terms)
     s.set_option("face_threads", threads)
@@ -126,6 +129,9 @@ def test_bad_options_rejected(gpu):
         s.set_option("conv_pairs", 2)
     with pytest.raises(PPPMError):
         s.set_option("terms_pairs", -1)
+    for bad in (1, 7, -2, 8192):  # chunks hold whole pairs of steps
+        with pytest.raises(PPPMError):
+            s.set_option("graph_chunk", bad)
     with pytest.raises(PPPMError):
         s.autotune()  # no mesh yet
     s.close()
@@ -153,6 +159,18 @@ def test_kernel_timing_leaves_the_run_unchanged(gpu, precision):
         s.close()
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("pairs", [0, 1])
+@pytest.mark.parametrize("call", [300, 69, 37])
+def test_graph_chunks_are_bit_identical(gpu, pairs, call):
+    """A long call replayed as chunk graphs plus a remainder graph (chunks of 32 and of 6 steps)
+    gives exactly the series of one graph per call, across motion frames and uneven call
+    lengths (the pairs of steps and the call's last-step work are the same)."""
+    a = _series("fp32", pairs, chunk=call, moving=True, graph_chunk=0)
+    for g in (32, 6):
+        b = _series("fp32", pairs, chunk=call, moving=True, graph_chunk=g)
+        assert np.array_equal(a, b), (g, call)
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
