@@ -301,6 +301,10 @@ int pppm_pair_weights_static(int device, void *stream, float dt, float dl, float
                                    steps left, so frames of uneven length record a few short
                                    graphs instead of one long graph per length; 0: one graph per
                                    call; otherwise an even number in [2, 4096].  Same results. */
+#define PPPM_OPT_STENCIL_VEC4 5 /* the FP32 interior stencil with res a multiple of 4: 1 four
+                                   consecutive z cells per thread with 16-byte loads, 0 one cell per
+                                   thread, -1 (default) four from res 96 up; pppm_autotune times both
+                                   and keeps the faster.  Same results.                          */
 int pppm_set_option(pppm_handle *h, int option, int value);
 int pppm_get_option(pppm_handle *h, int option, int *value);
 /* No counterpart in the reference.  Autotuner of the face stage, on the current mesh and state.

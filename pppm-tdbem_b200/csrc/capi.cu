@@ -1339,6 +1339,11 @@ int pppm_set_option(pppm_handle *ph, int option, int value)
             break;
         h.split_stencil = value != 0;
         return PPPM_OK;
+    case PPPM_OPT_STENCIL_VEC4:
+        if (value < -1 || value > 1)
+            break;
+        h.stencil_vec4 = value;
+        return PPPM_OK;
     case PPPM_OPT_GRAPH_CHUNK:
         if (value != 0 && (value < 2 || value > 4096 || (value & 1)))
             break;
@@ -1366,6 +1371,8 @@ int pppm_get_option(pppm_handle *ph, int option, int *value)
         *value = h.terms_pairs ? 1 : 0;
     else if (option == PPPM_OPT_SPLIT_STENCIL)
         *value = h.split_stencil ? 1 : 0;
+    else if (option == PPPM_OPT_STENCIL_VEC4)
+        *value = h.stencil_vec4;
     else if (option == PPPM_OPT_GRAPH_CHUNK)
         *value = h.graph_chunk;
     else

@@ -201,9 +201,12 @@ __device__ inline R leapfrog(R pc, R xm, R xp, R ym, R yp, R zm, R zp, R pprev, 
 // interior update with the long boundary solve; the boundary blocks come first, so they are
 // scheduled first and their long solves overlap the interior blocks instead of trailing them:
 //   [0, nb_bd)              boundary-layer cells (a coordinate equal to 1 or res-2), 256 per block
-//   [nb_bd, nb_bd + nb_in)  interior cells [2, res-3]^3 by x plane: a block covers zlen (a power of
-//                           two, at most 256) consecutive z of 256 / zlen consecutive y rows, so
-//                           threads find their cell without a division
+//   [nb_bd, nb_bd + nb_in)  interior cells [2, res-3]^3.  FP32 fields with res a multiple of 4
+//                           (vec4): one thread per group of four consecutive z of an interior
+//                           (x, y) row, 16-byte loads (stencil_interior4).  Otherwise by x plane: a
+//                           block covers zlen (a power of two, at most 256) consecutive z of
+//                           256 / zlen consecutive y rows, so threads find their cell without a
+//                           division
 //   the rest                Neumann ring write, one thread per triangle
 // skip_corrected: the bulk of a split step (corrected cells are left to stencil_corr_kernel).
 // The tiles of a plane are counted in powers of two (blocks past the last tile exit at once), so a
@@ -214,6 +217,7 @@ struct StencilSplit
     int zlog;              // log2 of the threads along z of an interior block
     int ytlog, ztlog;      // log2 of the interior blocks per x plane along y and along z
     int skip_corrected;
+    int vec4;              // interior in groups of four z (FP32, res % 4 == 0): res / 4 groups per row
 };
 
 inline int ceil_log2(long long v)
@@ -224,7 +228,11 @@ inline int ceil_log2(long long v)
     return l;
 }
 
-inline StencilSplit stencil_split(int res, int nt)
+// vec4: 1 four interior cells per thread where the layout allows it (FP32, res % 4 == 0), 0 one
+// cell per thread, -1 four from res 96 up (measured: at res 64 the bulk launch is bound by the
+// boundary layer's solves and the scalar interior finishes first; at res 128 the vector interior
+// halves the bulk).  The autotuner times both.
+inline StencilSplit stencil_split(int res, int nt, bool fp32, int vec4)
 {
     long long mi = res - 4, m = res - 2;
     long long n_bd = 2 * m * m + 2 * (m - 2) * m + 2 * (m - 2) * (m - 2);
@@ -233,6 +241,11 @@ inline StencilSplit stencil_split(int res, int nt)
     sp.ztlog = ceil_log2(div_up(mi, 1 << sp.zlog));
     sp.ytlog = ceil_log2(div_up(mi, 256 >> sp.zlog));
     sp.nb_in = (int)(mi << (sp.ytlog + sp.ztlog));
+    if (fp32 && res % 4 == 0 && (vec4 > 0 || (vec4 < 0 && res >= 96)))
+    {
+        sp.vec4 = res / 4;
+        sp.nb_in = (int)div_up(mi * mi * sp.vec4, 256);
+    }
     sp.nb_bd = div_up(n_bd, 256);
     sp.nb_nt = div_up(nt, 256);
     sp.skip_corrected = 0;
@@ -275,6 +288,70 @@ __device__ inline R interior_cell(const StepArgs &a, const R *__restrict__ cur, 
                        a.lap_coef, a.h2, a.rh2);
 }
 
+// Interior cells four at a time along z (FP32 fields, res a multiple of 4, so every group of four
+// starts on a 16-byte boundary): thread t of the interior range takes z-group g = t mod (res/4) of
+// interior row t div (res/4) (x, y in [2, res-3]).  It loads the group, its four x / y neighbour
+// groups and p^{t-2} as 16-byte vectors and the two z halo values singly, and computes each interior
+// cell of the group with the scalar leapfrog (same arithmetic: fields bit-identical).  A group of
+// four interior cells with no corrected cell and no listener is stored as one vector; any other
+// group goes cell by cell through finish_cell.
+__device__ inline void stencil_interior4(const StepArgs &a, const float *__restrict__ cur,
+                                         const float *__restrict__ prev, float *next, long long srow, int b,
+                                         const StencilSplit &sp, const unsigned *corr_mask, float *series)
+{
+    const int res = a.res, mi = res - 4, G = sp.vec4;
+    const long long t = (long long)b * 256 + threadIdx.x;
+    const long long row = t / G;
+    if (row >= (long long)mi * mi)
+        return;
+    const int g = (int)(t - row * G);
+    const int x = 2 + (int)(row / mi), y = 2 + (int)(row % mi), z0 = 4 * g;
+    const long long sx = (long long)res * res;
+    const long long c0 = ((long long)x * res + y) * res + z0;
+    const float4 cc = *(const float4 *)(cur + c0);
+    const float4 xm = *(const float4 *)(cur + c0 - sx), xp = *(const float4 *)(cur + c0 + sx);
+    const float4 ym = *(const float4 *)(cur + c0 - res), yp = *(const float4 *)(cur + c0 + res);
+    const float4 pp = *(const float4 *)(prev + c0);
+    // z - 1 of the group's first cell (read when that cell is interior: g >= 1) and z + 1 of its last
+    // (read when interior: g <= res/4 - 2)
+    const float zlo = g > 0 ? cur[c0 - 1] : 0.0f, zhi = g < G - 1 ? cur[c0 + 4] : 0.0f;
+    const float c[6] = {zlo, cc.x, cc.y, cc.z, cc.w, zhi};
+    const float vxm[4] = {xm.x, xm.y, xm.z, xm.w}, vxp[4] = {xp.x, xp.y, xp.z, xp.w};
+    const float vym[4] = {ym.x, ym.y, ym.z, ym.w}, vyp[4] = {yp.x, yp.y, yp.z, yp.w};
+    const float vp[4] = {pp.x, pp.y, pp.z, pp.w};
+    const unsigned bits = (corr_mask[c0 >> 5] >> (c0 & 31)) & 0xfu;  // c0 % 4 == 0: one word
+    bool listen = false;
+    for (int l = 0; l < a.n_listen; l++)
+        listen |= a.listen_cell[l] >= c0 && a.listen_cell[l] < c0 + 4;
+    float v[4];
+    int inside = 0;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+    {
+        v[u] = 0.0f;
+        if (z0 + u >= 2 && z0 + u <= res - 3)
+        {
+            inside |= 1 << u;
+            v[u] = leapfrog<float>(c[u + 1], vxm[u], vxp[u], vym[u], vyp[u], c[u], c[u + 2], vp[u], a.lap_coef, a.h2,
+                                   a.rh2);
+        }
+    }
+    if (inside == 0xf && !bits && !listen)
+    {
+        *(float4 *)(next + c0) = make_float4(v[0], v[1], v[2], v[3]);
+        return;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+        if ((inside >> u) & 1)
+        {
+            const bool corrected = (bits >> u) & 1u;
+            if (sp.skip_corrected && corrected)
+                continue;
+            finish_cell<float>(a, srow, c0 + u, v[u], next, corrected, series);
+        }
+}
+
 // the stencil work of block b of one scene's stencil grid (256 threads)
 template <typename R>
 __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, const StepDyn &dy, int b, StencilSplit sp,
@@ -303,6 +380,12 @@ __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, cons
     b -= sp.nb_bd;
     if (b < sp.nb_in)
     {
+        if constexpr (sizeof(R) == 4)
+            if (sp.vec4)
+            {
+                stencil_interior4(a, cur, prev, next, dy.row, b, sp, corr_mask, series);
+                return;
+            }
         const int mi = res - 4;
         const int plane = b >> (sp.ytlog + sp.ztlog), r = b & ((1 << (sp.ytlog + sp.ztlog)) - 1);
         const int yt = r >> sp.ztlog, zt = r & ((1 << sp.ztlog) - 1);
@@ -1093,7 +1176,7 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.ring.g[i] = (R *)h.grid[i];
         L.ring.p[i] = (R *)h.pml[i];
     }
-    L.sp = stencil_split(h.res, L.a.nt);
+    L.sp = stencil_split(h.res, L.a.nt, !h.fp64, h.stencil_vec4);
     L.st = h.d_state;
     L.corr_mask = h.d_corr_mask;
     L.ring.hist = (R *)h.d_hist;
@@ -1748,6 +1831,38 @@ int autotune(Handle &h, int reps, float *us, int *best)
     cudaError_t e = copy_state(true);
     StepState sg{h.t + 1, h.n3, h.series_count, zacc};
     sg.series = h.d_series;  // the timed graphs write listener rows past the recorded ones
+    // the interior stencil one or four cells per thread (FP32, res % 4 == 0): time the bulk launch
+    // (no listeners; the snapshot restore below undoes its writes) both ways and keep the faster
+    const int keep_vec4 = h.stencil_vec4;
+    if (!h.fp64 && h.res % 4 == 0 && e == cudaSuccess)
+    {
+        float tv[2] = {0, 0};
+        set_state_kernel<<<1, 1, 0, s>>>(h.d_state, sg);
+        for (int v = 0; v < 2 && rc == PPPM_OK && e == cudaSuccess; v++)
+        {
+            h.stencil_vec4 = v;
+            StepLaunch<R> S;
+            rc = make_launch<R>(h, S);
+            if (rc != PPPM_OK)
+                break;
+            S.a.n_listen = 0;
+            StencilSplit bsp = S.sp;
+            bsp.skip_corrected = 1;
+            const int nb = S.sp.nb_bd + S.sp.nb_in;
+            stencil_kernel<R><<<nb, 256, 0, s>>>(S.a, S.ring, S.st, 0, bsp, S.corr_mask);
+            e = cudaEventRecord(h.ev[0], s);
+            for (int r = 0; r < reps && e == cudaSuccess; r++)
+                stencil_kernel<R><<<nb, 256, 0, s>>>(S.a, S.ring, S.st, 0, bsp, S.corr_mask);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(h.ev[1], s);
+            if (e == cudaSuccess)
+                e = cudaEventSynchronize(h.ev[1]);
+            if (e == cudaSuccess)
+                e = cudaEventElapsedTime(&tv[v], h.ev[0], h.ev[1]);
+            h.launches += reps + 1;
+        }
+        h.stencil_vec4 = rc == PPPM_OK && e == cudaSuccess ? (tv[1] < tv[0] ? 1 : 0) : keep_vec4;
+    }
     for (int c = 0; c < kTuneConfigs && e == cudaSuccess && rc == PPPM_OK; c++)
     {
         h.conv_pairs = c / 6;
@@ -1800,6 +1915,7 @@ int autotune(Handle &h, int reps, float *us, int *best)
         h.conv_pairs = keep_pairs;
         h.face_threads = keep_threads;
         h.terms_pairs = keep_terms;
+        h.stencil_vec4 = keep_vec4;
         return rc;
     }
     h.conv_pairs = gbest / 6;

@@ -517,14 +517,16 @@ class Solver:
         check(lib.pppm_launch_count(self.h, ctypes.byref(v)), "launch_count")
         return v.value
 
-    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2, "split_stencil": 3, "graph_chunk": 4}
+    OPTIONS = {"conv_pairs": 0, "face_threads": 1, "terms_pairs": 2, "split_stencil": 3, "graph_chunk": 4,
+               "stencil_vec4": 5}
     TUNE_CANDIDATES = [(pairs, threads) for pairs in (0, 1) for threads in (64, 128, 256)]
     TUNE_CONFIGS = [(pairs, threads, terms) for pairs in (0, 1) for threads in (64, 128, 256) for terms in (0, 1)]
 
     def set_option(self, name, value):
         """Launch option of the recorded step graphs (pppm_set_option): conv_pairs (0: one pass
         per step, 1: two steps per pass), face_threads (64/128/256), terms_pairs (0/1),
-        split_stencil (0/1), graph_chunk (steps per chunk graph of a long call; 0: one graph)."""
+        split_stencil (0/1), graph_chunk (steps per chunk graph of a long call; 0: one graph),
+        stencil_vec4 (1: four interior cells per thread, 0: one, -1: by grid size)."""
         check(lib.pppm_set_option(self.h, self.OPTIONS[name], int(value)), "set_option")
 
     def get_option(self, name):
@@ -548,7 +550,7 @@ class Solver:
                 "finish_us": {"single": sum(per[n]), "pairs": sum(per[n + 1])},
                 "finish_launch_us": {"single": per[n], "pairs": per[n + 1]},
                 "step_us": dict(zip(self.TUNE_CONFIGS, step_us)) if any(step_us) else None,
-                "terms_pairs": self.get_option("terms_pairs")}
+                "terms_pairs": self.get_option("terms_pairs"), "stencil_vec4": self.get_option("stencil_vec4")}
 
     def enable_timing(self, on=True):
         check(lib.pppm_enable_timing(self.h, 1 if on else 0), "enable_timing")

@@ -18,13 +18,15 @@ pytestmark = pytest.mark.gpu
 
 
 def _series(precision, pairs, threads=256, steps=300, chunk=None, moving=False, terms=None, split=1,
-            graph_chunk=None):
+            graph_chunk=None, vec4=None):
     v0, f, h, mn, dt = sphere_small()
     res = 24
     s = Solver(res, h, dt, mn, precision=precision)
     s.set_option("split_stencil", split)
     if graph_chunk is not None:
         s.set_option("graph_chunk", graph_chunk)
+    if vec4 is not None:
+        s.set_option("stencil_vec4", vec4)
     s.set_option("conv_pairs", pairs)
     s.set_option("terms_pairs", (1 if pairs else 0) if terms is None else terms)
     s.set_option("face_threads", threads)
@@ -132,6 +134,9 @@ def test_bad_options_rejected(gpu):
     for bad in (1, 7, -2, 8192):  # chunks hold whole pairs of steps
         with pytest.raises(PPPMError):
             s.set_option("graph_chunk", bad)
+    for bad in (2, -2):
+        with pytest.raises(PPPMError):
+            s.set_option("stencil_vec4", bad)
     with pytest.raises(PPPMError):
         s.autotune()  # no mesh yet
     s.close()
@@ -171,6 +176,16 @@ def test_graph_chunks_are_bit_identical(gpu, pairs, call):
     for g in (32, 6):
         b = _series("fp32", pairs, chunk=call, moving=True, graph_chunk=g)
         assert np.array_equal(a, b), (g, call)
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_stencil_vec4_is_bit_identical(gpu, split):
+    """The interior stencil four cells per thread (16-byte loads) against one cell per thread: the
+    same arithmetic per cell, so the series are bit-identical, split or not, moving or not."""
+    for moving in (False, True):
+        a = _series("fp32", 1, steps=150, chunk=23, moving=moving, split=split, vec4=0)
+        b = _series("fp32", 1, steps=150, chunk=23, moving=moving, split=split, vec4=1)
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
