@@ -419,16 +419,14 @@ __global__ void __launch_bounds__(256) stencil_kernel(const __grid_constant__ St
 // triangles' cells, i.e. at corrected cells).  Threads stride over the corrected-cell list (its
 // length is read from the step state); the arithmetic per cell is that of stencil_body.
 template <typename R>
-__global__ void __launch_bounds__(256) stencil_corr_kernel(const __grid_constant__ StepArgs a0,
-                                                            const __grid_constant__ Ring<R> ring, const StepState *st,
-                                                            int k, const int *n3_cell)
+__device__ inline void stencil_corr_body(const StepArgs &a0, const Ring<R> &ring, const StepState *st, int k,
+                                         const int *n3_cell, int first, int stride)
 {
-    grid_dependency_wait();
     const StepDyn dy = bind_step(st, k, a0.nt);
     R *cur = ring.slot(dy.tnew - 1), *next = ring.slot(dy.tnew);
     const R *prev = ring.slot(dy.tnew - 2);
     const int res = a0.res, n3 = st->n3;
-    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < n3; ci += gridDim.x * blockDim.x)
+    for (int ci = first; ci < n3; ci += stride)
     {
         const int c = n3_cell[ci];
         const int x = c / (res * res), y = (c / res) % res, z = c % res;
@@ -441,6 +439,15 @@ __global__ void __launch_bounds__(256) stencil_corr_kernel(const __grid_constant
             continue;  // the ghost layer holds no unknown of the stencil
         next[c] = v - next[c];  // the FDTD-near correction the near stage left in this slot
     }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) stencil_corr_kernel(const __grid_constant__ StepArgs a0,
+                                                            const __grid_constant__ Ring<R> ring, const StepState *st,
+                                                            int k, const int *n3_cell)
+{
+    grid_dependency_wait();
+    stencil_corr_body<R>(a0, ring, st, k, n3_cell, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // split-field PML (fdtd.cu:162-232) on [1, res-2]^3; pml slots hold 6 values per cell
@@ -2166,14 +2173,28 @@ struct BatchScene
     R *conv;         // the scene's per-triangle convolution sums (pipelined graphs)
     R *conv1;        // partial sums of the second step of a pair (two steps per pass)
     int near_warps;  // warps of this scene's near grid
+    int corr_threads;  // threads of this scene's corrected-cell stencil grid (they stride over the cells)
 };
 
 template <typename R>
-__global__ void __launch_bounds__(256) batch_stencil_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+__global__ void __launch_bounds__(256) batch_stencil_kernel(const BatchScene<R> *sc, const int2 *map, int k,
+                                                             int skip_corrected)
 {
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    stencil_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), m.y, S.sp, S.corr_mask);
+    StencilSplit sp = S.sp;
+    sp.skip_corrected = skip_corrected;
+    stencil_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), m.y, sp, S.corr_mask);
+}
+
+// the stencil at every active scene's corrected cells (stencil_corr_kernel per scene)
+template <typename R>
+__global__ void __launch_bounds__(256) batch_corr_kernel(const BatchScene<R> *sc, const int2 *map, int k)
+{
+    grid_dependency_wait();
+    const int2 m = map[blockIdx.x];
+    const BatchScene<R> &S = sc[m.x];
+    stencil_corr_body<R>(S.a, S.ring, S.st, k, S.na.n3_cell, m.y * 256 + threadIdx.x, S.corr_threads);
 }
 
 template <typename R>
@@ -2181,7 +2202,7 @@ __global__ void __launch_bounds__(256) batch_face_kernel(const BatchScene<R> *sc
 {
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    const int tri = m.y * 8 + (threadIdx.x >> 5);
+    const int tri = m.y * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
     if (tri < S.a.nt)
         face_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), S.fa, tri, threadIdx.x & 31);
 }
@@ -2189,6 +2210,7 @@ __global__ void __launch_bounds__(256) batch_face_kernel(const BatchScene<R> *sc
 template <typename R>
 __global__ void __launch_bounds__(256) batch_near_kernel(const BatchScene<R> *sc, const int2 *map, int k)
 {
+    grid_dependency_wait();
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
     near_body<R>(S.a, S.ring, bind_step(S.st, k, S.a.nt), S.na, S.st->n3, m.y * 8 + (threadIdx.x >> 5), S.near_warps,
@@ -2206,7 +2228,7 @@ __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc
 {
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    const int w = m.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int w = m.y * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (w >= S.a.nt)
         return;
     const int tri = centre_of(S.fa, w);
@@ -2236,9 +2258,10 @@ __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc
 template <typename R>
 __global__ void __launch_bounds__(256) batch_finish_kernel(const BatchScene<R> *sc, const int2 *map, int k, int next)
 {
+    grid_dependency_wait();
     const int2 m = map[blockIdx.x];
     const BatchScene<R> &S = sc[m.x];
-    const int tri = m.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int tri = m.y * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (tri >= S.a.nt)
         return;
     const StepDyn dy = bind_step(S.st, k, S.a.nt);
@@ -2301,16 +2324,20 @@ struct Batch
     cudaEvent_t ev = nullptr;
     std::vector<unsigned char> host_scenes;
     // block maps: 0 stencil (with the Neumann range), 1 face (8 triangles per block), 2 near,
-    // 3 stencil without the Neumann range, 4 Neumann values (256 triangles per block)
-    std::vector<int2> host_map[5];
+    // 3 stencil without the Neumann range, 4 Neumann values (256 triangles per block), 5 the
+    // corrected-cell stencil
+    std::vector<int2> host_map[6];
+    int face_threads = 256;  // block size of the face-stage kernels (the first scene's launch option)
     std::vector<StepState *> host_states;
     std::vector<int> host_nt;
     void *d_scenes = nullptr;
     size_t scenes_cap = 0;
-    int2 *d_map[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    size_t map_cap[5] = {0, 0, 0, 0, 0};
+    int2 *d_map[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t map_cap[6] = {0, 0, 0, 0, 0, 0};
     cudaStream_t side = nullptr;                      // second branch while recording
+    cudaStream_t side2 = nullptr;                     // third branch: the bulk of the stencil
     cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;  // fork / join points while recording
+    cudaEvent_t ev_near = nullptr, ev_bulk = nullptr;
     StepState **d_states = nullptr;
     int *d_nt = nullptr;
     size_t states_cap = 0, nt_cap = 0;
@@ -2342,6 +2369,7 @@ int batch_tables(Batch &b, const std::vector<int> &active)
     const int T = 256;
     const size_t na = active.size();
     b.host_scenes.assign(na * sizeof(BatchScene<R>), 0);
+    b.face_threads = b.hs[active.empty() ? 0 : active[0]]->face_threads;
     for (auto &m : b.host_map)
         m.clear();
     b.host_states.resize(na);
@@ -2369,10 +2397,12 @@ int batch_tables(Batch &b, const std::vector<int> &active)
             h.batch_near_cells = h.n3 + h.n3 / 8 + 256;
         const int near_blocks = std::max(1, div_up((long long)h.batch_near_cells * 32, T));
         S.near_warps = near_blocks * (T / 32);
+        const int corr_blocks = std::max(1, div_up((long long)h.batch_near_cells, T));
+        S.corr_threads = corr_blocks * T;
         memcpy(b.host_scenes.data() + ai * sizeof(S), &S, sizeof(S));
         for (int k = 0; k < L.stencil_blocks; k++)
             b.host_map[0].push_back(make_int2((int)ai, k));
-        for (int k = 0; k < div_up(h.nt, T / 32); k++)
+        for (int k = 0; k < div_up(h.nt, b.face_threads / 32); k++)
             b.host_map[1].push_back(make_int2((int)ai, k));
         for (int k = 0; k < near_blocks; k++)
             b.host_map[2].push_back(make_int2((int)ai, k));
@@ -2380,6 +2410,8 @@ int batch_tables(Batch &b, const std::vector<int> &active)
             b.host_map[3].push_back(make_int2((int)ai, k));
         for (int k = 0; k < div_up(h.nt, T); k++)
             b.host_map[4].push_back(make_int2((int)ai, k));
+        for (int k = 0; k < corr_blocks; k++)
+            b.host_map[5].push_back(make_int2((int)ai, k));
         b.host_states[ai] = h.d_state;
         b.host_nt[ai] = h.nt;
     }
@@ -2387,7 +2419,7 @@ int batch_tables(Batch &b, const std::vector<int> &active)
     PB_TRY(grow((unsigned char **)&ds, b.scenes_cap, b.host_scenes.size()));
     b.d_scenes = ds;
     PB_CUDA(cudaMemcpyAsync(b.d_scenes, b.host_scenes.data(), b.host_scenes.size(), cudaMemcpyHostToDevice, b.stream));
-    for (int i = 0; i < 5; i++)
+    for (int i = 0; i < 6; i++)
     {
         PB_TRY(grow(&b.d_map[i], b.map_cap[i], b.host_map[i].size()));
         PB_CUDA(cudaMemcpyAsync(b.d_map[i], b.host_map[i].data(), b.host_map[i].size() * sizeof(int2),
@@ -2406,9 +2438,11 @@ template <typename R>
 int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
 {
     std::vector<unsigned char> sig(b.host_scenes);
-    const void *ptrs[] = {b.d_scenes, b.d_map[0], b.d_map[1], b.d_map[2], b.d_map[3], b.d_map[4], b.d_states, b.d_nt};
+    const void *ptrs[] = {b.d_scenes, b.d_map[0], b.d_map[1], b.d_map[2], b.d_map[3], b.d_map[4], b.d_map[5],
+                          b.d_states, b.d_nt};
     const size_t sizes[] = {b.host_map[0].size(), b.host_map[1].size(), b.host_map[2].size(), b.host_map[3].size(),
-                            b.host_map[4].size(), (size_t)g, (size_t)nactive};
+                            b.host_map[4].size(), b.host_map[5].size(), (size_t)g, (size_t)nactive,
+                            (size_t)b.face_threads};
     sig.insert(sig.end(), (const unsigned char *)ptrs, (const unsigned char *)ptrs + sizeof(ptrs));
     sig.insert(sig.end(), (const unsigned char *)sizes, (const unsigned char *)sizes + sizeof(sizes));
     for (auto &gr : b.graphs)
@@ -2426,33 +2460,46 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
     const int n0 = (int)b.host_map[0].size(), n1 = (int)b.host_map[1].size(), n2 = (int)b.host_map[2].size();
     cudaGraph_t graph = nullptr;
     const int n3 = (int)b.host_map[3].size(), n4 = (int)b.host_map[4].size();
+    const int FT = b.face_threads;
     PB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
-    if (n1 > 0 && n4 > 0 && b.side)
+    const int n5 = (int)b.host_map[5].size();
+    if (n1 > 0 && n4 > 0 && b.side && b.side2)
     {
-        // two branches as for one scene (capture_pipelined): each step's face-pair convolutions
-        // beside the previous near stage and this step's stencil
-        cudaStream_t s = b.stream;
+        // the branches of one scene's recorded steps (capture_pipelined): each step's face-pair
+        // convolutions beside the previous near stage, the corrected cells' stencil on the main
+        // branch (corrected-cell stencil -> finish -> near as dependent launches) and the rest of
+        // every grid on a third branch
+        cudaStream_t s = b.stream, bulk = b.side2;
+        const int2 *m1 = b.d_map[1], *m2 = b.d_map[2], *m5 = b.d_map[5];
         batch_nwrite_kernel<R><<<n4, 256, 0, s>>>(sc, b.d_map[4], 0);
         cudaEventRecord(b.ev_fin, s);
+        cudaEventRecord(b.ev_near, s);
         for (int k = 0; k < g; k++)
         {
             cudaStreamWaitEvent(b.side, b.ev_fin, 0);
-            batch_conv_kernel<R><<<n1, 256, 0, b.side>>>(sc, b.d_map[1], k);
+            batch_conv_kernel<R><<<n1, FT, 0, b.side>>>(sc, m1, k);
             cudaEventRecord(b.ev_conv, b.side);
-            batch_stencil_kernel<R><<<n3, 256, 0, s>>>(sc, b.d_map[3], k);
+            if (k > 0)
+                cudaStreamWaitEvent(s, b.ev_bulk, 0);  // bulk(k-1)
+            cudaStreamWaitEvent(bulk, b.ev_near, 0);   // near(k-1), or the graph's start
+            batch_stencil_kernel<R><<<n3, 256, 0, bulk>>>(sc, b.d_map[3], k, 1);
+            cudaEventRecord(b.ev_bulk, bulk);
+            launch_dependent(batch_corr_kernel<R>, n5, 256, s, sc, m5, k);
             cudaStreamWaitEvent(s, b.ev_conv, 0);
-            batch_finish_kernel<R><<<n1, 256, 0, s>>>(sc, b.d_map[1], k, k + 1 < g ? 1 : 0);
+            launch_dependent(batch_finish_kernel<R>, n1, FT, s, sc, m1, k, k + 1 < g ? 1 : 0);
             cudaEventRecord(b.ev_fin, s);
             if (n2 > 0)
-                batch_near_kernel<R><<<n2, 256, 0, s>>>(sc, b.d_map[2], k);
+                launch_dependent(batch_near_kernel<R>, n2, 256, s, sc, m2, k);
+            cudaEventRecord(b.ev_near, s);
         }
+        cudaStreamWaitEvent(s, b.ev_bulk, 0);
     }
     else
         for (int k = 0; k < g; k++)
         {
-            batch_stencil_kernel<R><<<n0, 256, 0, b.stream>>>(sc, b.d_map[0], k);
+            batch_stencil_kernel<R><<<n0, 256, 0, b.stream>>>(sc, b.d_map[0], k, 0);
             if (n1 > 0)
-                batch_face_kernel<R><<<n1, 256, 0, b.stream>>>(sc, b.d_map[1], k);
+                batch_face_kernel<R><<<n1, FT, 0, b.stream>>>(sc, b.d_map[1], k);
             if (n2 > 0)
                 batch_near_kernel<R><<<n2, 256, 0, b.stream>>>(sc, b.d_map[2], k);
         }
@@ -2522,7 +2569,10 @@ int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
             cudaGraphExec_t exec = nullptr;
             PB_TRY(batch_graph<R>(b, g, (int)active.size(), &exec));
             PB_CUDA(cudaGraphLaunch(exec, b.stream));
-            b.launches += 3ll * g + 1;
+            // pipelined graphs: conv, bulk stencil, corrected-cell stencil, finish and near per step,
+            // plus the Neumann write and the state advance; otherwise stencil, face and near
+            const bool piped = !b.host_map[1].empty() && !b.host_map[4].empty() && b.side && b.side2;
+            b.launches += piped ? 5ll * g + 2 : 3ll * g + 1;
             left -= g;
         }
         done = end;
@@ -2579,7 +2629,10 @@ int batch_create(Handle **hs, int n, Batch **out)
     if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_conv, cudaEventDisableTiming) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess)
+        cudaEventCreateWithFlags(&b->ev_near, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_bulk, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side2, cudaStreamNonBlocking) != cudaSuccess)
     {
         delete b;
         set_error("cudaEventCreate failed");
@@ -2615,8 +2668,14 @@ void batch_destroy(Batch *b)
         cudaEventDestroy(b->ev_fin);
     if (b->ev_conv)
         cudaEventDestroy(b->ev_conv);
+    if (b->ev_near)
+        cudaEventDestroy(b->ev_near);
+    if (b->ev_bulk)
+        cudaEventDestroy(b->ev_bulk);
     if (b->side)
         cudaStreamDestroy(b->side);
+    if (b->side2)
+        cudaStreamDestroy(b->side2);
     delete b;
 }
 
