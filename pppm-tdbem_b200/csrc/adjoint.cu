@@ -84,6 +84,11 @@ struct Adjoint
     // host-call staging
     void *d_g = nullptr, *d_out = nullptr;
     long long g_cap = 0, out_cap = 0;
+    // the call's reverse-step state on the device, and a recorded chunk of reverse steps with the
+    // launch arguments it was recorded for
+    void *d_step = nullptr;
+    cudaGraphExec_t chunk = nullptr;
+    std::vector<unsigned char> chunk_sig;
 };
 
 namespace
@@ -155,12 +160,27 @@ struct AdjArgs
     __device__ R *slot(int tau) const { return lam[((tau % 3) + 3) % 3]; }
 };
 
+// The reverse step a kernel launch covers: reverse step j of a pppm_adjoint call processes time
+// sigma = top - 1 - j; its dL/dsignal row is g + (sigma - bottom) * nl and its dL/dacc row
+// out + (sigma - bottom) * nt.  Read from device memory, so a recorded chunk of reverse steps
+// replays for any stretch of a sweep (advance_adj_kernel moves top on after each chunk).
+struct AdjStep
+{
+    int top, bottom;
+    const void *g;
+    void *out;
+};
+
+__device__ inline int adj_sigma(const AdjStep *st, int j) { return st->top - 1 - j; }
+
 // P1: the listener samples' adjoints
 template <typename R>
-__global__ void adj_listen_kernel(const __grid_constant__ AdjArgs<R> a, int sigma, const R *g)
+__global__ void adj_listen_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st, int jstep)
 {
     if (threadIdx.x != 0)
         return;
+    const int sigma = adj_sigma(st, jstep);
+    const R *g = (const R *)st->g + (long long)(sigma - st->bottom) * a.nl;
     for (int l = 0; l < a.nl; l++)  // one thread: listeners may share a cell
         a.slot(sigma)[a.listen_cell[l]] += g[l];
 }
@@ -225,8 +245,10 @@ __device__ inline void ring_add(R *ring, int j, int tau0, int q, const R (&v)[4]
 
 // P2: near BEM push, then lamF of triangle j (one warp per triangle)
 template <typename R>
-__global__ void __launch_bounds__(256) adj_bem_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_bem_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                      int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (j >= a.nt)
         return;
@@ -251,8 +273,11 @@ __global__ void __launch_bounds__(256) adj_bem_kernel(const __grid_constant__ Ad
 // P3: face push (one warp per triangle j over the centres i whose face list holds j), then
 // dL/dacc[sigma][j]
 template <typename R>
-__global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ AdjArgs<R> a, int sigma, R *out_row)
+__global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                       int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
+    R *out_row = st->out ? (R *)st->out + (long long)(sigma - st->bottom) * a.nt : nullptr;
     using W4 = typename AdjWRec<R>::W4;
     const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (j >= a.nt)
@@ -290,8 +315,10 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const __grid_constant__ A
 
 // P5: the stored FDTD-near sums of step sigma (one warp per triangle)
 template <typename R>
-__global__ void __launch_bounds__(256) adj_fdtd_near_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_fdtd_near_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                            int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (j >= a.nt)
         return;
@@ -308,8 +335,10 @@ __global__ void __launch_bounds__(256) adj_fdtd_near_kernel(const __grid_constan
 
 // P4: corner cells of the face interpolation
 template <typename R>
-__global__ void __launch_bounds__(256) adj_corner_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_corner_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                         int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ncorner)
         return;
@@ -327,8 +356,10 @@ __device__ inline int judge_of(int v, int res) { return -((int)(v == 1)) + ((int
 
 // P6: the boundary-layer solve transposed
 template <typename R>
-__global__ void __launch_bounds__(256) adj_boundary_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_boundary_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                           int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int res = a.res;
     if (i >= boundary_cells(res))
@@ -391,8 +422,10 @@ __global__ void __launch_bounds__(256) adj_boundary_kernel(const __grid_constant
 
 // P7: the transposed stencil, one thread per cell of the whole grid (ghost layer included)
 template <typename R>
-__global__ void __launch_bounds__(256) adj_stencil_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_stencil_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                          int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ncells)
         return;
@@ -477,8 +510,10 @@ __device__ inline bool in_pml(int x, int y, int z, int res, int w)
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) adj_pml_kernel(const __grid_constant__ AdjArgs<R> a, int sigma)
+__global__ void __launch_bounds__(256) adj_pml_kernel(const __grid_constant__ AdjArgs<R> a, const AdjStep *st,
+                                                      int jstep)
 {
+    const int sigma = adj_sigma(st, jstep);
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ncells)
         return;
@@ -746,7 +781,11 @@ void adj_free_tables(Adjoint &A)
 void adj_free_state(Adjoint &A)
 {
     void **ptrs[] = {&A.lam[0], &A.lam[1], &A.lam[2], &A.lam_b, &A.acc_n, &A.acc_d, &A.lam_f, &A.d_g, &A.d_out,
-                     &A.psi[0], &A.psi[1]};
+                     &A.psi[0], &A.psi[1], &A.d_step};
+    if (A.chunk)
+        cudaGraphExecDestroy(A.chunk);
+    A.chunk = nullptr;
+    A.chunk_sig.clear();
     for (void **p : ptrs)
     {
         dev_free(*p);
@@ -934,6 +973,36 @@ AdjArgs<R> make_adj_args(Handle &h, Adjoint &A)
     return a;
 }
 
+__global__ void set_adj_step_kernel(AdjStep *dst, AdjStep v) { *dst = v; }
+__global__ void advance_adj_kernel(AdjStep *st, int g) { st->top -= g; }
+
+// the kernels of reverse step j of the call (no error check: may run under stream capture)
+template <typename R>
+void adj_launch_step(const AdjArgs<R> &a, const AdjStep *st, int j, cudaStream_t s, long long nbd)
+{
+    const int T = 256, tw = div_up((long long)a.nt * 32, T);
+    if (a.nl > 0)
+        adj_listen_kernel<R><<<1, 32, 0, s>>>(a, st, j);
+    adj_bem_kernel<R><<<tw, T, 0, s>>>(a, st, j);
+    adj_face_kernel<R><<<tw, T, 0, s>>>(a, st, j);
+    if (a.ncorner > 0)
+        adj_corner_kernel<R><<<div_up(a.ncorner, T), T, 0, s>>>(a, st, j);
+    adj_fdtd_near_kernel<R><<<tw, T, 0, s>>>(a, st, j);
+    if (a.pml_w > 0)
+        adj_pml_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, st, j);
+    else
+    {
+        adj_boundary_kernel<R><<<div_up(nbd, T), T, 0, s>>>(a, st, j);
+        adj_stencil_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, st, j);
+    }
+}
+
+// A sweep's reverse steps cost five to seven launches each, so long sweeps with fixed tables
+// replay a recorded chunk of kAdjChunk reverse steps (about 0.1 ms of host time per step to record,
+// once per handle and launch arguments); the steps left over, short calls (a moving sweep's
+// frames) and calls on a stream being captured launch the kernels directly.
+constexpr int kAdjChunk = 32;
+
 template <typename R>
 int run_adjoint(Handle &h, const R *g, int nsteps, R *out, int fresh)
 {
@@ -958,28 +1027,61 @@ int run_adjoint(Handle &h, const R *g, int nsteps, R *out, int fresh)
         A.started = true;
     }
     const AdjArgs<R> a = make_adj_args<R>(h, A);
-    const int T = 256, top = A.pos, bottom = A.pos - nsteps;
+    const int top = A.pos, bottom = A.pos - nsteps;
     const long long nbd = boundary_cells(h.res);
     cudaStream_t s = h.stream;
-    const int tw = div_up((long long)a.nt * 32, T);
-    for (int sigma = top - 1; sigma >= bottom; sigma--)
+    if (!A.d_step)
+        PB_TRY(dev_alloc(&A.d_step, sizeof(AdjStep)));
+    AdjStep *dst = (AdjStep *)A.d_step;
+    set_adj_step_kernel<<<1, 1, 0, s>>>(dst, AdjStep{top, bottom, g, out});
+    PB_CHECK_LAUNCH();
+    const long long per_step = 5 + (a.nl > 0) + (a.ncorner > 0) - (a.pml_w > 0);
+    h.launches += 1;
+    int done = 0;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PB_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusNone && nsteps >= 2 * kAdjChunk)
     {
-        if (a.nl > 0)
-            adj_listen_kernel<R><<<1, 32, 0, s>>>(a, sigma, g + (long long)(sigma - bottom) * a.nl);
-        adj_bem_kernel<R><<<tw, T, 0, s>>>(a, sigma);
-        adj_face_kernel<R><<<tw, T, 0, s>>>(a, sigma, out + (long long)(sigma - bottom) * a.nt);
-        if (a.ncorner > 0)
-            adj_corner_kernel<R><<<div_up(a.ncorner, T), T, 0, s>>>(a, sigma);
-        adj_fdtd_near_kernel<R><<<tw, T, 0, s>>>(a, sigma);
-        if (a.pml_w > 0)
-            adj_pml_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
-        else
+        std::vector<unsigned char> sig((const unsigned char *)&a, (const unsigned char *)&a + sizeof(a));
+        const bool have = A.chunk && A.chunk_sig == sig;
+        if (!have && nsteps >= 4 * kAdjChunk)
         {
-            adj_boundary_kernel<R><<<div_up(nbd, T), T, 0, s>>>(a, sigma);
-            adj_stencil_kernel<R><<<div_up(a.ncells, T), T, 0, s>>>(a, sigma);
+            if (A.chunk)
+                cudaGraphExecDestroy(A.chunk);
+            A.chunk = nullptr;
+            A.chunk_sig.clear();
+            cudaGraph_t graph = nullptr;
+            PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int j = 0; j < kAdjChunk; j++)
+                adj_launch_step<R>(a, dst, j, s, nbd);
+            advance_adj_kernel<<<1, 1, 0, s>>>(dst, kAdjChunk);
+            cudaError_t e = cudaStreamEndCapture(s, &graph);
+            if (e == cudaSuccess)
+                e = cudaGraphInstantiate(&A.chunk, graph, 0);
+            if (graph)
+                cudaGraphDestroy(graph);
+            if (e != cudaSuccess)
+            {
+                A.chunk = nullptr;
+                set_error("recording the adjoint chunk graph failed: %s", cudaGetErrorString(e));
+                return PPPM_ERR_CUDA;
+            }
+            A.chunk_sig.swap(sig);
         }
+        if (A.chunk && A.chunk_sig.size() == sizeof(a) && memcmp(A.chunk_sig.data(), &a, sizeof(a)) == 0)
+        {
+            const int chunks = nsteps / kAdjChunk;
+            for (int c = 0; c < chunks; c++)
+                PB_CUDA(cudaGraphLaunch(A.chunk, s));
+            done = chunks * kAdjChunk;
+            h.launches += (long long)chunks * (per_step * kAdjChunk + 1);
+        }
+    }
+    for (int j = 0; j < nsteps - done; j++)  // relative to the state the chunks advanced
+    {
+        adj_launch_step<R>(a, dst, j, s, nbd);
         PB_CHECK_LAUNCH();
-        h.launches += 5 + (a.nl > 0) + (a.ncorner > 0);
+        h.launches += per_step;
     }
     A.pos = bottom;
     return PPPM_OK;

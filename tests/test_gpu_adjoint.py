@@ -117,6 +117,23 @@ def test_chunks_continue_the_sweep(gpu):
     s.close()
 
 
+@pytest.mark.parametrize("pml", [0, 4])
+def test_recorded_chunks_match_direct_launches(gpu, pml):
+    """A long sweep replays a recorded chunk of 32 reverse steps (the kernels read their time
+    from device memory) and launches the rest directly; the same sweep in calls of 50 steps, which
+    launch every kernel directly, gives bit-identical gradients."""
+    s = _solver("fp32", res=20, sub=1, pml_width=pml)
+    n = 300
+    g = np.random.default_rng(8).standard_normal((n, s.n_listeners))
+    whole = s.adjoint(g)
+    parts = []
+    for k, e in enumerate(range(n, 0, -50)):
+        parts.append(s.adjoint(g[e - 50:e], fresh=(k == 0)))
+    assert np.array_equal(np.concatenate(parts[::-1]), whole)
+    assert np.all(np.isfinite(whole)) and np.abs(whole).max() > 0
+    s.close()
+
+
 def _fd_check(s, acc, target, grad, rng, ndir):
     """worst relative gap between <grad, v> and central differences of the loss along v"""
 
