@@ -609,7 +609,33 @@ __device__ inline int centre_of(const int *face_start, int nt, int p)
 // Phase A: face-to-face spectra, one thread per (recomputed pair, k <= 8) evaluating both
 // layers; spec[18 w + k] single layer, spec[18 w + 9 + k] double layer.
 // mode: 0 = ref32 throughout, 1 = FP64 for panels sharing vertices (stored as float)
-__global__ void fc_spectra_kernel(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
+// The corner cells of centre ctr's interpolation that lie farther than 1.5 h from the neighbour's
+// centre along some axis, with their scale (-interpolation weight) (pppm_cache.cu:234-271)
+__device__ inline int far_corners(const DevConsts &dc, const int *basec, const float *interp, int ctr, f3 nbc,
+                                  f3 *pts, float *sc)
+{
+    int n = 0;
+    const int bx = basec[3 * ctr], by = basec[3 * ctr + 1], bz = basec[3 * ctr + 2];
+    for (int dx = 0; dx < 2; dx++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dz = 0; dz < 2; dz++)
+            {
+                const int widx = dx * 4 + dy * 2 + dz;
+                const f3 c = cell_center(bx + dx, by + dy, bz + dz, dc.h, dc.mn);
+                if (abs(c.x - nbc.x) > dc.h * 1.5 || abs(c.y - nbc.y) > dc.h * 1.5 || abs(c.z - nbc.z) > dc.h * 1.5)
+                {
+                    pts[n] = c;
+                    sc[n] = -interp[8 * ctr + widx];
+                    n++;
+                }
+            }
+    return n;
+}
+
+// Phase A, one thread per (pair, wave number): the face-to-face spectra of both layers plus the
+// neighbour's point integrals at the centre's far interpolation corners, the pair's record spectra
+__global__ void fc_spectra_kernel(DevConsts dc, const float *verts, const int *tris, const float *center,
+                                  const int *basec, const float *interp, const int *face_start, int nt,
                                   const int *face_nbr, const int *work, int nwork, int mode, cf *spec)
 {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -635,8 +661,13 @@ __global__ void fc_spectra_kernel(DevConsts dc, const float *verts, const int *t
     }
     else
         ref32::face_to_face2(sv, si, tv, ti, cf{dc.wave_re[k], dc.wave_im[k]}, dc.threshold, os, od);
-    spec[(size_t)w * 18 + k] = os;
-    spec[(size_t)w * 18 + 9 + k] = od;
+    f3 pts[8];
+    float sc[8];
+    const int n = far_corners(dc, basec, interp, ctr, load3(center, nbr), pts, sc);
+    cf ps, pd;
+    ref32::face_to_points2(sv, pts, sc, n, true, cf{dc.wave_re[k], dc.wave_im[k]}, ps, pd);
+    spec[(size_t)w * 18 + k] = cf{os.re + ps.re, os.im + ps.im};
+    spec[(size_t)w * 18 + 9 + k] = cf{od.re + pd.re, od.im + pd.im};
 }
 
 __global__ void fc_spectra_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *face_start, int nt,
@@ -659,47 +690,19 @@ __global__ void fc_spectra_kernel_d(DevConsts dc, const float *verts, const int 
         face_to_face(s, si, t, ti, cd{dc.wave_re_d[k], dc.wave_im_d[k]}, (double)dc.h * 0.1, layer == 1);
 }
 
-// Phase B: corner point integrals, FFT, packing into the pool record
-__global__ void fc_finish_kernel(DevConsts dc, const float *verts, const int *tris, const float *center,
-                                 const int *basec, const float *interp, const int *face_start, int nt,
-                                 const int *face_nbr, const int *face_pool, const int *work, int nwork, const cf *spec,
+// Phase B, one thread per pair: FFT of both record spectra, packing into the pool record
+__global__ void fc_finish_kernel(DevConsts dc, const int *face_pool, const int *work, int nwork, const cf *spec,
                                  __half2 *pool_w, float2 *pool_scale)
 {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nwork)
         return;
     int p = work[w];
-    int ctr = centre_of(face_start, nt, p), nbr = face_nbr[p];
-    f3 sv[3];
-    int si[3];
-    load_tri(verts, tris, nbr, sv, si);
-    f3 nbc = load3(center, nbr);
-    f3 pts[8];
-    float sc[8];
-    int n = 0;
-    int bx = basec[3 * ctr], by = basec[3 * ctr + 1], bz = basec[3 * ctr + 2];
-    for (int dx = 0; dx < 2; dx++)
-        for (int dy = 0; dy < 2; dy++)
-            for (int dz = 0; dz < 2; dz++)
-            {
-                int widx = dx * 4 + dy * 2 + dz;
-                f3 c = cell_center(bx + dx, by + dy, bz + dz, dc.h, dc.mn);
-                if (abs(c.x - nbc.x) > dc.h * 1.5 || abs(c.y - nbc.y) > dc.h * 1.5 || abs(c.z - nbc.z) > dc.h * 1.5)
-                {
-                    pts[n] = c;
-                    sc[n] = -interp[8 * ctr + widx];
-                    n++;
-                }
-            }
     cf ss[kTaps], sd[kTaps];
     for (int k = 0; k <= kTaps / 2; k++)
     {
-        cf a = spec[(size_t)w * 18 + k], b = spec[(size_t)w * 18 + 9 + k];
-        cf kk{dc.wave_re[k], dc.wave_im[k]};
-        cf ps, pd;
-        ref32::face_to_points2(sv, pts, sc, n, true, kk, ps, pd);
-        ss[k] = cf{a.re + ps.re, a.im + ps.im};
-        sd[k] = cf{b.re + pd.re, b.im + pd.im};
+        ss[k] = spec[(size_t)w * 18 + k];
+        sd[k] = spec[(size_t)w * 18 + 9 + k];
     }
     float ws[kTaps], wd[kTaps];
     spectrum_to_weights(ss, dc.lambda, ws, dc.tw);
@@ -1318,11 +1321,11 @@ int cache_refresh(Handle &h)
             {
                 int mode = h.prm.weights == PPPM_WEIGHTS_FP64 ? 1 : 0;
                 fc_spectra_kernel<<<div_up((long long)nwork * 9, 128), 128, 0, s>>>(
-                    dc, h.d_verts, h.d_tris, h.d_face_start, nt, h.d_face_nbr, work, nwork, mode, (cf *)h.d_spec);
-                fc_finish_kernel<<<div_up(nwork, 128), 128, 0, s>>>(
                     dc, h.d_verts, h.d_tris, h.d_center, h.d_basec, h.d_face_interp, h.d_face_start, nt,
-                    h.d_face_nbr, h.d_face_pool, work, nwork, (const cf *)h.d_spec, (__half2 *)h.d_pool_w,
-                    h.d_pool_scale);
+                    h.d_face_nbr, work, nwork, mode, (cf *)h.d_spec);
+                fc_finish_kernel<<<div_up(nwork, 128), 128, 0, s>>>(dc, h.d_face_pool, work, nwork,
+                                                                     (const cf *)h.d_spec, (__half2 *)h.d_pool_w,
+                                                                     h.d_pool_scale);
             }
             h.launches += 2;
             PB_CHECK_LAUNCH();
