@@ -174,6 +174,17 @@ struct PointTerms
     int valid;
 };
 
+// a / b in double, rounded to nearest, from y = RN(1 / b): q = RN(a y), then one correction with
+// the exact remainder a - b q (P. Markstein, IBM J. Res. Dev. 34(1), 1990), which gives the correctly
+// rounded quotient for the normal operands met here; a zero numerator keeps its sign, as in the
+// division.  Two quotients by the same b then cost one division instead of two.
+__device__ inline double div_by(double a, double b, double y)
+{
+    const double q = __dmul_rn(a, y);
+    const double r = __fma_rn(-b, q, a);
+    return a == 0.0 ? a : __fma_rn(r, y, q);
+}
+
 __device__ inline PointTerms point_terms(f3 src, f3 trg, f3 n, cf k)
 {
     PointTerms t{0, 0, 0, 0, 0};
@@ -185,10 +196,12 @@ __device__ inline PointTerms point_terms(f3 src, f3 trg, f3 n, cf k)
         cf ikr = ikr_of(r, k);
         cf e = cexp(ikr.re, ikr.im);
         double den1 = 4 * PB_PI * r;
-        t.qre = e.re / den1;
-        t.qim = e.im / den1;
+        const double y1 = 1.0 / den1;
+        t.qre = div_by(e.re, den1, y1);
+        t.qim = div_by(e.im, den1, y1);
         double den = 4 * PB_PI * r2 * r;
-        double are = -e.re / den, aim = -e.im / den;
+        const double y = 1.0 / den;
+        double are = div_by(-e.re, den, y), aim = div_by(-e.im, den, y);
         float bre = 1.0f - ikr.re, bim = -ikr.im;
         double mre = are * bre - aim * bim;
         double mim = are * bim + aim * bre;
