@@ -142,12 +142,10 @@ __device__ inline void gc_point_offset(int p, int &dx, int &dy, int &dz)
     dz = axis == 2 ? far : b;
 }
 
-__global__ void __launch_bounds__(256, 4) gc_block_kernel(DevConsts dc, const float *verts, const int *tris,
-                                                          const int *cellc, const float *center, const float *normal,
-                                                          const float *area, const int *flag, __half2 *gc_w,
-                                                          float2 *gc_scale, float *snap)
+__device__ inline void gc_block_body(int tri, const DevConsts &dc, const float *verts, const int *tris,
+                                     const int *cellc, const float *center, const float *normal, const float *area,
+                                     const int *flag, __half2 *gc_w, float2 *gc_scale, float *snap)
 {
-    const int tri = blockIdx.x;
     if (!flag[tri])
         return;
     // The point terms of steps 1-2 and, once they are consumed, the 16-tap weights, the two
@@ -287,6 +285,20 @@ __global__ void __launch_bounds__(256, 4) gc_block_kernel(DevConsts dc, const fl
     }
 }
 
+// Blocks take triangles tri = blockIdx.x, blockIdx.x + gridDim.x, ...: a grid of one block per
+// triangle, or a smaller one that leaves room on the SMs for the kernels of the same mesh update
+// running beside it (grid_cache_start)
+__global__ void __launch_bounds__(256, 4) gc_block_kernel(DevConsts dc, const float *verts, const int *tris, int nt,
+                                                          const int *cellc, const float *center, const float *normal,
+                                                          const float *area, const int *flag, __half2 *gc_w,
+                                                          float2 *gc_scale, float *snap)
+{
+    for (int tri = blockIdx.x; tri < nt; tri += gridDim.x)
+    {
+        gc_block_body(tri, dc, verts, tris, cellc, center, normal, area, flag, gc_w, gc_scale, snap);
+        __syncthreads();  // the next triangle reuses the shared buffers
+    }
+}
 
 // FP64 scheme: the same records entirely in double, unquantised
 __global__ void gc_compute_kernel_d(DevConsts dc, const float *verts, const int *tris, const int *cellc,
@@ -1146,12 +1158,12 @@ int journal_rewind(Handle &h, int id)
     return PPPM_OK;
 }
 
-int gc_factors(Handle &h)
+int gc_factors(Handle &h, cudaStream_t gs)
 {
     const long long n = (long long)h.nt * 54;
     if (!h.d_gc_f || n == 0)
         return PPPM_OK;
-    gc_factor_kernel<<<div_up(n, 256), 256, 0, h.stream>>>(
+    gc_factor_kernel<<<div_up(n, 256), 256, 0, gs>>>(
         h.fp64 ? nullptr : (const __half2 *)h.d_gc_w, h.d_gc_scale, h.fp64 ? (const double2 *)h.d_gc_w : nullptr, n,
         h.fp64 ? nullptr : (float *)h.d_gc_f, h.fp64 ? (double *)h.d_gc_f : nullptr);
     h.launches++;
@@ -1159,51 +1171,55 @@ int gc_factors(Handle &h)
     return PPPM_OK;
 }
 
-int cache_refresh(Handle &h)
+// One-time allocations of the caches (the first set_mesh)
+static int cache_alloc(Handle &h)
 {
+    if (h.d_gc_w)
+        return PPPM_OK;
     cudaStream_t s = h.stream;
-    const int nt = h.nt, T = 256;
+    const int nt = h.nt;
     const size_t rec_bytes = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    PB_TRY(dev_alloc(&h.d_gc_w, (size_t)nt * 54 * rec_bytes));
+    PB_TRY(dev_alloc(&h.d_gc_f, (size_t)nt * 54 * h.real_size));
+    if (!h.fp64)
+        PB_TRY(dalloc(&h.d_gc_scale, (size_t)nt * 54));
+    PB_TRY(dalloc(&h.d_gc_snap, (size_t)nt * 7));
+    PB_TRY(dalloc(&h.d_gc_flag, (size_t)nt));
+    PB_TRY(dalloc(&h.d_fc_keys, (size_t)nt * kFaceCacheSlots));
+    PB_TRY(dalloc(&h.d_fc_slot, (size_t)nt * kFaceCacheSlots));
+    PB_CUDA(cudaMemsetAsync(h.d_fc_keys, 0xff, sizeof(int) * (size_t)nt * kFaceCacheSlots, s));
+    PB_TRY(dalloc(&h.d_pool_count, 1));
+    PB_CUDA(cudaMemsetAsync(h.d_pool_count, 0, sizeof(int), s));
+    PB_TRY(dalloc(&h.d_log_count, 2));
+    PB_TRY(dalloc(&h.d_face_interp, (size_t)nt * 8));
+    if (h.fp64)
+        PB_TRY(dalloc(&h.d_face_interp_d, (size_t)nt * 8));
+    PB_TRY(dalloc(&h.d_face_denom, (size_t)nt));
+    PB_TRY(dalloc(&h.d_tw, (size_t)16));
+    twiddle_kernel<<<1, 1, 0, s>>>(h.d_tw);
+    h.launches++;
+    PB_CHECK_LAUNCH();
+    h.pool_used = 0;
+    h.gc_empty = true;
+    return PPPM_OK;
+}
+
+// The grid-cache refresh (recompute flags, records, the completion factors of the two-step terms)
+// on stream gs
+static int grid_cache_refresh(Handle &h, cudaStream_t gs)
+{
+    const int nt = h.nt, T = 256;
     DevConsts dc = make_consts(h);
-
-    // ---- one-time allocations
-    if (!h.d_gc_w)
-    {
-        PB_TRY(dev_alloc(&h.d_gc_w, (size_t)nt * 54 * rec_bytes));
-        PB_TRY(dev_alloc(&h.d_gc_f, (size_t)nt * 54 * h.real_size));
-        if (!h.fp64)
-            PB_TRY(dalloc(&h.d_gc_scale, (size_t)nt * 54));
-        PB_TRY(dalloc(&h.d_gc_snap, (size_t)nt * 7));
-        PB_TRY(dalloc(&h.d_gc_flag, (size_t)nt));
-        PB_TRY(dalloc(&h.d_fc_keys, (size_t)nt * kFaceCacheSlots));
-        PB_TRY(dalloc(&h.d_fc_slot, (size_t)nt * kFaceCacheSlots));
-        PB_CUDA(cudaMemsetAsync(h.d_fc_keys, 0xff, sizeof(int) * (size_t)nt * kFaceCacheSlots, s));
-        PB_TRY(dalloc(&h.d_pool_count, 1));
-        PB_CUDA(cudaMemsetAsync(h.d_pool_count, 0, sizeof(int), s));
-        PB_TRY(dalloc(&h.d_log_count, 2));
-        PB_TRY(dalloc(&h.d_face_interp, (size_t)nt * 8));
-        if (h.fp64)
-            PB_TRY(dalloc(&h.d_face_interp_d, (size_t)nt * 8));
-        PB_TRY(dalloc(&h.d_face_denom, (size_t)nt));
-        PB_TRY(dalloc(&h.d_tw, (size_t)16));
-        twiddle_kernel<<<1, 1, 0, s>>>(h.d_tw);
-        h.launches++;
-        PB_CHECK_LAUNCH();
-        dc.tw = h.d_tw;
-        h.pool_used = 0;
-        h.gc_empty = true;
-    }
-
-    // ---- grid cache
-    gc_flag_kernel<<<div_up(nt, T), T, 0, s>>>(h.d_center, h.d_normal, h.d_area, h.d_gc_snap, nt, h.prm.dl,
-                                               h.gc_empty ? 1 : 0, h.d_gc_flag);
+    dc.tw = h.d_tw;
+    gc_flag_kernel<<<div_up(nt, T), T, 0, gs>>>(h.d_center, h.d_normal, h.d_area, h.d_gc_snap, nt, h.prm.dl,
+                                                h.gc_empty ? 1 : 0, h.d_gc_flag);
     h.launches++;
     PB_CHECK_LAUNCH();
     if (h.fp64)
-        gc_compute_kernel_d<<<div_up((long long)nt * 27, 128), 128, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc,
-                                                                             h.d_center, h.d_normal, h.d_area,
-                                                                             h.d_gc_flag, nt, (double2 *)h.d_gc_w,
-                                                                             h.d_gc_snap);
+        gc_compute_kernel_d<<<div_up((long long)nt * 27, 128), 128, 0, gs>>>(dc, h.d_verts, h.d_tris, h.d_cellc,
+                                                                              h.d_center, h.d_normal, h.d_area,
+                                                                              h.d_gc_flag, nt, (double2 *)h.d_gc_w,
+                                                                              h.d_gc_snap);
     else
     {
         // four blocks of 37 KB shared memory per SM: ask for the largest shared-memory carve-out
@@ -1214,13 +1230,67 @@ int cache_refresh(Handle &h)
                                          cudaSharedmemCarveoutMaxShared));
             carveout_set = true;
         }
-        gc_block_kernel<<<nt, 256, 0, s>>>(dc, h.d_verts, h.d_tris, h.d_cellc, h.d_center, h.d_normal, h.d_area,
-                                           h.d_gc_flag, (__half2 *)h.d_gc_w, h.d_gc_scale, h.d_gc_snap);
+        // beside the rest of the update (side stream): two blocks per SM, half of what fits
+        int blocks = nt;
+        if (gs != h.stream)
+        {
+            int sms = 0;
+            PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h.prm.device));
+            blocks = std::max(1, std::min(nt, 2 * sms));
+        }
+        gc_block_kernel<<<blocks, 256, 0, gs>>>(dc, h.d_verts, h.d_tris, nt, h.d_cellc, h.d_center, h.d_normal,
+                                                h.d_area, h.d_gc_flag, (__half2 *)h.d_gc_w, h.d_gc_scale,
+                                                h.d_gc_snap);
     }
     h.launches++;
     PB_CHECK_LAUNCH();
     h.gc_empty = false;
-    PB_TRY(gc_factors(h));
+    return gc_factors(h, gs);
+}
+
+// The grid-cache refresh reads only the triangle geometry of this update (mesh_build's first
+// kernel: centres, normals, areas, cells) and nothing else reads or writes its arrays until the
+// step tables are primed, so update_mesh starts it on side2 right after the geometry kernel, where
+// it runs (transcendental-bound) beside the list builds and the face-cache refresh (latency- and
+// synchronisation-bound); cache_refresh joins it before returning.
+int grid_cache_start(Handle &h)
+{
+    PB_TRY(cache_alloc(h));
+    if (!h.side2 || !h.ev_upd_fork || !h.ev_upd_join)
+        return PPPM_OK;  // cache_refresh then refreshes the grid cache on the handle's stream
+    PB_CUDA(cudaEventRecord(h.ev_upd_fork, h.stream));
+    PB_CUDA(cudaStreamWaitEvent(h.side2, h.ev_upd_fork, 0));
+    PB_TRY(grid_cache_refresh(h, h.side2));
+    PB_CUDA(cudaEventRecord(h.ev_upd_join, h.side2));
+    h.gc_launched = true;
+    return PPPM_OK;
+}
+
+void join_grid_cache(Handle &h)
+{
+    if (h.gc_launched)
+        cudaStreamWaitEvent(h.stream, h.ev_upd_join, 0);
+    h.gc_launched = false;
+}
+
+int cache_refresh(Handle &h)
+{
+    // whatever path this returns by, the handle's stream waits for the grid-cache branch
+    struct Join
+    {
+        Handle &h;
+        ~Join() { join_grid_cache(h); }
+    } join{h};
+    cudaStream_t s = h.stream;
+    const int nt = h.nt, T = 256;
+    const size_t rec_bytes = h.fp64 ? kTaps * sizeof(double2) : kTaps * sizeof(__half2);
+    DevConsts dc = make_consts(h);
+    PB_TRY(cache_alloc(h));
+    dc.tw = h.d_tw;
+
+    // ---- grid cache (already running on side2 when update_mesh started it with the geometry)
+    if (!h.gc_launched)
+        PB_TRY(grid_cache_refresh(h, s));
 
     // ---- face cache
     const f3 mn{h.prm.min_pos[0], h.prm.min_pos[1], h.prm.min_pos[2]};
@@ -1599,7 +1669,7 @@ int cache_import_grid(Handle &h, const void *records)
     PB_CUDA(cudaStreamSynchronize(s));
     dev_free(tmp);
     h.gc_empty = false;
-    PB_TRY(gc_factors(h));
+    PB_TRY(gc_factors(h, h.stream));
     return cache_regather(h);
 }
 

@@ -381,7 +381,9 @@ int pppm_create(const pppm_params *p, pppm_handle **out)
         cudaEventCreateWithFlags(&h.ev_fin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h.ev_conv, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h.ev_near, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h.ev_bulk, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&h.ev_bulk, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_upd_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.ev_upd_join, cudaEventDisableTiming) != cudaSuccess)
     {
         set_error("cudaStreamCreate / cudaEventCreate failed");
         return fail(PPPM_ERR_CUDA);
@@ -445,6 +447,10 @@ int pppm_destroy(pppm_handle *ph)
         cudaEventDestroy(h.ev_near);
     if (h.ev_bulk)
         cudaEventDestroy(h.ev_bulk);
+    if (h.ev_upd_fork)
+        cudaEventDestroy(h.ev_upd_fork);
+    if (h.ev_upd_join)
+        cudaEventDestroy(h.ev_upd_join);
     if (h.side)
         cudaStreamDestroy(h.side);
     if (h.side2)
@@ -499,6 +505,8 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_CUDA(cudaMemsetAsync(h.d_dlast, 0, (size_t)nt * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
     int rc = mesh_build(h);
+    if (rc != PPPM_OK)
+        join_grid_cache(h);
     if (rc == PPPM_OK && h.prm.method == PPPM_METHOD_GHOST)
     {
         // GhostCellSolver::set_mesh (ghost_cell.h:84-99): labels, ghost system, zero accelerations
@@ -551,7 +559,14 @@ int pppm_update_mesh(pppm_handle *ph, const float *verts, int verts_on_device)
                             verts_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h.stream));
     h.mesh_version++;
     h.tables_stale = false;
-    PB_TRY(mesh_build(h));
+    {
+        const int rc = mesh_build(h);
+        if (rc != PPPM_OK)
+        {
+            join_grid_cache(h);
+            return rc;
+        }
+    }
     if (h.prm.method == PPPM_METHOD_GHOST)
     {
         // GhostCellSolver::update_mesh (ghost_cell.h:101-117): new labels, fresh cells filled from

@@ -89,6 +89,8 @@ struct Handle
     cudaStream_t side2 = nullptr;                        // third branch: the bulk of the split stencil
     cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;     // fork / join points while recording
     cudaEvent_t ev_near = nullptr, ev_bulk = nullptr;
+    cudaEvent_t ev_upd_fork = nullptr, ev_upd_join = nullptr;  // the grid-cache branch of a mesh update
+    bool gc_launched = false;  // this update's grid-cache refresh runs on side2 (grid_cache_start)
     int res = 0;
     long long n_cells = 0;
     int t = -1;
@@ -295,6 +297,8 @@ void ghost_free(Handle &h);
 
 // cache.cu
 int cache_refresh(Handle &h);  // grid cache + face cache refresh, dense gathers, denominators
+int grid_cache_start(Handle &h);  // the grid-cache refresh on side2, joined by cache_refresh
+void join_grid_cache(Handle &h);  // the handle's stream waits for that branch (error paths)
 int cache_free(Handle &h);
 size_t cache_state_bytes(Handle &h);                               // pppm_cache_state_size
 int cache_state_save(Handle &h, void *dst, size_t bytes);          // host or device buffer
@@ -312,7 +316,7 @@ int cache_import_face(Handle &h, const int *pairs, const void *records, int n); 
 int step_prime(Handle &h);
 int step_autotune(Handle &h, int reps, float *us, int *best);
 int step_time_kernels(Handle &h, int reps, float *us);  // us: PPPM_KERNEL_KINDS entries
-int gc_factors(Handle &h);
+int gc_factors(Handle &h, cudaStream_t gs);
 int step_run(Handle &h, const float *acc_dev, int nsteps);
 int step_free(Handle &h);  // recorded graphs and the step state
 // batched scenes (step.cu): one set of stage launches advances every scene

@@ -520,6 +520,9 @@ int mesh_build(Handle &h)
                                                  h.d_area, h.d_cellc, h.d_basec, h.d_cell, h.d_base, h.d_status);
     h.launches++;
     PB_CHECK_LAUNCH();
+    // the grid-cache refresh needs only this geometry: it runs on a side stream from here on
+    if (h.prm.method == PPPM_METHOD_PPPM)
+        PB_TRY(grid_cache_start(h));
     // (the status is read with the list sizes below: triangles outside the interior get no cell,
     // so the list builds in between stay in bounds)
 
