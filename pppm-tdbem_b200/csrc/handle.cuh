@@ -189,6 +189,7 @@ struct Handle
     int face_threads = 256;   // threads per block of their face-stage kernels (step_autotune)
     bool terms_pairs = true;  // ... and the grid-cache near-field terms two steps per pass
     bool split_stencil = true;  // ... and the stencil split into corrected cells and the bulk
+    bool corr_near_boundary = false;  // a corrected cell may neighbour the boundary layer (mesh_build)
     int stencil_vec4 = -1;      // interior stencil four cells per thread: 1 on, 0 off, -1 by grid size
     int graph_chunk = 32;       // steps per chunk graph of a long pppm_step call (0: one graph per call)
 

@@ -153,6 +153,12 @@ __global__ void geometry_kernel(const float *verts, const int *tris, int nt, int
     }
     cell[i] = (gx * res + gy) * res + gz;
     base[i] = (bx * res + by) * res + bz;
+    // status[1]: a triangle within three cells of the grid's faces, so that a corrected cell (its
+    // 3^3 block) may be the inward neighbour of a boundary-layer cell that is not corrected; that
+    // cell's 4x4 solve reads p^{t-1} at the corrected cell, which the split step's near stage
+    // overwrites beside it (make_launch records the step unsplit then)
+    if (gx <= 3 || gy <= 3 || gz <= 3 || gx >= res - 4 || gy >= res - 4 || gz >= res - 4)
+        atomicExch(status + 1, 1);
 }
 
 __global__ void count_kernel(const int *key, int n, int *count)
@@ -597,9 +603,11 @@ int mesh_build(Handle &h)
     h.launches++;
     PB_CHECK_LAUNCH();
     PB_TRY(exclusive_scan(h, face_len, h.d_face_start, nt));
-    int v[6];
-    const int *src[6] = {h.d_status, pos3 + nc, b4_pos + (nc - 1), st3 + nc, st4 + nc, h.d_face_start + nt};
-    PB_TRY(read_ints(h, src, 6, v));
+    int v[7];
+    const int *src[7] = {h.d_status,       pos3 + nc, b4_pos + (nc - 1), st3 + nc, st4 + nc, h.d_face_start + nt,
+                         h.d_status + 1};
+    PB_TRY(read_ints(h, src, 7, v));
+    h.corr_near_boundary = v[6] != 0;
     if (v[0])
     {
         set_error("mesh leaves the grid interior: every triangle must lie at least two cells inside the grid");

@@ -1066,6 +1066,10 @@ __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const S
     R *cur = ring.slot(dy.tnew), *nextslot = ring.slot(dy.tnew + 1);
     for (int ci = warp0; ci < n3; ci += nwarps)
     {
+        // the cell and its far-field value are fetched before the pair sums, so their latency
+        // overlaps the term gathers
+        const int c = lane == 0 ? na.n3_cell[ci] : 0;
+        const R far = lane == 0 && !prime ? cur[c] : (R)0;
         const int b = na.n3_start[ci], e = na.n3_start[ci + 1];
         R acc_f = 0, acc_b = 0;
         for (int p = b + lane; p < e; p += 32)
@@ -1080,11 +1084,10 @@ __device__ inline void near_body(const StepArgs &a, const Ring<R> &ring, const S
             acc_b = warp_sum(acc_b);
         if (lane == 0)
         {
-            int c = na.n3_cell[ci];
             nextslot[c] = acc_f;
             if (!prime)
             {
-                R v = (R)((double)cur[c] + (double)acc_b * 0.98);
+                R v = (R)((double)far + (double)acc_b * 0.98);
                 cur[c] = v;
                 for (int l = 0; l < a.n_listen; l++)
                     if (a.listen_cell[l] == c)
@@ -1221,7 +1224,10 @@ int make_launch(Handle &h, StepLaunch<R> &L)
         L.pairs = h.conv_pairs;
         L.face_threads = h.face_threads;
         L.tpairs = h.terms_pairs ? 1 : 0;
-        L.split = h.split_stencil ? 1 : 0;
+        // the split step's bulk runs beside the near stage, which overwrites p^{t-1} at corrected
+        // cells with the next step's sums: only when no corrected cell neighbours a boundary-layer
+        // cell whose solve reads it (mesh_build's check)
+        L.split = h.split_stencil && !h.corr_near_boundary ? 1 : 0;
         L.fa.face_d1 = (const R *)h.d_face_d1;
         L.fa.order = h.d_base_tris;
         L.fa.dlast = (R *)h.d_dlast;
@@ -2338,6 +2344,7 @@ struct Batch
     cudaStream_t side2 = nullptr;                     // third branch: the bulk of the stencil
     cudaEvent_t ev_fin = nullptr, ev_conv = nullptr;  // fork / join points while recording
     cudaEvent_t ev_near = nullptr, ev_bulk = nullptr;
+    bool split = true;  // every active scene's step may run split (make_launch's L.split)
     StepState **d_states = nullptr;
     int *d_nt = nullptr;
     size_t states_cap = 0, nt_cap = 0;
@@ -2374,11 +2381,13 @@ int batch_tables(Batch &b, const std::vector<int> &active)
         m.clear();
     b.host_states.resize(na);
     b.host_nt.resize(na);
+    b.split = true;
     for (size_t ai = 0; ai < na; ai++)
     {
         Handle &h = *b.hs[active[ai]];
         StepLaunch<R> L;
         PB_TRY(make_launch<R>(h, L));
+        b.split = b.split && L.split;
         BatchScene<R> S;
         memset(&S, 0, sizeof(S));
         S.a = L.a;
@@ -2442,7 +2451,7 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
                           b.d_states, b.d_nt};
     const size_t sizes[] = {b.host_map[0].size(), b.host_map[1].size(), b.host_map[2].size(), b.host_map[3].size(),
                             b.host_map[4].size(), b.host_map[5].size(), (size_t)g, (size_t)nactive,
-                            (size_t)b.face_threads};
+                            (size_t)b.face_threads, (size_t)b.split};
     sig.insert(sig.end(), (const unsigned char *)ptrs, (const unsigned char *)ptrs + sizeof(ptrs));
     sig.insert(sig.end(), (const unsigned char *)sizes, (const unsigned char *)sizes + sizeof(sizes));
     for (auto &gr : b.graphs)
@@ -2466,9 +2475,9 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
     if (n1 > 0 && n4 > 0 && b.side && b.side2)
     {
         // the branches of one scene's recorded steps (capture_pipelined): each step's face-pair
-        // convolutions beside the previous near stage, the corrected cells' stencil on the main
-        // branch (corrected-cell stencil -> finish -> near as dependent launches) and the rest of
-        // every grid on a third branch
+        // convolutions beside the previous near stage, and with the split stencil (every active
+        // scene's L.split) the corrected cells' stencil on the main branch (corrected-cell stencil
+        // -> finish -> near as dependent launches) and the rest of every grid on a third branch
         cudaStream_t s = b.stream, bulk = b.side2;
         const int2 *m1 = b.d_map[1], *m2 = b.d_map[2], *m5 = b.d_map[5];
         batch_nwrite_kernel<R><<<n4, 256, 0, s>>>(sc, b.d_map[4], 0);
@@ -2479,12 +2488,18 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
             cudaStreamWaitEvent(b.side, b.ev_fin, 0);
             batch_conv_kernel<R><<<n1, FT, 0, b.side>>>(sc, m1, k);
             cudaEventRecord(b.ev_conv, b.side);
-            if (k > 0)
-                cudaStreamWaitEvent(s, b.ev_bulk, 0);  // bulk(k-1)
-            cudaStreamWaitEvent(bulk, b.ev_near, 0);   // near(k-1), or the graph's start
-            batch_stencil_kernel<R><<<n3, 256, 0, bulk>>>(sc, b.d_map[3], k, 1);
-            cudaEventRecord(b.ev_bulk, bulk);
-            launch_dependent(batch_corr_kernel<R>, n5, 256, s, sc, m5, k);
+            if (b.split)
+            {
+                if (k > 0)
+                    cudaStreamWaitEvent(s, b.ev_bulk, 0);  // bulk(k-1)
+                cudaStreamWaitEvent(bulk, b.ev_near, 0);   // near(k-1), or the graph's start
+                batch_stencil_kernel<R><<<n3, 256, 0, bulk>>>(sc, b.d_map[3], k, 1);
+                cudaEventRecord(b.ev_bulk, bulk);
+                launch_dependent(batch_corr_kernel<R>, n5, 256, s, sc, m5, k);
+            }
+            else
+                // the whole stencil but its Neumann block range (finish / nwrite wrote N[t])
+                batch_stencil_kernel<R><<<n3, 256, 0, s>>>(sc, b.d_map[3], k, 0);
             cudaStreamWaitEvent(s, b.ev_conv, 0);
             launch_dependent(batch_finish_kernel<R>, n1, FT, s, sc, m1, k, k + 1 < g ? 1 : 0);
             cudaEventRecord(b.ev_fin, s);
@@ -2492,7 +2507,8 @@ int batch_graph(Batch &b, int g, int nactive, cudaGraphExec_t *out)
                 launch_dependent(batch_near_kernel<R>, n2, 256, s, sc, m2, k);
             cudaEventRecord(b.ev_near, s);
         }
-        cudaStreamWaitEvent(s, b.ev_bulk, 0);
+        if (b.split)
+            cudaStreamWaitEvent(s, b.ev_bulk, 0);
     }
     else
         for (int k = 0; k < g; k++)
@@ -2572,7 +2588,7 @@ int batch_run_t(Batch &b, const float *const *dacc, const int *nsteps)
             // pipelined graphs: conv, bulk stencil, corrected-cell stencil, finish and near per step,
             // plus the Neumann write and the state advance; otherwise stencil, face and near
             const bool piped = !b.host_map[1].empty() && !b.host_map[4].empty() && b.side && b.side2;
-            b.launches += piped ? 5ll * g + 2 : 3ll * g + 1;
+            b.launches += piped ? (b.split ? 5ll : 4ll) * g + 2 : 3ll * g + 1;
             left -= g;
         }
         done = end;

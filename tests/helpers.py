@@ -24,6 +24,18 @@ def sphere_small(res=24, sub=2, radius=0.1, offset=True):
     return v, f, h, mn, dt
 
 
+def edge_sphere(axis, cell):
+    """sphere_small moved along one axis so that its triangles' cells reach `cell` there at one end
+    (the lowest cell when cell < 12, else the highest)"""
+    v0, f, h, mn, dt = sphere_small()
+    c = v0[f].mean(1)
+    rel = (c[:, axis] - mn[axis]) / h
+    shift = (cell + 0.5 - rel.min()) if cell < 12 else (cell + 0.5 - rel.max())
+    v = v0.copy()
+    v[:, axis] += np.float32(shift * h)
+    return v, f, h, mn, dt
+
+
 def moving_small_verts(v0, step, dt):
     t = step * float(dt)
     R = scenes.rotation_matrix([0.3, 0.5, 0.8], 40.0 * t)

@@ -8,7 +8,7 @@ steps.
 import numpy as np
 import pytest
 
-from helpers import sine_acc
+from helpers import edge_sphere, sine_acc
 from pppm_b200 import Batch, PPPMError, Solver, scenes
 
 pytestmark = pytest.mark.gpu
@@ -131,4 +131,35 @@ def test_batch_with_motion_frames_matches_single_scenes(gpu):
             assert np.array_equal(s1.grid(rel), s2.grid(rel))
     b.close()
     for s, _, _, _ in alone + together:
+        s.close()
+
+
+def test_batch_with_a_scene_near_the_boundary(gpu):
+    """A scene whose mesh reaches cell 3 of an axis steps unsplit (its corrected cells neighbour the
+    boundary layer); a batch holding it records the unsplit stencil for every scene, with results
+    bit-identical to the scenes stepped one by one."""
+    def make():
+        v, f, h, mn, dt = edge_sphere(0, 3)
+        e = Solver(24, h, dt, mn)
+        e.set_mesh(v, f)
+        e.add_listener(20, 12, 12)
+        e.add_listener(1, 12, 12)
+        s, f2, dt2 = _scene(24, 2, 2)
+        return [(e, sine_acc(80, len(f), 1500.0, dt), 61), (s, sine_acc(80, len(f2), 1100.0, dt2), 45)]
+
+    alone = make()
+    for s, acc, steps in alone:
+        s.step(acc[:steps])
+    together = make()
+    b = Batch([s for s, _, _ in together])
+    b.run([acc[:steps] for _, acc, steps in together])
+    for (s1, acc, steps), (s2, _, _) in zip(alone, together):
+        assert np.array_equal(s1.listeners(), s2.listeners())
+        for rel in (0, -1, -2):
+            assert np.array_equal(s1.grid(rel), s2.grid(rel))
+        s1.step(acc[steps:])
+        s2.step(acc[steps:])
+        assert np.array_equal(s1.listeners(), s2.listeners())
+    b.close()
+    for s, _, _ in alone + together:
         s.close()

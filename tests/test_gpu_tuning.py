@@ -10,7 +10,7 @@ within the oracle bounds of the parity tests (1e-5 over the first 50 steps with 
 import numpy as np
 import pytest
 
-from helpers import moving_small_verts, rel_l2, sine_acc, sphere_small
+from helpers import edge_sphere, moving_small_verts, rel_l2, sine_acc, sphere_small
 from oracle.oracle import Oracle
 from pppm_b200 import Solver
 
@@ -226,3 +226,43 @@ def test_measurement_mode_profiles_every_kernel(gpu, split):
     assert n["conv2"] == 20 and n["fix"] == 20 and n["near"] == 42 and n["face"] == 2
     assert n["finish1"] == 20 and n["finish2"] == 10 and n["finish"] == 10
     assert n["nwrite"] == 10 and n["empty"] == 10
+
+
+def _edge_series(axis, cell, split, steps=150, chunk=23, profile=False):
+    v, f, h, mn, dt = edge_sphere(axis, cell)
+    s = Solver(24, h, dt, mn)
+    s.set_option("split_stencil", split)
+    s.set_option("conv_pairs", 1)
+    s.set_option("terms_pairs", 1)
+    s.set_mesh(v, f)
+    s.add_listener(20, 12, 12)
+    s.add_listener(1, 12, 12)
+    acc = sine_acc(steps, len(f), 1500.0, dt)
+    if profile:
+        s.enable_timing(True)
+    for s0 in range(0, steps, chunk):
+        s.step(acc[s0: s0 + chunk])
+    prof = s.kernel_profile() if profile else None
+    out = s.listeners().astype(np.float64), s.grid(0).copy()
+    s.close()
+    return out, prof
+
+
+@pytest.mark.parametrize("axis,cell,split", [(0, 3, False), (1, 20, False), (2, 3, False), (0, 4, True),
+                                             (1, 19, True)])
+def test_split_stencil_off_near_the_boundary(gpu, axis, cell, split):
+    """A corrected cell two cells from the grid's face is the inward neighbour of a boundary-layer
+    cell that is not corrected: that cell's 4x4 solve reads p^{t-1} there, which the split step's
+    near stage overwrites with the next step's sums beside the bulk.  Such a mesh (a triangle in
+    cell 3 or res-4 of an axis) runs the step unsplit, with the same results; one cell further in,
+    the split stays."""
+    (a, ga), prof = _edge_series(axis, cell, 1, steps=42, chunk=42, profile=True)
+    n = {k: c for k, (us, c) in prof.items()}
+    if split:
+        assert n["stencil_bulk"] == 40 and n["stencil_corr"] == 40
+    else:
+        assert n["stencil"] == 42 and "stencil_bulk" not in n
+    (b, gb), _ = _edge_series(axis, cell, 1)
+    (c, gc), _ = _edge_series(axis, cell, 0)
+    assert np.all(np.isfinite(b)) and np.abs(b).max() > 0
+    assert np.array_equal(b, c) and np.array_equal(gb, gc)
