@@ -496,14 +496,14 @@ int pppm_set_mesh(pppm_handle *ph, const float *verts, int nv, const int *tris, 
     PB_TRY(dev_alloc(&h.d_dirichlet, (size_t)nt * kRing * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_neumann, 0, (size_t)nt * kRing * h.real_size, h.stream));
     PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)nt * kRing * h.real_size, h.stream));
-    PB_TRY(dev_alloc(&h.d_hist, (size_t)8 * nt * kRing * h.real_size));
+    PB_TRY(dev_alloc(&h.d_hist, (size_t)4 * nt * kHistRow * h.real_size));
     PB_TRY(dev_alloc(&h.d_terms, (size_t)54 * nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_conv, (size_t)nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_conv1, (size_t)nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_dlast, (size_t)nt * h.real_size));
     PB_TRY(dev_alloc(&h.d_terms1, (size_t)54 * nt * h.real_size));
     PB_CUDA(cudaMemsetAsync(h.d_dlast, 0, (size_t)nt * h.real_size, h.stream));
-    PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * nt * kRing * h.real_size, h.stream));
+    PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)4 * nt * kHistRow * h.real_size, h.stream));
     int rc = mesh_build(h);
     if (rc != PPPM_OK)
         join_grid_cache(h);
@@ -898,7 +898,7 @@ int pppm_reset_fields(pppm_handle *ph)
     {
         PB_CUDA(cudaMemsetAsync(h.d_neumann, 0, (size_t)h.nt * kRing * h.real_size, h.stream));
         PB_CUDA(cudaMemsetAsync(h.d_dirichlet, 0, (size_t)h.nt * kRing * h.real_size, h.stream));
-        PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)8 * h.nt * kRing * h.real_size, h.stream));
+        PB_CUDA(cudaMemsetAsync(h.d_hist, 0, (size_t)4 * h.nt * kHistRow * h.real_size, h.stream));
     }
     PB_TRY(step_prime(h));
     PB_TRY(clear_step_status(h));
@@ -946,7 +946,6 @@ int pppm_save_state(pppm_handle *ph, void *dst, size_t bytes)
     if (h.mesh_set)
     {
         size_t hb = (size_t)h.nt * kRing * h.real_size;
-        PB_TRY(hist_export(h));
         PB_CUDA(cudaMemcpyAsync(p, h.d_neumann, hb, cudaMemcpyDeviceToHost, h.stream));
         p += hb;
         PB_CUDA(cudaMemcpyAsync(p, h.d_dirichlet, hb, cudaMemcpyDeviceToHost, h.stream));
@@ -1059,8 +1058,8 @@ int pppm_dump(pppm_handle *ph, int what, void *dst, size_t bytes)
     case PPPM_DUMP_GRID_T: return copy(h.slot(h.t), need);
     case PPPM_DUMP_GRID_TM1: return copy(h.slot(h.t - 1), need);
     case PPPM_DUMP_GRID_TM2: return copy(h.slot(h.t - 2), need);
-    case PPPM_DUMP_NEUMANN: PB_TRY(hist_export(h)); return copy(h.d_neumann, need);
-    case PPPM_DUMP_DIRICHLET: PB_TRY(hist_export(h)); return copy(h.d_dirichlet, need);
+    case PPPM_DUMP_NEUMANN: return copy(h.d_neumann, need);
+    case PPPM_DUMP_DIRICHLET: return copy(h.d_dirichlet, need);
     case PPPM_DUMP_TRI_GEOM:
     {
         std::vector<float> c, nn, a;
@@ -1242,8 +1241,6 @@ int pppm_load(pppm_handle *ph, int what, const void *src, size_t bytes)
     if (bytes < need)
         return PPPM_ERR_ARG;
     const bool ring = what == PPPM_DUMP_NEUMANN || what == PPPM_DUMP_DIRICHLET;
-    if (ring)
-        PB_TRY(hist_export(h));  // the other ring keeps its current values
     PB_CUDA(cudaMemcpyAsync(dst, src, need, cudaMemcpyHostToDevice, h.stream));
     if (ring)
         PB_TRY(hist_import(h));

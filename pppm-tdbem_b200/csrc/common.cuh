@@ -14,6 +14,10 @@ namespace pb
 // (reference CMakeLists.txt:30, bem.h:55).
 constexpr int kTaps = 16;
 constexpr int kRing = 32;
+// The step's own history copies keep the 16 times the taps reach (kHist slots), Neumann and
+// Dirichlet interleaved by 4-tap chunks in one row of kHistRow values per triangle (step.cu).
+constexpr int kHist = 16;
+constexpr int kHistRow = 2 * kHist;
 // Reference capacities that define parity-mode limits (particle_grid.h:9-11,
 // pppm_cache.h:79); the B200 lists are CSR and only the face cache keeps a per-face bound.
 constexpr int kFaceCacheSlots = 1024;

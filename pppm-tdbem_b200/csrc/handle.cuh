@@ -179,7 +179,7 @@ struct Handle
 
     // ---- histories
     void *d_neumann = nullptr, *d_dirichlet = nullptr;  // reference layout: read-out and loading
-    void *d_hist = nullptr;  // the step's copies: [Neumann, Dirichlet][4 copies][nt][kRing] (step.cu)
+    void *d_hist = nullptr;  // the step's copies: [4 copies][nt][kHistRow], both fields (step.cu)
     void *d_terms = nullptr;  // nt x 54 near-field terms of the current step (step.cu: near_terms)
     void *d_conv = nullptr;   // nt face-pair convolution sums of the pipelined step (step.cu)
     void *d_conv1 = nullptr;  // nt partial sums of the following step (step.cu: conv2_kernel)
@@ -325,8 +325,8 @@ struct Batch;
 int batch_create(Handle **hs, int n, Batch **out);
 int batch_run(Batch *b, const float *const *dacc, const int *nsteps);  // dacc: device rows per scene
 void batch_destroy(Batch *b);
-int hist_import(Handle &h);  // reference-layout rings -> the step's history copies
-int hist_export(Handle &h);  // the step's history copies -> reference-layout rings
+int hist_import(Handle &h);  // reference-layout rings -> the step's history copies (the rings are
+                             // kept current by every history write)
 
 // cells.cu
 int cells_classify(Handle &h, int *ghost_count);

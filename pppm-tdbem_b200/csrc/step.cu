@@ -80,34 +80,50 @@ __device__ inline void flag_nonfinite(int *status, R v)
 
 
 // History rings in the step.  The reference keeps per triangle a ring of 32 values indexed by
-// time mod 32 and reads the 16 taps t, t-1, ..., t-15 (bem.h:55).  The step keeps every ring in
-// four copies instead; copy c holds time tau at index (c - tau) mod 32, so taps 4q..4q+3 of time
-// t sit at indices (c - t + 4q) .. +3 of copy c, ascending with the tap, and for c = t mod 4
-// they start on a multiple of 4: one aligned 16-byte load (FP32) reads 4 taps.  A new value is
-// written into all four copies.  The reference-layout rings stay beside them for read-out and
-// loading (hist_export / hist_import).
-__host__ __device__ inline int hist_index(int copy, int time) { return (copy - time) & (kRing - 1); }
+// time mod 32 and reads the 16 taps t, t-1, ..., t-15 (bem.h:55).  Those rings (the canonical
+// rings, reference layout) are kept current by every history write and serve read-out, loading
+// and the Neumann value of a step without an acceleration row (the value 32 steps old, as the
+// reference's ring holds it).  The taps are read from four copies of 16 slots instead: copy c
+// holds time tau at slot (c - tau) mod 16, so taps 4q..4q+3 of time t sit at slots
+// (c - t + 4q) .. +3 of copy c, ascending with the tap, and for c = t mod 4 they start on a
+// multiple of 4.  A copy's row interleaves the two fields by 4-tap chunks: chunk j holds Neumann
+// slots 4j..4j+3 then Dirichlet slots 4j..4j+3, so the Neumann and Dirichlet taps 4q..4q+3 of a
+// triangle are one aligned 32-byte load (FP32) and a triangle's whole window is one 128-byte
+// line.  A new value is written into all four copies and the canonical ring.
+__host__ __device__ inline int hist_index(int copy, int time) { return (copy - time) & (kHist - 1); }
 
-// the three grid time levels (and PML fields) by time index, and the history copies
-// [field 0 = Neumann, 1 = Dirichlet][copy 0..3][nt][kRing]
+// the three grid time levels (and PML fields) by time index, the history copies
+// [copy 0..3][nt][kHistRow] and the canonical rings [nt][kRing] of both fields
 template <typename R>
 struct Ring
 {
     R *g[3];
     R *p[3];
     R *hist;
+    R *canon[2];  // field 0 = Neumann, 1 = Dirichlet
     int nt;
     __device__ R *slot(int time) const { return g[((time % 3) + 3) % 3]; }
     __device__ R *pml(int time) const { return p[((time % 3) + 3) % 3]; }
-    __device__ R *hrow(int field, int copy, int tri) const
+    __device__ R *hrow(int copy, int tri) const { return hist + ((long long)copy * nt + tri) * kHistRow; }
+    // position of slot s of a field inside a copy's row
+    __device__ static int hpos(int field, int s) { return ((s >> 2) << 3) + (field << 2) + (s & 3); }
+    __device__ R &hat(int field, int copy, int tri, int s) const { return hrow(copy, tri)[hpos(field, s)]; }
+    __device__ R &canon_at(int field, int tri, int time) const
     {
-        return hist + ((long long)(field * 4 + copy) * nt + tri) * kRing;
+        return canon[field][(long long)tri * kRing + (time & (kRing - 1))];
     }
     __device__ void hwrite(int field, int tri, int time, R v) const
     {
 #pragma unroll
         for (int c = 0; c < 4; c++)
-            hrow(field, c, tri)[hist_index(c, time)] = v;
+            hat(field, c, tri, hist_index(c, time)) = v;
+        canon_at(field, tri, time) = v;
+    }
+    // N[time] of triangle tri: the acceleration row's value, or without one the value the
+    // canonical ring holds for that slot (written 32 steps before, as the reference's ring)
+    __device__ void nwrite(int tri, int time, const float *acc) const
+    {
+        hwrite(0, tri, time, acc ? (R)acc[tri] : canon_at(0, tri, time));
     }
 };
 
@@ -402,8 +418,8 @@ __device__ inline void stencil_body(const StepArgs &a, const Ring<R> &ring, cons
     }
     b -= sp.nb_in;
     int i = b * 256 + threadIdx.x;
-    if (i < a.nt && dy.acc)
-        ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
+    if (i < a.nt)
+        ring.nwrite(i, dy.tnew, dy.acc);
 }
 
 template <typename R>
@@ -470,8 +486,8 @@ __global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepAr
     R *pnext = ring.pml(dy.tnew);
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int res = a.res, m = res - 2, w = a.pml_width;
-    if (gid < a.nt && dy.acc)
-        ring.hwrite(0, (int)gid, dy.tnew, (R)dy.acc[gid]);
+    if (gid < a.nt)
+        ring.nwrite((int)gid, dy.tnew, dy.acc);
     if (gid >= (long long)m * m * m)
         return;
     int q[3] = {1 + (int)(gid / ((long long)m * m)), 1 + (int)((gid / m) % m), 1 + (int)(gid % m)};
@@ -566,6 +582,26 @@ struct WRec<double>
     using H4 = Vec<double, 4>;
 };
 
+// Taps 4q..4q+3 of time t of both fields of one triangle: chunk (slot of tap 0) / 4 + q of copy
+// t mod 4, which starts 8 values into the row per chunk.  FP32: one 32-byte load (PTX
+// ld.global.v8.f32, sm_100), so a quad reads a triangle's two windows as one 128-byte line.  The
+// asm is ordered against the kernel's own history writes (memory clobber).
+__device__ inline int window_offset(int t, int q) { return (((hist_index(t & 3, t) >> 2) + q) & 3) << 3; }
+
+__device__ inline void load_window(const float *p, Vec<float, 4> &n, Vec<float, 4> &d)
+{
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(n.v[0]), "=f"(n.v[1]), "=f"(n.v[2]), "=f"(n.v[3]), "=f"(d.v[0]), "=f"(d.v[1]), "=f"(d.v[2]),
+                   "=f"(d.v[3])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ inline void load_window(const double *p, Vec<double, 4> &n, Vec<double, 4> &d)
+{
+    n = *(const Vec<double, 4> *)p;
+    d = *(const Vec<double, 4> *)(p + 4);
+}
+
 constexpr unsigned kFull = 0xffffffffu;
 
 template <typename R>
@@ -618,9 +654,8 @@ __device__ inline void near_terms(const Ring<R> &ring, int t, const FaceArgs<R> 
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
     const int g = lane >> 2, q = lane & 3;
-    const int copy = t & 3, off = (hist_index(copy, t) + 4 * q) & (kRing - 1);
-    const H4 hn = *(const H4 *)(ring.hrow(0, copy, tri) + off);
-    H4 hd = *(const H4 *)(ring.hrow(1, copy, tri) + off);
+    H4 hn, hd;
+    load_window(ring.hrow(t & 3, tri) + window_offset(t, q), hn, hd);
     if (d0 && q == 0)
         hd.v[0] = dnew;
     // history taps 4q-1 .. 4q+2 for the shifted FDTD-near records (tap -1 does not exist: 0)
@@ -676,9 +711,8 @@ __device__ inline void near_terms2(const Ring<R> &ring, int t, const FaceArgs<R>
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
     const int g = lane >> 2, q = lane & 3;
-    const int copy = t & 3, off = (hist_index(copy, t) + 4 * q) & (kRing - 1);
-    const H4 hn = *(const H4 *)(ring.hrow(0, copy, tri) + off);
-    H4 hd = *(const H4 *)(ring.hrow(1, copy, tri) + off);
+    H4 hn, hd;
+    load_window(ring.hrow(t & 3, tri) + window_offset(t, q), hn, hd);
     if (q == 0)
         hd.v[0] = dnew;
     // time-t taps shifted by one (4q+i-1) and by two (4q+i-2)
@@ -766,8 +800,7 @@ __device__ inline R face_conv(const Ring<R> &ring, int tnew, const FaceArgs<R> &
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
     const int g = lane >> 2, q = lane & 3;
-    const int copy = tnew & 3, off = (hist_index(copy, tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
-    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
+    const R *base = ring.hrow(tnew & 3, 0) + window_offset(tnew, q);
     const int b = f.face_start[tri], e = f.face_start[tri + 1];
     R acc = 0;
     for (int p = b + g; p < e; p += 8)
@@ -775,8 +808,8 @@ __device__ inline R face_conv(const Ring<R> &ring, int tnew, const FaceArgs<R> &
         const W4 w = *(const W4 *)(f.face_w + (long long)p * kTaps + 4 * q);
         const float2 s = f.face_scale ? f.face_scale[p] : make_float2(1, 1);
         const int nb = f.face_nbr[p];
-        const H4 hn = *(const H4 *)(nbase + (long long)nb * kRing);
-        const H4 hd = *(const H4 *)(dbase + (long long)nb * kRing);
+        H4 hn, hd;
+        load_window(base + (long long)nb * kHistRow, hn, hd);
 #pragma unroll
         for (int i = 0; i < 4; i++)
         {
@@ -804,9 +837,7 @@ __device__ inline void face_conv2(const Ring<R> &ring, int tnew, const float *ac
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
     const int g = lane >> 2, q = lane & 3;
-    const int copy = tnew & 3, off = (hist_index(copy, tnew) + 4 * q) & (kRing - 1);  // off % 4 == 0
-    const R *nbase = ring.hrow(0, copy, 0) + off, *dbase = ring.hrow(1, copy, 0) + off;
-    const int nslot = hist_index(0, tnew + 1);  // N[t+1] in copy 0 (used when no acceleration row)
+    const R *base = ring.hrow(tnew & 3, 0) + window_offset(tnew, q);
     const unsigned quad = 0xfu << (lane & ~3);
     const int b = f.face_start[tri], e = f.face_start[tri + 1];
     R a0 = 0, a1 = 0;
@@ -815,11 +846,11 @@ __device__ inline void face_conv2(const Ring<R> &ring, int tnew, const float *ac
         const W4 w = *(const W4 *)(f.face_w + (long long)p * kTaps + 4 * q);
         const float2 s = f.face_scale ? f.face_scale[p] : make_float2(1, 1);
         const int nb = f.face_nbr[p];
-        const H4 hn = *(const H4 *)(nbase + (long long)nb * kRing);
-        const H4 hd = *(const H4 *)(dbase + (long long)nb * kRing);
+        H4 hn, hd;
+        load_window(base + (long long)nb * kHistRow, hn, hd);
         R nnew = 0;
-        if (q == 0)
-            nnew = acc_next ? (R)acc_next[nb] : ring.hrow(0, 0, nb)[nslot];
+        if (q == 0)  // N[t+1]: the next acceleration row, or the canonical ring's value
+            nnew = acc_next ? (R)acc_next[nb] : ring.canon_at(0, nb, tnew + 1);
         const R un = __shfl_up_sync(quad, hn.v[3], 1, 4), ud = __shfl_up_sync(quad, hd.v[3], 1, 4);
 #pragma unroll
         for (int i = 0; i < 4; i++)
@@ -871,11 +902,13 @@ __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs
     R num = far_sum * (R)f.reflect + conv;
     const R dnew = (R)(num / f.denom[tri]);
     if (commit && lane < 4)
-        ring.hrow(1, lane, tri)[hist_index(lane, tnew)] = dnew;  // lane c: copy c
+        ring.hat(1, lane, tri, hist_index(lane, tnew)) = dnew;  // lane c: copy c
     else if (commit && lane == 4 && f.dlast)
         f.dlast[tri] = dnew;
     else if (commit && lane == 5)
         flag_nonfinite(f.status, dnew);  // a NaN acceleration or field reaches D within a step or two
+    else if (commit && lane == 6)
+        ring.canon_at(1, tri, tnew) = dnew;
     if (mode == 1)
         near_terms2<R>(ring, tnew, f, tri, lane, dnew, nnext);
     else if (mode == 2)
@@ -889,7 +922,7 @@ __device__ inline void face_finish(const Ring<R> &ring, int tnew, const FaceArgs
 template <typename R>
 __device__ inline R next_neumann(const Ring<R> &ring, const StepDyn &dn, int tri)
 {
-    return dn.acc ? (R)dn.acc[tri] : ring.hrow(0, 0, tri)[hist_index(0, dn.tnew)];
+    return dn.acc ? (R)dn.acc[tri] : ring.canon_at(0, tri, dn.tnew);
 }
 
 // the fused face stage (corner loads issued first so their latency overlaps the convolution)
@@ -992,8 +1025,8 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Rin
     face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
     face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri], mode,
                    mode == 1 ? next_neumann<R>(ring, dn, tri) : (R)0);
-    if (next && lane == 0 && dn.acc)
-        ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
+    if (next && lane == 0)
+        ring.nwrite(tri, dn.tnew, dn.acc);
 }
 
 // the autotuner's finish: the same work without the history and Dirichlet writes, so that timing
@@ -1022,8 +1055,8 @@ __global__ void nwrite_kernel(const __grid_constant__ Ring<R> ring, const StepSt
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const StepDyn dy = bind_step(st, kstep, nt);
-    if (i < nt && dy.acc)
-        ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
+    if (i < nt)
+        ring.nwrite(i, dy.tnew, dy.acc);
 }
 
 // the near-field terms of time t for every triangle without a face step (priming)
@@ -1190,6 +1223,8 @@ int make_launch(Handle &h, StepLaunch<R> &L)
     L.st = h.d_state;
     L.corr_mask = h.d_corr_mask;
     L.ring.hist = (R *)h.d_hist;
+    L.ring.canon[0] = (R *)h.d_neumann;
+    L.ring.canon[1] = (R *)h.d_dirichlet;
     L.ring.nt = h.mesh_set ? h.nt : 0;
     L.mesh = h.mesh_set && h.prm.method == PPPM_METHOD_PPPM ? 1 : 0;
     L.pml = h.prm.pml_width > 0 ? 1 : 0;
@@ -1820,7 +1855,9 @@ int autotune(Handle &h, int reps, float *us, int *best)
     // (conv_pairs = i / 6, threads = {64, 128, 256}[(i / 2) % 3], terms_pairs = i % 2).  The steps
     // write listener rows past the recorded ones, which the next call overwrites; the fields and
     // histories are restored from the snapshot at the end; h.t and the series count do not move.
-    const size_t gbytes = (size_t)h.n_cells * h.real_size, hbytes = (size_t)8 * nt * kRing * h.real_size;
+    // histories: the copies, then the two canonical rings
+    const size_t gbytes = (size_t)h.n_cells * h.real_size, cbytes = (size_t)4 * nt * kHistRow * h.real_size,
+                 rbytes = (size_t)nt * kRing * h.real_size, hbytes = cbytes + 2 * rbytes;
     const size_t abytes = (size_t)kTuneGraphSteps * nt * sizeof(float);
     void *snap = nullptr;
     PB_TRY(dev_alloc(&snap, 3 * gbytes + hbytes + abytes));
@@ -1832,9 +1869,12 @@ int autotune(Handle &h, int reps, float *us, int *best)
         for (int i = 0; i < 3 && e == cudaSuccess; i++)
             e = save ? cudaMemcpyAsync((char *)snap + i * gbytes, h.grid[i], gbytes, cudaMemcpyDeviceToDevice, s)
                      : cudaMemcpyAsync(h.grid[i], (char *)snap + i * gbytes, gbytes, cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess)
-            e = save ? cudaMemcpyAsync((char *)snap + 3 * gbytes, h.d_hist, hbytes, cudaMemcpyDeviceToDevice, s)
-                     : cudaMemcpyAsync(h.d_hist, (char *)snap + 3 * gbytes, hbytes, cudaMemcpyDeviceToDevice, s);
+        void *hist[3] = {h.d_hist, h.d_neumann, h.d_dirichlet};
+        const size_t hb[3] = {cbytes, rbytes, rbytes};
+        char *at = (char *)snap + 3 * gbytes;
+        for (int i = 0; i < 3 && e == cudaSuccess; at += hb[i], i++)
+            e = save ? cudaMemcpyAsync(at, hist[i], hb[i], cudaMemcpyDeviceToDevice, s)
+                     : cudaMemcpyAsync(hist[i], at, hb[i], cudaMemcpyDeviceToDevice, s);
         return e;
     };
     const int keep_pairs = h.conv_pairs, keep_threads = h.face_threads;
@@ -1959,36 +1999,33 @@ int prime(Handle &h)
     return PPPM_OK;
 }
 
-// reference-layout rings (index = time mod 32) <-> the four history copies
+// the canonical rings (index = time mod 32) -> the four history copies: the 16 times t-15..t
+// that the taps of the next step and the near-field terms of time t reach (the canonical rings
+// are current at all times, so nothing flows the other way)
 template <typename R>
-__global__ void hist_copy_kernel(R *canon_n, R *canon_d, R *hist, int nt, int to_copies)
+__global__ void hist_import_kernel(const R *canon_n, const R *canon_d, R *hist, int nt, int t)
 {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long per = (long long)nt * kRing;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per = (long long)nt * kHist;
     if (i >= 2 * per)
         return;
     const int field = (int)(i / per);
     const long long r = i % per;
-    const int tri = (int)(r / kRing), slot = (int)(r % kRing);
-    R *canon = field ? canon_d : canon_n;
-    if (to_copies)
-    {
-        const R v = canon[r];
-        for (int c = 0; c < 4; c++)
-            hist[((long long)(field * 4 + c) * nt + tri) * kRing + hist_index(c, slot)] = v;
-    }
-    else
-        canon[r] = hist[((long long)(field * 4) * nt + tri) * kRing + hist_index(0, slot)];
+    const int tri = (int)(r / kHist), tau = t - (int)(r % kHist);
+    const R v = (field ? canon_d : canon_n)[(long long)tri * kRing + (tau & (kRing - 1))];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        hist[((long long)c * nt + tri) * kHistRow + Ring<R>::hpos(field, hist_index(c, tau))] = v;
 }
 
 template <typename R>
-int hist_copy(Handle &h, int to_copies)
+int hist_copy(Handle &h)
 {
     if (!h.mesh_set || !h.d_hist)
         return PPPM_OK;
-    const long long n = 2ll * h.nt * kRing;
-    hist_copy_kernel<R><<<div_up(n, 256), 256, 0, h.stream>>>((R *)h.d_neumann, (R *)h.d_dirichlet, (R *)h.d_hist,
-                                                               h.nt, to_copies);
+    const long long n = 2ll * h.nt * kHist;
+    hist_import_kernel<R><<<div_up(n, 256), 256, 0, h.stream>>>((const R *)h.d_neumann, (const R *)h.d_dirichlet,
+                                                                 (R *)h.d_hist, h.nt, h.t);
     h.launches++;
     PB_CHECK_LAUNCH();
     return PPPM_OK;
@@ -2122,8 +2159,7 @@ int step_time_kernels(Handle &h, int reps, float *us)
     return h.fp64 ? time_kernels<double>(h, reps, us) : time_kernels<float>(h, reps, us);
 }
 
-int hist_import(Handle &h) { return h.fp64 ? hist_copy<double>(h, 1) : hist_copy<float>(h, 1); }
-int hist_export(Handle &h) { return h.fp64 ? hist_copy<double>(h, 0) : hist_copy<float>(h, 0); }
+int hist_import(Handle &h) { return h.fp64 ? hist_copy<double>(h) : hist_copy<float>(h); }
 
 int step_prime(Handle &h) { return h.fp64 ? prime<double>(h) : prime<float>(h); }
 
@@ -2279,8 +2315,8 @@ __global__ void __launch_bounds__(256) batch_finish_kernel(const BatchScene<R> *
     face_corners<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv);
     face_finish<R>(S.ring, dy.tnew, S.fa, tri, lane, iw, pv, S.conv[tri], mode,
                    mode == 1 ? next_neumann<R>(S.ring, dn, tri) : (R)0);
-    if (next && lane == 0 && dn.acc)
-        S.ring.hwrite(0, tri, dn.tnew, (R)dn.acc[tri]);
+    if (next && lane == 0)
+        S.ring.nwrite(tri, dn.tnew, dn.acc);
 }
 
 template <typename R>
@@ -2290,8 +2326,8 @@ __global__ void batch_nwrite_kernel(const BatchScene<R> *sc, const int2 *map, in
     const BatchScene<R> &S = sc[m.x];
     const int i = m.y * blockDim.x + threadIdx.x;
     const StepDyn dy = bind_step(S.st, k, S.a.nt);
-    if (i < S.a.nt && dy.acc)
-        S.ring.hwrite(0, i, dy.tnew, (R)dy.acc[i]);
+    if (i < S.a.nt)
+        S.ring.nwrite(i, dy.tnew, dy.acc);
 }
 
 // after G steps: every active scene's state moves on by G steps
