@@ -125,6 +125,15 @@ struct Ring
     {
         hwrite(0, tri, time, acc ? (R)acc[tri] : canon_at(0, tri, time));
     }
+    // N[time + 1] of triangle tri into the Dirichlet slot of `time` in copy time mod 4: that slot
+    // is tap 0 of the Dirichlet window of `time` (the step's unknown, which no reader of the
+    // window uses; finish of that step overwrites it with D[time]), so a two-step pass over the
+    // face pairs at `time` receives N[time + 1] with the window (face_conv2).  acc_next: the
+    // acceleration row of time + 1, or none.
+    __device__ void stash_next(int tri, int time, const float *acc_next) const
+    {
+        hat(1, time & 3, tri, hist_index(time & 3, time)) = acc_next ? (R)acc_next[tri] : canon_at(0, tri, time + 1);
+    }
 };
 
 template <typename Real>
@@ -831,8 +840,8 @@ __device__ inline R face_conv(const Ring<R> &ring, int tnew, const FaceArgs<R> &
 // lane before it in the quad (tap -1: N[t+1]; for D, taps 0 and 1 of time t+1 are left out).
 // The face weights, scales and neighbour indices are read once for both steps.
 template <typename R>
-__device__ inline void face_conv2(const Ring<R> &ring, int tnew, const float *acc_next, const FaceArgs<R> &f, int tri,
-                                  int lane, R &c0, R &c1)
+__device__ inline void face_conv2(const Ring<R> &ring, int tnew, const FaceArgs<R> &f, int tri, int lane, R &c0,
+                                  R &c1)
 {
     using W4 = typename WRec<R>::W4;
     using H4 = typename WRec<R>::H4;
@@ -848,9 +857,7 @@ __device__ inline void face_conv2(const Ring<R> &ring, int tnew, const float *ac
         const int nb = f.face_nbr[p];
         H4 hn, hd;
         load_window(base + (long long)nb * kHistRow, hn, hd);
-        R nnew = 0;
-        if (q == 0)  // N[t+1]: the next acceleration row, or the canonical ring's value
-            nnew = acc_next ? (R)acc_next[nb] : ring.canon_at(0, nb, tnew + 1);
+        const R nnew = hd.v[0];  // lane q = 0: N[t+1], stashed in Dirichlet tap 0 (Ring::stash_next)
         const R un = __shfl_up_sync(quad, hn.v[3], 1, 4), ud = __shfl_up_sync(quad, hd.v[3], 1, 4);
 #pragma unroll
         for (int i = 0; i < 4; i++)
@@ -970,9 +977,8 @@ __global__ void __launch_bounds__(256) conv2_kernel(const __grid_constant__ Ring
     if (w >= nt)
         return;
     const int tri = centre_of(f, w);
-    const StepDyn dn = bind_step(st, kstep + 1, nt);
     R c0, c1;
-    face_conv2<R>(ring, st->tnew0 + kstep, dn.acc, f, tri, threadIdx.x & 31, c0, c1);
+    face_conv2<R>(ring, st->tnew0 + kstep, f, tri, threadIdx.x & 31, c0, c1);
     if ((threadIdx.x & 31) == 0)
     {
         conv[tri] = c0;
@@ -1004,9 +1010,11 @@ __global__ void __launch_bounds__(256) fix_kernel(int nt, const __grid_constant_
     face_fix<R>(f, conv1, conv, centre_of(f, w), threadIdx.x & 31);
 }
 
-// pipelined step: the rest of the face stage of step kstep; next != 0: also the Neumann value of
+// pipelined step: the rest of the face stage of step kstep; next & 1: also the Neumann value of
 // step kstep + 1 into the history (its slot is outside every window of this step), so the next
-// step's convolution can start before that step's stencil
+// step's convolution can start before that step's stencil; next & 2: step kstep + 1 starts a
+// two-step pass over the face pairs, which receives N of step kstep + 2 with its history windows
+// (Ring::stash_next)
 // (one instantiation per mode: the two-step variants need more registers, which the one-step
 // path should not carry)
 template <typename R, int mode>
@@ -1025,8 +1033,10 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Rin
     face_corners<R>(ring, dy.tnew, f, tri, lane, iw, pv);
     face_finish<R>(ring, dy.tnew, f, tri, lane, iw, pv, conv[tri], mode,
                    mode == 1 ? next_neumann<R>(ring, dn, tri) : (R)0);
-    if (next && lane == 0)
+    if ((next & 1) && lane == 0)
         ring.nwrite(tri, dn.tnew, dn.acc);
+    else if ((next & 2) && lane == 1)
+        ring.stash_next(tri, dn.tnew, bind_step(st, kstep + 2, nt).acc);
 }
 
 // the autotuner's finish: the same work without the history and Dirichlet writes, so that timing
@@ -1049,14 +1059,19 @@ __global__ void __launch_bounds__(256) finish_dry_kernel(const __grid_constant__
                    mode == 1 ? next_neumann<R>(ring, dn, tri) : (R)0, false);
 }
 
-// the Neumann value of step kstep into the history (first step of a pipelined call)
+// the Neumann value of step kstep into the history (first step of a pipelined call); stash: the step
+// starts a two-step pass over the face pairs (Ring::stash_next)
 template <typename R>
-__global__ void nwrite_kernel(const __grid_constant__ Ring<R> ring, const StepState *st, int kstep, int nt)
+__global__ void nwrite_kernel(const __grid_constant__ Ring<R> ring, const StepState *st, int kstep, int nt, int stash)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const StepDyn dy = bind_step(st, kstep, nt);
     if (i < nt)
+    {
         ring.nwrite(i, dy.tnew, dy.acc);
+        if (stash)
+            ring.stash_next(i, dy.tnew, bind_step(st, kstep + 1, nt).acc);
+    }
 }
 
 // the near-field terms of time t for every triangle without a face step (priming)
@@ -1359,7 +1374,9 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair,
     const bool split = L.split && bulk;
     StencilSplit bsp = L.sp;
     bsp.skip_corrected = 1;
-    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
+    // step j's convolution is a two-step pass (conv2_kernel)
+    auto conv2_at = [&](int j) { return pair && !(j & 1) && j < nsteps && (open || j + 1 < nsteps); };
+    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt, conv2_at(0) ? 1 : 0);
     cudaEventRecord(h.ev_fin, s);
     if (split)
         cudaEventRecord(h.ev_near, s);
@@ -1391,7 +1408,7 @@ void capture_pipelined(Handle &h, const StepLaunch<R> &L, int nsteps, bool pair,
         // leaves for the next call are then exactly those that prime() rebuilds after a state
         // restore or a mesh update
         const int mode = L.tpairs && more ? ((k & 1) ? 2 : 1) : 0;
-        const int nx = more ? 1 : 0;
+        const int nx = (more ? 1 : 0) | (conv2_at(k + 1) ? 2 : 0);
         const R *conv = L.conv;
         if (mode == 1)
             launch_dependent(finish_kernel<R, 1>, wblocks, FT, s, L.ring, L.st, k, nt, L.fa, conv, nx);
@@ -1447,8 +1464,9 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
     };
     cudaGraph_t graph = nullptr;
     PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    auto conv2_at = [&](int j) { return pair && !(j & 1) && j + 1 < n; };
     mark(PPPM_KERNEL_NWRITE);
-    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt);
+    nwrite_kernel<R><<<div_up(nt, T), T, 0, s>>>(L.ring, L.st, 0, nt, conv2_at(0) ? 1 : 0);
     mark(PPPM_KERNEL_EMPTY);
     empty_kernel<<<1, 32, 0, s>>>();
     for (int k = 0; k < n; k++)
@@ -1483,7 +1501,7 @@ int profile_graph(Handle &h, const StepLaunch<R> &L, cudaGraphExec_t *out)
             stencil_kernel<R><<<L.sp.nb_bd + L.sp.nb_in, T, 0, s>>>(L.a, L.ring, L.st, k, L.sp, L.corr_mask);
         }
         const int mode = L.tpairs && k + 1 < n ? ((k & 1) ? 2 : 1) : 0;
-        const int nx = k + 1 < n ? 1 : 0;
+        const int nx = (k + 1 < n ? 1 : 0) | (conv2_at(k + 1) ? 2 : 0);
         if (mode == 1)
         {
             mark(PPPM_KERNEL_FINISH1);
@@ -2265,6 +2283,12 @@ __global__ void __launch_bounds__(256) batch_near_kernel(const BatchScene<R> *sc
 // (conv2_kernel / fix_kernel) as the scene's state says: a scene's steps pair up from the first
 // step of its batched run (pair0), so the pairs, and the results, are those of the same steps
 // run alone in one pppm_step call, wherever the batch's graphs and phases begin and end.
+// a scene's step of time t starts a two-step pass over the face pairs (batch_conv_kernel)
+__device__ inline bool batch_conv2_at(const StepState &st, int t)
+{
+    return st.pair_end >= st.pair0 && st.conv_pairs && !((t - st.pair0) & 1) && t + 1 <= st.pair_end;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc, const int2 *map, int k)
 {
@@ -2278,11 +2302,10 @@ __global__ void __launch_bounds__(256) batch_conv_kernel(const BatchScene<R> *sc
     const bool paired = pe >= p0 && S.st->conv_pairs;
     if (paired && ((tnew - p0) & 1))
         face_fix<R>(S.fa, S.conv1, S.conv, tri, lane);  // second step of a pair
-    else if (paired && tnew + 1 <= pe)
+    else if (batch_conv2_at(*S.st, tnew))
     {
-        const StepDyn dn = bind_step(S.st, k + 1, S.a.nt);
         R c0, c1;
-        face_conv2<R>(S.ring, tnew, dn.acc, S.fa, tri, lane, c0, c1);
+        face_conv2<R>(S.ring, tnew, S.fa, tri, lane, c0, c1);
         if (lane == 0)
         {
             S.conv[tri] = c0;
@@ -2317,6 +2340,8 @@ __global__ void __launch_bounds__(256) batch_finish_kernel(const BatchScene<R> *
                    mode == 1 ? next_neumann<R>(S.ring, dn, tri) : (R)0);
     if (next && lane == 0)
         S.ring.nwrite(tri, dn.tnew, dn.acc);
+    else if (next && lane == 1 && batch_conv2_at(*S.st, dn.tnew))
+        S.ring.stash_next(tri, dn.tnew, bind_step(S.st, k + 2, S.a.nt).acc);
 }
 
 template <typename R>
@@ -2327,7 +2352,11 @@ __global__ void batch_nwrite_kernel(const BatchScene<R> *sc, const int2 *map, in
     const int i = m.y * blockDim.x + threadIdx.x;
     const StepDyn dy = bind_step(S.st, k, S.a.nt);
     if (i < S.a.nt)
+    {
         S.ring.nwrite(i, dy.tnew, dy.acc);
+        if (batch_conv2_at(*S.st, dy.tnew))
+            S.ring.stash_next(i, dy.tnew, bind_step(S.st, k + 1, S.a.nt).acc);
+    }
 }
 
 // after G steps: every active scene's state moves on by G steps
