@@ -7,9 +7,11 @@
 //                  t+1 the dead slot t+1 carries, at corrected cells only, the FDTD-near
 //                  correction of step t+1 (see step.cu).
 //   pml[3]         res^3 x 6 real (PML only)
-//   neumann/dirichlet  nt x 32 real rings in the reference layout (slot = t mod 32), for
-//                  read-out and loading; the step works on hist, four shifted copies of each
-//                  ring (copy c holds time tau at (c - tau) mod 32) so 4 taps are one aligned load
+//   neumann/dirichlet  nt x 32 real rings in the reference layout (slot = t mod 32), kept
+//                  current by every history write, for read-out and loading; the step reads
+//                  hist, four shifted 16-slot copies (copy c holds time tau at (c - tau) mod 16)
+//                  with both fields of a triangle in one row, so a lane's 4 Neumann and 4
+//                  Dirichlet taps are one aligned load
 //   cell CSR       cell_start[res^3 + 1] / cell_tris[nt] (sorted by triangle id per cell),
 //                  same for base cells
 //   3^3 pairs      n3 corrected cells: n3_cell, n3_start[n3 + 1]; p3 pairs: p3_tri, p3_woff

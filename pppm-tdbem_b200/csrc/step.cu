@@ -558,9 +558,9 @@ __global__ void __launch_bounds__(256) pml_kernel(const __grid_constant__ StepAr
 
 // ---- convolution helpers
 // A pair is handled by a quad of 4 lanes: lane q takes taps 4q..4q+3 with one 16-byte load of
-// the pair's weights (4 fp16 (single, double) tap pairs) and one 16-byte load each of the
-// neighbour's Neumann and Dirichlet windows from the history copy whose taps 4q..4q+3 are
-// aligned at this time step; the 8 quads of a warp take pairs g, g + 8, ...  Each lane sums its
+// the pair's weights (4 fp16 (single, double) tap pairs) and one load of the neighbour's Neumann
+// and Dirichlet taps 4q..4q+3 from the history copy in which they are aligned at this time step
+// (load_window); the 8 quads of a warp take pairs g, g + 8, ...  Each lane sums its
 // taps in increasing pair and tap order; the warp reduces once per triangle / cell.
 __device__ inline float conv_tap(__half2 w, float2 s, float n, float d)
 {
